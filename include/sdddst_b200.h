@@ -1,0 +1,165 @@
+/*
+ * sdddst_b200 -- C ABI of the B200 (sm_100a) implicit-step engine.
+ *
+ * Plain pointers and sizes only; every call returns an int status
+ * (SDDDST_OK = 0, negative on error; sdddst_last_error() describes the last
+ * failure on the calling thread).  Unlike the reference, which ignores the
+ * UMFPACK status (src/simulation.cpp:388-395, cast to void), no status is
+ * dropped.  One context is driven by one host thread; it owns one CUDA stream
+ * and all device memory of one simulated system.
+ *
+ * Configuration arrays use the reference's layouts: dislocations as N rows of
+ * {x, y, b} doubles (include/dislocation.h:27-31), point defects as P rows of
+ * {x, y} (include/point_defect.h:27-30).  Host pointers unless a name says
+ * "_device".
+ */
+#ifndef SDDDST_B200_H
+#define SDDDST_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SDDDST_OK 0
+#define SDDDST_ERR_INVALID (-1)   /* bad argument or size */
+#define SDDDST_ERR_CUDA (-2)      /* CUDA runtime error (message in sdddst_last_error) */
+#define SDDDST_ERR_NOMEM (-3)     /* device or host allocation failed */
+#define SDDDST_ERR_SOLVER (-4)    /* linear solve did not reach its tolerance */
+#define SDDDST_ERR_CAPACITY (-5)  /* caller buffer too small (required size returned) */
+#define SDDDST_ERR_NONFINITE (-6) /* NaN/Inf in a state or result */
+
+/* StressProtocol family: getType() "zero-stress" (stress_protocol.cpp:54-57),
+ * "fixed-rate-stress" (fixed_rate_protocol.cpp:80-83), "spring-stress"
+ * (spring_protocol.cpp:56-59), and a constant value (any other type string). */
+enum {
+    SDDDST_STRESS_ZERO = 0,
+    SDDDST_STRESS_FIXED_RATE = 1,
+    SDDDST_STRESS_SPRING = 2,
+    SDDDST_STRESS_CONSTANT = 3
+};
+
+/* StressProtocolStepType (stress_protocol.h:31-37). */
+enum {
+    SDDDST_STAGE_ORIGINAL = 0,
+    SDDDST_STAGE_END_OF_BIG_STEP = 1,
+    SDDDST_STAGE_END_OF_FIRST_SMALL_STEP = 2,
+    SDDDST_STAGE_END_OF_SECOND_SMALL_STEP = 3
+};
+
+/* Arithmetic of the O(N^2) pair sum. */
+enum {
+    SDDDST_PAIRSUM_FP64 = 0, /* plain: FP64 throughout */
+    SDDDST_PAIRSUM_FP32 = 1  /* FP32 pair terms, FP64 (compensated) accumulation */
+};
+
+/* Linear solver replacing UMFPACK (simulation.cpp:386-396). */
+enum {
+    SDDDST_SOLVER_GMRES = 0,      /* restarted GMRES, FP64, unpreconditioned */
+    SDDDST_SOLVER_GMRES_JACOBI = 1 /* restarted GMRES, FP64, diagonal preconditioner */
+};
+
+/* Field kernels (Field plug-in): the analytic periodic field
+ * (Fields/AnalyticField.cpp). */
+enum { SDDDST_FIELD_ANALYTIC = 0 };
+
+typedef struct {
+    int n;                    /* dislocation count (SimulationData::dc) */
+    int p;                    /* point-defect count (SimulationData::pc) */
+    double cutoff_multiplier; /* SimulationData::cutOffMultiplier */
+    double prec;              /* SimulationData::prec */
+    double step_size;         /* SimulationData::stepSize (initial) */
+    double A;                 /* SimulationData::A (after any scaling) */
+    double KASQR;             /* SimulationData::KASQR (after any scaling) */
+    int ic;                   /* SimulationData::ic, chord-Newton iterations */
+    int stress_kind;          /* SDDDST_STRESS_* */
+    double stress_rate;       /* FixedRateProtocol::rate */
+    double spring_constant;   /* SpringProtocol::springConstant */
+    double stress_value;      /* constant protocol */
+    int calculate_strain;     /* SimulationData::calculateStrainDuringSimulation */
+    int max_step_limited;     /* SimulationData::isMaxStepSizeLimit */
+    double max_step;          /* SimulationData::maxStepSizeLimit */
+    int field;                /* SDDDST_FIELD_* */
+    int pairsum;              /* SDDDST_PAIRSUM_* */
+    int solver;               /* SDDDST_SOLVER_* */
+    double solver_tol;        /* relative residual target of the iterative solve */
+    int gmres_restart;        /* Krylov subspace size per cycle */
+    int max_iters;            /* iteration cap per solve */
+    int device;               /* CUDA device ordinal */
+} sdddst_params;
+
+/* Defaults of SimulationData() (simulation_data.cpp:43-109, constants.h):
+ * cutoff multiplier 1, prec 1e-8, step 1, A = 1.6e-3, KASQR = 1.65^2*1e6/256,
+ * ic = 2, zero stress, FP64 pair sum, GMRES to 1e-14. */
+void sdddst_default_params(sdddst_params *prm);
+
+/* Creates a context and uploads the configuration.  Replaces constructing
+ * SimulationData + Simulation (simulation_data.cpp:111-117,
+ * simulation.cpp:38-55); the cutoff follows SimulationData::updateCutOff
+ * (simulation_data.cpp:208-218). */
+int sdddst_ctx_create(const sdddst_params *prm, const double *xyb, const double *pd, void **ctx);
+int sdddst_ctx_destroy(void *ctx);
+
+/* Error text of the last failing call on this thread. */
+const char *sdddst_last_error(void);
+
+/* Replaces the state: positions, step size, time, energy, strain.  With
+ * first_step = 0 the state is taken as just accepted (initial velocities
+ * re-evaluated as at simulation.cpp:543-550, tolerances reset as at :644);
+ * with first_step = 1 the next step behaves as a fresh Simulation's first
+ * step (simulation.cpp:450-479). */
+int sdddst_set_state(void *ctx, const double *xyb, double step_size, double sim_time, double energy,
+                     double strain, int first_step);
+
+/* Scalars after the last step, same order as the oracle:
+ * [0] simTime [1] stepSize [2] successful steps [3] failed steps [4] energy
+ * [5] accumulated strain [6] max error ratio^2 of the last attempt
+ * [7] <|v|> [8] sum v^2 [9] energy increment [10] cutoff [11] stress(Original) */
+int sdddst_get_scalars(void *ctx, double *out12);
+
+/* which: 0 accepted configuration, 1 big step, 2 first small step,
+ * 3 second small step; writes N x {x, y, b}. */
+int sdddst_get_config(void *ctx, int which, double *xyb);
+
+/* which: 0 initSpeed, 1 initSpeed2, 2 speed, 3 speed2, 4 dVec, 5 g,
+ * 6 tolerance at the end of the last step (before its reset). */
+int sdddst_get_vector(void *ctx, int which, double *out);
+
+/* Simulation::calculateSpeeds (simulation.cpp:86-131) on a given
+ * configuration with a fresh precision handler: velocities v[N] and the
+ * per-dislocation tolerance tol[N] (precision_handler.cpp:72-87).
+ * stress_type selects the stored stress value (after calculateStress at
+ * sim_time for that step type). */
+int sdddst_speeds(void *ctx, const double *xyb, double sim_time, int stress_type, double *v, double *tol);
+
+/* Simulation::calculateJacobian (simulation.cpp:236-384) at step size h on a
+ * given configuration, returned as CSR of J (row i = dislocation i; the
+ * reference's CSC column j is row j of J^T).  row_ptr[N+1], col[cap],
+ * val[cap], dvec[N].  On SDDDST_ERR_CAPACITY, *nnz holds the size needed. */
+int sdddst_jacobian(void *ctx, double h, const double *xyb, int *row_ptr, int *col, double *val, double *dvec,
+                    long cap, long *nnz);
+
+/* Solves J(h, xyb) x = rhs with the context's solver (the UMFPACK
+ * symbolic + numeric + solve sequence, simulation.cpp:386-396). */
+int sdddst_solve(void *ctx, double h, const double *xyb, const double *rhs, double *x, int *iterations);
+
+/* Simulation::step (simulation.cpp:435-441): one adaptive implicit step
+ * (full step, two half steps, error control, accept/reject, new step size). */
+int sdddst_step(void *ctx, int *accepted);
+
+/* Repeats sdddst_step until `accepted_target` steps were accepted or
+ * `max_attempts` attempts were made. */
+int sdddst_run(void *ctx, int accepted_target, int max_attempts, int *accepted, int *attempts);
+
+/* Device-resident access for callers that keep the state on the GPU:
+ * pointers to the accepted configuration's x, y and b arrays (N doubles each,
+ * structure of arrays) on the context's device. */
+int sdddst_state_device(void *ctx, double **x_device, double **y_device, double **b_device);
+
+/* Launch statistics: number of kernels this context has launched so far. */
+long sdddst_kernel_launches(void *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,221 @@
+"""ctypes binding of the engine's C ABI (``include/sdddst_b200.h``).
+
+This is the path tests and the bench call through: plain pointers and sizes,
+no torch types.  Loading fails loudly when the CUDA library has not been
+built; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsdddst_b200.so")
+
+OK = 0
+ERR_INVALID = -1
+ERR_CUDA = -2
+ERR_NOMEM = -3
+ERR_SOLVER = -4
+ERR_CAPACITY = -5
+ERR_NONFINITE = -6
+
+STRESS_ZERO, STRESS_FIXED_RATE, STRESS_SPRING, STRESS_CONSTANT = 0, 1, 2, 3
+PAIRSUM_FP64, PAIRSUM_FP32 = 0, 1
+SOLVER_GMRES, SOLVER_GMRES_JACOBI = 0, 1
+
+# Every extern "C" symbol of include/sdddst_b200.h.
+EXPORTS = [
+    "sdddst_default_params", "sdddst_ctx_create", "sdddst_ctx_destroy", "sdddst_last_error",
+    "sdddst_set_state", "sdddst_get_scalars", "sdddst_get_config", "sdddst_get_vector",
+    "sdddst_speeds", "sdddst_jacobian", "sdddst_solve", "sdddst_step", "sdddst_run",
+    "sdddst_state_device", "sdddst_kernel_launches",
+]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("n", C.c_int), ("p", C.c_int),
+        ("cutoff_multiplier", C.c_double), ("prec", C.c_double), ("step_size", C.c_double),
+        ("A", C.c_double), ("KASQR", C.c_double), ("ic", C.c_int),
+        ("stress_kind", C.c_int), ("stress_rate", C.c_double), ("spring_constant", C.c_double),
+        ("stress_value", C.c_double), ("calculate_strain", C.c_int), ("max_step_limited", C.c_int),
+        ("max_step", C.c_double), ("field", C.c_int), ("pairsum", C.c_int), ("solver", C.c_int),
+        ("solver_tol", C.c_double), ("gmres_restart", C.c_int), ("max_iters", C.c_int), ("device", C.c_int),
+    ]
+
+
+class EngineError(RuntimeError):
+    def __init__(self, rc: int, msg: str):
+        super().__init__(f"sdddst_b200 error {rc}: {msg}")
+        self.rc = rc
+
+
+_lib = None
+_D = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_I = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def load(path: str = LIB_PATH):
+    """Load the CUDA engine library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with `python -m sdddst_b200.build`")
+    lib = C.CDLL(path)
+    lib.sdddst_default_params.argtypes = [C.POINTER(Params)]
+    lib.sdddst_default_params.restype = None
+    lib.sdddst_last_error.restype = C.c_char_p
+    lib.sdddst_ctx_create.argtypes = [C.POINTER(Params), _D, C.c_void_p, C.POINTER(C.c_void_p)]
+    lib.sdddst_ctx_destroy.argtypes = [C.c_void_p]
+    lib.sdddst_set_state.argtypes = [C.c_void_p, _D, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int]
+    lib.sdddst_get_scalars.argtypes = [C.c_void_p, _D]
+    lib.sdddst_get_config.argtypes = [C.c_void_p, C.c_int, _D]
+    lib.sdddst_get_vector.argtypes = [C.c_void_p, C.c_int, _D]
+    lib.sdddst_speeds.argtypes = [C.c_void_p, _D, C.c_double, C.c_int, _D, _D]
+    lib.sdddst_jacobian.argtypes = [C.c_void_p, C.c_double, _D, _I, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_long, C.POINTER(C.c_long)]
+    lib.sdddst_solve.argtypes = [C.c_void_p, C.c_double, _D, _D, _D, C.POINTER(C.c_int)]
+    lib.sdddst_step.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+    lib.sdddst_run.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.sdddst_state_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.sdddst_kernel_launches.argtypes = [C.c_void_p]
+    lib.sdddst_kernel_launches.restype = C.c_long
+    _lib = lib
+    return lib
+
+
+def _check(rc: int):
+    if rc != OK:
+        raise EngineError(rc, load().sdddst_last_error().decode(errors="replace"))
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    load().sdddst_default_params(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p
+
+
+def cli_params(n: int, cutoff_multiplier: float, prec: float, step_size: float = 1e-6, p: int = 0,
+               pd_scaling: bool = False, **kw) -> Params:
+    """Parameters as the reference CLI sets them (project_parser.cpp:137-298):
+    SimulationData defaults, then step size, precision, cutoff multiplier and,
+    when a point-defect file is given, A *= 1/sqrt(N) and KASQR *= N."""
+    prm = default_params(n=n, p=p, cutoff_multiplier=cutoff_multiplier, prec=prec, step_size=step_size)
+    if pd_scaling:
+        prm.A = prm.A * (1.0 / np.sqrt(float(n)))
+        prm.KASQR = prm.KASQR * float(n)
+    for k, v in kw.items():
+        setattr(prm, k, v)
+    return prm
+
+
+SCALAR_NAMES = ["sim_time", "step_size", "successful_steps", "failed_steps", "energy", "strain",
+                "max_error_ratio_sqr", "avg_speed", "vsquare", "energy_accum", "cutoff", "stress"]
+
+
+class Engine:
+    """One device context (one simulated system on one GPU)."""
+
+    def __init__(self, prm: Params, xyb: np.ndarray, pd: Optional[np.ndarray] = None):
+        lib = load()
+        self.lib = lib
+        self.prm = prm
+        xyb = np.ascontiguousarray(xyb, dtype=np.float64).reshape(-1)
+        self.n = prm.n
+        if xyb.size != 3 * self.n:
+            raise ValueError("xyb must hold n rows of (x, y, b)")
+        self._pd = None
+        pdp = None
+        if prm.p > 0:
+            self._pd = np.ascontiguousarray(pd, dtype=np.float64).reshape(-1)
+            if self._pd.size != 2 * prm.p:
+                raise ValueError("pd must hold p rows of (x, y)")
+            pdp = self._pd.ctypes.data_as(C.c_void_p)
+        h = C.c_void_p()
+        _check(lib.sdddst_ctx_create(C.byref(prm), xyb, pdp, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.sdddst_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, xyb, step_size, sim_time=0.0, energy=0.0, strain=0.0, first_step=False):
+        a = np.ascontiguousarray(xyb, dtype=np.float64).reshape(-1)
+        _check(self.lib.sdddst_set_state(self.h, a, float(step_size), float(sim_time), float(energy),
+                                         float(strain), int(first_step)))
+
+    def scalars(self) -> dict:
+        out = np.zeros(12)
+        _check(self.lib.sdddst_get_scalars(self.h, out))
+        return dict(zip(SCALAR_NAMES, out))
+
+    def config(self, which: int = 0) -> np.ndarray:
+        out = np.zeros(3 * self.n)
+        _check(self.lib.sdddst_get_config(self.h, which, out))
+        return out.reshape(self.n, 3)
+
+    def vector(self, which: int) -> np.ndarray:
+        out = np.zeros(self.n)
+        _check(self.lib.sdddst_get_vector(self.h, which, out))
+        return out
+
+    def speeds(self, xyb, sim_time=0.0, stress_type=0):
+        a = np.ascontiguousarray(xyb, dtype=np.float64).reshape(-1)
+        v = np.zeros(self.n)
+        tol = np.zeros(self.n)
+        _check(self.lib.sdddst_speeds(self.h, a, float(sim_time), int(stress_type), v, tol))
+        return v, tol
+
+    def jacobian(self, h, xyb):
+        """CSR of J: (row_ptr, col, val, dvec)."""
+        a = np.ascontiguousarray(xyb, dtype=np.float64).reshape(-1)
+        rp = np.zeros(self.n + 1, dtype=np.int32)
+        nnz = C.c_long(0)
+        rc = self.lib.sdddst_jacobian(self.h, float(h), a, rp, None, None, None, 0, C.byref(nnz))
+        if rc not in (OK, ERR_CAPACITY):
+            _check(rc)
+        cap = nnz.value
+        col = np.zeros(cap, dtype=np.int32)
+        val = np.zeros(cap)
+        d = np.zeros(self.n)
+        _check(self.lib.sdddst_jacobian(self.h, float(h), a, rp, col.ctypes.data_as(C.c_void_p),
+                                        val.ctypes.data_as(C.c_void_p), d.ctypes.data_as(C.c_void_p),
+                                        cap, C.byref(nnz)))
+        return rp, col[:nnz.value], val[:nnz.value], d
+
+    def solve(self, h, xyb, rhs):
+        a = np.ascontiguousarray(xyb, dtype=np.float64).reshape(-1)
+        r = np.ascontiguousarray(rhs, dtype=np.float64)
+        x = np.zeros(self.n)
+        it = C.c_int(0)
+        _check(self.lib.sdddst_solve(self.h, float(h), a, r, x, C.byref(it)))
+        return x, it.value
+
+    def step(self) -> bool:
+        a = C.c_int(0)
+        _check(self.lib.sdddst_step(self.h, C.byref(a)))
+        return bool(a.value)
+
+    def run(self, accepted_target: int, max_attempts: int):
+        a, t = C.c_int(0), C.c_int(0)
+        _check(self.lib.sdddst_run(self.h, int(accepted_target), int(max_attempts), C.byref(a), C.byref(t)))
+        return a.value, t.value
+
+    def launches(self) -> int:
+        return int(self.lib.sdddst_kernel_launches(self.h))

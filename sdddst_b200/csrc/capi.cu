@@ -1,0 +1,300 @@
+// extern "C" boundary of the engine (include/sdddst_b200.h).  Every entry
+// point catches C++ exceptions and CUDA errors and turns them into status
+// codes with a per-thread message.
+#include "engine.h"
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int rc, const std::string &msg)
+{
+    g_last_error = msg;
+    return rc;
+}
+
+int from_engine(sd::Engine *e, int rc)
+{
+    if (rc != 0) g_last_error = e->err.empty() ? std::string("engine error") : e->err;
+    return rc;
+}
+
+sd::Engine *E(void *ctx) { return static_cast<sd::Engine *>(ctx); }
+
+// Uploads a caller configuration into the engine's scratch arrays and
+// temporarily routes y and b to them; restores on destruction.
+struct ScratchConfig {
+    sd::Engine *e;
+    double *y_saved, *b_saved;
+    ScratchConfig(sd::Engine *e_, const double *xyb) : e(e_), y_saved(e_->d_y), b_saved(e_->d_b)
+    {
+        const int n = e->n;
+        std::vector<double> hx(n), hy(n), hb(n);
+        for (int i = 0; i < n; ++i) {
+            hx[i] = xyb[3 * i];
+            hy[i] = xyb[3 * i + 1];
+            hb[i] = xyb[3 * i + 2];
+        }
+        cudaMemcpyAsync(e->d_xs, hx.data(), sizeof(double) * n, cudaMemcpyHostToDevice, e->st);
+        cudaMemcpyAsync(e->d_ys, hy.data(), sizeof(double) * n, cudaMemcpyHostToDevice, e->st);
+        cudaMemcpyAsync(e->d_bs, hb.data(), sizeof(double) * n, cudaMemcpyHostToDevice, e->st);
+        cudaStreamSynchronize(e->st);
+        e->d_y = e->d_ys;
+        e->d_b = e->d_bs;
+    }
+    ~ScratchConfig()
+    {
+        e->d_y = y_saved;
+        e->d_b = b_saved;
+    }
+};
+
+} // namespace
+
+extern "C" {
+
+void sdddst_default_params(sdddst_params *p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->n = 0;
+    p->p = 0;
+    p->cutoff_multiplier = 1.0;           // DEFAULT_CUTOFF_MULTIPLIER, constants.h:26
+    p->prec = 1e-8;                       // DEFAULT_PRECISION, constants.h:28
+    p->step_size = 1.0;                   // DEFAULT_STEP_SIZE, constants.h:31
+    p->A = 1e-4 * 16.0;                   // DEFAULT_A, constants.h:34
+    p->KASQR = 1.65 * 1.65 * 1e6 / 256.0; // DEFAULT_KASQR, constants.h:33
+    p->ic = 2;                            // DEFAULT_ITERATION_COUNT, constants.h:29
+    p->stress_kind = SDDDST_STRESS_ZERO;
+    p->spring_constant = 1.0;             // SpringProtocol(), spring_protocol.cpp:22-26
+    p->field = SDDDST_FIELD_ANALYTIC;
+    p->pairsum = SDDDST_PAIRSUM_FP64;
+    p->solver = SDDDST_SOLVER_GMRES;
+    p->solver_tol = 1e-13;
+    p->gmres_restart = 30;
+    p->max_iters = 1000;
+    p->device = 0;
+}
+
+const char *sdddst_last_error(void) { return g_last_error.c_str(); }
+
+int sdddst_ctx_create(const sdddst_params *prm, const double *xyb, const double *pd, void **ctx)
+{
+    if (!prm || !ctx) return fail(SDDDST_ERR_INVALID, "null argument");
+    *ctx = nullptr;
+    if (prm->field != SDDDST_FIELD_ANALYTIC) return fail(SDDDST_ERR_INVALID, "unsupported field kind");
+    if (prm->pairsum != SDDDST_PAIRSUM_FP64 && prm->pairsum != SDDDST_PAIRSUM_FP32)
+        return fail(SDDDST_ERR_INVALID, "unsupported pair-sum mode");
+    if (prm->solver != SDDDST_SOLVER_GMRES && prm->solver != SDDDST_SOLVER_GMRES_JACOBI)
+        return fail(SDDDST_ERR_INVALID, "unsupported solver");
+    if (!(prm->prec > 0) || !(prm->step_size > 0) || !(prm->cutoff_multiplier > 0))
+        return fail(SDDDST_ERR_INVALID, "prec, step size and cutoff multiplier must be positive");
+    sd::Engine *e = new (std::nothrow) sd::Engine();
+    if (!e) return fail(SDDDST_ERR_NOMEM, "host allocation failed");
+    int rc;
+    try {
+        rc = e->init(*prm, xyb, pd);
+    } catch (const std::exception &ex) {
+        rc = SDDDST_ERR_NOMEM;
+        e->err = ex.what();
+    }
+    if (rc) {
+        g_last_error = e->err;
+        delete e;
+        return rc;
+    }
+    *ctx = e;
+    return SDDDST_OK;
+}
+
+int sdddst_ctx_destroy(void *ctx)
+{
+    if (!ctx) return SDDDST_OK;
+    delete E(ctx);
+    return SDDDST_OK;
+}
+
+int sdddst_set_state(void *ctx, const double *xyb, double step_size, double sim_time, double energy, double strain,
+                     int first_step)
+{
+    if (!ctx || !xyb) return fail(SDDDST_ERR_INVALID, "null argument");
+    if (!(step_size > 0)) return fail(SDDDST_ERR_INVALID, "step size must be positive");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    try {
+        return from_engine(e, e->set_state_host(xyb, step_size, sim_time, energy, strain, first_step));
+    } catch (const std::exception &ex) {
+        return fail(SDDDST_ERR_NOMEM, ex.what());
+    }
+}
+
+int sdddst_get_scalars(void *ctx, double *out)
+{
+    if (!ctx || !out) return fail(SDDDST_ERR_INVALID, "null argument");
+    sd::Engine *e = E(ctx);
+    out[0] = e->sim_time;
+    out[1] = e->step_size;
+    out[2] = (double)e->succ;
+    out[3] = (double)e->failed;
+    out[4] = e->energy;
+    out[5] = e->strain;
+    out[6] = e->last_ratio;
+    out[7] = e->sum_avg_speed;
+    out[8] = e->vsquare;
+    out[9] = e->energy_accum;
+    out[10] = e->cutoff;
+    out[11] = e->stress_get(SDDDST_STAGE_ORIGINAL);
+    return SDDDST_OK;
+}
+
+int sdddst_get_config(void *ctx, int which, double *xyb)
+{
+    if (!ctx || !xyb || which < 0 || which > 3) return fail(SDDDST_ERR_INVALID, "bad argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    const int n = e->n;
+    const double *src = which == 0 ? e->d_x0 : which == 1 ? e->d_xb : which == 2 ? e->d_x1 : e->d_x2;
+    std::vector<double> hx(n), hy(n), hb(n);
+    cudaMemcpyAsync(hx.data(), src, sizeof(double) * n, cudaMemcpyDeviceToHost, e->st);
+    cudaMemcpyAsync(hy.data(), e->d_y, sizeof(double) * n, cudaMemcpyDeviceToHost, e->st);
+    cudaMemcpyAsync(hb.data(), e->d_b, sizeof(double) * n, cudaMemcpyDeviceToHost, e->st);
+    if (int rc = e->sync_check("get_config")) return from_engine(e, rc);
+    for (int i = 0; i < n; ++i) {
+        xyb[3 * i] = hx[i];
+        xyb[3 * i + 1] = hy[i];
+        xyb[3 * i + 2] = hb[i];
+    }
+    return SDDDST_OK;
+}
+
+int sdddst_get_vector(void *ctx, int which, double *out)
+{
+    if (!ctx || !out || which < 0 || which > 6) return fail(SDDDST_ERR_INVALID, "bad argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    const double *src[] = {e->d_v0, e->d_v0b, e->d_vs, e->d_vs2, e->d_dvec, e->d_g, e->d_tol_last};
+    cudaMemcpyAsync(out, src[which], sizeof(double) * e->n, cudaMemcpyDeviceToHost, e->st);
+    return from_engine(e, e->sync_check("get_vector"));
+}
+
+int sdddst_speeds(void *ctx, const double *xyb, double sim_time, int stress_type, double *v, double *tol)
+{
+    if (!ctx || !xyb || !v || !tol || stress_type < 0 || stress_type > 3)
+        return fail(SDDDST_ERR_INVALID, "bad argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    try {
+        ScratchConfig sc(e, xyb);
+        e->stress_calc(sim_time, stress_type, e->strain);
+        std::vector<double> t0(e->n, e->prec * e->prec);
+        // fresh precision handler for this evaluation
+        cudaMemcpyAsync(e->d_tol_last, e->d_tol, sizeof(double) * e->n, cudaMemcpyDeviceToDevice, e->st);
+        cudaMemcpyAsync(e->d_tol, t0.data(), sizeof(double) * e->n, cudaMemcpyHostToDevice, e->st);
+        e->speeds(e->d_xs, e->d_Stmp + 0, e->d_w, stress_type, true);
+        cudaMemcpyAsync(v, e->d_Stmp, sizeof(double) * e->n, cudaMemcpyDeviceToHost, e->st);
+        cudaMemcpyAsync(tol, e->d_tol, sizeof(double) * e->n, cudaMemcpyDeviceToHost, e->st);
+        cudaMemcpyAsync(e->d_tol, e->d_tol_last, sizeof(double) * e->n, cudaMemcpyDeviceToDevice, e->st);
+        return from_engine(e, e->sync_check("speeds"));
+    } catch (const std::exception &ex) {
+        return fail(SDDDST_ERR_NOMEM, ex.what());
+    }
+}
+
+int sdddst_jacobian(void *ctx, double h, const double *xyb, int *row_ptr, int *col, double *val, double *dvec,
+                    long cap, long *nnz)
+{
+    if (!ctx || !xyb || !row_ptr || !nnz) return fail(SDDDST_ERR_INVALID, "null argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    try {
+        ScratchConfig sc(e, xyb);
+        if (int rc = e->assemble(e->d_xs)) return from_engine(e, rc);
+        *nnz = e->nnz;
+        if (e->nnz > cap || !col || !val || !dvec) return fail(SDDDST_ERR_CAPACITY, "output capacity too small");
+        sd::launch_make_dvec(*e, h, e->d_dvec, e->st);
+        double *tmp = nullptr;
+        if (cudaMalloc(&tmp, sizeof(double) * e->nnz) != cudaSuccess) return fail(SDDDST_ERR_NOMEM, "export buffer");
+        sd::launch_export_jacobian(*e, h, e->d_dvec, tmp, e->st);
+        cudaMemcpyAsync(row_ptr, e->d_rowptr, sizeof(int) * (e->n + 1), cudaMemcpyDeviceToHost, e->st);
+        cudaMemcpyAsync(col, e->d_col, sizeof(int) * e->nnz, cudaMemcpyDeviceToHost, e->st);
+        cudaMemcpyAsync(val, tmp, sizeof(double) * e->nnz, cudaMemcpyDeviceToHost, e->st);
+        cudaMemcpyAsync(dvec, e->d_dvec, sizeof(double) * e->n, cudaMemcpyDeviceToHost, e->st);
+        int rc = e->sync_check("jacobian export");
+        cudaFree(tmp);
+        return from_engine(e, rc);
+    } catch (const std::exception &ex) {
+        return fail(SDDDST_ERR_NOMEM, ex.what());
+    }
+}
+
+int sdddst_solve(void *ctx, double h, const double *xyb, const double *rhs, double *x, int *iterations)
+{
+    if (!ctx || !xyb || !rhs || !x) return fail(SDDDST_ERR_INVALID, "null argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    try {
+        ScratchConfig sc(e, xyb);
+        if (int rc = e->assemble(e->d_xs)) return from_engine(e, rc);
+        sd::launch_make_dvec(*e, h, e->d_dvec, e->st);
+        cudaMemcpyAsync(e->d_g, rhs, sizeof(double) * e->n, cudaMemcpyHostToDevice, e->st);
+        int rc = e->solve(h, e->d_g, e->d_sol);
+        if (iterations) *iterations = e->last_iters;
+        if (rc) return from_engine(e, rc);
+        cudaMemcpyAsync(x, e->d_sol, sizeof(double) * e->n, cudaMemcpyDeviceToHost, e->st);
+        return from_engine(e, e->sync_check("solve"));
+    } catch (const std::exception &ex) {
+        return fail(SDDDST_ERR_NOMEM, ex.what());
+    }
+}
+
+int sdddst_step(void *ctx, int *accepted)
+{
+    if (!ctx) return fail(SDDDST_ERR_INVALID, "null argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    try {
+        return from_engine(e, e->step(accepted));
+    } catch (const std::exception &ex) {
+        return fail(SDDDST_ERR_NOMEM, ex.what());
+    }
+}
+
+int sdddst_run(void *ctx, int accepted_target, int max_attempts, int *accepted, int *attempts)
+{
+    if (!ctx) return fail(SDDDST_ERR_INVALID, "null argument");
+    int acc = 0, att = 0;
+    while (acc < accepted_target && att < max_attempts) {
+        int a = 0;
+        int rc = sdddst_step(ctx, &a);
+        att++;
+        if (rc) {
+            if (accepted) *accepted = acc;
+            if (attempts) *attempts = att;
+            return rc;
+        }
+        acc += a;
+    }
+    if (accepted) *accepted = acc;
+    if (attempts) *attempts = att;
+    return SDDDST_OK;
+}
+
+int sdddst_state_device(void *ctx, double **x, double **y, double **b)
+{
+    if (!ctx) return fail(SDDDST_ERR_INVALID, "null argument");
+    sd::Engine *e = E(ctx);
+    if (x) *x = e->d_x0;
+    if (y) *y = e->d_y;
+    if (b) *b = e->d_b;
+    return SDDDST_OK;
+}
+
+long sdddst_kernel_launches(void *ctx) { return ctx ? E(ctx)->launches : 0; }
+
+} // extern "C"

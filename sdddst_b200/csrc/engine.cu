@@ -1,0 +1,401 @@
+// Step driver of the implicit scheme on the device (reference:
+// src/simulation.cpp:62-84 integrate, :133-193 calculateG, :398-405
+// calculateXError, :435-650 step / stepStageI-III; precision handler
+// src/precision_handler.cpp:62-119; stress protocols
+// src/StressProtocols/*.cpp; cutoff src/simulation_data.cpp:208-218).
+//
+// All vectors stay in HBM.  The host keeps the scalars the reference keeps
+// in SimulationData / Simulation (step size, time, energy, counters, stress
+// values) and issues the kernels on the context's stream.  Stage I and stage
+// II share one Jacobian assembly: both are built at the accepted
+// configuration, and H(h/2) = H(h)/2 exactly, so only d(h) differs.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace sd {
+
+static const int kOrig = SDDDST_STAGE_ORIGINAL;
+static const int kEndBig = SDDDST_STAGE_END_OF_BIG_STEP;
+static const int kEndFirst = SDDDST_STAGE_END_OF_FIRST_SMALL_STEP;
+static const int kEndSecond = SDDDST_STAGE_END_OF_SECOND_SMALL_STEP;
+
+template <typename T>
+static int dalloc(T **p, size_t count)
+{
+    if (count == 0) count = 1;
+    return cudaMalloc((void **)p, sizeof(T) * count) == cudaSuccess ? 0 : SDDDST_ERR_NOMEM;
+}
+
+Engine::~Engine()
+{
+    if (device >= 0) cudaSetDevice(device);
+    void *bufs[] = {d_x0, d_y, d_b, d_xb, d_x1, d_x2, d_xs, d_v0, d_v0b, d_vs, d_vs2, d_S0, d_S1, d_Stmp,
+                    d_g, d_sol, d_dvec, d_tol, d_tol_last, d_minr2, d_part, d_pdx, d_pdy, d_cell,
+                    d_cell_count, d_cell_start, d_cell_fill, d_sorted, d_rowcnt, d_rowptr, d_col, d_val,
+                    d_V, d_w, d_z, d_r, d_hcol, d_partials, d_scal, d_y_small, d_ys, d_bs, d_flag};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (h_scal) cudaFreeHost(h_scal);
+    if (st) cudaStreamDestroy(st);
+}
+
+int Engine::sync_check(const char *what)
+{
+    cudaError_t e1 = cudaStreamSynchronize(st);
+    cudaError_t e2 = cudaGetLastError();
+    cudaError_t e = e1 != cudaSuccess ? e1 : e2;
+    if (e != cudaSuccess) {
+        err = std::string(what) + ": " + cudaGetErrorString(e);
+        return SDDDST_ERR_CUDA;
+    }
+    return 0;
+}
+
+// SimulationData::updateCutOff (simulation_data.cpp:208-218) and the cell
+// grid of the neighbour search.
+void Engine::update_cutoff()
+{
+    double m = cutoff_multiplier;
+    if (cutoff_multiplier >= 1. / 12. * std::sqrt(2.0 * double(n))) m = 1e20;
+    cutoff = 1. / std::sqrt((double)n) * m;
+    cutoff_sqr = cutoff * cutoff;
+    one_per_cutoff_sqr = 1. / cutoff_sqr;
+    // pairs are kept while (r - c)^2 < 36.8 c^2, i.e. r < (1 + sqrt(36.8)) c
+    double rc = cutoff * (1.0 + std::sqrt(36.8)) * (1.0 + 1e-9);
+    int g = rc >= 1.0 / 3.0 ? 1 : (int)std::floor(1.0 / rc);
+    if (g < 3) g = 1;
+    if (g > 1024) g = 1024;
+    G = g;
+}
+
+int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
+{
+    prm = p_;
+    n = prm.n;
+    p = prm.p;
+    device = prm.device;
+    if (n < 2 || p < 0) {
+        err = "n must be >= 2 and p >= 0";
+        return SDDDST_ERR_INVALID;
+    }
+    if (!xyb || (p > 0 && !pd)) {
+        err = "missing configuration arrays";
+        return SDDDST_ERR_INVALID;
+    }
+    if (prm.ic < 1) prm.ic = 2;
+    if (prm.gmres_restart < 2) prm.gmres_restart = 30;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        err = "cudaSetDevice failed";
+        return SDDDST_ERR_CUDA;
+    }
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+        err = "stream creation failed";
+        return SDDDST_ERR_CUDA;
+    }
+    cudaDeviceProp dp;
+    cudaGetDeviceProperties(&dp, device);
+    red_blocks = 2 * dp.multiProcessorCount;
+    cutoff_multiplier = prm.cutoff_multiplier;
+    prec = prm.prec;
+    A = prm.A;
+    KASQR = prm.KASQR;
+    ic = prm.ic;
+    step_size = prm.step_size;
+    restart = prm.gmres_restart;
+    update_cutoff();
+
+    int rc = 0;
+    double **vecs[] = {&d_x0, &d_y, &d_b, &d_xb, &d_x1, &d_x2, &d_xs, &d_v0, &d_v0b, &d_vs, &d_vs2,
+                       &d_S0, &d_S1, &d_Stmp, &d_g, &d_sol, &d_dvec, &d_tol, &d_tol_last, &d_w, &d_z,
+                       &d_r, &d_ys, &d_bs};
+    for (double **v : vecs) rc |= dalloc(v, n);
+    rc |= dalloc(&d_minr2, n);
+    rc |= dalloc(&d_part, pair_part_doubles(n));
+    rc |= dalloc(&d_pdx, p);
+    rc |= dalloc(&d_pdy, p);
+    const int ncell = G * G;
+    rc |= dalloc(&d_cell, n);
+    rc |= dalloc(&d_cell_count, ncell + 1);
+    rc |= dalloc(&d_cell_start, ncell + 1);
+    rc |= dalloc(&d_cell_fill, ncell + 1);
+    rc |= dalloc(&d_sorted, n);
+    rc |= dalloc(&d_rowcnt, n);
+    rc |= dalloc(&d_rowptr, n + 1);
+    rc |= dalloc(&d_flag, 4);
+    rc |= dalloc(&d_V, (size_t)(restart + 1) * n);
+    rc |= dalloc(&d_hcol, 2 * (restart + 1) + 4);
+    rc |= dalloc(&d_partials, (size_t)red_blocks * (restart + 2));
+    rc |= dalloc(&d_scal, 8);
+    rc |= dalloc(&d_y_small, (size_t)n + restart + 8);
+    if (cudaMallocHost((void **)&h_scal, sizeof(double) * (2 * (restart + 1) + 8)) != cudaSuccess)
+        rc |= SDDDST_ERR_NOMEM;
+    if (rc) {
+        err = "device allocation failed";
+        return SDDDST_ERR_NOMEM;
+    }
+    // initial CSR capacity from the expected neighbour count
+    double rcut = cutoff * (1.0 + std::sqrt(36.8));
+    double area = std::min(1.0, 3.14159265358979 * rcut * rcut);
+    long est = (long)((double)n * (1.0 + 1.3 * area * n)) + n + 1024;
+    if (est > (long)n * n + n) est = (long)n * n + n;
+    nnz_cap = est;
+    rc |= dalloc(&d_col, nnz_cap);
+    rc |= dalloc(&d_val, nnz_cap);
+    if (!rc) cudaMemsetAsync(d_col, 0, sizeof(int) * nnz_cap, st);
+    if (rc) {
+        err = "CSR allocation failed";
+        return SDDDST_ERR_NOMEM;
+    }
+    // upload the configuration (AoS {x,y,b} -> SoA)
+    std::vector<double> hx(n), hy(n), hb(n);
+    for (int i = 0; i < n; ++i) {
+        hx[i] = xyb[3 * i];
+        hy[i] = xyb[3 * i + 1];
+        hb[i] = xyb[3 * i + 2];
+    }
+    cudaMemcpyAsync(d_x0, hx.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_y, hy.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_b, hb.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    if (p > 0) {
+        std::vector<double> px(p), py(p);
+        for (int i = 0; i < p; ++i) {
+            px[i] = pd[2 * i];
+            py[i] = pd[2 * i + 1];
+        }
+        cudaMemcpyAsync(d_pdx, px.data(), sizeof(double) * p, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_pdy, py.data(), sizeof(double) * p, cudaMemcpyHostToDevice, st);
+    }
+    std::vector<double> t0(n, prec * prec);
+    cudaMemcpyAsync(d_tol, t0.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_tol_last, t0.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(d_dvec, 0, sizeof(double) * n, st);
+    return sync_check("init");
+}
+
+// ---------------------------------------------------------------- stress
+
+void Engine::stress_calc(double t, int type, double strain_now)
+{
+    if (prm.stress_kind == SDDDST_STRESS_FIXED_RATE) {
+        stress_vals[type] = t * prm.stress_rate; // fixed_rate_protocol.cpp:39-57
+    } else if (prm.stress_kind == SDDDST_STRESS_SPRING) {
+        double v = prm.spring_constant * (t * prm.stress_rate - strain_now); // spring_protocol.cpp:33-54
+        if (v < 0) v = 0;
+        stress_vals[type] = v;
+    }
+}
+
+double Engine::stress_get(int type) const
+{
+    if (prm.stress_kind == SDDDST_STRESS_FIXED_RATE || prm.stress_kind == SDDDST_STRESS_SPRING)
+        return stress_vals[type];
+    if (prm.stress_kind == SDDDST_STRESS_CONSTANT) return prm.stress_value;
+    return 0.0;
+}
+
+// ---------------------------------------------------------------- pieces
+
+static void reset_tol(Engine &e)
+{
+    // PrecisionHandler::reset (precision_handler.cpp:62-70)
+    std::vector<double> t0(e.n, e.prec * e.prec);
+    cudaMemcpyAsync(e.d_tol, t0.data(), sizeof(double) * e.n, cudaMemcpyHostToDevice, e.st);
+    cudaStreamSynchronize(e.st);
+}
+
+int Engine::speeds(const double *x, double *v_out, double *S_out, int stress_type, bool update_tol)
+{
+    const double tau_ext = stress_get(stress_type);
+    const double r2_track = update_tol ? 400.0 * prec * prec * (1.0 + 1e-9) : 0.0;
+    launch_pair_sum(*this, x, st, prm.pairsum, r2_track);
+    launch_speeds_finish(*this, x, tau_ext, S_out, v_out, update_tol ? 1 : 0, st);
+    launches += 3;
+    return 0;
+}
+
+int Engine::assemble(const double *x)
+{
+    int rc = jacobian_assemble(*this, x);
+    return rc;
+}
+
+int Engine::solve(double h, const double *rhs, double *x_out)
+{
+    int precond = prm.solver == SDDDST_SOLVER_GMRES_JACOBI;
+    return gmres_solve(*this, h, d_dvec, rhs, x_out, precond);
+}
+
+// Simulation::integrate (simulation.cpp:62-84) with calculateG
+// (simulation.cpp:133-193) inlined.
+int Engine::integrate(double h, double *xn, const double *xo, bool use2, bool init_speed, int origin, int end,
+                      bool reuse_assembly)
+{
+    if (!reuse_assembly)
+        if (int rc = assemble(xn)) return rc;
+    launch_make_dvec(*this, h, d_dvec, st);
+    launches++;
+    double *isp = use2 ? d_v0b : d_v0;
+    double *csp0 = use2 ? d_vs2 : d_vs;
+    double *Sorig = use2 ? d_S1 : d_S0;
+    for (int it = 0; it < ic; ++it) {
+        const bool calc_init = it == 0 ? init_speed : false;
+        const bool use_init_first = it == 0 ? zero_stress() : false;
+        double *csp = csp0;
+        if (calc_init) {
+            double t = sim_time, tasi = strain;
+            if (origin == kEndFirst) {
+                t += step_size * 0.5;
+                if (prm.stress_kind == SDDDST_STRESS_SPRING) {
+                    double inc;
+                    if (int rc = strain_inc(d_x0, d_x1, &inc)) return rc;
+                    tasi += inc;
+                }
+            }
+            stress_calc(t, origin, tasi);
+            cur_stress = origin;
+            speeds(xo, isp, Sorig, origin, true);
+        }
+        if (use_init_first) {
+            csp = isp;
+        } else {
+            double t = sim_time + step_size, tasi = strain;
+            if (prm.stress_kind == SDDDST_STRESS_SPRING) {
+                double inc1 = 0, inc2 = 0;
+                if (end == kEndFirst) {
+                    if (int rc = strain_inc(d_x0, d_x1, &inc1)) return rc;
+                } else if (end == kEndSecond) {
+                    if (int rc = strain_inc(d_x0, d_x1, &inc1)) return rc;
+                    if (int rc = strain_inc(d_x1, d_x2, &inc2)) return rc;
+                } else if (end == kEndBig) {
+                    if (int rc = strain_inc(d_x0, d_xb, &inc1)) return rc;
+                }
+                tasi += inc1 + inc2;
+            }
+            if (end == kEndFirst) t -= step_size * 0.5;
+            stress_calc(t, end, tasi);
+            cur_stress = end;
+            speeds(xn, csp, d_Stmp, end, true);
+        }
+        launch_residual_g(*this, h, xn, xo, csp, isp, d_dvec, d_g, st);
+        launches++;
+        if (int rc = solve(h, d_g, d_sol)) return rc;
+        launch_axpy_update(*this, xn, d_sol, st);
+        launches++;
+    }
+    return 0;
+}
+
+// Simulation::step = stepStageI + II + III (simulation.cpp:435-650).
+int Engine::step(int *accepted)
+{
+    const size_t bytes = sizeof(double) * n;
+    // ---- stage I (simulation.cpp:443-492)
+    energy_accum = 0;
+    vsquare = 0;
+    cur_stress = kOrig;
+    if (first_step) {
+        stress_calc(sim_time, kOrig, strain);
+        speeds(d_x0, d_v0, d_S0, kOrig, true);
+        init_speed_needed = false;
+        if (int rc = sum_sq(d_v0, &vsquare)) return rc;
+        first_step = false;
+    }
+    cudaMemcpyAsync(d_xb, d_x0, bytes, cudaMemcpyDeviceToDevice, st);
+    if (int rc = integrate(step_size, d_xb, d_x0, false, init_speed_needed, kOrig, kEndBig, false)) return rc;
+    successful_step = false;
+    // ---- stage II (simulation.cpp:494-499): same configuration, same G
+    cudaMemcpyAsync(d_x1, d_x0, bytes, cudaMemcpyDeviceToDevice, st);
+    if (int rc = integrate(0.5 * step_size, d_x1, d_x0, false, false, kOrig, kEndFirst, true)) return rc;
+    // ---- stage III (simulation.cpp:501-650)
+    sum_avg_speed = 0;
+    cudaMemcpyAsync(d_x2, d_x1, bytes, cudaMemcpyDeviceToDevice, st);
+    if (int rc = integrate(0.5 * step_size, d_x2, d_x1, true, true, kEndFirst, kEndSecond, false)) return rc;
+    if (int rc = sum_sq(d_v0, &vsquare1)) return rc;
+    if (int rc = sum_sq(d_v0b, &vsquare2)) return rc;
+    energy_accum = (vsquare1 + vsquare2) * 0.5 * step_size * 0.5;
+    double ratio = 0.0;
+    if (int rc = max_ratio(&ratio)) return rc;
+    if (!std::isfinite(ratio)) {
+        err = "step: non-finite error ratio";
+        return SDDDST_ERR_NONFINITE;
+    }
+    if (ratio < 1.0) {
+        successful_step = true;
+        init_speed_needed = true;
+        if (prm.calculate_strain) {
+            double a, b2;
+            if (int rc = strain_inc(d_x0, d_x1, &a)) return rc;
+            strain += a;
+            if (int rc = strain_inc(d_x1, d_x2, &b2)) return rc;
+            strain += b2;
+        }
+        std::swap(d_x0, d_x2);
+        sim_time += step_size;
+        succ++;
+        cur_stress = kOrig;
+        stress_calc(sim_time, kOrig, strain);
+        speeds(d_x0, d_v0, d_S0, kOrig, true);
+        init_speed_needed = false;
+        double sa;
+        if (int rc = sum_abs(d_v0, &sa)) return rc;
+        sum_avg_speed = sa / double(n);
+        if (int rc = sum_sq(d_v0, &vsquare)) return rc;
+        energy_accum += (vsquare2 + vsquare) * 0.5 * step_size * 0.5;
+        energy += energy_accum;
+    } else {
+        failed++;
+    }
+    // PrecisionHandler::getNewStepSize (precision_handler.cpp:103-119)
+    double hn;
+    if (0.0 == ratio) {
+        hn = step_size * 2.0;
+    } else {
+        double t = 1. / std::sqrt(ratio);
+        t = std::pow(t, 1. / 3.);
+        if (t > 2.0) t = 2.0;
+        hn = 0.9 * step_size * t;
+    }
+    step_size = hn;
+    last_ratio = ratio;
+    cudaMemcpyAsync(d_tol_last, d_tol, bytes, cudaMemcpyDeviceToDevice, st);
+    reset_tol(*this);
+    if (prm.max_step_limited && prm.max_step < step_size) step_size = prm.max_step;
+    if (accepted) *accepted = successful_step ? 1 : 0;
+    return sync_check("step");
+}
+
+int Engine::set_state_host(const double *xyb, double h, double t, double e, double s, int first)
+{
+    std::vector<double> hx(n), hy(n), hb(n);
+    for (int i = 0; i < n; ++i) {
+        hx[i] = xyb[3 * i];
+        hy[i] = xyb[3 * i + 1];
+        hb[i] = xyb[3 * i + 2];
+    }
+    cudaMemcpyAsync(d_x0, hx.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_y, hy.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_b, hb.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    step_size = h;
+    sim_time = t;
+    strain = s;
+    energy = e;
+    reset_tol(*this);
+    if (first) {
+        first_step = true;
+        init_speed_needed = true;
+        return sync_check("set_state");
+    }
+    first_step = false;
+    cur_stress = kOrig;
+    stress_calc(sim_time, kOrig, strain);
+    speeds(d_x0, d_v0, d_S0, kOrig, true);
+    init_speed_needed = false;
+    reset_tol(*this);
+    return sync_check("set_state");
+}
+
+} // namespace sd

@@ -1,0 +1,119 @@
+// Host-side engine of one simulated system: device buffers, parameters and
+// the step driver.  Mirrors the state of the reference's SimulationData +
+// Simulation + PrecisionHandler (include/simulation_data.h:69-144,
+// include/simulation.h:73-85, include/precision_handler.h:54-59) with the
+// vectors resident in HBM as structure-of-arrays doubles.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/sdddst_b200.h"
+
+namespace sd {
+
+struct Engine {
+    // ---- sizes and parameters
+    int n = 0, p = 0, device = 0;
+    sdddst_params prm{};
+    double cutoff_multiplier = 1.0, cutoff = 1.0, cutoff_sqr = 1.0, one_per_cutoff_sqr = 1.0;
+    double prec = 1e-8, A = 0, KASQR = 0;
+    int ic = 2;
+    cudaStream_t st = nullptr;
+
+    // ---- configuration and step vectors (N doubles each)
+    double *d_x0 = nullptr, *d_y = nullptr, *d_b = nullptr; // accepted configuration
+    double *d_xb = nullptr, *d_x1 = nullptr, *d_x2 = nullptr, *d_xs = nullptr;
+    double *d_v0 = nullptr, *d_v0b = nullptr, *d_vs = nullptr, *d_vs2 = nullptr;
+    double *d_S0 = nullptr, *d_S1 = nullptr, *d_Stmp = nullptr; // pair+defect sums without tau_ext
+    double *d_g = nullptr, *d_sol = nullptr, *d_dvec = nullptr;
+    double *d_tol = nullptr, *d_tol_last = nullptr;
+    unsigned long long *d_minr2 = nullptr;
+    double *d_part = nullptr;
+    double *d_pdx = nullptr, *d_pdy = nullptr;
+    double *d_ys = nullptr, *d_bs = nullptr; // scratch y, b of caller-supplied configurations
+
+    // ---- cell list of the cutoff-neighbour search
+    int G = 1; // cells per axis
+    int *d_cell = nullptr, *d_cell_count = nullptr, *d_cell_start = nullptr, *d_cell_fill = nullptr;
+    int *d_sorted = nullptr;
+
+    // ---- CSR of the unit-step Jacobian part G = H / h (diagonal in slot 0 of each row)
+    int *d_rowcnt = nullptr, *d_rowptr = nullptr, *d_col = nullptr;
+    double *d_val = nullptr;
+    long nnz_cap = 0, nnz = 0;
+    int *d_flag = nullptr; // device-side error flag of the assembly
+    bool assembled_valid = false;
+    const double *assembled_for = nullptr;
+
+    // ---- Krylov workspace
+    int restart = 30;
+    double *d_V = nullptr, *d_w = nullptr, *d_z = nullptr, *d_r = nullptr, *d_hcol = nullptr;
+    double *d_partials = nullptr, *d_scal = nullptr, *d_y_small = nullptr;
+    int red_blocks = 0;
+    double *h_scal = nullptr; // pinned
+    int last_iters = 0;
+    double last_resid = 0.0;
+
+    // ---- host scalars (SimulationData / Simulation members)
+    double step_size = 1.0, sim_time = 0.0, strain = 0.0;
+    double energy = 0.0, energy_accum = 0.0, vsquare = 0.0, vsquare1 = 0.0, vsquare2 = 0.0;
+    double sum_avg_speed = 0.0, last_ratio = 0.0;
+    double stress_vals[4] = {0, 0, 0, 0};
+    long succ = 0, failed = 0;
+    bool first_step = true, init_speed_needed = true, successful_step = true;
+    int cur_stress = 0;
+
+    long launches = 0;
+    std::string err;
+
+    ~Engine();
+    int init(const sdddst_params &prm, const double *xyb, const double *pd);
+    void update_cutoff();
+
+    // reference operations
+    int speeds(const double *x, double *v_out, double *S_out, int stress_type, bool update_tol);
+    int assemble(const double *x);
+    int solve(double h, const double *rhs, double *x_out);
+    int integrate(double h, double *xn, const double *xo, bool use2, bool init_speed, int origin, int end,
+                  bool reuse_assembly);
+    int step(int *accepted);
+    int set_state_host(const double *xyb, double step, double t, double e, double strain, int first);
+
+    // stress protocol (host scalars)
+    void stress_calc(double t, int type, double strain_now);
+    double stress_get(int type) const;
+    bool zero_stress() const { return prm.stress_kind == SDDDST_STRESS_ZERO; }
+
+    // device reductions (results on host)
+    int sum_sq(const double *v, double *out);
+    int sum_abs(const double *v, double *out);
+    int strain_inc(const double *xo, const double *xn, double *out);
+    int max_ratio(double *out);
+    int sync_check(const char *what);
+};
+
+// ---- launchers (one .cu file each)
+int pair_tile_size(int n);
+size_t pair_part_doubles(int n);
+void launch_pair_sum(const Engine &e, const double *x, cudaStream_t st, int mode, double r2_track);
+void launch_speeds_finish(const Engine &e, const double *x, double tau_ext, double *S, double *v, int update_tol,
+                          cudaStream_t st);
+void launch_add_stress(const Engine &e, const double *S, double tau_ext, double *v, cudaStream_t st);
+
+int jacobian_assemble(Engine &e, const double *x);
+void launch_make_dvec(const Engine &e, double h, double *dvec, cudaStream_t st);
+void launch_export_jacobian(const Engine &e, double h, const double *dvec, double *val_out, cudaStream_t st);
+
+void launch_spmv_J(const Engine &e, double h, const double *dvec, const double *v, double *y, cudaStream_t st);
+int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, double *x, int precond);
+
+void launch_residual_g(const Engine &e, double h, const double *xn, const double *xo, const double *csp,
+                       const double *isp, const double *dvec, double *g, cudaStream_t st);
+void launch_axpy_update(const Engine &e, double *xn, const double *sol, cudaStream_t st);
+
+int reduce_sum(Engine &e, const double *a, const double *b, int n, int op, double *out);
+
+} // namespace sd

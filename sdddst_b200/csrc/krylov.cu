@@ -1,0 +1,391 @@
+// Linear solve of the chord-Newton system J(h) x = g (the UMFPACK
+// symbolic + numeric + solve sequence of the reference,
+// src/simulation.cpp:386-396), plus the small vector kernels of the step.
+//
+// J(h) = I + diag((1 + d)/2) h G is applied matrix-free from the CSR of G
+// (warp per row).  The solver is restarted GMRES with classical Gram-Schmidt
+// and one re-orthogonalisation pass (CGS2), FP64 throughout, optionally right
+// preconditioned by diag(J)^-1.  The (m+1) x m Hessenberg matrix and its
+// Givens rotations live on the host; each iteration moves one packed vector
+// of 2m+3 doubles device-to-host.  All reductions are two-stage with a fixed
+// grid, so results are bit-reproducible run to run.
+#include "engine.h"
+#include "common.cuh"
+
+#include <cmath>
+#include <vector>
+
+namespace sd {
+
+// y = J v  (warp per row)
+__global__ void spmv_j_kernel(int n, double h, const int *__restrict__ rowptr, const int *__restrict__ col,
+                              const double *__restrict__ val, const double *__restrict__ dvec,
+                              const double *__restrict__ v, double *__restrict__ y)
+{
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const int s = rowptr[row], e = rowptr[row + 1];
+    double acc = 0.0;
+    for (int q = s + lane; q < e; q += 32) acc += val[q] * v[col[q]];
+    acc = warp_sum(acc);
+    if (lane == 0) y[row] = v[row] + (1.0 + dvec[row]) * 0.5 * h * acc;
+}
+
+// diag(J)_i = 1 + (1 + d_i)/2 h G_ii
+__global__ void jdiag_inv_kernel(int n, double h, const int *__restrict__ rowptr, const double *__restrict__ val,
+                                 const double *__restrict__ dvec, double *__restrict__ dinv)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dinv[i] = 1.0 / (1.0 + (1.0 + dvec[i]) * 0.5 * h * val[rowptr[i]]);
+}
+
+__global__ void mul_kernel(int n, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ c)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) c[i] = a[i] * b[i];
+}
+
+__global__ void scale_kernel(int n, double s, const double *__restrict__ a, double *__restrict__ c)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) c[i] = a[i] * s;
+}
+
+__global__ void sub_kernel(int n, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ c)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) c[i] = a[i] - b[i];
+}
+
+// partials[blk * kk + k] = sum over the block's slice of V[k][i] w[i]
+__global__ void multi_dot_partial_kernel(int n, int kk, const double *__restrict__ V, size_t ldv,
+                                         const double *__restrict__ w, double *__restrict__ partials)
+{
+    __shared__ double red[32];
+    const int nb = gridDim.x;
+    const int chunk = (n + nb - 1) / nb;
+    const int s = blockIdx.x * chunk;
+    const int e = min(n, s + chunk);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = 0; k < kk; ++k) {
+        const double *vk = V + (size_t)k * ldv;
+        double acc = 0.0;
+        for (int i = s + threadIdx.x; i < e; i += blockDim.x) acc += vk[i] * w[i];
+        acc = warp_sum(acc);
+        if (lane == 0) red[wid] = acc;
+        __syncthreads();
+        if (wid == 0) {
+            double t = lane < nw ? red[lane] : 0.0;
+            t = warp_sum(t);
+            if (lane == 0) partials[(size_t)blockIdx.x * kk + k] = t;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void multi_dot_final_kernel(int nb, int kk, const double *__restrict__ partials, double *__restrict__ out)
+{
+    const int k = blockIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) acc += partials[(size_t)b * kk + k];
+    acc = warp_sum(acc);
+    if (lane == 0) red[wid] = acc;
+    __syncthreads();
+    if (wid == 0) {
+        double t = lane < nw ? red[lane] : 0.0;
+        t = warp_sum(t);
+        if (lane == 0) out[k] = t;
+    }
+}
+
+// w -= sum_k V[k] c[k]
+__global__ void gs_update_kernel(int n, int kk, const double *__restrict__ V, size_t ldv,
+                                 const double *__restrict__ c, double *__restrict__ w)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double acc = w[i];
+    for (int k = 0; k < kk; ++k) acc -= V[(size_t)k * ldv + i] * c[k];
+    w[i] = acc;
+}
+
+// x += sum_k V[k] y[k]  (optionally times dinv)
+__global__ void combine_kernel(int n, int kk, const double *__restrict__ V, size_t ldv, const double *__restrict__ y,
+                               const double *__restrict__ dinv, double *__restrict__ x)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double acc = 0.0;
+    for (int k = 0; k < kk; ++k) acc += V[(size_t)k * ldv + i] * y[k];
+    if (dinv) acc *= dinv[i];
+    x[i] += acc;
+}
+
+// g_i = x_new - (1+d)/2 h v_new - x_old - (1-d)/2 h v_old (simulation.cpp:189-192)
+__global__ void residual_g_kernel(int n, double h, const double *__restrict__ xn, const double *__restrict__ xo,
+                                  const double *__restrict__ csp, const double *__restrict__ isp,
+                                  const double *__restrict__ dvec, double *__restrict__ g)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double d = dvec[i];
+    const double a = __dmul_rn(__dmul_rn(__dmul_rn(__dadd_rn(1.0, d), 0.5), h), csp[i]);
+    const double c = __dmul_rn(__dmul_rn(__dmul_rn(__dsub_rn(1.0, d), 0.5), h), isp[i]);
+    g[i] = __dsub_rn(__dsub_rn(__dsub_rn(xn[i], a), xo[i]), c);
+}
+
+// x_new[j] -= x[j] (simulation.cpp:78-81)
+__global__ void update_kernel(int n, double *__restrict__ xn, const double *__restrict__ sol)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) xn[i] -= sol[i];
+}
+
+// ---- generic reductions: op 0 sum a^2, 1 sum |a|, 2 sum b (a - c),
+//      3 max over i of (|a - c| > 0 ? (a - c)^2 / b : 0), 4 sum a b
+template <int OP>
+__device__ __forceinline__ double red_term(int i, const double *a, const double *b, const double *c)
+{
+    if (OP == 0) return a[i] * a[i];
+    if (OP == 1) return fabs(a[i]);
+    if (OP == 2) return b[i] * (a[i] - c[i]);
+    if (OP == 3) {
+        double e = fabs(a[i] - c[i]);
+        return e > 0.0 ? __ddiv_rn(__dmul_rn(e, e), b[i]) : 0.0; // precision_handler.cpp:94
+    }
+    return a[i] * b[i];
+}
+
+template <int OP>
+__global__ void reduce_partial_kernel(int n, const double *__restrict__ a, const double *__restrict__ b,
+                                      const double *__restrict__ c, double *__restrict__ partials)
+{
+    __shared__ double red[32];
+    const int nb = gridDim.x;
+    const int chunk = (n + nb - 1) / nb;
+    const int s = blockIdx.x * chunk, e = min(n, s + chunk);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double acc = 0.0;
+    for (int i = s + threadIdx.x; i < e; i += blockDim.x) {
+        double t = red_term<OP>(i, a, b, c);
+        acc = OP == 3 ? fmax(acc, t) : acc + t;
+    }
+    acc = OP == 3 ? warp_max(acc) : warp_sum(acc);
+    if (lane == 0) red[wid] = acc;
+    __syncthreads();
+    if (wid == 0) {
+        double t = lane < nw ? red[lane] : 0.0;
+        t = OP == 3 ? warp_max(t) : warp_sum(t);
+        if (lane == 0) partials[blockIdx.x] = t;
+    }
+}
+
+template <int OP>
+__global__ void reduce_final_kernel(int nb, const double *__restrict__ partials, double *__restrict__ out)
+{
+    __shared__ double red[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) acc = OP == 3 ? fmax(acc, partials[k]) : acc + partials[k];
+    acc = OP == 3 ? warp_max(acc) : warp_sum(acc);
+    if (lane == 0) red[wid] = acc;
+    __syncthreads();
+    if (wid == 0) {
+        double t = lane < nw ? red[lane] : 0.0;
+        t = OP == 3 ? warp_max(t) : warp_sum(t);
+        if (lane == 0) *out = t;
+    }
+}
+
+template <int OP>
+static void launch_reduce(Engine &e, int n, const double *a, const double *b, const double *c, double *dst)
+{
+    reduce_partial_kernel<OP><<<e.red_blocks, 256, 0, e.st>>>(n, a, b, c, e.d_partials);
+    reduce_final_kernel<OP><<<1, 256, 0, e.st>>>(e.red_blocks, e.d_partials, dst);
+    e.launches += 2;
+}
+
+// Reduction with its result copied to the host (synchronises the stream).
+int reduce_sum(Engine &e, const double *a, const double *b, int n, int op, double *out)
+{
+    switch (op) {
+    case 0: launch_reduce<0>(e, n, a, nullptr, nullptr, e.d_scal); break;
+    case 1: launch_reduce<1>(e, n, a, nullptr, nullptr, e.d_scal); break;
+    case 4: launch_reduce<4>(e, n, a, b, nullptr, e.d_scal); break;
+    default: return SDDDST_ERR_INVALID;
+    }
+    cudaMemcpyAsync(e.h_scal, e.d_scal, sizeof(double), cudaMemcpyDeviceToHost, e.st);
+    if (int rc = e.sync_check("reduce")) return rc;
+    *out = e.h_scal[0];
+    return 0;
+}
+
+int Engine::sum_sq(const double *v, double *out) { return reduce_sum(*this, v, nullptr, n, 0, out); }
+int Engine::sum_abs(const double *v, double *out) { return reduce_sum(*this, v, nullptr, n, 1, out); }
+
+int Engine::strain_inc(const double *xo, const double *xn, double *out)
+{
+    launch_reduce<2>(*this, n, xn, d_b, xo, d_scal);
+    cudaMemcpyAsync(h_scal, d_scal, sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (int rc = sync_check("strain")) return rc;
+    *out = h_scal[0];
+    return 0;
+}
+
+int Engine::max_ratio(double *out)
+{
+    launch_reduce<3>(*this, n, d_xb, d_tol, d_x2, d_scal);
+    cudaMemcpyAsync(h_scal, d_scal, sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (int rc = sync_check("error ratio")) return rc;
+    *out = h_scal[0];
+    return 0;
+}
+
+void launch_spmv_J(const Engine &e, double h, const double *dvec, const double *v, double *y, cudaStream_t st)
+{
+    const int wpb = 8;
+    spmv_j_kernel<<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_rowptr, e.d_col, e.d_val, dvec, v, y);
+}
+
+void launch_residual_g(const Engine &e, double h, const double *xn, const double *xo, const double *csp,
+                       const double *isp, const double *dvec, double *g, cudaStream_t st)
+{
+    residual_g_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, h, xn, xo, csp, isp, dvec, g);
+}
+
+void launch_axpy_update(const Engine &e, double *xn, const double *sol, cudaStream_t st)
+{
+    update_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, xn, sol);
+}
+
+// Restarted GMRES(m) on J(h) x = rhs, x0 = 0.  Returns 0 on convergence to
+// e.prm.solver_tol relative residual, SDDDST_ERR_SOLVER otherwise.
+int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, double *x, int precond)
+{
+    const int n = e.n, m = e.restart;
+    const size_t ldv = (size_t)n;
+    cudaStream_t st = e.st;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    const double tol = e.prm.solver_tol > 0 ? e.prm.solver_tol : 1e-13;
+    const int max_it = e.prm.max_iters > 0 ? e.prm.max_iters : 1000;
+    double *V = e.d_V, *w = e.d_w, *z = e.d_z, *r = e.d_r;
+    double *dinv = nullptr;
+    cudaMemsetAsync(x, 0, sizeof(double) * n, st);
+    if (precond) {
+        dinv = e.d_y_small; // n doubles reserved for the diagonal
+        jdiag_inv_kernel<<<nb, 256, 0, st>>>(n, h, e.d_rowptr, e.d_val, dvec, dinv);
+        e.launches++;
+    }
+    double beta0;
+    if (int rc = reduce_sum(e, rhs, rhs, n, 4, &beta0)) return rc;
+    beta0 = std::sqrt(beta0);
+    e.last_iters = 0;
+    e.last_resid = 0.0;
+    if (beta0 == 0.0) return 0;
+    if (!std::isfinite(beta0)) {
+        e.err = "solve: non-finite right-hand side";
+        return SDDDST_ERR_NONFINITE;
+    }
+    cudaMemcpyAsync(r, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
+    double beta = beta0;
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), gv(m + 1), yv(m);
+    double *hpk = e.h_scal; // pinned, 2m+3 doubles
+    int total = 0;
+    bool converged = false;
+    const int wpb = 8;
+    while (!converged) {
+        scale_kernel<<<nb, 256, 0, st>>>(n, 1.0 / beta, r, V);
+        e.launches++;
+        std::fill(gv.begin(), gv.end(), 0.0);
+        gv[0] = beta;
+        int k = 0;
+        for (int j = 0; j < m; ++j) {
+            const double *vj = V + (size_t)j * ldv;
+            const double *src = vj;
+            if (precond) {
+                mul_kernel<<<nb, 256, 0, st>>>(n, vj, dinv, z);
+                src = z;
+                e.launches++;
+            }
+            spmv_j_kernel<<<(n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, src, w);
+            const int kk = j + 1;
+            // CGS2
+            multi_dot_partial_kernel<<<e.red_blocks, 256, 0, st>>>(n, kk, V, ldv, w, e.d_partials);
+            multi_dot_final_kernel<<<kk, 256, 0, st>>>(e.red_blocks, kk, e.d_partials, e.d_hcol);
+            gs_update_kernel<<<nb, 256, 0, st>>>(n, kk, V, ldv, e.d_hcol, w);
+            multi_dot_partial_kernel<<<e.red_blocks, 256, 0, st>>>(n, kk, V, ldv, w, e.d_partials);
+            multi_dot_final_kernel<<<kk, 256, 0, st>>>(e.red_blocks, kk, e.d_partials, e.d_hcol + (m + 1));
+            gs_update_kernel<<<nb, 256, 0, st>>>(n, kk, V, ldv, e.d_hcol + (m + 1), w);
+            reduce_partial_kernel<4><<<e.red_blocks, 256, 0, st>>>(n, w, w, nullptr, e.d_partials);
+            reduce_final_kernel<4><<<1, 256, 0, st>>>(e.red_blocks, e.d_partials, e.d_hcol + 2 * (m + 1));
+            e.launches += 9;
+            cudaMemcpyAsync(hpk, e.d_hcol, sizeof(double) * (2 * (m + 1) + 1), cudaMemcpyDeviceToHost, st);
+            if (int rc = e.sync_check("gmres iteration")) return rc;
+            double hn = std::sqrt(std::max(hpk[2 * (m + 1)], 0.0));
+            for (int i = 0; i < kk; ++i) H[(size_t)i * m + j] = hpk[i] + hpk[(m + 1) + i];
+            H[(size_t)(j + 1) * m + j] = hn;
+            if (!std::isfinite(hn)) {
+                e.err = "solve: non-finite Krylov vector";
+                return SDDDST_ERR_NONFINITE;
+            }
+            if (hn > 0.0) {
+                scale_kernel<<<nb, 256, 0, st>>>(n, 1.0 / hn, w, V + (size_t)(j + 1) * ldv);
+                e.launches++;
+            }
+            // Givens
+            for (int i = 0; i < j; ++i) {
+                double a = H[(size_t)i * m + j], b2 = H[(size_t)(i + 1) * m + j];
+                H[(size_t)i * m + j] = cs[i] * a + sn[i] * b2;
+                H[(size_t)(i + 1) * m + j] = -sn[i] * a + cs[i] * b2;
+            }
+            double a = H[(size_t)j * m + j], b2 = H[(size_t)(j + 1) * m + j];
+            double rr = std::hypot(a, b2);
+            cs[j] = rr > 0 ? a / rr : 1.0;
+            sn[j] = rr > 0 ? b2 / rr : 0.0;
+            H[(size_t)j * m + j] = rr;
+            H[(size_t)(j + 1) * m + j] = 0.0;
+            gv[j + 1] = -sn[j] * gv[j];
+            gv[j] = cs[j] * gv[j];
+            ++total;
+            k = j + 1;
+            if (std::fabs(gv[j + 1]) <= tol * beta0 || hn == 0.0) {
+                converged = true;
+                break;
+            }
+            if (total >= max_it) break;
+        }
+        // back substitution
+        for (int i = k - 1; i >= 0; --i) {
+            double s = gv[i];
+            for (int q = i + 1; q < k; ++q) s -= H[(size_t)i * m + q] * yv[q];
+            yv[i] = s / H[(size_t)i * m + i];
+        }
+        cudaMemcpyAsync(e.d_y_small + n, yv.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st);
+        combine_kernel<<<nb, 256, 0, st>>>(n, k, V, ldv, e.d_y_small + n, dinv, x);
+        e.launches++;
+        if (converged) break;
+        if (total >= max_it) break;
+        // true residual for the restart
+        spmv_j_kernel<<<(n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, x, w);
+        sub_kernel<<<nb, 256, 0, st>>>(n, rhs, w, r);
+        e.launches += 2;
+        double b2;
+        if (int rc = reduce_sum(e, r, r, n, 4, &b2)) return rc;
+        beta = std::sqrt(b2);
+        if (beta <= tol * beta0) {
+            converged = true;
+            break;
+        }
+    }
+    e.last_iters = total;
+    if (!converged) {
+        e.err = "solve: GMRES did not reach the residual target";
+        return SDDDST_ERR_SOLVER;
+    }
+    return 0;
+}
+
+} // namespace sd

@@ -1,0 +1,199 @@
+// O(N^2) velocity pair sum (reference: Simulation::calculateSpeeds,
+// src/simulation.cpp:86-131).
+//
+// Work is split into T x T tiles (I, J), I <= J, over the unique pairs
+// i < j (the reference's antisymmetry res[i] += t, res[j] -= t).  A CTA stages
+// the J block's x, y, b in shared memory; each thread owns one row i of the
+// I block and walks the block's columns.  Row sums stay in registers; column
+// sums are transposed through shared memory per 32-column chunk and reduced
+// across warps.  Every partial lands in a private slot of part[nblk][N]:
+//   part[J][i] <- row partial of tile (I, J) for i in block I
+//   part[I][j] <- column partial of tile (I, J) for j in block J
+//   part[I][i] <- both partials of the diagonal tile (I, I)
+// so no two tiles write the same slot and the final per-dislocation sum over
+// the nblk slots runs in a fixed order (bit-reproducible run to run).
+//
+// The precision handler needs min r^2 per dislocation only below
+// 400 prec^2 (updateTolerance, precision_handler.cpp:72-87, acts only when
+// r^2/400 < prec^2), so close pairs alone do an atomicMin on the bit pattern.
+#include "engine.h"
+#include "field_f64.cuh"
+#include "field_f32.cuh"
+
+namespace sd {
+
+__device__ __forceinline__ void tile_coords(long t, int &I, int &J)
+{
+    int j = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((long)j * (j + 1) / 2 > t) --j;
+    while ((long)(j + 1) * (j + 2) / 2 <= t) ++j;
+    J = j;
+    I = (int)(t - (long)j * (j + 1) / 2);
+}
+
+template <int T, int kMode>
+__global__ void __launch_bounds__(T) pair_tiles_kernel(const double *__restrict__ x, const double *__restrict__ y,
+                                                       const double *__restrict__ b, int n, int nblk,
+                                                       double *__restrict__ part,
+                                                       unsigned long long *__restrict__ minr2, double r2_track)
+{
+    constexpr int W = T / 32;
+    __shared__ double sx[T], sy[T], sb[T];
+    __shared__ double tbuf[W][32][33];
+    __shared__ double colsum[W][T];
+
+    int I, J;
+    tile_coords((long)blockIdx.x, I, J);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int j0 = J * T;
+    {
+        int j = j0 + tid;
+        bool ok = j < n;
+        sx[tid] = ok ? x[j] : 0.0;
+        sy[tid] = ok ? y[j] : 0.0;
+        sb[tid] = ok ? b[j] : 0.0;
+    }
+    const int i = I * T + tid;
+    const bool row_ok = i < n;
+    const double xi = row_ok ? x[i] : 0.0;
+    const double yi = row_ok ? y[i] : 0.0;
+    const double bi = row_ok ? b[i] : 0.0;
+    const bool diag = (I == J);
+    __syncthreads();
+
+    double acc = 0.0;
+    for (int c0 = 0; c0 < T; c0 += 32) {
+#pragma unroll 2
+        for (int k = 0; k < 32; ++k) {
+            const int jj = c0 + k;
+            const bool valid = row_ok && (j0 + jj < n) && (!diag || jj > tid);
+            double dx = wrap_half(xi - sx[jj]);
+            double dy = wrap_half(yi - sy[jj]);
+            double r2 = r2_exact(dx, dy);
+            if (!valid) {
+                dx = 0.25;
+                dy = 0.25;
+            }
+            double t;
+            if (kMode == 0) t = bi * sb[jj] * tau_xy_f64(dx, dy);
+            else t = bi * sb[jj] * (double)tau_xy_f32(dx, dy);
+            t = valid ? t : 0.0;
+            acc += t;
+            if (valid && r2 < r2_track) { // rare: only pairs that can set a tolerance
+                atomic_min_nonneg(&minr2[i], r2);
+                atomic_min_nonneg(&minr2[j0 + jj], r2);
+            }
+            tbuf[warp][k][lane] = t;
+        }
+        __syncwarp();
+        double cs = 0.0;
+#pragma unroll 8
+        for (int m = 0; m < 32; ++m) cs += tbuf[warp][lane][m];
+        colsum[warp][c0 + lane] = cs;
+        __syncwarp();
+    }
+    __syncthreads();
+    double ctot = 0.0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) ctot += colsum[w][tid];
+
+    if (diag) {
+        if (row_ok) part[(size_t)I * n + i] = acc - ctot;
+    } else {
+        if (row_ok) part[(size_t)J * n + i] = acc;
+        if (j0 + tid < n) part[(size_t)I * n + j0 + tid] = -ctot;
+    }
+}
+
+// Per-dislocation finish: sum of the nblk partials in fixed order, point
+// defects (simulation.cpp:111-128), S = pair + defect sum, v = S + b tau_ext
+// (simulation.cpp:129), and the tolerance update from min r^2.
+__global__ void speeds_finish_kernel(int n, int nblk, const double *__restrict__ part, const double *__restrict__ x,
+                                     const double *__restrict__ y, const double *__restrict__ b, int p,
+                                     const double *__restrict__ pdx, const double *__restrict__ pdy, double A,
+                                     double K, double tau_ext, double *__restrict__ S, double *__restrict__ v,
+                                     const unsigned long long *__restrict__ minr2, double *__restrict__ tol,
+                                     double prec_sqr, int update_tol)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double acc = 0.0;
+    for (int L = 0; L < nblk; ++L) acc += part[(size_t)L * n + i];
+    double smin = __longlong_as_double((long long)minr2[i]);
+    const double xi = x[i], yi = y[i], bi = b[i];
+    for (int q = 0; q < p; ++q) {
+        double dx = wrap_half(xi - pdx[q]);
+        double dy = wrap_half(yi - pdy[q]);
+        double s;
+        double g = pd_force_f64(dx, dy, A, K, &s);
+        acc -= g * bi;
+        if (s < smin) smin = s;
+    }
+    S[i] = acc;
+    v[i] = acc + bi * tau_ext;
+    if (update_tol) {
+        double t = __dmul_rn(__dmul_rn(smin, 0.25), 1e-2); // precision_handler.cpp:74
+        double cur = tol[i];
+        if (t < prec_sqr && t < cur) tol[i] = (t == 0.0) ? kEps : t;
+    }
+}
+
+__global__ void add_stress_kernel(int n, const double *__restrict__ S, const double *__restrict__ b, double tau_ext,
+                                  double *__restrict__ v)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = S[i] + b[i] * tau_ext;
+}
+
+__global__ void fill_u64_kernel(unsigned long long *p, unsigned long long v, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+int pair_tile_size(int n) { return n >= 8192 ? 128 : 64; }
+
+void launch_pair_sum(const Engine &e, const double *x, cudaStream_t st, int mode, double r2_track)
+{
+    const int n = e.n;
+    const int T = pair_tile_size(n);
+    const int nblk = (n + T - 1) / T;
+    const long tiles = (long)nblk * (nblk + 1) / 2;
+    fill_u64_kernel<<<(n + 255) / 256, 256, 0, st>>>(e.d_minr2, 0x7FF0000000000000ull, n);
+    if (T == 128) {
+        if (mode == 0)
+            pair_tiles_kernel<128, 0><<<(unsigned)tiles, 128, 0, st>>>(x, e.d_y, e.d_b, n, nblk, e.d_part, e.d_minr2, r2_track);
+        else
+            pair_tiles_kernel<128, 1><<<(unsigned)tiles, 128, 0, st>>>(x, e.d_y, e.d_b, n, nblk, e.d_part, e.d_minr2, r2_track);
+    } else {
+        if (mode == 0)
+            pair_tiles_kernel<64, 0><<<(unsigned)tiles, 64, 0, st>>>(x, e.d_y, e.d_b, n, nblk, e.d_part, e.d_minr2, r2_track);
+        else
+            pair_tiles_kernel<64, 1><<<(unsigned)tiles, 64, 0, st>>>(x, e.d_y, e.d_b, n, nblk, e.d_part, e.d_minr2, r2_track);
+    }
+}
+
+void launch_speeds_finish(const Engine &e, const double *x, double tau_ext, double *S, double *v, int update_tol,
+                          cudaStream_t st)
+{
+    const int n = e.n;
+    const int T = pair_tile_size(n);
+    const int nblk = (n + T - 1) / T;
+    speeds_finish_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, nblk, e.d_part, x, e.d_y, e.d_b, e.p, e.d_pdx, e.d_pdy,
+                                                         e.A, e.KASQR, tau_ext, S, v, e.d_minr2, e.d_tol,
+                                                         e.prec * e.prec, update_tol);
+}
+
+void launch_add_stress(const Engine &e, const double *S, double tau_ext, double *v, cudaStream_t st)
+{
+    add_stress_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, S, e.d_b, tau_ext, v);
+}
+
+size_t pair_part_doubles(int n)
+{
+    const int T = pair_tile_size(n);
+    const int nblk = (n + T - 1) / T;
+    return (size_t)nblk * (size_t)n;
+}
+
+} // namespace sd

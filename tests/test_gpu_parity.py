@@ -1,0 +1,196 @@
+"""GPU parity of the CUDA path against the oracle, through the C ABI.
+
+The oracle is the C restatement (oracle/sdddst_oracle.c), itself pinned
+bit-for-bit to the reference (tests/test_oracle.py); the committed golden
+fixtures of the reference are checked directly too.
+
+Tolerances (FP64 plain path):
+  * velocities: |dv_i| <= 1e-10 * max|v| + 1e-9 |v_i|  (the device sums pairs
+    in a different order and evaluates the field with a shared exp and exact
+    near-field identities instead of per-image cosh and a Taylor branch);
+  * tolerances: bit-exact without point defects (same r^2 arithmetic);
+  * Jacobian: same sparsity pattern, |dJ_ij| <= 1e-10 * max|J offdiag|;
+  * positions after a teacher-forced step: 1e-10 relative, error ratio 1e-6
+    relative (it divides a ~1e-6 position difference by a ~1e-12 tolerance),
+    identical accept/reject decisions and step sizes to 1e-6 relative.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import ref
+from sdddst_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def make_pair(n, seed, m, prec, p=0, sk=0, sv=0.0, step=1e-6, **kw):
+    from sdddst_b200 import capi
+    xyb, pd = workloads.dislocations(n, seed, p)
+    rp = ref.params(cutoff_multiplier=m, prec=prec, step_size=step, stress_kind=sk, stress_value=sv,
+                    pd_scaling=p > 0)
+    oracle = ref.Sim(xyb, pd if p else None, rp, "port")
+    prm = capi.cli_params(n, m, prec, step_size=step, p=p, pd_scaling=p > 0, stress_kind=sk, stress_value=sv, **kw)
+    eng = capi.Engine(prm, xyb, pd if p else None)
+    return xyb, pd, oracle, eng
+
+
+def assert_speeds_close(v, v_ref):
+    scale = np.abs(v_ref).max()
+    err = np.abs(v - v_ref)
+    bound = 1e-10 * scale + 1e-9 * np.abs(v_ref)
+    assert np.all(err <= bound), (err.max(), scale, (err / np.maximum(np.abs(v_ref), 1e-300)).max())
+
+
+@pytest.mark.parametrize("n,seed,m,p,sk,sv", [(256, 0, 0.5, 0, 0, 0.0), (1000, 5, 1.0, 64, 3, 0.01),
+                                              (4096, 1, 1.0, 256, 3, 0.01)])
+def test_speeds_match_oracle(engine_lib, port_lib, n, seed, m, p, sk, sv):
+    xyb, pd, o, e = make_pair(n, seed, m, 1e-6, p, sk, sv)
+    for stype in (0, 2):
+        v_ref, tol_ref = o.speeds(xyb, 0.0, stype)
+        v, tol = e.speeds(xyb, 0.0, stype)
+        assert_speeds_close(v, v_ref)
+        if p == 0:
+            assert np.array_equal(tol, tol_ref)
+        else:
+            assert np.allclose(tol, tol_ref, rtol=1e-9, atol=0)
+
+
+@pytest.mark.parametrize("name", ["n64_zero", "n96_pd8_const", "n128_m1_zero"])
+def test_speeds_and_jacobian_match_golden(engine_lib, name):
+    from sdddst_b200 import capi
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    n, seed, p, m, prec, sk, sv, steps = g["params"]
+    n, p = int(n), int(p)
+    prm = capi.cli_params(n, m, prec, step_size=1e-6, p=p, pd_scaling=p > 0, stress_kind=int(sk), stress_value=sv)
+    e = capi.Engine(prm, g["xyb"], g["pd"] if p else None)
+    v, tol = e.speeds(g["xyb"])
+    assert_speeds_close(v, g["v"])
+    _compare_jacobian(e, float(g["h"]), g["xyb"], g["Ap"], g["Ai"], g["Ax"], g["dvec"], n)
+
+
+def _dense_from_csc(Ap, Ai, Ax, n):
+    return ref.csc_to_dense(Ap, Ai, Ax, n)
+
+
+def _compare_jacobian(e, h, xyb, Ap, Ai, Ax, dvec_ref, n):
+    rp, col, val, d = e.jacobian(h, xyb)
+    J = np.zeros((n, n))
+    pat = np.zeros((n, n), dtype=bool)
+    for i in range(n):
+        for q in range(rp[i], rp[i + 1]):
+            J[i, col[q]] += val[q]
+            pat[i, col[q]] = True
+    Jr = _dense_from_csc(Ap, Ai, Ax, n)
+    pr = np.zeros((n, n), dtype=bool)
+    for j in range(n):
+        for q in range(Ap[j], Ap[j + 1]):
+            pr[Ai[q], j] = True
+    pr = pr | pr.T
+    assert np.array_equal(pat, pr), "sparsity pattern differs"
+    off = ~np.eye(n, dtype=bool)
+    scale = np.abs(Jr[off]).max() if np.any(off & pr) else 1.0
+    assert np.abs(J - Jr).max() <= 1e-10 * max(scale, 1.0)
+    assert np.allclose(d, dvec_ref, rtol=1e-9, atol=1e-14)
+
+
+@pytest.mark.parametrize("n,seed,m,p,h", [(256, 0, 0.5, 0, 3e-6), (600, 3, 1.0, 32, 1e-5)])
+def test_jacobian_matches_oracle(engine_lib, port_lib, n, seed, m, p, h):
+    xyb, pd, o, e = make_pair(n, seed, m, 1e-6, p, 3 if p else 0, 0.01 if p else 0.0)
+    Ap, Ai, Ax, d = o.jacobian(h, xyb)
+    _compare_jacobian(e, h, xyb, Ap, Ai, Ax, d, n)
+
+
+def test_solve_matches_dense(engine_lib, port_lib):
+    n = 800
+    xyb, pd, o, e = make_pair(n, 4, 1.0, 1e-6)
+    h = 2e-5
+    Ap, Ai, Ax, d = o.jacobian(h, xyb)
+    J = ref.csc_to_dense(Ap, Ai, Ax, n)
+    rng = np.random.default_rng(0)
+    b = rng.standard_normal(n) * 1e-4
+    x, iters = e.solve(h, xyb, b)
+    x_ref = np.linalg.solve(J, b)
+    assert iters > 0
+    assert np.abs(x - x_ref).max() <= 1e-11 * np.abs(x_ref).max()
+
+
+def _teacher_forced(n, seed, m, prec, p=0, sk=0, sv=0.0, steps=12, **kw):
+    xyb, pd, o, e = make_pair(n, seed, m, prec, p, sk, sv, **kw)
+    first = True
+    worst = 0.0
+    decisions = 0
+    for k in range(steps):
+        x = o.config(0)
+        sc = o.scalars()
+        h = sc["step_size"]
+        e.set_state(x, h, sc["sim_time"], sc["energy"], sc["strain"], first)
+        if not first:
+            o.set_state(x, h, sc["sim_time"], sc["energy"], sc["strain"], False)
+        first = False
+        a_ref = o.step()
+        a = e.step()
+        so, se = o.scalars(), e.scalars()
+        assert a == a_ref, (k, so, se)
+        decisions += 1
+        for which in (1, 2, 3):
+            xr = o.config(which)[:, 0]
+            xd = e.config(which)[:, 0]
+            worst = max(worst, np.abs(xd - xr).max())
+            assert np.abs(xd - xr).max() <= 1e-10 * max(1.0, np.abs(xr).max()), (k, which)
+        assert np.isclose(se["max_error_ratio_sqr"], so["max_error_ratio_sqr"], rtol=1e-6, atol=1e-12), (k, so, se)
+        assert np.isclose(se["step_size"], so["step_size"], rtol=1e-6), k
+        assert np.isclose(se["energy"], so["energy"], rtol=1e-9, atol=1e-300), k
+        assert np.allclose(e.vector(6), o.vector(6), rtol=1e-9, atol=0)
+    return worst, decisions
+
+
+def test_step_teacher_forced_small(engine_lib, port_lib):
+    worst, k = _teacher_forced(256, 0, 0.5, 1e-6, steps=16)
+    assert k == 16
+
+
+def test_step_teacher_forced_defects_constant_stress(engine_lib, port_lib):
+    worst, k = _teacher_forced(600, 1, 1.0, 1e-7, p=40, sk=3, sv=0.01, steps=5)
+    assert k == 5
+
+
+def test_free_running_trajectory_small(engine_lib, port_lib):
+    """200 accepted steps of the N=256 workload, free running on both sides;
+    per-step positions, error ratio and energy are compared while the two
+    trajectories take the same accept/reject decisions."""
+    w = workloads.SMALL_256
+    xyb, _ = w.state()
+    from sdddst_b200 import capi
+    o = ref.Sim(xyb, None, ref.params(cutoff_multiplier=w.cutoff_multiplier, prec=w.prec, step_size=w.step_size), "port")
+    e = capi.Engine(capi.cli_params(w.n, w.cutoff_multiplier, w.prec, step_size=w.step_size), xyb)
+    acc = 0
+    attempts = 0
+    while acc < w.steps and attempts < 600:
+        a_ref = o.step()
+        a = e.step()
+        attempts += 1
+        assert a == a_ref, attempts
+        acc += a
+        so, se = o.scalars(), e.scalars()
+        xr, xd = o.config(0)[:, 0], e.config(0)[:, 0]
+        assert np.abs(xd - xr).max() <= 1e-9, attempts
+        assert np.isclose(se["max_error_ratio_sqr"], so["max_error_ratio_sqr"], rtol=1e-5, atol=1e-12)
+        assert np.isclose(se["energy"], so["energy"], rtol=1e-8)
+    assert acc == w.steps
+
+
+def test_fp32_pairsum_accuracy(engine_lib, port_lib):
+    """Mixed precision: FP32 pair terms with FP64 accumulation against the
+    FP64 oracle (reported error, bounded here)."""
+    from sdddst_b200 import capi
+    n = 4096
+    xyb, _ = workloads.dislocations(n, 2)
+    o = ref.Sim(xyb, None, ref.params(cutoff_multiplier=1.0, prec=1e-5), "port")
+    v_ref, _ = o.speeds(xyb)
+    e = capi.Engine(capi.cli_params(n, 1.0, 1e-5, pairsum=capi.PAIRSUM_FP32), xyb)
+    v, _ = e.speeds(xyb)
+    rel = np.abs(v - v_ref).max() / np.abs(v_ref).max()
+    assert rel < 1e-5, rel
