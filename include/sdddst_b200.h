@@ -54,8 +54,9 @@ enum {
 
 /* Linear solver replacing UMFPACK (simulation.cpp:386-396). */
 enum {
-    SDDDST_SOLVER_GMRES = 0,      /* restarted GMRES, FP64, unpreconditioned */
-    SDDDST_SOLVER_GMRES_JACOBI = 1 /* restarted GMRES, FP64, diagonal preconditioner */
+    SDDDST_SOLVER_GMRES = 0,         /* restarted GMRES, FP64, unpreconditioned */
+    SDDDST_SOLVER_GMRES_JACOBI = 1,  /* restarted GMRES, FP64, diagonal preconditioner */
+    SDDDST_SOLVER_GMRES_CLUSTER = 2  /* restarted GMRES, FP64, block-Jacobi on strongly coupled clusters */
 };
 
 /* Field kernels (Field plug-in): the analytic periodic field
@@ -84,12 +85,13 @@ typedef struct {
     double solver_tol;        /* relative residual target of the iterative solve */
     int gmres_restart;        /* Krylov subspace size per cycle */
     int max_iters;            /* iteration cap per solve */
+    double precond_theta;     /* coupling strength that joins two dislocations in a cluster */
     int device;               /* CUDA device ordinal */
 } sdddst_params;
 
 /* Defaults of SimulationData() (simulation_data.cpp:43-109, constants.h):
  * cutoff multiplier 1, prec 1e-8, step 1, A = 1.6e-3, KASQR = 1.65^2*1e6/256,
- * ic = 2, zero stress, FP64 pair sum, GMRES to 1e-14. */
+ * ic = 2, zero stress, FP64 pair sum, cluster-preconditioned GMRES to 1e-13. */
 void sdddst_default_params(sdddst_params *prm);
 
 /* Creates a context and uploads the configuration.  Replaces constructing
@@ -154,6 +156,30 @@ int sdddst_run(void *ctx, int accepted_target, int max_attempts, int *accepted, 
  * pointers to the accepted configuration's x, y and b arrays (N doubles each,
  * structure of arrays) on the context's device. */
 int sdddst_state_device(void *ctx, double **x_device, double **y_device, double **b_device);
+
+/* Replaces the accepted configuration's x coordinates (N doubles, host)
+ * without re-evaluating the initial velocities: for round trips of a state
+ * the context already holds (y, b and the step state are unchanged).  With
+ * recompute = 1 the initial velocities are re-evaluated as after an accepted
+ * step (simulation.cpp:543-550). */
+int sdddst_upload_positions(void *ctx, const double *x, int recompute);
+
+/* Copies the accepted configuration's x coordinates (N doubles) to the host. */
+int sdddst_download_positions(void *ctx, double *x);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that time or
+ * order work against it. */
+int sdddst_stream(void *ctx, void **stream);
+
+/* Roofline denominators of the CUDA-core pipes on `device`: sustained FP64
+ * and FP32 fused multiply-add throughput in TFLOP/s (2 FLOP per FMA),
+ * measured by a short dependent-chain microbenchmark (~0.1 s). */
+int sdddst_vector_peaks(int device, double *fp64_tflops, double *fp32_tflops);
+
+/* Times `reps` back-to-back launches of the pair-sum kernels on the accepted
+ * configuration with CUDA events on the context's stream; writes the mean
+ * device time of one launch (tile kernel and its min-distance reset). */
+int sdddst_profile_pair_sum(void *ctx, int reps, double *ms_per_launch);
 
 /* Launch statistics: number of kernels this context has launched so far. */
 long sdddst_kernel_launches(void *ctx);

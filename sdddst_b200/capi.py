@@ -25,14 +25,15 @@ ERR_NONFINITE = -6
 
 STRESS_ZERO, STRESS_FIXED_RATE, STRESS_SPRING, STRESS_CONSTANT = 0, 1, 2, 3
 PAIRSUM_FP64, PAIRSUM_FP32 = 0, 1
-SOLVER_GMRES, SOLVER_GMRES_JACOBI = 0, 1
+SOLVER_GMRES, SOLVER_GMRES_JACOBI, SOLVER_GMRES_CLUSTER = 0, 1, 2
 
 # Every extern "C" symbol of include/sdddst_b200.h.
 EXPORTS = [
     "sdddst_default_params", "sdddst_ctx_create", "sdddst_ctx_destroy", "sdddst_last_error",
     "sdddst_set_state", "sdddst_get_scalars", "sdddst_get_config", "sdddst_get_vector",
     "sdddst_speeds", "sdddst_jacobian", "sdddst_solve", "sdddst_step", "sdddst_run",
-    "sdddst_state_device", "sdddst_kernel_launches",
+    "sdddst_state_device", "sdddst_kernel_launches", "sdddst_upload_positions",
+    "sdddst_download_positions", "sdddst_stream", "sdddst_vector_peaks", "sdddst_profile_pair_sum",
 ]
 
 
@@ -44,7 +45,8 @@ class Params(C.Structure):
         ("stress_kind", C.c_int), ("stress_rate", C.c_double), ("spring_constant", C.c_double),
         ("stress_value", C.c_double), ("calculate_strain", C.c_int), ("max_step_limited", C.c_int),
         ("max_step", C.c_double), ("field", C.c_int), ("pairsum", C.c_int), ("solver", C.c_int),
-        ("solver_tol", C.c_double), ("gmres_restart", C.c_int), ("max_iters", C.c_int), ("device", C.c_int),
+        ("solver_tol", C.c_double), ("gmres_restart", C.c_int), ("max_iters", C.c_int),
+        ("precond_theta", C.c_double), ("device", C.c_int),
     ]
 
 
@@ -83,6 +85,11 @@ def load(path: str = LIB_PATH):
     lib.sdddst_step.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
     lib.sdddst_run.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.sdddst_state_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.sdddst_upload_positions.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    lib.sdddst_download_positions.argtypes = [C.c_void_p, C.c_void_p]
+    lib.sdddst_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    lib.sdddst_profile_pair_sum.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
+    lib.sdddst_vector_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.sdddst_kernel_launches.argtypes = [C.c_void_p]
     lib.sdddst_kernel_launches.restype = C.c_long
     _lib = lib
@@ -92,6 +99,13 @@ def load(path: str = LIB_PATH):
 def _check(rc: int):
     if rc != OK:
         raise EngineError(rc, load().sdddst_last_error().decode(errors="replace"))
+
+
+def vector_peaks(device: int = 0):
+    """Measured FP64 and FP32 FMA throughput (TFLOP/s) of the GPU."""
+    a, b = C.c_double(0), C.c_double(0)
+    _check(load().sdddst_vector_peaks(int(device), C.byref(a), C.byref(b)))
+    return a.value, b.value
 
 
 def default_params(**kw) -> Params:
@@ -216,6 +230,26 @@ class Engine:
         a, t = C.c_int(0), C.c_int(0)
         _check(self.lib.sdddst_run(self.h, int(accepted_target), int(max_attempts), C.byref(a), C.byref(t)))
         return a.value, t.value
+
+    def upload_positions(self, x, recompute: bool = False):
+        """x: a C-contiguous float64 array (pinned host memory is fastest)."""
+        _check(self.lib.sdddst_upload_positions(self.h, C.c_void_p(x.ctypes.data if isinstance(x, np.ndarray)
+                                                                    else int(x)), int(recompute)))
+
+    def download_positions(self, x):
+        _check(self.lib.sdddst_download_positions(self.h, C.c_void_p(x.ctypes.data if isinstance(x, np.ndarray)
+                                                                      else int(x))))
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(self.lib.sdddst_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def profile_pair_sum(self, reps: int = 3) -> float:
+        """Mean device milliseconds of one pair-sum launch (CUDA events)."""
+        ms = C.c_double(0)
+        _check(self.lib.sdddst_profile_pair_sum(self.h, int(reps), C.byref(ms)))
+        return ms.value
 
     def launches(self) -> int:
         return int(self.lib.sdddst_kernel_launches(self.h))

@@ -75,8 +75,9 @@ void sdddst_default_params(sdddst_params *p)
     p->spring_constant = 1.0;             // SpringProtocol(), spring_protocol.cpp:22-26
     p->field = SDDDST_FIELD_ANALYTIC;
     p->pairsum = SDDDST_PAIRSUM_FP64;
-    p->solver = SDDDST_SOLVER_GMRES;
+    p->solver = SDDDST_SOLVER_GMRES_CLUSTER;
     p->solver_tol = 1e-13;
+    p->precond_theta = 0.1;
     p->gmres_restart = 30;
     p->max_iters = 1000;
     p->device = 0;
@@ -91,7 +92,8 @@ int sdddst_ctx_create(const sdddst_params *prm, const double *xyb, const double 
     if (prm->field != SDDDST_FIELD_ANALYTIC) return fail(SDDDST_ERR_INVALID, "unsupported field kind");
     if (prm->pairsum != SDDDST_PAIRSUM_FP64 && prm->pairsum != SDDDST_PAIRSUM_FP32)
         return fail(SDDDST_ERR_INVALID, "unsupported pair-sum mode");
-    if (prm->solver != SDDDST_SOLVER_GMRES && prm->solver != SDDDST_SOLVER_GMRES_JACOBI)
+    if (prm->solver != SDDDST_SOLVER_GMRES && prm->solver != SDDDST_SOLVER_GMRES_JACOBI &&
+        prm->solver != SDDDST_SOLVER_GMRES_CLUSTER)
         return fail(SDDDST_ERR_INVALID, "unsupported solver");
     if (!(prm->prec > 0) || !(prm->step_size > 0) || !(prm->cutoff_multiplier > 0))
         return fail(SDDDST_ERR_INVALID, "prec, step size and cutoff multiplier must be positive");
@@ -242,6 +244,7 @@ int sdddst_solve(void *ctx, double h, const double *xyb, const double *rhs, doub
         ScratchConfig sc(e, xyb);
         if (int rc = e->assemble(e->d_xs)) return from_engine(e, rc);
         sd::launch_make_dvec(*e, h, e->d_dvec, e->st);
+        if (int rc = e->prepare_solver(h)) return from_engine(e, rc);
         cudaMemcpyAsync(e->d_g, rhs, sizeof(double) * e->n, cudaMemcpyHostToDevice, e->st);
         int rc = e->solve(h, e->d_g, e->d_sol);
         if (iterations) *iterations = e->last_iters;
@@ -293,6 +296,58 @@ int sdddst_state_device(void *ctx, double **x, double **y, double **b)
     if (y) *y = e->d_y;
     if (b) *b = e->d_b;
     return SDDDST_OK;
+}
+
+int sdddst_upload_positions(void *ctx, const double *x, int recompute)
+{
+    if (!ctx || !x) return fail(SDDDST_ERR_INVALID, "null argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    cudaMemcpyAsync(e->d_x0, x, sizeof(double) * e->n, cudaMemcpyHostToDevice, e->st);
+    if (recompute) {
+        e->cur_stress = SDDDST_STAGE_ORIGINAL;
+        e->stress_calc(e->sim_time, SDDDST_STAGE_ORIGINAL, e->strain);
+        e->speeds(e->d_x0, e->d_v0, e->d_S0, SDDDST_STAGE_ORIGINAL, false);
+    }
+    return from_engine(e, e->sync_check("upload positions"));
+}
+
+int sdddst_download_positions(void *ctx, double *x)
+{
+    if (!ctx || !x) return fail(SDDDST_ERR_INVALID, "null argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    cudaMemcpyAsync(x, e->d_x0, sizeof(double) * e->n, cudaMemcpyDeviceToHost, e->st);
+    return from_engine(e, e->sync_check("download positions"));
+}
+
+int sdddst_stream(void *ctx, void **stream)
+{
+    if (!ctx || !stream) return fail(SDDDST_ERR_INVALID, "null argument");
+    *stream = (void *)E(ctx)->st;
+    return SDDDST_OK;
+}
+
+int sdddst_profile_pair_sum(void *ctx, int reps, double *ms_per_launch)
+{
+    if (!ctx || !ms_per_launch || reps < 1) return fail(SDDDST_ERR_INVALID, "bad argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    sd::launch_pair_sum(*e, e->d_x0, e->st, e->prm.pairsum, 0.0); // warm-up
+    cudaEventRecord(a, e->st);
+    for (int r = 0; r < reps; ++r) sd::launch_pair_sum(*e, e->d_x0, e->st, e->prm.pairsum, 0.0);
+    cudaEventRecord(b, e->st);
+    int rc = e->sync_check("profile pair sum");
+    float ms = 0.f;
+    if (!rc) cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    e->launches += 2 * (reps + 1);
+    *ms_per_launch = ms / reps;
+    return from_engine(e, rc);
 }
 
 long sdddst_kernel_launches(void *ctx) { return ctx ? E(ctx)->launches : 0; }

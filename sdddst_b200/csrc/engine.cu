@@ -40,6 +40,7 @@ Engine::~Engine()
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (h_scal) cudaFreeHost(h_scal);
+    precond_free(*this);
     if (st) cudaStreamDestroy(st);
 }
 
@@ -133,6 +134,7 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     rc |= dalloc(&d_y_small, (size_t)n + restart + 8);
     if (cudaMallocHost((void **)&h_scal, sizeof(double) * (2 * (restart + 1) + 8)) != cudaSuccess)
         rc |= SDDDST_ERR_NOMEM;
+    rc |= precond_alloc(*this);
     if (rc) {
         err = "device allocation failed";
         return SDDDST_ERR_NOMEM;
@@ -225,8 +227,14 @@ int Engine::assemble(const double *x)
 
 int Engine::solve(double h, const double *rhs, double *x_out)
 {
-    int precond = prm.solver == SDDDST_SOLVER_GMRES_JACOBI;
+    int precond = prm.solver == SDDDST_SOLVER_GMRES_JACOBI ? 1 : prm.solver == SDDDST_SOLVER_GMRES_CLUSTER ? 2 : 0;
     return gmres_solve(*this, h, d_dvec, rhs, x_out, precond);
+}
+
+int Engine::prepare_solver(double h)
+{
+    if (prm.solver == SDDDST_SOLVER_GMRES_CLUSTER) return precond_build(*this, h, d_dvec);
+    return 0;
 }
 
 // Simulation::integrate (simulation.cpp:62-84) with calculateG
@@ -238,6 +246,7 @@ int Engine::integrate(double h, double *xn, const double *xo, bool use2, bool in
         if (int rc = assemble(xn)) return rc;
     launch_make_dvec(*this, h, d_dvec, st);
     launches++;
+    if (int rc = prepare_solver(h)) return rc;
     double *isp = use2 ? d_v0b : d_v0;
     double *csp0 = use2 ? d_vs2 : d_vs;
     double *Sorig = use2 ? d_S1 : d_S0;

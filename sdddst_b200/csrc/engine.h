@@ -57,6 +57,15 @@ struct Engine {
     int last_iters = 0;
     double last_resid = 0.0;
 
+    // ---- cluster block-Jacobi preconditioner (precond.cu)
+    int *pc_ptr = nullptr, *pc_parent = nullptr, *pc_tmp = nullptr, *pc_tmp2 = nullptr, *pc_members = nullptr;
+    int *pc_blk_of = nullptr, *pc_loc = nullptr, *pc_count = nullptr, *pc_fill = nullptr, *pc_start = nullptr;
+    int *pc_nblk = nullptr, *pc_bbase = nullptr, *pc_bstart = nullptr, *pc_blen = nullptr, *pc_sq = nullptr;
+    int *pc_off = nullptr;
+    double *pc_binv = nullptr;
+    long pc_binv_cap = 0;
+    int pc_nb = 0;
+
     // ---- host scalars (SimulationData / Simulation members)
     double step_size = 1.0, sim_time = 0.0, strain = 0.0;
     double energy = 0.0, energy_accum = 0.0, vsquare = 0.0, vsquare1 = 0.0, vsquare2 = 0.0;
@@ -77,6 +86,7 @@ struct Engine {
     int speeds(const double *x, double *v_out, double *S_out, int stress_type, bool update_tol);
     int assemble(const double *x);
     int solve(double h, const double *rhs, double *x_out);
+    int prepare_solver(double h); // per matrix: preconditioner set-up
     int integrate(double h, double *xn, const double *xo, bool use2, bool init_speed, int origin, int end,
                   bool reuse_assembly);
     int step(int *accepted);
@@ -115,5 +125,10 @@ void launch_residual_g(const Engine &e, double h, const double *xn, const double
 void launch_axpy_update(const Engine &e, double *xn, const double *sol, cudaStream_t st);
 
 int reduce_sum(Engine &e, const double *a, const double *b, int n, int op, double *out);
+
+int precond_alloc(Engine &e);
+void precond_free(Engine &e);
+int precond_build(Engine &e, double h, const double *dvec);
+void precond_apply(Engine &e, const double *v, double *z);
 
 } // namespace sd

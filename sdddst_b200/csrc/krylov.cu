@@ -52,6 +52,12 @@ __global__ void scale_kernel(int n, double s, const double *__restrict__ a, doub
     if (i < n) c[i] = a[i] * s;
 }
 
+__global__ void add_kernel(int n, const double *__restrict__ a, double *__restrict__ x)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += a[i];
+}
+
 __global__ void sub_kernel(int n, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ c)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -274,7 +280,7 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
     double *V = e.d_V, *w = e.d_w, *z = e.d_z, *r = e.d_r;
     double *dinv = nullptr;
     cudaMemsetAsync(x, 0, sizeof(double) * n, st);
-    if (precond) {
+    if (precond == 1) {
         dinv = e.d_y_small; // n doubles reserved for the diagonal
         jdiag_inv_kernel<<<nb, 256, 0, st>>>(n, h, e.d_rowptr, e.d_val, dvec, dinv);
         e.launches++;
@@ -305,10 +311,13 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
         for (int j = 0; j < m; ++j) {
             const double *vj = V + (size_t)j * ldv;
             const double *src = vj;
-            if (precond) {
+            if (precond == 1) {
                 mul_kernel<<<nb, 256, 0, st>>>(n, vj, dinv, z);
                 src = z;
                 e.launches++;
+            } else if (precond == 2) {
+                precond_apply(e, vj, z);
+                src = z;
             }
             spmv_j_kernel<<<(n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, src, w);
             const int kk = j + 1;
@@ -364,8 +373,17 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
             yv[i] = s / H[(size_t)i * m + i];
         }
         cudaMemcpyAsync(e.d_y_small + n, yv.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st);
-        combine_kernel<<<nb, 256, 0, st>>>(n, k, V, ldv, e.d_y_small + n, dinv, x);
-        e.launches++;
+        if (precond == 2) {
+            // x += M^-1 (V y)
+            cudaMemsetAsync(r, 0, sizeof(double) * n, st);
+            combine_kernel<<<nb, 256, 0, st>>>(n, k, V, ldv, e.d_y_small + n, nullptr, r);
+            precond_apply(e, r, z);
+            add_kernel<<<nb, 256, 0, st>>>(n, z, x);
+            e.launches += 2;
+        } else {
+            combine_kernel<<<nb, 256, 0, st>>>(n, k, V, ldv, e.d_y_small + n, dinv, x);
+            e.launches++;
+        }
         if (converged) break;
         if (total >= max_it) break;
         // true residual for the restart

@@ -1,0 +1,351 @@
+// Cluster block-Jacobi preconditioner for J(h) = I + diag(c) h G,
+// c_i = (1 + d_i)/2.
+//
+// Close dislocation pairs couple through entries of size h |dtau/dx| ~ h/r^2
+// that can exceed the identity by orders of magnitude; such a pair forms a
+// stiff 2x2 block whose soft mode (both dislocations moving together) a
+// diagonal scaling cannot reach.  Strongly coupled dislocations are therefore
+// grouped and their diagonal blocks of J inverted exactly:
+//   * strength s_ij = h |G_ij| / sqrt(M_ii M_jj) on the symmetric form
+//     M = diag(c)^-1 J (M_ii = 1/c_i + h G_ii, M_ij = h G_ij);
+//   * every dislocation points to its strongest neighbour with s >= theta;
+//     following pointers never decreases s, so each chain ends in a mutual
+//     pair, whose smaller index roots the cluster (pointer jumping);
+//   * clusters are listed contiguously, members in ascending index order,
+//     and cut into blocks of at most kMaxBlock;
+//   * one warp per block builds the dense block of J, inverts it by
+//     Gauss-Jordan elimination with partial pivoting in shared memory, and
+//     stores the inverse; applying M^-1 is one small dense product per block.
+#include "engine.h"
+#include "common.cuh"
+
+#include <vector>
+
+namespace sd {
+
+constexpr int kMaxBlock = 32;
+
+__global__ void strongest_kernel(int n, double h, double theta, const int *__restrict__ rowptr,
+                                 const int *__restrict__ col, const double *__restrict__ val,
+                                 const double *__restrict__ dvec, int *__restrict__ ptr)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const int s = rowptr[i], e = rowptr[i + 1];
+    const double mii = 2.0 / (1.0 + dvec[i]) + h * val[s];
+    double best = -1.0;
+    int bj = i;
+    for (int q = s + 1 + lane; q < e; q += 32) {
+        const int j = col[q];
+        const double mjj = 2.0 / (1.0 + dvec[j]) + h * val[rowptr[j]];
+        const double den = sqrt(fabs(mii) * fabs(mjj));
+        const double sij = den > 0 ? h * fabs(val[q]) / den : 0.0;
+        if (sij >= theta && (sij > best || (sij == best && j < bj))) {
+            best = sij;
+            bj = j;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        int oj = __shfl_xor_sync(0xffffffffu, bj, o);
+        if (ob > best || (ob == best && oj < bj)) {
+            best = ob;
+            bj = oj;
+        }
+    }
+    if (lane == 0) ptr[i] = best >= theta ? bj : i;
+}
+
+__global__ void root_init_kernel(int n, const int *__restrict__ ptr, int *__restrict__ parent)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int p = ptr[i];
+    if (p == i || (ptr[p] == i && i < p)) parent[i] = i;
+    else parent[i] = p;
+}
+
+__global__ void jump_kernel(int n, const int *__restrict__ in, int *__restrict__ out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[in[i]];
+}
+
+// After jumping, a node whose parent is not a root (a chain longer than the
+// jumps covered, or a tie cycle) becomes its own root.
+__global__ void root_fix_kernel(int n, int *__restrict__ parent, int *__restrict__ count)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int r = parent[i];
+    if (parent[r] != r) r = i;
+    parent[i] = r;
+    atomicAdd(&count[r], 1);
+}
+
+__global__ void member_scatter_kernel(int n, const int *__restrict__ root, const int *__restrict__ start,
+                                      int *__restrict__ fill, int *__restrict__ members)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int r = root[i];
+    members[start[r] + atomicAdd(&fill[r], 1)] = i;
+}
+
+// one thread per cluster root: members in ascending order (rank sort, for
+// clusters of up to 256; larger ones keep their arrival order) and the
+// cluster's block count
+__global__ void cluster_sort_kernel(int n, const int *__restrict__ count, const int *__restrict__ start,
+                                    const int *__restrict__ in, int *__restrict__ out, int *__restrict__ nblocks)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    int k = count[r];
+    nblocks[r] = k > 0 ? (k + kMaxBlock - 1) / kMaxBlock : 0;
+    if (k == 0) return;
+    int s = start[r];
+    if (k > 256) {
+        for (int a = 0; a < k; ++a) out[s + a] = in[s + a];
+        return;
+    }
+    for (int a = 0; a < k; ++a) {
+        int v = in[s + a], rank = 0;
+        for (int b2 = 0; b2 < k; ++b2) rank += in[s + b2] < v;
+        out[s + rank] = v;
+    }
+}
+
+__global__ void block_list_kernel(int n, const int *__restrict__ count, const int *__restrict__ start,
+                                  const int *__restrict__ bbase, int *__restrict__ bstart, int *__restrict__ blen)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    int k = count[r];
+    if (k == 0) return;
+    int s = start[r], b0 = bbase[r];
+    for (int t = 0; t * kMaxBlock < k; ++t) {
+        bstart[b0 + t] = s + t * kMaxBlock;
+        int len = k - t * kMaxBlock;
+        blen[b0 + t] = len < kMaxBlock ? len : kMaxBlock;
+    }
+}
+
+__global__ void block_meta_kernel(int nb, const int *__restrict__ bstart, const int *__restrict__ blen,
+                                  const int *__restrict__ members, int *__restrict__ blk_of, int *__restrict__ loc,
+                                  int *__restrict__ sq)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    int s = bstart[b], k = blen[b];
+    for (int t = 0; t < k; ++t) {
+        int i = members[s + t];
+        blk_of[i] = b;
+        loc[i] = t;
+    }
+    sq[b] = k * k;
+}
+
+// One warp per block: dense J block, Gauss-Jordan inverse with partial
+// pivoting, written row-major at binv[off[b]].
+__global__ void block_invert_kernel(int nb, double h, const int *__restrict__ bstart, const int *__restrict__ blen,
+                                    const int *__restrict__ members, const int *__restrict__ blk_of,
+                                    const int *__restrict__ loc, const int *__restrict__ off,
+                                    const int *__restrict__ rowptr, const int *__restrict__ col,
+                                    const double *__restrict__ val, const double *__restrict__ dvec,
+                                    double *__restrict__ binv, int *__restrict__ flag)
+{
+    __shared__ double A[2][kMaxBlock][2 * kMaxBlock + 1];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.x * 2 + wib;
+    if (b >= nb) return;
+    const int k = blen[b], s = bstart[b];
+    double(*M)[2 * kMaxBlock + 1] = A[wib];
+    if (k == 1) {
+        if (lane == 0) {
+            const int i = members[s];
+            const double jii = 1.0 + (1.0 + dvec[i]) * 0.5 * h * val[rowptr[i]];
+            binv[off[b]] = 1.0 / jii;
+        }
+        return;
+    }
+    for (int r = 0; r < k; ++r)
+        for (int c = lane; c < 2 * k; c += 32) M[r][c] = (c - k == r) ? 1.0 : 0.0;
+    __syncwarp();
+    // gather the block: each lane owns rows lane, lane + 32 (k <= 32: one)
+    if (lane < k) {
+        const int i = members[s + lane];
+        const double ci = (1.0 + dvec[i]) * 0.5 * h;
+        for (int q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+            const int j = col[q];
+            if (blk_of[j] == b) M[lane][loc[j]] += ci * val[q];
+        }
+        M[lane][lane] += 1.0;
+    }
+    __syncwarp();
+    bool singular = false;
+    for (int p = 0; p < k; ++p) {
+        // pivot search in column p (rows p..k-1)
+        double v = lane >= p && lane < k ? fabs(M[lane][p]) : -1.0;
+        int idx = lane;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_xor_sync(0xffffffffu, v, o);
+            int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+            if (ov > v || (ov == v && oi < idx)) {
+                v = ov;
+                idx = oi;
+            }
+        }
+        if (!(v > 0.0)) {
+            singular = true;
+            break;
+        }
+        if (idx != p)
+            for (int c = lane; c < 2 * k; c += 32) {
+                double t = M[p][c];
+                M[p][c] = M[idx][c];
+                M[idx][c] = t;
+            }
+        __syncwarp();
+        const double inv = 1.0 / M[p][p];
+        __syncwarp();
+        for (int c = lane; c < 2 * k; c += 32) M[p][c] *= inv;
+        __syncwarp();
+        if (lane < k && lane != p) {
+            const double f = M[lane][p];
+            if (f != 0.0)
+                for (int c = 0; c < 2 * k; ++c) M[lane][c] -= f * M[p][c];
+        }
+        __syncwarp();
+    }
+    if (singular) {
+        if (lane == 0) atomicExch(flag, 1);
+        return;
+    }
+    double *dst = binv + off[b];
+    for (int r = 0; r < k; ++r)
+        for (int c = lane; c < k; c += 32) dst[r * k + c] = M[r][k + c];
+}
+
+__global__ void block_apply_kernel(int nb, const int *__restrict__ bstart, const int *__restrict__ blen,
+                                   const int *__restrict__ members, const int *__restrict__ off,
+                                   const double *__restrict__ binv, const double *__restrict__ v,
+                                   double *__restrict__ z)
+{
+    const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (b >= nb) return;
+    const int k = blen[b], s = bstart[b];
+    const double *B = binv + off[b];
+    if (k == 1) {
+        if (lane == 0) z[members[s]] = B[0] * v[members[s]];
+        return;
+    }
+    double vl = lane < k ? v[members[s + lane]] : 0.0;
+    double acc = 0.0;
+    for (int c = 0; c < k; ++c) {
+        double vc = __shfl_sync(0xffffffffu, vl, c);
+        if (lane < k) acc += B[lane * k + c] * vc;
+    }
+    if (lane < k) z[members[s + lane]] = acc;
+}
+
+// scan helper from jacobian.cu
+__global__ void scan_kernel(const int *__restrict__ in, int m, int *__restrict__ out);
+
+// Builds the cluster block-Jacobi inverse of J(h) for the assembled G.
+int precond_build(Engine &e, double h, const double *dvec)
+{
+    const int n = e.n;
+    cudaStream_t st = e.st;
+    const unsigned nb256 = (unsigned)((n + 255) / 256);
+    const double theta = e.prm.precond_theta > 0 ? e.prm.precond_theta : 0.1;
+    int *ptr = e.pc_ptr, *par = e.pc_parent, *par2 = e.pc_tmp;
+    strongest_kernel<<<(n + 7) / 8, 256, 0, st>>>(n, h, theta, e.d_rowptr, e.d_col, e.d_val, dvec, ptr);
+    root_init_kernel<<<nb256, 256, 0, st>>>(n, ptr, par);
+    for (int it = 0; it < 12; ++it) {
+        jump_kernel<<<nb256, 256, 0, st>>>(n, par, par2);
+        std::swap(par, par2);
+    }
+    cudaMemsetAsync(e.pc_count, 0, sizeof(int) * (n + 1), st);
+    cudaMemsetAsync(e.pc_fill, 0, sizeof(int) * (n + 1), st);
+    root_fix_kernel<<<nb256, 256, 0, st>>>(n, par, e.pc_count);
+    scan_kernel<<<1, 1024, 0, st>>>(e.pc_count, n, e.pc_start);
+    member_scatter_kernel<<<nb256, 256, 0, st>>>(n, par, e.pc_start, e.pc_fill, e.pc_tmp2);
+    cluster_sort_kernel<<<nb256, 256, 0, st>>>(n, e.pc_count, e.pc_start, e.pc_tmp2, e.pc_members, e.pc_nblk);
+    scan_kernel<<<1, 1024, 0, st>>>(e.pc_nblk, n, e.pc_bbase);
+    e.launches += 19;
+    int nb = 0;
+    cudaMemcpyAsync(&nb, e.pc_bbase + n, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (int rc = e.sync_check("precond clusters")) return rc;
+    if (nb <= 0 || nb > n) {
+        e.err = "precond: bad block count";
+        return SDDDST_ERR_SOLVER;
+    }
+    block_list_kernel<<<nb256, 256, 0, st>>>(n, e.pc_count, e.pc_start, e.pc_bbase, e.pc_bstart, e.pc_blen);
+    block_meta_kernel<<<(nb + 255) / 256, 256, 0, st>>>(nb, e.pc_bstart, e.pc_blen, e.pc_members, e.pc_blk_of,
+                                                        e.pc_loc, e.pc_sq);
+    scan_kernel<<<1, 1024, 0, st>>>(e.pc_sq, nb, e.pc_off);
+    e.launches += 3;
+    int total = 0;
+    cudaMemcpyAsync(&total, e.pc_off + nb, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (int rc = e.sync_check("precond blocks")) return rc;
+    if (total > e.pc_binv_cap) {
+        if (e.pc_binv) cudaFree(e.pc_binv);
+        e.pc_binv = nullptr;
+        long cap = total + total / 4 + 1024;
+        if (cudaMalloc(&e.pc_binv, sizeof(double) * cap) != cudaSuccess) {
+            e.err = "precond: allocation failed";
+            return SDDDST_ERR_NOMEM;
+        }
+        e.pc_binv_cap = cap;
+    }
+    cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
+    block_invert_kernel<<<(nb + 1) / 2, 64, 0, st>>>(nb, h, e.pc_bstart, e.pc_blen, e.pc_members, e.pc_blk_of,
+                                                     e.pc_loc, e.pc_off, e.d_rowptr, e.d_col, e.d_val, dvec,
+                                                     e.pc_binv, e.d_flag);
+    e.launches += 1;
+    int flag = 0;
+    cudaMemcpyAsync(&flag, e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (int rc = e.sync_check("precond invert")) return rc;
+    if (flag) {
+        e.err = "precond: singular cluster block";
+        return SDDDST_ERR_SOLVER;
+    }
+    e.pc_nb = nb;
+    return 0;
+}
+
+void precond_apply(Engine &e, const double *v, double *z)
+{
+    block_apply_kernel<<<(e.pc_nb + 7) / 8, 256, 0, e.st>>>(e.pc_nb, e.pc_bstart, e.pc_blen, e.pc_members, e.pc_off,
+                                                            e.pc_binv, v, z);
+    e.launches++;
+}
+
+int precond_alloc(Engine &e)
+{
+    const int n = e.n;
+    int **arrs[] = {&e.pc_ptr, &e.pc_parent, &e.pc_tmp, &e.pc_tmp2, &e.pc_members, &e.pc_blk_of, &e.pc_loc};
+    for (int **a : arrs)
+        if (cudaMalloc(a, sizeof(int) * n) != cudaSuccess) return SDDDST_ERR_NOMEM;
+    int **arrs1[] = {&e.pc_count, &e.pc_fill, &e.pc_start, &e.pc_nblk, &e.pc_bbase, &e.pc_bstart, &e.pc_blen,
+                     &e.pc_sq, &e.pc_off};
+    for (int **a : arrs1)
+        if (cudaMalloc(a, sizeof(int) * (n + 1)) != cudaSuccess) return SDDDST_ERR_NOMEM;
+    return 0;
+}
+
+void precond_free(Engine &e)
+{
+    int *arrs[] = {e.pc_ptr, e.pc_parent, e.pc_tmp, e.pc_tmp2, e.pc_members, e.pc_blk_of, e.pc_loc,
+                   e.pc_count, e.pc_fill, e.pc_start, e.pc_nblk, e.pc_bbase, e.pc_bstart, e.pc_blen,
+                   e.pc_sq, e.pc_off};
+    for (int *a : arrs)
+        if (a) cudaFree(a);
+    if (e.pc_binv) cudaFree(e.pc_binv);
+}
+
+} // namespace sd
