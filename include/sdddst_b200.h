@@ -181,6 +181,30 @@ int sdddst_vector_peaks(int device, double *fp64_tflops, double *fp32_tflops);
  * device time of one launch (tile kernel and its min-distance reset). */
 int sdddst_profile_pair_sum(void *ctx, int reps, double *ms_per_launch);
 
+/* Allocation-free velocity evaluation, for callers that cannot allocate
+ * device memory (their memory is budgeted by another framework, or a
+ * cudaMalloc and its implicit device-wide synchronisation would stall the
+ * work they interleave with).  No counterpart in the reference.
+ *
+ * Computes v_i = sum_{j != i} b_i b_j tau_xy(x_i - x_j, y_i - y_j) + b_i tau_ext
+ * (the pair sum of calculateSpeeds without point defects or tolerances) in
+ * FP64, the same kernels as sdddst_speeds.  Inputs x, y, b and the output v
+ * are N doubles each in device memory; the work is queued on `stream`
+ * (a cudaStream_t, NULL for the default stream) and not synchronised.
+ *
+ * Scratch: a static 2 MiB __device__ array inside this library, held by every
+ * GPU that loads the library until the process exits; N is limited to 4096
+ * (larger N returns SDDDST_ERR_CAPACITY).  The first call on each device
+ * looks up the array's device address (with that device current); make that
+ * first call before any stream capture.  No cudaMalloc, cudaFree or other
+ * allocating call is made.  All calls share the one array, which keeps the
+ * last call's contents: calls that overlap on the GPU (different streams, or
+ * host threads using the same device) race and must be serialised by the
+ * caller.  Every scratch slot is written before it is read, so nothing needs
+ * clearing between calls. */
+int sdddst_speeds_noalloc(int n, const double *x_device, const double *y_device, const double *b_device,
+                          double tau_ext, double *v_device, void *stream);
+
 /* Launch statistics: number of kernels this context has launched so far. */
 long sdddst_kernel_launches(void *ctx);
 

@@ -34,6 +34,7 @@ EXPORTS = [
     "sdddst_speeds", "sdddst_jacobian", "sdddst_solve", "sdddst_step", "sdddst_run",
     "sdddst_state_device", "sdddst_kernel_launches", "sdddst_upload_positions",
     "sdddst_download_positions", "sdddst_stream", "sdddst_vector_peaks", "sdddst_profile_pair_sum",
+    "sdddst_speeds_noalloc",
 ]
 
 
@@ -88,6 +89,8 @@ def load(path: str = LIB_PATH):
     lib.sdddst_upload_positions.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
     lib.sdddst_download_positions.argtypes = [C.c_void_p, C.c_void_p]
     lib.sdddst_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    lib.sdddst_speeds_noalloc.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
+                                          C.c_void_p]
     lib.sdddst_profile_pair_sum.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
     lib.sdddst_vector_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.sdddst_kernel_launches.argtypes = [C.c_void_p]

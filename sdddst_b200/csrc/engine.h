@@ -112,6 +112,8 @@ void launch_pair_sum(const Engine &e, const double *x, cudaStream_t st, int mode
 void launch_speeds_finish(const Engine &e, const double *x, double tau_ext, double *S, double *v, int update_tol,
                           cudaStream_t st);
 void launch_add_stress(const Engine &e, const double *S, double tau_ext, double *v, cudaStream_t st);
+void launch_speeds_raw(int n, const double *x, const double *y, const double *b, double tau_ext, double *part,
+                       double *v, cudaStream_t st);
 
 int jacobian_assemble(Engine &e, const double *x);
 void launch_make_dvec(const Engine &e, double h, double *dvec, cudaStream_t st);

@@ -119,7 +119,7 @@ __global__ void speeds_finish_kernel(int n, int nblk, const double *__restrict__
     if (i >= n) return;
     double acc = 0.0;
     for (int L = 0; L < nblk; ++L) acc += part[(size_t)L * n + i];
-    double smin = __longlong_as_double((long long)minr2[i]);
+    double smin = update_tol ? __longlong_as_double((long long)minr2[i]) : 0.0;
     const double xi = x[i], yi = y[i], bi = b[i];
     for (int q = 0; q < p; ++q) {
         double dx = wrap_half(xi - pdx[q]);
@@ -129,7 +129,7 @@ __global__ void speeds_finish_kernel(int n, int nblk, const double *__restrict__
         acc -= g * bi;
         if (s < smin) smin = s;
     }
-    S[i] = acc;
+    if (S) S[i] = acc;
     v[i] = acc + bi * tau_ext;
     if (update_tol) {
         double t = __dmul_rn(__dmul_rn(smin, 0.25), 1e-2); // precision_handler.cpp:74
@@ -187,6 +187,23 @@ void launch_speeds_finish(const Engine &e, const double *x, double tau_ext, doub
 void launch_add_stress(const Engine &e, const double *S, double tau_ext, double *v, cudaStream_t st)
 {
     add_stress_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, S, e.d_b, tau_ext, v);
+}
+
+// Launches with caller-provided buffers (no engine): FP64 pair sum without
+// tolerance tracking, then v = sum + b tau_ext.  `part` must hold
+// pair_part_doubles(n) doubles; every slot of it is written before it is read.
+void launch_speeds_raw(int n, const double *x, const double *y, const double *b, double tau_ext, double *part,
+                       double *v, cudaStream_t st)
+{
+    const int T = pair_tile_size(n);
+    const int nblk = (n + T - 1) / T;
+    const long tiles = (long)nblk * (nblk + 1) / 2;
+    if (T == 128)
+        pair_tiles_kernel<128, 0><<<(unsigned)tiles, 128, 0, st>>>(x, y, b, n, nblk, part, nullptr, 0.0);
+    else
+        pair_tiles_kernel<64, 0><<<(unsigned)tiles, 64, 0, st>>>(x, y, b, n, nblk, part, nullptr, 0.0);
+    speeds_finish_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, nblk, part, x, y, b, 0, nullptr, nullptr, 0.0, 0.0,
+                                                         tau_ext, nullptr, v, nullptr, nullptr, 0.0, 0);
 }
 
 size_t pair_part_doubles(int n)
