@@ -152,6 +152,7 @@ def time_steps(torch, eng, steps, warmup, flush, per_kernel=True):
     total_ms = 0.0
     accepted = 0
     l0 = eng.launches()
+    s0 = eng.solver_stats()
     for _ in range(steps):
         flush.zero_()  # L2 flush between timed steps (outside the events)
         torch.cuda.synchronize()
@@ -163,6 +164,8 @@ def time_steps(torch, eng, steps, warmup, flush, per_kernel=True):
         b.synchronize()
         total_ms += a.elapsed_time(b)
     torch.cuda.synchronize()
+    s1 = eng.solver_stats()
+    time_steps.last_solver = {"solves": s1[0] - s0[0], "iterations": s1[1] - s0[1]}
     return total_ms, accepted, eng.launches() - l0
 
 
@@ -325,6 +328,7 @@ def main():
     clocks.start()
     total_ms, accepted, launches = time_steps(torch, eng, args.steps, args.warmup, flush)
     clk = clocks.stop()
+    solver_stats = dict(time_steps.last_solver)
     if dist:
         t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -388,7 +392,8 @@ def main():
         "config": {"workload": f"n{args.n}_m{CUTOFF_M}_seed{SEED}", "N": args.n, "cutoff_multiplier": CUTOFF_M,
                    "prec": PREC, "initial_step": H0, "pairsum": args.pairsum, "solver": "gmres(30) fp64",
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas" if ws > 1 else "none",
-                   "accepted": accepted, "attempts": args.steps, "final_step_size": sc["step_size"]},
+                   "accepted": accepted, "attempts": args.steps, "final_step_size": sc["step_size"],
+                   "solver_stats": solver_stats},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "roofline": roof,

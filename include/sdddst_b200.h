@@ -205,6 +205,10 @@ int sdddst_profile_pair_sum(void *ctx, int reps, double *ms_per_launch);
 int sdddst_speeds_noalloc(int n, const double *x_device, const double *y_device, const double *b_device,
                           double tau_ext, double *v_device, void *stream);
 
+/* Linear-solver statistics of this context: solves performed and their
+ * total Krylov iterations. */
+int sdddst_solver_stats(void *ctx, long *solves, long *iterations);
+
 /* Launch statistics: number of kernels this context has launched so far. */
 long sdddst_kernel_launches(void *ctx);
 

@@ -34,7 +34,7 @@ EXPORTS = [
     "sdddst_speeds", "sdddst_jacobian", "sdddst_solve", "sdddst_step", "sdddst_run",
     "sdddst_state_device", "sdddst_kernel_launches", "sdddst_upload_positions",
     "sdddst_download_positions", "sdddst_stream", "sdddst_vector_peaks", "sdddst_profile_pair_sum",
-    "sdddst_speeds_noalloc",
+    "sdddst_speeds_noalloc", "sdddst_solver_stats",
 ]
 
 
@@ -91,6 +91,7 @@ def load(path: str = LIB_PATH):
     lib.sdddst_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     lib.sdddst_speeds_noalloc.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
                                           C.c_void_p]
+    lib.sdddst_solver_stats.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long)]
     lib.sdddst_profile_pair_sum.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
     lib.sdddst_vector_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.sdddst_kernel_launches.argtypes = [C.c_void_p]
@@ -253,6 +254,11 @@ class Engine:
         ms = C.c_double(0)
         _check(self.lib.sdddst_profile_pair_sum(self.h, int(reps), C.byref(ms)))
         return ms.value
+
+    def solver_stats(self):
+        a, b = C.c_long(0), C.c_long(0)
+        _check(self.lib.sdddst_solver_stats(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def launches(self) -> int:
         return int(self.lib.sdddst_kernel_launches(self.h))

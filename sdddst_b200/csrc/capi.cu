@@ -345,9 +345,17 @@ int sdddst_profile_pair_sum(void *ctx, int reps, double *ms_per_launch)
     if (!rc) cudaEventElapsedTime(&ms, a, b);
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    e->launches += 2 * (reps + 1);
+    e->launches += (e->prm.pairsum == SDDDST_PAIRSUM_FP32 ? 3 : 2) * (reps + 1);
     *ms_per_launch = ms / reps;
     return from_engine(e, rc);
+}
+
+int sdddst_solver_stats(void *ctx, long *solves, long *iterations)
+{
+    if (!ctx) return fail(SDDDST_ERR_INVALID, "null argument");
+    if (solves) *solves = E(ctx)->solves;
+    if (iterations) *iterations = E(ctx)->iterations;
+    return SDDDST_OK;
 }
 
 long sdddst_kernel_launches(void *ctx) { return ctx ? E(ctx)->launches : 0; }

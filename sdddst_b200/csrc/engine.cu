@@ -36,10 +36,13 @@ Engine::~Engine()
     void *bufs[] = {d_x0, d_y, d_b, d_xb, d_x1, d_x2, d_xs, d_v0, d_v0b, d_vs, d_vs2, d_S0, d_S1, d_Stmp,
                     d_g, d_sol, d_dvec, d_tol, d_tol_last, d_minr2, d_part, d_pdx, d_pdy, d_cell,
                     d_cell_count, d_cell_start, d_cell_fill, d_sorted, d_rowcnt, d_rowptr, d_col, d_val,
-                    d_V, d_w, d_z, d_r, d_hcol, d_partials, d_scal, d_y_small, d_ys, d_bs, d_flag};
+                    d_V, d_w, d_z, d_r, d_hcol, d_partials, d_scal, d_y_small, d_ys, d_bs, d_flag, d_xw};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (h_scal) cudaFreeHost(h_scal);
+    if (h_hrec) cudaFreeHost(h_hrec);
+    if (d_hrec) cudaFree(d_hrec);
+    if (d_counter) cudaFree(d_counter);
     precond_free(*this);
     if (st) cudaStreamDestroy(st);
 }
@@ -89,6 +92,7 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     }
     if (prm.ic < 1) prm.ic = 2;
     if (prm.gmres_restart < 2) prm.gmres_restart = 30;
+    if (prm.gmres_restart > 31) prm.gmres_restart = 31; // fused Gram-Schmidt kernels hold 32 partial sums
     if (cudaSetDevice(device) != cudaSuccess) {
         err = "cudaSetDevice failed";
         return SDDDST_ERR_CUDA;
@@ -112,7 +116,7 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     int rc = 0;
     double **vecs[] = {&d_x0, &d_y, &d_b, &d_xb, &d_x1, &d_x2, &d_xs, &d_v0, &d_v0b, &d_vs, &d_vs2,
                        &d_S0, &d_S1, &d_Stmp, &d_g, &d_sol, &d_dvec, &d_tol, &d_tol_last, &d_w, &d_z,
-                       &d_r, &d_ys, &d_bs};
+                       &d_r, &d_ys, &d_bs, &d_xw};
     for (double **v : vecs) rc |= dalloc(v, n);
     rc |= dalloc(&d_minr2, n);
     rc |= dalloc(&d_part, pair_part_doubles(n));
@@ -129,7 +133,11 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     rc |= dalloc(&d_flag, 4);
     rc |= dalloc(&d_V, (size_t)(restart + 1) * n);
     rc |= dalloc(&d_hcol, 2 * (restart + 1) + 4);
-    rc |= dalloc(&d_partials, (size_t)red_blocks * (restart + 2));
+    rc |= dalloc(&d_partials, (size_t)red_blocks * 32 + 64);
+    rc |= dalloc(&d_hrec, (size_t)(restart + 1) * (2 * (restart + 1) + 1));
+    rc |= dalloc(&d_counter, 4);
+    if (cudaMallocHost((void **)&h_hrec, sizeof(double) * (restart + 1) * (2 * (restart + 1) + 1)) != cudaSuccess)
+        rc |= SDDDST_ERR_NOMEM;
     rc |= dalloc(&d_scal, 8);
     rc |= dalloc(&d_y_small, (size_t)n + restart + 8);
     if (cudaMallocHost((void **)&h_scal, sizeof(double) * (2 * (restart + 1) + 8)) != cudaSuccess)
@@ -175,6 +183,7 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     cudaMemcpyAsync(d_tol, t0.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(d_tol_last, t0.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(d_dvec, 0, sizeof(double) * n, st);
+    cudaMemsetAsync(d_counter, 0, sizeof(unsigned int), st);
     return sync_check("init");
 }
 
@@ -215,7 +224,7 @@ int Engine::speeds(const double *x, double *v_out, double *S_out, int stress_typ
     const double r2_track = update_tol ? 400.0 * prec * prec * (1.0 + 1e-9) : 0.0;
     launch_pair_sum(*this, x, st, prm.pairsum, r2_track);
     launch_speeds_finish(*this, x, tau_ext, S_out, v_out, update_tol ? 1 : 0, st);
-    launches += 3;
+    launches += prm.pairsum == SDDDST_PAIRSUM_FP32 ? 4 : 3;
     return 0;
 }
 

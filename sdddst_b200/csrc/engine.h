@@ -34,6 +34,7 @@ struct Engine {
     double *d_part = nullptr;
     double *d_pdx = nullptr, *d_pdy = nullptr;
     double *d_ys = nullptr, *d_bs = nullptr; // scratch y, b of caller-supplied configurations
+    double *d_xw = nullptr;                  // positions wrapped into [-0.5, 0.5) (mixed pair sum)
 
     // ---- cell list of the cutoff-neighbour search
     int G = 1; // cells per axis
@@ -56,6 +57,10 @@ struct Engine {
     double *h_scal = nullptr; // pinned
     int last_iters = 0;
     double last_resid = 0.0;
+    long solves = 0, iterations = 0;      // solver statistics
+    double *d_hrec = nullptr;             // per-iteration Gram-Schmidt records
+    double *h_hrec = nullptr;             // pinned copy
+    unsigned int *d_counter = nullptr;    // last-block ticket of the fused reductions
 
     // ---- cluster block-Jacobi preconditioner (precond.cu)
     int *pc_ptr = nullptr, *pc_parent = nullptr, *pc_tmp = nullptr, *pc_tmp2 = nullptr, *pc_members = nullptr;

@@ -1,18 +1,22 @@
 // FP32 field kernel for the mixed-precision pair sum.
 //
-// Same image structure as field_f64.cuh (AnalyticField.cpp:145-160): the
-// separation is formed and wrapped in FP64 (so close pairs keep full relative
-// accuracy) and rounded to FP32 once; the image terms run in FP32 with the
-// SFU (ex2, rcp); the caller accumulates the per-pair results in FP64.
+// Same image structure as field_f64.cuh (AnalyticField.cpp:145-160).  The
+// separation is formed and wrapped in FP64 by the caller (so close pairs keep
+// full relative accuracy) and rounded to FP32 once; the image terms run in
+// FP32 with the SFU (ex2, rcp); the caller accumulates in FP64.
+//  * sin(pi dy), |dy| <= 0.5, is an odd degree-13 polynomial (Taylor; the
+//    remainder is below 7e-10);
 //  * k = 0 uses cosh 2a - cos 2b = 2(sinh^2 a + sin^2 b) and
 //    cosh 2a cos 2b - 1 = 2(sinh^2 a - sin^2 b) - 4 sinh^2 a sin^2 b, with
-//    sinh a from its odd Taylor series below |a| = 0.5 (truncation < 4e-9
+//    sinh a from its odd Taylor series below |a| = 0.5 (remainder < 4e-9
 //    relative) and from e^{+-a} above;
 //  * |k| = 1 images are exact: (C cy - 1) / (C - cy)^2 with C = cosh 2pi u;
-//  * |u| >= 1.5 images use t = 1/C = 2 e^{-2 pi |u|} (the dropped e^{-4 pi |u|}
-//    part is below 7e-9 relative) and N/D^2 = cy t + (2 cy^2 - 1) t^2 +
-//    O(t^3) (|t| <= 1.6e-4, so the remainder is below 3e-8 relative), which
-//    needs neither a division nor an SFU op.
+//  * |u| >= 1.5 images use t = 1/C = 2 e^{-2 pi |u|} (dropped part below
+//    7e-9 relative) and N/D^2 = cy t + (2 cy^2 - 1) t^2 + O(t^3); with
+//    t = 2 E^{-+1} e^{-2 pi k} the sums over k = 2..4 collapse to
+//    polynomials in dx with constant coefficients (the t^2 part is kept for
+//    k = 2 only; for k >= 3 it is below 3e-7 of a term that is itself below
+//    1e-7 of tau).
 #pragma once
 
 #include "common.cuh"
@@ -22,82 +26,75 @@ namespace sd {
 constexpr float kPiF = 3.14159265358979f;
 constexpr float kTwoPiSqF = 19.7392088021787f;
 
-// e^{-2 pi k} in FP32, k = 1..5
-__device__ __forceinline__ float qnegf(int k)
+// e^{+-2 pi k} and the far-image sums
+constexpr float kQP1 = 535.4916555247647f;                       // e^{2 pi}
+constexpr float kQN1 = 1.8674427317079889e-03f;                  // e^{-2 pi}
+constexpr float kQN2 = 3.4873423562089956e-06f;
+constexpr float kQN3 = 6.512412136079901e-09f;
+constexpr float kQN4 = 1.2161556709409309e-11f;
+constexpr float kQN5 = 2.2711010683240937e-14f;
+constexpr float kA1 = 3.4938669795049805e-06f;                   // qn2 + qn3 + qn4
+constexpr float kB1 = 6.994256639099779e-06f;                    // 2 qn2 + 3 qn3 + 4 qn4
+constexpr float kQN2SQ = 1.2161556709409309e-11f;                // qn2^2 = qn4
+
+__device__ __forceinline__ float sinpi_poly(float y)
 {
-    switch (k) {
-    case 1: return 1.8674427317079889e-03f;
-    case 2: return 3.4873423562089956e-06f;
-    case 3: return 6.512412136079901e-09f;
-    case 4: return 1.2161556709409309e-11f;
-    default: return 2.2711010683240937e-14f;
-    }
-}
-__device__ __forceinline__ float qposf(int k)
-{
-    switch (k) {
-    case 1: return 535.4916555247647f;
-    case 2: return 286751.3131366533f;
-    case 3: return 153552935.3954467f;
-    case 4: return 82226315585.595f;
-    default: return 44031505860632.03f;
-    }
+    const float y2 = y * y;
+    float p = 0.00046630280576761f;   //  pi^13 / 13!
+    p = fmaf(p, y2, -0.00737043094571435f); // -pi^11 / 11!
+    p = fmaf(p, y2, 0.08214588661112823f);  //  pi^9 / 9!
+    p = fmaf(p, y2, -0.59926452932079207f); // -pi^7 / 7!
+    p = fmaf(p, y2, 2.55016403987734549f);  //  pi^5 / 5!
+    p = fmaf(p, y2, -5.16771278004997003f); // -pi^3 / 3!
+    p = fmaf(p, y2, 3.14159265358979324f);  //  pi
+    return y * p;
 }
 
-__device__ __forceinline__ float sinh_small_or_exp(float a, float ep, float epi)
+// tau_xy(dx, dy) in FP32; dx, dy already minimum-image in [-0.5, 0.5].
+__device__ __forceinline__ float tau_xy_f32(float dx, float dy)
 {
-    float a2 = a * a;
-    float poly = a * (1.0f + a2 * (1.0f / 6.0f + a2 * (1.0f / 120.0f + a2 * (1.0f / 5040.0f))));
-    return fabsf(a) < 0.5f ? poly : 0.5f * (ep - epi);
-}
-
-// tau_xy(dx, dy) in FP32 from FP64 separations.
-__device__ __forceinline__ float tau_xy_f32(double dxd, double dyd)
-{
-    const float dx = (float)dxd, dy = (float)dyd;
-    const float sn = sinpif(dy);
+    const float sn = sinpi_poly(dy);
     const float sn2 = sn * sn;
-    const float cy = 1.0f - 2.0f * sn2;
+    const float cy = fmaf(-2.0f, sn2, 1.0f);
     const float a = kPiF * dx;
     const float ep = __expf(a);
     const float epi = __expf(-a);
-    const float sh = sinh_small_or_exp(a, ep, epi);
+    const float a2 = a * a;
+    const float poly = a * fmaf(a2, fmaf(a2, fmaf(a2, 1.0f / 5040.0f, 1.0f / 120.0f), 1.0f / 6.0f), 1.0f);
+    const float sh = fabsf(a) < 0.5f ? poly : 0.5f * (ep - epi);
     const float sh2 = sh * sh;
     const float E = ep * ep, Ei = epi * epi;
     const bool pos = dx >= 0.0f;
 
     // k = 0
     const float D0 = 2.0f * (sh2 + sn2);
-    const float N0 = 2.0f * (sh2 - sn2) - 4.0f * sh2 * sn2;
+    const float N0 = fmaf(-4.0f * sh2, sn2, 2.0f * (sh2 - sn2));
     const float r0 = __frcp_rn(D0);
     float acc = dx * N0 * r0 * r0;
 
     // |k| = 1, exact
     {
-        float Cp = 0.5f * (E * qposf(1) + Ei * qnegf(1));
-        float Dp = Cp - cy;
-        float rp = __frcp_rn(Dp * Dp);
-        float Cm = 0.5f * (E * qnegf(1) + Ei * qposf(1));
-        float Dm = Cm - cy;
-        float rm = __frcp_rn(Dm * Dm);
-        acc += (dx + 1.0f) * (Cp * cy - 1.0f) * rp + (dx - 1.0f) * (Cm * cy - 1.0f) * rm;
+        const float Cp = 0.5f * fmaf(E, kQP1, Ei * kQN1);
+        const float Dp = Cp - cy;
+        const float rp = __frcp_rn(Dp * Dp);
+        const float Cm = 0.5f * fmaf(E, kQN1, Ei * kQP1);
+        const float Dm = Cm - cy;
+        const float rm = __frcp_rn(Dm * Dm);
+        acc = fmaf((dx + 1.0f) * fmaf(Cp, cy, -1.0f), rp, acc);
+        acc = fmaf((dx - 1.0f) * fmaf(Cm, cy, -1.0f), rm, acc);
     }
-    // far images: t = 2 e^{-2 pi |u|}
-    const float c2 = 2.0f * cy * cy - 1.0f;
-    float far = 0.0f;
-#pragma unroll
-    for (int k = 2; k <= 4; ++k) {
-        float tp = 2.0f * Ei * qnegf(k); // u = dx + k > 0
-        float tm = 2.0f * E * qnegf(k);  // u = dx - k < 0
-        float wp = (k == 4 && pos) ? 1.0f - dx : 1.0f;
-        float wm = (k == 4 && !pos) ? 1.0f + dx : 1.0f;
-        far += wp * (dx + (float)k) * tp * (cy + c2 * tp) + wm * (dx - (float)k) * tm * (cy + c2 * tm);
-    }
-    {
-        float t5 = pos ? 2.0f * E * qnegf(5) : 2.0f * Ei * qnegf(5);
-        float u5 = pos ? dx - 5.0f : dx + 5.0f;
-        far += fabsf(dx) * u5 * t5 * (cy + c2 * t5);
-    }
+    // |u| >= 1.5: first-order sums over k = 2..4 (+k side uses E^-1, -k side E)
+    const float c2 = fmaf(2.0f * cy, cy, -1.0f);
+    const float base = dx * kA1;
+    const float w4 = pos ? -dx * (dx + 4.0f) * kQN4 : dx * (dx - 4.0f) * kQN4;
+    const float S1p = base + kB1 + (pos ? w4 : 0.0f);
+    const float S1m = base - kB1 + (pos ? 0.0f : w4);
+    float far = 2.0f * cy * fmaf(Ei, S1p, E * S1m);
+    far = fmaf(4.0f * c2 * kQN2SQ, fmaf(Ei * Ei, dx + 2.0f, E * E * (dx - 2.0f)), far);
+    // end image: -5 (dx >= 0) or +5 (dx < 0), weight |dx|
+    const float t5 = 2.0f * (pos ? E : Ei) * kQN5;
+    const float u5 = pos ? dx - 5.0f : dx + 5.0f;
+    far = fmaf(fabsf(dx) * u5 * t5, fmaf(c2, t5, cy), far);
     return (acc + far) * kTwoPiSqF;
 }
 

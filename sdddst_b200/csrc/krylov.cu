@@ -267,8 +267,91 @@ void launch_axpy_update(const Engine &e, double *xn, const double *sol, cudaStre
     update_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, xn, sol);
 }
 
-// Restarted GMRES(m) on J(h) x = rhs, x0 = 0.  Returns 0 on convergence to
-// e.prm.solver_tol relative residual, SDDDST_ERR_SOLVER otherwise.
+// ---- fused Gram-Schmidt passes: one kernel per pass, each ending in a
+// deterministic last-block reduction of the per-block partials.
+//   OP 0: out[k] = V[k] . w                       (k < kk)
+//   OP 1: w -= V c;  out[k] = V[k] . w            (classical GS, second pass)
+//   OP 2: w -= V c;  out[0] = w . w
+//   OP 3: out[0] = w . w
+template <int OP>
+__global__ void __launch_bounds__(256) gs_fused_kernel(int n, int kk, const double *__restrict__ V, size_t ldv,
+                                                       double *__restrict__ w, const double *__restrict__ c,
+                                                       double *__restrict__ out, double *__restrict__ partials,
+                                                       unsigned int *__restrict__ counter)
+{
+    constexpr int KM = 32;
+    __shared__ double cs[KM];
+    __shared__ double red[8][KM + 1];
+    __shared__ bool last;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if ((OP == 1 || OP == 2) && tid < kk) cs[tid] = c[tid];
+    __syncthreads();
+    double acc[KM];
+#pragma unroll
+    for (int k = 0; k < KM; ++k) acc[k] = 0.0;
+    const int nb = gridDim.x;
+    const int chunk = (n + nb - 1) / nb;
+    const int s0 = blockIdx.x * chunk, e0 = min(n, s0 + chunk);
+    for (int i = s0 + tid; i < e0; i += blockDim.x) {
+        double wi = w[i];
+        if (OP == 1 || OP == 2) {
+            double u = 0.0;
+            for (int k = 0; k < kk; ++k) u += V[(size_t)k * ldv + i] * cs[k];
+            wi -= u;
+            w[i] = wi;
+        }
+        if (OP == 0 || OP == 1) {
+#pragma unroll
+            for (int k = 0; k < KM; ++k)
+                if (k < kk) acc[k] += V[(size_t)k * ldv + i] * wi;
+        } else {
+            acc[0] += wi * wi;
+        }
+    }
+    const int nout = (OP == 0 || OP == 1) ? kk : 1;
+#pragma unroll
+    for (int k = 0; k < KM; ++k) {
+        if (k < nout) {
+            double v = warp_sum(acc[k]);
+            if (lane == 0) red[wid][k] = v;
+        }
+    }
+    __syncthreads();
+    if (tid < nout) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[q][tid];
+        partials[(size_t)blockIdx.x * KM + tid] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (tid < nout) {
+        double t = 0.0;
+        for (int b = 0; b < nb; ++b) t += partials[(size_t)b * KM + tid];
+        out[tid] = t;
+    }
+    if (tid == 0) *counter = 0u;
+}
+
+// V_{j+1} = w / sqrt(nrm2) (zero vector on breakdown)
+__global__ void normalize_kernel(int n, const double *__restrict__ w, const double *__restrict__ nrm2,
+                                 double *__restrict__ v)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double s = *nrm2;
+    v[i] = s > 0.0 ? w[i] * rsqrt(s) : 0.0;
+}
+
+// Restarted GMRES(m) on J(h) x = rhs, x0 = 0, right preconditioned
+// (precond 0: none, 1: diagonal, 2: cluster blocks).  Iterations run without
+// host synchronisation; every `chk` iterations the Hessenberg columns come
+// back in one copy, the host applies the Givens rotations and tests
+// convergence (so at most chk-1 iterations past convergence are computed).
+// Returns 0 on reaching e.prm.solver_tol relative residual.
 int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, double *x, int precond)
 {
     const int n = e.n, m = e.restart;
@@ -277,17 +360,37 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
     const unsigned nb = (unsigned)((n + 255) / 256);
     const double tol = e.prm.solver_tol > 0 ? e.prm.solver_tol : 1e-13;
     const int max_it = e.prm.max_iters > 0 ? e.prm.max_iters : 1000;
+    const int chk = 4;
+    const int stride = 2 * (m + 1) + 1; // per-iteration record: c1[m+1], c2[m+1], nrm2
     double *V = e.d_V, *w = e.d_w, *z = e.d_z, *r = e.d_r;
     double *dinv = nullptr;
+    const int wpb = 8;
     cudaMemsetAsync(x, 0, sizeof(double) * n, st);
     if (precond == 1) {
         dinv = e.d_y_small; // n doubles reserved for the diagonal
         jdiag_inv_kernel<<<nb, 256, 0, st>>>(n, h, e.d_rowptr, e.d_val, dvec, dinv);
         e.launches++;
     }
-    double beta0;
-    if (int rc = reduce_sum(e, rhs, rhs, n, 4, &beta0)) return rc;
-    beta0 = std::sqrt(beta0);
+    auto apply_precond = [&](const double *in, double *out) -> const double * {
+        if (precond == 1) {
+            mul_kernel<<<nb, 256, 0, st>>>(n, in, dinv, out);
+            e.launches++;
+            return out;
+        }
+        if (precond == 2) {
+            precond_apply(e, in, out);
+            return out;
+        }
+        return in;
+    };
+    // beta0 = ||rhs||
+    cudaMemcpyAsync(r, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
+    gs_fused_kernel<3><<<e.red_blocks, 256, 0, st>>>(n, 1, nullptr, ldv, r, nullptr, e.d_scal, e.d_partials,
+                                                     e.d_counter);
+    e.launches++;
+    cudaMemcpyAsync(e.h_scal, e.d_scal, sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (int rc = e.sync_check("gmres start")) return rc;
+    double beta0 = std::sqrt(e.h_scal[0]);
     e.last_iters = 0;
     e.last_resid = 0.0;
     if (beta0 == 0.0) return 0;
@@ -295,78 +398,72 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
         e.err = "solve: non-finite right-hand side";
         return SDDDST_ERR_NONFINITE;
     }
-    cudaMemcpyAsync(r, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
     double beta = beta0;
     std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), gv(m + 1), yv(m);
-    double *hpk = e.h_scal; // pinned, 2m+3 doubles
+    double *hrec = e.h_hrec;
     int total = 0;
     bool converged = false;
-    const int wpb = 8;
     while (!converged) {
-        scale_kernel<<<nb, 256, 0, st>>>(n, 1.0 / beta, r, V);
+        normalize_kernel<<<nb, 256, 0, st>>>(n, r, e.d_scal, V); // d_scal holds ||r||^2
         e.launches++;
         std::fill(gv.begin(), gv.end(), 0.0);
         gv[0] = beta;
         int k = 0;
-        for (int j = 0; j < m; ++j) {
-            const double *vj = V + (size_t)j * ldv;
-            const double *src = vj;
-            if (precond == 1) {
-                mul_kernel<<<nb, 256, 0, st>>>(n, vj, dinv, z);
-                src = z;
-                e.launches++;
-            } else if (precond == 2) {
-                precond_apply(e, vj, z);
-                src = z;
+        int j = 0;
+        bool stop = false;
+        while (j < m && !stop) {
+            const int jend = std::min(m, j + chk);
+            for (int jj = j; jj < jend; ++jj) {
+                const double *src = apply_precond(V + (size_t)jj * ldv, z);
+                spmv_j_kernel<<<(n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec,
+                                                                        src, w);
+                double *rec = e.d_hrec + (size_t)jj * stride;
+                const int kk = jj + 1;
+                gs_fused_kernel<0><<<e.red_blocks, 256, 0, st>>>(n, kk, V, ldv, w, nullptr, rec, e.d_partials,
+                                                                 e.d_counter);
+                gs_fused_kernel<1><<<e.red_blocks, 256, 0, st>>>(n, kk, V, ldv, w, rec, rec + (m + 1), e.d_partials,
+                                                                 e.d_counter);
+                gs_fused_kernel<2><<<e.red_blocks, 256, 0, st>>>(n, kk, V, ldv, w, rec + (m + 1), rec + 2 * (m + 1),
+                                                                 e.d_partials, e.d_counter);
+                normalize_kernel<<<nb, 256, 0, st>>>(n, w, rec + 2 * (m + 1), V + (size_t)(jj + 1) * ldv);
+                e.launches += 5;
             }
-            spmv_j_kernel<<<(n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, src, w);
-            const int kk = j + 1;
-            // CGS2
-            multi_dot_partial_kernel<<<e.red_blocks, 256, 0, st>>>(n, kk, V, ldv, w, e.d_partials);
-            multi_dot_final_kernel<<<kk, 256, 0, st>>>(e.red_blocks, kk, e.d_partials, e.d_hcol);
-            gs_update_kernel<<<nb, 256, 0, st>>>(n, kk, V, ldv, e.d_hcol, w);
-            multi_dot_partial_kernel<<<e.red_blocks, 256, 0, st>>>(n, kk, V, ldv, w, e.d_partials);
-            multi_dot_final_kernel<<<kk, 256, 0, st>>>(e.red_blocks, kk, e.d_partials, e.d_hcol + (m + 1));
-            gs_update_kernel<<<nb, 256, 0, st>>>(n, kk, V, ldv, e.d_hcol + (m + 1), w);
-            reduce_partial_kernel<4><<<e.red_blocks, 256, 0, st>>>(n, w, w, nullptr, e.d_partials);
-            reduce_final_kernel<4><<<1, 256, 0, st>>>(e.red_blocks, e.d_partials, e.d_hcol + 2 * (m + 1));
-            e.launches += 9;
-            cudaMemcpyAsync(hpk, e.d_hcol, sizeof(double) * (2 * (m + 1) + 1), cudaMemcpyDeviceToHost, st);
+            cudaMemcpyAsync(hrec + (size_t)j * stride, e.d_hrec + (size_t)j * stride,
+                            sizeof(double) * stride * (jend - j), cudaMemcpyDeviceToHost, st);
             if (int rc = e.sync_check("gmres iteration")) return rc;
-            double hn = std::sqrt(std::max(hpk[2 * (m + 1)], 0.0));
-            for (int i = 0; i < kk; ++i) H[(size_t)i * m + j] = hpk[i] + hpk[(m + 1) + i];
-            H[(size_t)(j + 1) * m + j] = hn;
-            if (!std::isfinite(hn)) {
-                e.err = "solve: non-finite Krylov vector";
-                return SDDDST_ERR_NONFINITE;
+            for (int jj = j; jj < jend && !stop; ++jj) {
+                const double *rc = hrec + (size_t)jj * stride;
+                const double hn = std::sqrt(std::max(rc[2 * (m + 1)], 0.0));
+                for (int i = 0; i <= jj; ++i) H[(size_t)i * m + jj] = rc[i] + rc[(m + 1) + i];
+                H[(size_t)(jj + 1) * m + jj] = hn;
+                if (!std::isfinite(hn)) {
+                    e.err = "solve: non-finite Krylov vector";
+                    return SDDDST_ERR_NONFINITE;
+                }
+                for (int i = 0; i < jj; ++i) {
+                    double a = H[(size_t)i * m + jj], b2 = H[(size_t)(i + 1) * m + jj];
+                    H[(size_t)i * m + jj] = cs[i] * a + sn[i] * b2;
+                    H[(size_t)(i + 1) * m + jj] = -sn[i] * a + cs[i] * b2;
+                }
+                double a = H[(size_t)jj * m + jj], b2 = H[(size_t)(jj + 1) * m + jj];
+                double rr = std::hypot(a, b2);
+                cs[jj] = rr > 0 ? a / rr : 1.0;
+                sn[jj] = rr > 0 ? b2 / rr : 0.0;
+                H[(size_t)jj * m + jj] = rr;
+                H[(size_t)(jj + 1) * m + jj] = 0.0;
+                gv[jj + 1] = -sn[jj] * gv[jj];
+                gv[jj] = cs[jj] * gv[jj];
+                ++total;
+                k = jj + 1;
+                if (std::fabs(gv[jj + 1]) <= tol * beta0 || hn == 0.0) {
+                    converged = true;
+                    stop = true;
+                }
+                if (total >= max_it) stop = true;
             }
-            if (hn > 0.0) {
-                scale_kernel<<<nb, 256, 0, st>>>(n, 1.0 / hn, w, V + (size_t)(j + 1) * ldv);
-                e.launches++;
-            }
-            // Givens
-            for (int i = 0; i < j; ++i) {
-                double a = H[(size_t)i * m + j], b2 = H[(size_t)(i + 1) * m + j];
-                H[(size_t)i * m + j] = cs[i] * a + sn[i] * b2;
-                H[(size_t)(i + 1) * m + j] = -sn[i] * a + cs[i] * b2;
-            }
-            double a = H[(size_t)j * m + j], b2 = H[(size_t)(j + 1) * m + j];
-            double rr = std::hypot(a, b2);
-            cs[j] = rr > 0 ? a / rr : 1.0;
-            sn[j] = rr > 0 ? b2 / rr : 0.0;
-            H[(size_t)j * m + j] = rr;
-            H[(size_t)(j + 1) * m + j] = 0.0;
-            gv[j + 1] = -sn[j] * gv[j];
-            gv[j] = cs[j] * gv[j];
-            ++total;
-            k = j + 1;
-            if (std::fabs(gv[j + 1]) <= tol * beta0 || hn == 0.0) {
-                converged = true;
-                break;
-            }
-            if (total >= max_it) break;
+            j = jend;
         }
-        // back substitution
+        // back substitution and x += M^-1 V y
         for (int i = k - 1; i >= 0; --i) {
             double s = gv[i];
             for (int q = i + 1; q < k; ++q) s -= H[(size_t)i * m + q] * yv[q];
@@ -374,7 +471,6 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
         }
         cudaMemcpyAsync(e.d_y_small + n, yv.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st);
         if (precond == 2) {
-            // x += M^-1 (V y)
             cudaMemsetAsync(r, 0, sizeof(double) * n, st);
             combine_kernel<<<nb, 256, 0, st>>>(n, k, V, ldv, e.d_y_small + n, nullptr, r);
             precond_apply(e, r, z);
@@ -384,21 +480,24 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
             combine_kernel<<<nb, 256, 0, st>>>(n, k, V, ldv, e.d_y_small + n, dinv, x);
             e.launches++;
         }
-        if (converged) break;
-        if (total >= max_it) break;
-        // true residual for the restart
+        if (converged || total >= max_it) break;
+        // restart from the true residual
         spmv_j_kernel<<<(n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, x, w);
         sub_kernel<<<nb, 256, 0, st>>>(n, rhs, w, r);
-        e.launches += 2;
-        double b2;
-        if (int rc = reduce_sum(e, r, r, n, 4, &b2)) return rc;
-        beta = std::sqrt(b2);
+        gs_fused_kernel<3><<<e.red_blocks, 256, 0, st>>>(n, 1, nullptr, ldv, r, nullptr, e.d_scal, e.d_partials,
+                                                         e.d_counter);
+        e.launches += 3;
+        cudaMemcpyAsync(e.h_scal, e.d_scal, sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (int rc = e.sync_check("gmres restart")) return rc;
+        beta = std::sqrt(e.h_scal[0]);
         if (beta <= tol * beta0) {
             converged = true;
             break;
         }
     }
     e.last_iters = total;
+    e.solves++;
+    e.iterations += total;
     if (!converged) {
         e.err = "solve: GMRES did not reach the residual target";
         return SDDDST_ERR_SOLVER;

@@ -74,9 +74,7 @@ __global__ void __launch_bounds__(T) pair_tiles_kernel(const double *__restrict_
                 dx = 0.25;
                 dy = 0.25;
             }
-            double t;
-            if (kMode == 0) t = bi * sb[jj] * tau_xy_f64(dx, dy);
-            else t = bi * sb[jj] * (double)tau_xy_f32(dx, dy);
+            double t = bi * sb[jj] * tau_xy_f64(dx, dy);
             t = valid ? t : 0.0;
             acc += t;
             if (valid && r2 < r2_track) { // rare: only pairs that can set a tolerance
@@ -103,6 +101,109 @@ __global__ void __launch_bounds__(T) pair_tiles_kernel(const double *__restrict_
         if (row_ok) part[(size_t)J * n + i] = acc;
         if (j0 + tid < n) part[(size_t)I * n + j0 + tid] = -ctot;
     }
+}
+
+// Mixed-precision tiles: separations in FP64 from positions pre-wrapped into
+// [-0.5, 0.5) (so x_i - x_j lies in (-1, 1) and one rint() gives the minimum
+// image), rounded once to FP32; field terms in FP32; row and column sums in
+// FP64.  Interior tiles (I < J, full blocks) skip every validity test.
+template <int T, bool kChecked>
+__device__ __forceinline__ void f32_tile_body(const double *sx, const double *sy, const float *sb, double xi,
+                                              double yi, float bi, int n, int j0, int tid, bool row_ok, bool diag,
+                                              int i, float (*tb)[33], double *colsum_w, double &acc,
+                                              unsigned long long *minr2, float r2_track)
+{
+    const int lane = tid & 31;
+    for (int c0 = 0; c0 < T; c0 += 32) {
+#pragma unroll 4
+        for (int k = 0; k < 32; ++k) {
+            const int jj = c0 + k;
+            double dd = xi - sx[jj];
+            dd -= rint(dd);
+            double ee = yi - sy[jj];
+            ee -= rint(ee);
+            float dx = __double2float_rn(dd), dy = __double2float_rn(ee);
+            bool valid = true;
+            if (kChecked) {
+                valid = row_ok && (j0 + jj < n) && (!diag || jj > tid);
+                if (!valid) {
+                    dx = 0.25f;
+                    dy = 0.25f;
+                }
+            }
+            float t = bi * sb[jj] * tau_xy_f32(dx, dy);
+            if (kChecked) t = valid ? t : 0.0f;
+            acc += (double)t;
+            const float r2 = fmaf(dx, dx, dy * dy);
+            if (r2 < r2_track && valid) { // rare: pairs that can set a tolerance
+                atomic_min_nonneg(&minr2[i], (double)r2);
+                atomic_min_nonneg(&minr2[j0 + jj], (double)r2);
+            }
+            tb[k][lane] = t;
+        }
+        __syncwarp();
+        double cs = 0.0;
+#pragma unroll 8
+        for (int m = 0; m < 32; ++m) cs += (double)tb[lane][m];
+        colsum_w[c0 + lane] = cs;
+        __syncwarp();
+    }
+}
+
+template <int T>
+__global__ void __launch_bounds__(T) pair_tiles_f32_kernel(const double *__restrict__ xw, const double *__restrict__ y,
+                                                           const double *__restrict__ b, int n, int nblk,
+                                                           double *__restrict__ part,
+                                                           unsigned long long *__restrict__ minr2, float r2_track)
+{
+    constexpr int W = T / 32;
+    __shared__ double sx[T], sy[T];
+    __shared__ float sb[T];
+    __shared__ float tbuf[W][32][33];
+    __shared__ double colsum[W][T];
+
+    int I, J;
+    tile_coords((long)blockIdx.x, I, J);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int j0 = J * T;
+    {
+        const int j = j0 + tid;
+        const bool ok = j < n;
+        sx[tid] = ok ? xw[j] : 0.0;
+        sy[tid] = ok ? y[j] : 0.0;
+        sb[tid] = ok ? (float)b[j] : 0.0f;
+    }
+    const int i = I * T + tid;
+    const bool row_ok = i < n;
+    const double xi = row_ok ? xw[i] : 0.0;
+    const double yi = row_ok ? y[i] : 0.0;
+    const float bi = row_ok ? (float)b[i] : 0.0f;
+    const bool diag = (I == J);
+    const bool checked = diag || (j0 + T > n) || (I * T + T > n);
+    __syncthreads();
+    double acc = 0.0;
+    if (checked)
+        f32_tile_body<T, true>(sx, sy, sb, xi, yi, bi, n, j0, tid, row_ok, diag, i, tbuf[warp], colsum[warp], acc,
+                               minr2, r2_track);
+    else
+        f32_tile_body<T, false>(sx, sy, sb, xi, yi, bi, n, j0, tid, row_ok, diag, i, tbuf[warp], colsum[warp], acc,
+                                minr2, r2_track);
+    __syncthreads();
+    double ctot = 0.0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) ctot += colsum[w][tid];
+    if (diag) {
+        if (row_ok) part[(size_t)I * n + i] = acc - ctot;
+    } else {
+        if (row_ok) part[(size_t)J * n + i] = acc;
+        if (j0 + tid < n) part[(size_t)I * n + j0 + tid] = -ctot;
+    }
+}
+
+__global__ void wrap_kernel(int n, const double *__restrict__ x, double *__restrict__ xw)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) xw[i] = wrap_half(x[i]);
 }
 
 // Per-dislocation finish: sum of the nblk partials in fixed order, point
@@ -160,16 +261,18 @@ void launch_pair_sum(const Engine &e, const double *x, cudaStream_t st, int mode
     const int nblk = (n + T - 1) / T;
     const long tiles = (long)nblk * (nblk + 1) / 2;
     fill_u64_kernel<<<(n + 255) / 256, 256, 0, st>>>(e.d_minr2, 0x7FF0000000000000ull, n);
-    if (T == 128) {
-        if (mode == 0)
+    if (mode == 0) {
+        if (T == 128)
             pair_tiles_kernel<128, 0><<<(unsigned)tiles, 128, 0, st>>>(x, e.d_y, e.d_b, n, nblk, e.d_part, e.d_minr2, r2_track);
         else
-            pair_tiles_kernel<128, 1><<<(unsigned)tiles, 128, 0, st>>>(x, e.d_y, e.d_b, n, nblk, e.d_part, e.d_minr2, r2_track);
-    } else {
-        if (mode == 0)
             pair_tiles_kernel<64, 0><<<(unsigned)tiles, 64, 0, st>>>(x, e.d_y, e.d_b, n, nblk, e.d_part, e.d_minr2, r2_track);
+    } else {
+        wrap_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, x, e.d_xw);
+        const float tr = (float)r2_track;
+        if (T == 128)
+            pair_tiles_f32_kernel<128><<<(unsigned)tiles, 128, 0, st>>>(e.d_xw, e.d_y, e.d_b, n, nblk, e.d_part, e.d_minr2, tr);
         else
-            pair_tiles_kernel<64, 1><<<(unsigned)tiles, 64, 0, st>>>(x, e.d_y, e.d_b, n, nblk, e.d_part, e.d_minr2, r2_track);
+            pair_tiles_f32_kernel<64><<<(unsigned)tiles, 64, 0, st>>>(e.d_xw, e.d_y, e.d_b, n, nblk, e.d_part, e.d_minr2, tr);
     }
 }
 
