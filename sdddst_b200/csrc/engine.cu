@@ -36,7 +36,8 @@ Engine::~Engine()
     void *bufs[] = {d_x0, d_y, d_b, d_xb, d_x1, d_x2, d_xs, d_v0, d_v0b, d_vs, d_vs2, d_S0, d_S1, d_Stmp,
                     d_g, d_sol, d_dvec, d_tol, d_tol_last, d_minr2, d_part, d_pdx, d_pdy, d_cell,
                     d_cell_count, d_cell_start, d_cell_fill, d_sorted, d_rowcnt, d_rowptr, d_col, d_val,
-                    d_V, d_w, d_z, d_r, d_hcol, d_partials, d_scal, d_y_small, d_ys, d_bs, d_flag, d_xw};
+                    d_V, d_w, d_z, d_r, d_hcol, d_partials, d_scal, d_y_small, d_ys, d_bs, d_flag, d_xw,
+                    d_gdiag, d_valf};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (h_scal) cudaFreeHost(h_scal);
@@ -104,6 +105,7 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     cudaDeviceProp dp;
     cudaGetDeviceProperties(&dp, device);
     red_blocks = 2 * dp.multiProcessorCount;
+    gs_blocks = dp.multiProcessorCount;
     cutoff_multiplier = prm.cutoff_multiplier;
     prec = prm.prec;
     A = prm.A;
@@ -116,7 +118,7 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     int rc = 0;
     double **vecs[] = {&d_x0, &d_y, &d_b, &d_xb, &d_x1, &d_x2, &d_xs, &d_v0, &d_v0b, &d_vs, &d_vs2,
                        &d_S0, &d_S1, &d_Stmp, &d_g, &d_sol, &d_dvec, &d_tol, &d_tol_last, &d_w, &d_z,
-                       &d_r, &d_ys, &d_bs, &d_xw};
+                       &d_r, &d_ys, &d_bs, &d_xw, &d_gdiag};
     for (double **v : vecs) rc |= dalloc(v, n);
     rc |= dalloc(&d_minr2, n);
     rc |= dalloc(&d_part, pair_part_doubles(n));
@@ -153,8 +155,8 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     long est = (long)((double)n * (1.0 + 1.3 * area * n)) + n + 1024;
     if (est > (long)n * n + n) est = (long)n * n + n;
     nnz_cap = est;
-    rc |= dalloc(&d_col, nnz_cap);
-    rc |= dalloc(&d_val, nnz_cap);
+    valf = prm.pairsum == SDDDST_PAIRSUM_FP32;
+    rc |= alloc_csr_values(*this, nnz_cap);
     if (!rc) cudaMemsetAsync(d_col, 0, sizeof(int) * nnz_cap, st);
     if (rc) {
         err = "CSR allocation failed";

@@ -43,7 +43,10 @@ struct Engine {
 
     // ---- CSR of the unit-step Jacobian part G = H / h (diagonal in slot 0 of each row)
     int *d_rowcnt = nullptr, *d_rowptr = nullptr, *d_col = nullptr;
-    double *d_val = nullptr;
+    double *d_val = nullptr;   // FP64 values (plain path)
+    float *d_valf = nullptr;   // FP32 values (mixed path)
+    bool valf = false;         // which of the two holds G
+    double *d_gdiag = nullptr; // G_ii in FP64 (both paths)
     long nnz_cap = 0, nnz = 0;
     int *d_flag = nullptr; // device-side error flag of the assembly
     bool assembled_valid = false;
@@ -53,7 +56,7 @@ struct Engine {
     int restart = 30;
     double *d_V = nullptr, *d_w = nullptr, *d_z = nullptr, *d_r = nullptr, *d_hcol = nullptr;
     double *d_partials = nullptr, *d_scal = nullptr, *d_y_small = nullptr;
-    int red_blocks = 0;
+    int red_blocks = 0, gs_blocks = 0;
     double *h_scal = nullptr; // pinned
     int last_iters = 0;
     double last_resid = 0.0;
@@ -121,6 +124,7 @@ void launch_speeds_raw(int n, const double *x, const double *y, const double *b,
                        double *v, cudaStream_t st);
 
 int jacobian_assemble(Engine &e, const double *x);
+int alloc_csr_values(Engine &e, long cap);
 void launch_make_dvec(const Engine &e, double h, double *dvec, cudaStream_t st);
 void launch_export_jacobian(const Engine &e, double h, const double *dvec, double *val_out, cudaStream_t st);
 

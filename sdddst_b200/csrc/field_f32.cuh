@@ -99,3 +99,75 @@ __device__ __forceinline__ float tau_xy_f32(float dx, float dy)
 }
 
 } // namespace sd
+
+namespace sd {
+
+// d tau_xy / d dx in FP32 (the Jacobian of the mixed path), same image
+// structure as tau_xy_dx_f64:  sum_k w_k f'(u_k) + sigma (f(u_end) - f(u_edge)),
+//   f'(u) = 2 pi^2 / D^2 [N + 2 pi u S (cy - 2 N / D)]   (k = 0, +-1 exact);
+// for |u| >= 1.5, t = 1/C = 2 e^{-2 pi |u|}:
+//   f'(u) = 2 pi^2 [ (1 - 2 pi |u|) cy t
+//                   + ((2 cy^2 - 1) + 2 pi |u| (2 - 4 cy^2)) t^2 ] + O(t^3),
+//   f(u)  = 2 pi^2 u cy t + O(t^2),
+// with the second order kept for k = 2 only and the k = 2..4 first-order sums
+// collapsed to polynomials in dx.
+__device__ __forceinline__ float tau_xy_dx_f32(float dx, float dy)
+{
+    const float twopi = 6.28318530717959f;
+    const float sn = sinpi_poly(dy);
+    const float sn2 = sn * sn;
+    const float cy = fmaf(-2.0f, sn2, 1.0f);
+    const float a = kPiF * dx;
+    const float ep = __expf(a);
+    const float epi = __expf(-a);
+    const float a2 = a * a;
+    const float poly = a * fmaf(a2, fmaf(a2, fmaf(a2, 1.0f / 5040.0f, 1.0f / 120.0f), 1.0f / 6.0f), 1.0f);
+    const float sh = fabsf(a) < 0.5f ? poly : 0.5f * (ep - epi);
+    const float ch = 0.5f * (ep + epi);
+    const float sh2 = sh * sh;
+    const float E = ep * ep, Ei = epi * epi;
+    const bool pos = dx >= 0.0f;
+
+    // k = 0
+    const float D0 = 2.0f * (sh2 + sn2);
+    const float N0 = fmaf(-4.0f * sh2, sn2, 2.0f * (sh2 - sn2));
+    const float S0 = 2.0f * sh * ch;
+    const float r0 = __frcp_rn(D0);
+    float acc = r0 * r0 * fmaf(twopi * dx * S0, fmaf(-2.0f * N0, r0, cy), N0);
+    // |k| = 1
+    {
+        const float ap = E * kQP1, bp = Ei * kQN1;
+        const float Cp = 0.5f * (ap + bp), Sp = 0.5f * (ap - bp);
+        const float Dp = Cp - cy, Np = fmaf(Cp, cy, -1.0f);
+        const float rp = __frcp_rn(Dp);
+        acc = fmaf(rp * rp, fmaf(twopi * (dx + 1.0f) * Sp, fmaf(-2.0f * Np, rp, cy), Np), acc);
+        const float am = E * kQN1, bm = Ei * kQP1;
+        const float Cm = 0.5f * (am + bm), Sm = 0.5f * (am - bm);
+        const float Dm = Cm - cy, Nm = fmaf(Cm, cy, -1.0f);
+        const float rm = __frcp_rn(Dm);
+        acc = fmaf(rm * rm, fmaf(twopi * (dx - 1.0f) * Sm, fmaf(-2.0f * Nm, rm, cy), Nm), acc);
+    }
+    // |k| = 2..4, first order, + side (E^-1) and - side (E)
+    const float sp = fmaf(1.0f - twopi * dx, kA1, -twopi * kB1) -
+                     (pos ? dx * kQN4 * (1.0f - twopi * (dx + 4.0f)) : 0.0f);
+    const float sm = fmaf(1.0f + twopi * dx, kA1, -twopi * kB1) +
+                     (pos ? 0.0f : dx * kQN4 * (1.0f - twopi * (4.0f - dx)));
+    float far = 2.0f * cy * fmaf(Ei, sp, E * sm);
+    // second order, k = 2
+    {
+        const float c2 = fmaf(2.0f * cy, cy, -1.0f), c4 = fmaf(-4.0f * cy, cy, 2.0f);
+        const float tp = 2.0f * Ei * kQN2, tm = 2.0f * E * kQN2;
+        far = fmaf(tp * tp, fmaf(twopi * (dx + 2.0f), c4, c2), far);
+        far = fmaf(tm * tm, fmaf(twopi * (2.0f - dx), c4, c2), far);
+    }
+    // end image (weight |dx|) and sigma (f(u_end) - f(u_edge))
+    const float te = 2.0f * (pos ? E : Ei) * kQN5;
+    const float ue_abs = pos ? 5.0f - dx : 5.0f + dx;
+    far = fmaf(fabsf(dx) * cy * te, fmaf(-twopi, ue_abs, 1.0f), far);
+    const float fe = (pos ? dx - 5.0f : dx + 5.0f) * te * cy;
+    const float fg = (pos ? (dx + 4.0f) * 2.0f * Ei * kQN4 : (dx - 4.0f) * 2.0f * E * kQN4) * cy;
+    far += pos ? fe - fg : fg - fe;
+    return (acc + far) * kTwoPiSqF;
+}
+
+} // namespace sd

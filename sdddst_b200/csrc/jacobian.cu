@@ -16,6 +16,7 @@
 // symmetric.
 #include "engine.h"
 #include "field_f64.cuh"
+#include "field_f32.cuh"
 
 namespace sd {
 
@@ -162,11 +163,12 @@ __global__ void row_count_kernel(int n, const double *__restrict__ x, const doub
     if (lane == 0) rowcnt[i] = cnt + 1;
 }
 
+template <typename VT>
 __global__ void row_fill_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
                                 const double *__restrict__ b, CellScan cs, double c, double c2, double ic2,
-                                const int *__restrict__ rowptr, int *__restrict__ col, double *__restrict__ val,
-                                int p, const double *__restrict__ pdx, const double *__restrict__ pdy, double A,
-                                double K, int *__restrict__ flag)
+                                const int *__restrict__ rowptr, int *__restrict__ col, VT *__restrict__ val,
+                                double *__restrict__ gdiag, int p, const double *__restrict__ pdx,
+                                const double *__restrict__ pdy, double A, double K, int *__restrict__ flag)
 {
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -214,9 +216,12 @@ __global__ void row_fill_kernel(int n, const double *__restrict__ x, const doubl
         double dy = wrap_half(y[hi] - y[lo]);
         double w;
         pair_kept(r2_exact(dx, dy), c, c2, ic2, &w);
-        double v = bi * b[j] * tau_xy_dx_f64(dx, dy) * w;
+        double tdx;
+        if (sizeof(VT) == sizeof(double)) tdx = tau_xy_dx_f64(dx, dy);
+        else tdx = (double)tau_xy_dx_f32(__double2float_rn(dx), __double2float_rn(dy));
+        const VT v = (VT)(bi * b[j] * tdx * w);
         val[q] = v;
-        rs += v;
+        rs += (double)v;
     }
     // 3) point-defect seed of the diagonal (simulation.cpp:274-325)
     double pd = 0.0;
@@ -230,17 +235,17 @@ __global__ void row_fill_kernel(int n, const double *__restrict__ x, const doubl
     pd = warp_sum(pd);
     if (lane == 0) {
         col[base] = i;
-        val[base] = -(rs + pd);
+        val[base] = (VT)(-(rs + pd));
+        gdiag[i] = -(rs + pd);
     }
 }
 
 // d_i = (s / (1 + s))^2 for s = h G_ii > 0 (simulation.cpp:349-374).
-__global__ void make_dvec_kernel(int n, double h, const int *__restrict__ rowptr, const double *__restrict__ val,
-                                 double *__restrict__ dvec)
+__global__ void make_dvec_kernel(int n, double h, const double *__restrict__ gdiag, double *__restrict__ dvec)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double s = __dmul_rn(h, val[rowptr[i]]);
+    double s = __dmul_rn(h, gdiag[i]);
     double d = 0.0;
     if (s > 0) {
         s = __drcp_rn(s);
@@ -253,7 +258,8 @@ __global__ void make_dvec_kernel(int n, double h, const int *__restrict__ rowptr
 
 // J values of the CSR (simulation.cpp:376-383): h G_ij (1 + d_i)/2, +1 on the
 // diagonal.
-__global__ void export_j_kernel(int n, double h, const int *__restrict__ rowptr, const double *__restrict__ val,
+template <typename VT>
+__global__ void export_j_kernel(int n, double h, const int *__restrict__ rowptr, const VT *__restrict__ val,
                                 const double *__restrict__ dvec, double *__restrict__ out)
 {
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -262,21 +268,33 @@ __global__ void export_j_kernel(int n, double h, const int *__restrict__ rowptr,
     const double ci = (1.0 + dvec[gw]) * 0.5;
     const int s = rowptr[gw], e = rowptr[gw + 1];
     for (int q = s + lane; q < e; q += 32) {
-        double v = h * val[q] * ci;
+        double v = h * (double)val[q] * ci;
         out[q] = (q == s) ? v + 1.0 : v;
     }
+}
+
+int alloc_csr_values(Engine &e, long cap)
+{
+    if (e.d_col) cudaFree(e.d_col);
+    if (e.d_val) cudaFree(e.d_val);
+    if (e.d_valf) cudaFree(e.d_valf);
+    e.d_col = nullptr;
+    e.d_val = nullptr;
+    e.d_valf = nullptr;
+    if (cudaMalloc(&e.d_col, sizeof(int) * cap) != cudaSuccess) return SDDDST_ERR_NOMEM;
+    if (e.valf) {
+        if (cudaMalloc(&e.d_valf, sizeof(float) * cap) != cudaSuccess) return SDDDST_ERR_NOMEM;
+    } else {
+        if (cudaMalloc(&e.d_val, sizeof(double) * cap) != cudaSuccess) return SDDDST_ERR_NOMEM;
+    }
+    return 0;
 }
 
 static int grow_csr(Engine &e, long need)
 {
     if (need <= e.nnz_cap) return 0;
     long cap = need + need / 4 + 1024;
-    if (e.d_col) cudaFree(e.d_col);
-    if (e.d_val) cudaFree(e.d_val);
-    e.d_col = nullptr;
-    e.d_val = nullptr;
-    if (cudaMalloc(&e.d_col, sizeof(int) * cap) != cudaSuccess) return SDDDST_ERR_NOMEM;
-    if (cudaMalloc(&e.d_val, sizeof(double) * cap) != cudaSuccess) return SDDDST_ERR_NOMEM;
+    if (alloc_csr_values(e, cap)) return SDDDST_ERR_NOMEM;
     cudaMemsetAsync(e.d_col, 0, sizeof(int) * cap, e.st);
     e.nnz_cap = cap;
     return 0;
@@ -314,9 +332,14 @@ int jacobian_assemble(Engine &e, const double *x)
     }
     e.nnz = total;
     cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
-    row_fill_kernel<<<rb, 32 * wpb, 0, st>>>(n, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr,
-                                            e.d_rowptr, e.d_col, e.d_val, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR,
-                                            e.d_flag);
+    if (e.valf)
+        row_fill_kernel<float><<<rb, 32 * wpb, 0, st>>>(n, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr,
+                                                       e.one_per_cutoff_sqr, e.d_rowptr, e.d_col, e.d_valf,
+                                                       e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag);
+    else
+        row_fill_kernel<double><<<rb, 32 * wpb, 0, st>>>(n, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr,
+                                                        e.one_per_cutoff_sqr, e.d_rowptr, e.d_col, e.d_val,
+                                                        e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag);
     e.launches += 1;
     int flag = 0;
     cudaMemcpyAsync(&flag, e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -330,13 +353,16 @@ int jacobian_assemble(Engine &e, const double *x)
 
 void launch_make_dvec(const Engine &e, double h, double *dvec, cudaStream_t st)
 {
-    make_dvec_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, h, e.d_rowptr, e.d_val, dvec);
+    make_dvec_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, h, e.d_gdiag, dvec);
 }
 
 void launch_export_jacobian(const Engine &e, double h, const double *dvec, double *val_out, cudaStream_t st)
 {
     const int wpb = 8;
-    export_j_kernel<<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_rowptr, e.d_val, dvec, val_out);
+    if (e.valf)
+        export_j_kernel<float><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_rowptr, e.d_valf, dvec, val_out);
+    else
+        export_j_kernel<double><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_rowptr, e.d_val, dvec, val_out);
 }
 
 } // namespace sd

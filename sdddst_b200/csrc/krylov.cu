@@ -17,9 +17,10 @@
 
 namespace sd {
 
-// y = J v  (warp per row)
+// y = J v  (warp per row; G values FP64 or FP32, arithmetic FP64)
+template <typename VT>
 __global__ void spmv_j_kernel(int n, double h, const int *__restrict__ rowptr, const int *__restrict__ col,
-                              const double *__restrict__ val, const double *__restrict__ dvec,
+                              const VT *__restrict__ val, const double *__restrict__ dvec,
                               const double *__restrict__ v, double *__restrict__ y)
 {
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -27,17 +28,17 @@ __global__ void spmv_j_kernel(int n, double h, const int *__restrict__ rowptr, c
     if (row >= n) return;
     const int s = rowptr[row], e = rowptr[row + 1];
     double acc = 0.0;
-    for (int q = s + lane; q < e; q += 32) acc += val[q] * v[col[q]];
+    for (int q = s + lane; q < e; q += 32) acc += (double)val[q] * v[col[q]];
     acc = warp_sum(acc);
     if (lane == 0) y[row] = v[row] + (1.0 + dvec[row]) * 0.5 * h * acc;
 }
 
 // diag(J)_i = 1 + (1 + d_i)/2 h G_ii
-__global__ void jdiag_inv_kernel(int n, double h, const int *__restrict__ rowptr, const double *__restrict__ val,
-                                 const double *__restrict__ dvec, double *__restrict__ dinv)
+__global__ void jdiag_inv_kernel(int n, double h, const double *__restrict__ gdiag, const double *__restrict__ dvec,
+                                 double *__restrict__ dinv)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dinv[i] = 1.0 / (1.0 + (1.0 + dvec[i]) * 0.5 * h * val[rowptr[i]]);
+    if (i < n) dinv[i] = 1.0 / (1.0 + (1.0 + dvec[i]) * 0.5 * h * gdiag[i]);
 }
 
 __global__ void mul_kernel(int n, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ c)
@@ -253,7 +254,12 @@ int Engine::max_ratio(double *out)
 void launch_spmv_J(const Engine &e, double h, const double *dvec, const double *v, double *y, cudaStream_t st)
 {
     const int wpb = 8;
-    spmv_j_kernel<<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_rowptr, e.d_col, e.d_val, dvec, v, y);
+    if (e.valf)
+        spmv_j_kernel<float><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_rowptr, e.d_col, e.d_valf, dvec,
+                                                                         v, y);
+    else
+        spmv_j_kernel<double><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_rowptr, e.d_col, e.d_val, dvec,
+                                                                          v, y);
 }
 
 void launch_residual_g(const Engine &e, double h, const double *xn, const double *xo, const double *csp,
@@ -368,7 +374,7 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
     cudaMemsetAsync(x, 0, sizeof(double) * n, st);
     if (precond == 1) {
         dinv = e.d_y_small; // n doubles reserved for the diagonal
-        jdiag_inv_kernel<<<nb, 256, 0, st>>>(n, h, e.d_rowptr, e.d_val, dvec, dinv);
+        jdiag_inv_kernel<<<nb, 256, 0, st>>>(n, h, e.d_gdiag, dvec, dinv);
         e.launches++;
     }
     auto apply_precond = [&](const double *in, double *out) -> const double * {
@@ -385,7 +391,7 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
     };
     // beta0 = ||rhs||
     cudaMemcpyAsync(r, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
-    gs_fused_kernel<3><<<e.red_blocks, 256, 0, st>>>(n, 1, nullptr, ldv, r, nullptr, e.d_scal, e.d_partials,
+    gs_fused_kernel<3><<<e.gs_blocks, 256, 0, st>>>(n, 1, nullptr, ldv, r, nullptr, e.d_scal, e.d_partials,
                                                      e.d_counter);
     e.launches++;
     cudaMemcpyAsync(e.h_scal, e.d_scal, sizeof(double), cudaMemcpyDeviceToHost, st);
@@ -415,15 +421,14 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
             const int jend = std::min(m, j + chk);
             for (int jj = j; jj < jend; ++jj) {
                 const double *src = apply_precond(V + (size_t)jj * ldv, z);
-                spmv_j_kernel<<<(n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec,
-                                                                        src, w);
+                launch_spmv_J(e, h, dvec, src, w, st);
                 double *rec = e.d_hrec + (size_t)jj * stride;
                 const int kk = jj + 1;
-                gs_fused_kernel<0><<<e.red_blocks, 256, 0, st>>>(n, kk, V, ldv, w, nullptr, rec, e.d_partials,
+                gs_fused_kernel<0><<<e.gs_blocks, 256, 0, st>>>(n, kk, V, ldv, w, nullptr, rec, e.d_partials,
                                                                  e.d_counter);
-                gs_fused_kernel<1><<<e.red_blocks, 256, 0, st>>>(n, kk, V, ldv, w, rec, rec + (m + 1), e.d_partials,
+                gs_fused_kernel<1><<<e.gs_blocks, 256, 0, st>>>(n, kk, V, ldv, w, rec, rec + (m + 1), e.d_partials,
                                                                  e.d_counter);
-                gs_fused_kernel<2><<<e.red_blocks, 256, 0, st>>>(n, kk, V, ldv, w, rec + (m + 1), rec + 2 * (m + 1),
+                gs_fused_kernel<2><<<e.gs_blocks, 256, 0, st>>>(n, kk, V, ldv, w, rec + (m + 1), rec + 2 * (m + 1),
                                                                  e.d_partials, e.d_counter);
                 normalize_kernel<<<nb, 256, 0, st>>>(n, w, rec + 2 * (m + 1), V + (size_t)(jj + 1) * ldv);
                 e.launches += 5;
@@ -482,9 +487,9 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
         }
         if (converged || total >= max_it) break;
         // restart from the true residual
-        spmv_j_kernel<<<(n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, x, w);
+        launch_spmv_J(e, h, dvec, x, w, st);
         sub_kernel<<<nb, 256, 0, st>>>(n, rhs, w, r);
-        gs_fused_kernel<3><<<e.red_blocks, 256, 0, st>>>(n, 1, nullptr, ldv, r, nullptr, e.d_scal, e.d_partials,
+        gs_fused_kernel<3><<<e.gs_blocks, 256, 0, st>>>(n, 1, nullptr, ldv, r, nullptr, e.d_scal, e.d_partials,
                                                          e.d_counter);
         e.launches += 3;
         cudaMemcpyAsync(e.h_scal, e.d_scal, sizeof(double), cudaMemcpyDeviceToHost, st);

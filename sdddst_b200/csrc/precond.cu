@@ -25,22 +25,24 @@ namespace sd {
 
 constexpr int kMaxBlock = 32;
 
+template <typename VT>
 __global__ void strongest_kernel(int n, double h, double theta, const int *__restrict__ rowptr,
-                                 const int *__restrict__ col, const double *__restrict__ val,
-                                 const double *__restrict__ dvec, int *__restrict__ ptr)
+                                 const int *__restrict__ col, const VT *__restrict__ val,
+                                 const double *__restrict__ gdiag, const double *__restrict__ dvec,
+                                 int *__restrict__ ptr)
 {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (i >= n) return;
     const int s = rowptr[i], e = rowptr[i + 1];
-    const double mii = 2.0 / (1.0 + dvec[i]) + h * val[s];
+    const double mii = 2.0 / (1.0 + dvec[i]) + h * gdiag[i];
     double best = -1.0;
     int bj = i;
     for (int q = s + 1 + lane; q < e; q += 32) {
         const int j = col[q];
-        const double mjj = 2.0 / (1.0 + dvec[j]) + h * val[rowptr[j]];
+        const double mjj = 2.0 / (1.0 + dvec[j]) + h * gdiag[j];
         const double den = sqrt(fabs(mii) * fabs(mjj));
-        const double sij = den > 0 ? h * fabs(val[q]) / den : 0.0;
+        const double sij = den > 0 ? h * fabs((double)val[q]) / den : 0.0;
         if (sij >= theta && (sij > best || (sij == best && j < bj))) {
             best = sij;
             bj = j;
@@ -149,12 +151,14 @@ __global__ void block_meta_kernel(int nb, const int *__restrict__ bstart, const 
 
 // One warp per block: dense J block, Gauss-Jordan inverse with partial
 // pivoting, written row-major at binv[off[b]].
+template <typename VT>
 __global__ void block_invert_kernel(int nb, double h, const int *__restrict__ bstart, const int *__restrict__ blen,
                                     const int *__restrict__ members, const int *__restrict__ blk_of,
                                     const int *__restrict__ loc, const int *__restrict__ off,
                                     const int *__restrict__ rowptr, const int *__restrict__ col,
-                                    const double *__restrict__ val, const double *__restrict__ dvec,
-                                    double *__restrict__ binv, int *__restrict__ flag)
+                                    const VT *__restrict__ val, const double *__restrict__ gdiag,
+                                    const double *__restrict__ dvec, double *__restrict__ binv,
+                                    int *__restrict__ flag)
 {
     __shared__ double A[2][kMaxBlock][2 * kMaxBlock + 1];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -165,7 +169,7 @@ __global__ void block_invert_kernel(int nb, double h, const int *__restrict__ bs
     if (k == 1) {
         if (lane == 0) {
             const int i = members[s];
-            const double jii = 1.0 + (1.0 + dvec[i]) * 0.5 * h * val[rowptr[i]];
+            const double jii = 1.0 + (1.0 + dvec[i]) * 0.5 * h * gdiag[i];
             binv[off[b]] = 1.0 / jii;
         }
         return;
@@ -177,9 +181,10 @@ __global__ void block_invert_kernel(int nb, double h, const int *__restrict__ bs
     if (lane < k) {
         const int i = members[s + lane];
         const double ci = (1.0 + dvec[i]) * 0.5 * h;
-        for (int q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+        M[lane][lane] += ci * gdiag[i];
+        for (int q = rowptr[i] + 1; q < rowptr[i + 1]; ++q) {
             const int j = col[q];
-            if (blk_of[j] == b) M[lane][loc[j]] += ci * val[q];
+            if (blk_of[j] == b) M[lane][loc[j]] += ci * (double)val[q];
         }
         M[lane][lane] += 1.0;
     }
@@ -263,7 +268,12 @@ int precond_build(Engine &e, double h, const double *dvec)
     const unsigned nb256 = (unsigned)((n + 255) / 256);
     const double theta = e.prm.precond_theta > 0 ? e.prm.precond_theta : 0.1;
     int *ptr = e.pc_ptr, *par = e.pc_parent, *par2 = e.pc_tmp;
-    strongest_kernel<<<(n + 7) / 8, 256, 0, st>>>(n, h, theta, e.d_rowptr, e.d_col, e.d_val, dvec, ptr);
+    if (e.valf)
+        strongest_kernel<float><<<(n + 7) / 8, 256, 0, st>>>(n, h, theta, e.d_rowptr, e.d_col, e.d_valf, e.d_gdiag,
+                                                             dvec, ptr);
+    else
+        strongest_kernel<double><<<(n + 7) / 8, 256, 0, st>>>(n, h, theta, e.d_rowptr, e.d_col, e.d_val, e.d_gdiag,
+                                                              dvec, ptr);
     root_init_kernel<<<nb256, 256, 0, st>>>(n, ptr, par);
     for (int it = 0; it < 12; ++it) {
         jump_kernel<<<nb256, 256, 0, st>>>(n, par, par2);
@@ -303,9 +313,14 @@ int precond_build(Engine &e, double h, const double *dvec)
         e.pc_binv_cap = cap;
     }
     cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
-    block_invert_kernel<<<(nb + 1) / 2, 64, 0, st>>>(nb, h, e.pc_bstart, e.pc_blen, e.pc_members, e.pc_blk_of,
-                                                     e.pc_loc, e.pc_off, e.d_rowptr, e.d_col, e.d_val, dvec,
-                                                     e.pc_binv, e.d_flag);
+    if (e.valf)
+        block_invert_kernel<float><<<(nb + 1) / 2, 64, 0, st>>>(nb, h, e.pc_bstart, e.pc_blen, e.pc_members,
+                                                                e.pc_blk_of, e.pc_loc, e.pc_off, e.d_rowptr, e.d_col,
+                                                                e.d_valf, e.d_gdiag, dvec, e.pc_binv, e.d_flag);
+    else
+        block_invert_kernel<double><<<(nb + 1) / 2, 64, 0, st>>>(nb, h, e.pc_bstart, e.pc_blen, e.pc_members,
+                                                                 e.pc_blk_of, e.pc_loc, e.pc_off, e.d_rowptr, e.d_col,
+                                                                 e.d_val, e.d_gdiag, dvec, e.pc_binv, e.d_flag);
     e.launches += 1;
     int flag = 0;
     cudaMemcpyAsync(&flag, e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);

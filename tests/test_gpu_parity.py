@@ -197,3 +197,22 @@ def test_fp32_pairsum_accuracy(engine_lib, port_lib):
     v, _ = e.speeds(xyb)
     rel = np.abs(v - v_ref).max() / np.abs(v_ref).max()
     assert rel < 1e-5, rel
+
+
+def test_mixed_jacobian_close_to_oracle(engine_lib, port_lib):
+    """Mixed path: FP32 dtau/dx and FP32 storage of G; J within FP32
+    accuracy of the oracle's (the pattern is the same test in FP64)."""
+    from sdddst_b200 import capi
+    n, h = 600, 1e-5
+    xyb, pd, o, _ = make_pair(n, 3, 1.0, 1e-6)
+    e = capi.Engine(capi.cli_params(n, 1.0, 1e-6, pairsum=capi.PAIRSUM_FP32), xyb)
+    Ap, Ai, Ax, d = o.jacobian(h, xyb)
+    rp, col, val, dd = e.jacobian(h, xyb)
+    J = np.zeros((n, n))
+    for i in range(n):
+        for q in range(rp[i], rp[i + 1]):
+            J[i, col[q]] += val[q]
+    Jr = ref.csc_to_dense(Ap, Ai, Ax, n)
+    off = ~np.eye(n, dtype=bool)
+    assert np.abs(J - Jr)[off].max() <= 2e-5 * np.abs(Jr[off]).max()
+    assert np.abs(np.diag(J) - np.diag(Jr)).max() <= 2e-5 * np.abs(np.diag(Jr)).max()
