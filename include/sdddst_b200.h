@@ -133,6 +133,32 @@ int sdddst_get_vector(void *ctx, int which, double *out);
  * sim_time for that step type). */
 int sdddst_speeds(void *ctx, const double *xyb, double sim_time, int stress_type, double *v, double *tol);
 
+/* calculateSpeeds with an explicit external stress: v[N] = pair sum + point
+ * defects + b tau_ext on the given configuration, and minr2[N], the
+ * smallest distance measure each dislocation saw (r^2 to dislocations,
+ * X2(dx)+X2(dy) to point defects) among those below 400 prec^2 (+inf
+ * otherwise) -- the argument the reference passes to
+ * PrecisionHandler::updateTolerance (precision_handler.cpp:72-87). */
+int sdddst_speeds_ext(void *ctx, const double *xyb, double tau_ext, double *v, double *minr2);
+
+/* Replaces the step state scalars without touching the configuration:
+ * SimulationData::stepSize, simTime, totalAccumulatedStrainIncrease and the
+ * Simulation's accumulated energy. */
+int sdddst_set_scalars(void *ctx, double step_size, double sim_time, double energy, double strain);
+
+/* Updates the mutable parameters of a live context from prm (cutoff
+ * multiplier with SimulationData::updateCutOff, precision, max step size,
+ * stress protocol parameters, solver settings); sizes and the field kind
+ * must be unchanged. */
+int sdddst_update_params(void *ctx, const sdddst_params *prm);
+
+/* Solves A x = b for a general N x N matrix given in CSC (Ap[N+1], Ai, Ax:
+ * UMFPACK's layout, as the reference's solveEQSys passes it,
+ * simulation.cpp:393-396) with the context's device solver.  The context's
+ * assembled Jacobian is replaced (the next step reassembles). */
+int sdddst_solve_csc(void *ctx, const int *Ap, const int *Ai, const double *Ax, const double *b, double *x,
+                     int *iterations);
+
 /* Simulation::calculateJacobian (simulation.cpp:236-384) at step size h on a
  * given configuration, returned as CSR of J (row i = dislocation i; the
  * reference's CSC column j is row j of J^T).  row_ptr[N+1], col[cap],

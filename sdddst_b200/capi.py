@@ -34,7 +34,8 @@ EXPORTS = [
     "sdddst_speeds", "sdddst_jacobian", "sdddst_solve", "sdddst_step", "sdddst_run",
     "sdddst_state_device", "sdddst_kernel_launches", "sdddst_upload_positions",
     "sdddst_download_positions", "sdddst_stream", "sdddst_vector_peaks", "sdddst_profile_pair_sum",
-    "sdddst_speeds_noalloc", "sdddst_solver_stats",
+    "sdddst_speeds_noalloc", "sdddst_solver_stats", "sdddst_speeds_ext", "sdddst_set_scalars",
+    "sdddst_update_params", "sdddst_solve_csc",
 ]
 
 
@@ -91,6 +92,10 @@ def load(path: str = LIB_PATH):
     lib.sdddst_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     lib.sdddst_speeds_noalloc.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
                                           C.c_void_p]
+    lib.sdddst_speeds_ext.argtypes = [C.c_void_p, _D, C.c_double, _D, _D]
+    lib.sdddst_set_scalars.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double]
+    lib.sdddst_update_params.argtypes = [C.c_void_p, C.POINTER(Params)]
+    lib.sdddst_solve_csc.argtypes = [C.c_void_p, _I, _I, _D, _D, _D, C.POINTER(C.c_int)]
     lib.sdddst_solver_stats.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long)]
     lib.sdddst_profile_pair_sum.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
     lib.sdddst_vector_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -223,6 +228,22 @@ class Engine:
         x = np.zeros(self.n)
         it = C.c_int(0)
         _check(self.lib.sdddst_solve(self.h, float(h), a, r, x, C.byref(it)))
+        return x, it.value
+
+    def speeds_ext(self, xyb, tau_ext=0.0):
+        a = np.ascontiguousarray(xyb, dtype=np.float64).reshape(-1)
+        v = np.zeros(self.n)
+        m = np.zeros(self.n)
+        _check(self.lib.sdddst_speeds_ext(self.h, a, float(tau_ext), v, m))
+        return v, m
+
+    def solve_csc(self, Ap, Ai, Ax, b):
+        x = np.zeros(self.n)
+        it = C.c_int(0)
+        _check(self.lib.sdddst_solve_csc(self.h, np.ascontiguousarray(Ap, dtype=np.int32),
+                                         np.ascontiguousarray(Ai, dtype=np.int32),
+                                         np.ascontiguousarray(Ax, dtype=np.float64),
+                                         np.ascontiguousarray(b, dtype=np.float64), x, C.byref(it)))
         return x, it.value
 
     def step(self) -> bool:

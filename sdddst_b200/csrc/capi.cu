@@ -3,6 +3,7 @@
 // codes with a per-thread message.
 #include "engine.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -203,6 +204,144 @@ int sdddst_speeds(void *ctx, const double *xyb, double sim_time, int stress_type
         cudaMemcpyAsync(tol, e->d_tol, sizeof(double) * e->n, cudaMemcpyDeviceToHost, e->st);
         cudaMemcpyAsync(e->d_tol, e->d_tol_last, sizeof(double) * e->n, cudaMemcpyDeviceToDevice, e->st);
         return from_engine(e, e->sync_check("speeds"));
+    } catch (const std::exception &ex) {
+        return fail(SDDDST_ERR_NOMEM, ex.what());
+    }
+}
+
+int sdddst_speeds_ext(void *ctx, const double *xyb, double tau_ext, double *v, double *minr2)
+{
+    if (!ctx || !xyb || !v) return fail(SDDDST_ERR_INVALID, "bad argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    try {
+        ScratchConfig sc(e, xyb);
+        const double r2_track = 400.0 * e->prec * e->prec * (1.0 + 1e-9);
+        sd::launch_pair_sum(*e, e->d_xs, e->st, e->prm.pairsum, r2_track);
+        e->d_minr2_out = e->d_z;
+        sd::launch_speeds_finish(*e, e->d_xs, tau_ext, nullptr, e->d_Stmp, 0, e->st);
+        e->d_minr2_out = nullptr;
+        e->launches += e->prm.pairsum == SDDDST_PAIRSUM_FP32 ? 4 : 3;
+        cudaMemcpyAsync(v, e->d_Stmp, sizeof(double) * e->n, cudaMemcpyDeviceToHost, e->st);
+        if (minr2) cudaMemcpyAsync(minr2, e->d_z, sizeof(double) * e->n, cudaMemcpyDeviceToHost, e->st);
+        return from_engine(e, e->sync_check("speeds_ext"));
+    } catch (const std::exception &ex) {
+        return fail(SDDDST_ERR_NOMEM, ex.what());
+    }
+}
+
+int sdddst_set_scalars(void *ctx, double step_size, double sim_time, double energy, double strain)
+{
+    if (!ctx) return fail(SDDDST_ERR_INVALID, "null argument");
+    if (!(step_size > 0)) return fail(SDDDST_ERR_INVALID, "step size must be positive");
+    sd::Engine *e = E(ctx);
+    e->step_size = step_size;
+    e->sim_time = sim_time;
+    e->energy = energy;
+    e->strain = strain;
+    return SDDDST_OK;
+}
+
+int sdddst_update_params(void *ctx, const sdddst_params *prm)
+{
+    if (!ctx || !prm) return fail(SDDDST_ERR_INVALID, "null argument");
+    sd::Engine *e = E(ctx);
+    if (prm->n != e->n || prm->p != e->p || prm->field != e->prm.field || prm->pairsum != e->prm.pairsum)
+        return fail(SDDDST_ERR_INVALID, "sizes, field and pair-sum mode cannot change on a live context");
+    if (!(prm->prec > 0) || !(prm->cutoff_multiplier > 0)) return fail(SDDDST_ERR_INVALID, "bad parameter");
+    cudaSetDevice(e->device);
+    const int restart_alloc = e->restart;
+    e->prm.cutoff_multiplier = prm->cutoff_multiplier;
+    e->prm.prec = prm->prec;
+    e->prm.max_step_limited = prm->max_step_limited;
+    e->prm.max_step = prm->max_step;
+    e->prm.stress_kind = prm->stress_kind;
+    e->prm.stress_rate = prm->stress_rate;
+    e->prm.spring_constant = prm->spring_constant;
+    e->prm.stress_value = prm->stress_value;
+    e->prm.calculate_strain = prm->calculate_strain;
+    e->prm.solver = prm->solver;
+    e->prm.solver_tol = prm->solver_tol;
+    e->prm.max_iters = prm->max_iters;
+    e->prm.precond_theta = prm->precond_theta;
+    e->prm.gmres_restart = prm->gmres_restart < 2 ? restart_alloc : std::min(prm->gmres_restart, restart_alloc);
+    e->restart = e->prm.gmres_restart;
+    e->prec = prm->prec;
+    e->cutoff_multiplier = prm->cutoff_multiplier;
+    e->update_cutoff();
+    const int ncell = e->G * e->G;
+    if (ncell > e->ncell_alloc) {
+        int **arrs[] = {&e->d_cell_count, &e->d_cell_start, &e->d_cell_fill};
+        for (int **a : arrs) {
+            cudaFree(*a);
+            *a = nullptr;
+            if (cudaMalloc(a, sizeof(int) * (ncell + 1)) != cudaSuccess) return fail(SDDDST_ERR_NOMEM, "cell arrays");
+        }
+        e->ncell_alloc = ncell;
+    }
+    return SDDDST_OK;
+}
+
+int sdddst_solve_csc(void *ctx, const int *Ap, const int *Ai, const double *Ax, const double *b, double *x,
+                     int *iterations)
+{
+    if (!ctx || !Ap || !Ai || !Ax || !b || !x) return fail(SDDDST_ERR_INVALID, "null argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    const int n = e->n;
+    try {
+        // CSC of A -> CSR rows of G = A - I with the diagonal in each row's first slot
+        std::vector<int> cnt(n + 1, 1);
+        for (int j = 0; j < n; ++j)
+            for (int q = Ap[j]; q < Ap[j + 1]; ++q) {
+                int i = Ai[q];
+                if (i < 0 || i >= n) return fail(SDDDST_ERR_INVALID, "row index out of range");
+                if (i != j) cnt[i]++;
+            }
+        std::vector<int> rp(n + 1, 0);
+        for (int i = 0; i < n; ++i) rp[i + 1] = rp[i] + cnt[i];
+        const long nnz = rp[n];
+        std::vector<int> cl(nnz), fill(n);
+        std::vector<double> vl(nnz, 0.0), gd(n, -1.0), ones(n, 1.0);
+        for (int i = 0; i < n; ++i) {
+            fill[i] = rp[i] + 1;
+            cl[rp[i]] = i;
+        }
+        for (int j = 0; j < n; ++j)
+            for (int q = Ap[j]; q < Ap[j + 1]; ++q) {
+                int i = Ai[q];
+                if (i == j) gd[i] += Ax[q];
+                else {
+                    cl[fill[i]] = j;
+                    vl[fill[i]++] = Ax[q];
+                }
+            }
+        for (int i = 0; i < n; ++i) vl[rp[i]] = gd[i];
+        if (nnz > e->nnz_cap) {
+            if (sd::alloc_csr_values(*e, nnz + nnz / 4)) return fail(SDDDST_ERR_NOMEM, "CSR allocation");
+            e->nnz_cap = nnz + nnz / 4;
+        }
+        e->nnz = nnz;
+        cudaMemcpyAsync(e->d_rowptr, rp.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, e->st);
+        cudaMemcpyAsync(e->d_col, cl.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, e->st);
+        std::vector<float> vf;
+        if (e->valf) {
+            vf.assign(vl.begin(), vl.end());
+            cudaMemcpyAsync(e->d_valf, vf.data(), sizeof(float) * nnz, cudaMemcpyHostToDevice, e->st);
+        } else {
+            cudaMemcpyAsync(e->d_val, vl.data(), sizeof(double) * nnz, cudaMemcpyHostToDevice, e->st);
+        }
+        cudaMemcpyAsync(e->d_gdiag, gd.data(), sizeof(double) * n, cudaMemcpyHostToDevice, e->st);
+        cudaMemcpyAsync(e->d_dvec, ones.data(), sizeof(double) * n, cudaMemcpyHostToDevice, e->st);
+        cudaMemcpyAsync(e->d_g, b, sizeof(double) * n, cudaMemcpyHostToDevice, e->st);
+        if (int rc = e->sync_check("solve_csc upload")) return from_engine(e, rc);
+        // J(h=1, d=1) = I + (1+1)/2 * 1 * (A - I) = A
+        if (int rc = e->prepare_solver(1.0)) return from_engine(e, rc);
+        int rc = e->solve(1.0, e->d_g, e->d_sol);
+        if (iterations) *iterations = e->last_iters;
+        if (rc) return from_engine(e, rc);
+        cudaMemcpyAsync(x, e->d_sol, sizeof(double) * n, cudaMemcpyDeviceToHost, e->st);
+        return from_engine(e, e->sync_check("solve_csc"));
     } catch (const std::exception &ex) {
         return fail(SDDDST_ERR_NOMEM, ex.what());
     }

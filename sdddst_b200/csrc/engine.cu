@@ -125,6 +125,7 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     rc |= dalloc(&d_pdx, p);
     rc |= dalloc(&d_pdy, p);
     const int ncell = G * G;
+    ncell_alloc = ncell;
     rc |= dalloc(&d_cell, n);
     rc |= dalloc(&d_cell_count, ncell + 1);
     rc |= dalloc(&d_cell_start, ncell + 1);

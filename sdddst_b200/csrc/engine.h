@@ -35,9 +35,11 @@ struct Engine {
     double *d_pdx = nullptr, *d_pdy = nullptr;
     double *d_ys = nullptr, *d_bs = nullptr; // scratch y, b of caller-supplied configurations
     double *d_xw = nullptr;                  // positions wrapped into [-0.5, 0.5) (mixed pair sum)
+    double *d_minr2_out = nullptr;           // optional per-dislocation min distance output
 
     // ---- cell list of the cutoff-neighbour search
     int G = 1; // cells per axis
+    int ncell_alloc = 0; // cell arrays hold ncell_alloc + 1 entries
     int *d_cell = nullptr, *d_cell_count = nullptr, *d_cell_start = nullptr, *d_cell_fill = nullptr;
     int *d_sorted = nullptr;
 

@@ -214,7 +214,7 @@ __global__ void speeds_finish_kernel(int n, int nblk, const double *__restrict__
                                      const double *__restrict__ pdx, const double *__restrict__ pdy, double A,
                                      double K, double tau_ext, double *__restrict__ S, double *__restrict__ v,
                                      const unsigned long long *__restrict__ minr2, double *__restrict__ tol,
-                                     double prec_sqr, int update_tol)
+                                     double prec_sqr, int update_tol, double *__restrict__ minr2_out)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -232,6 +232,7 @@ __global__ void speeds_finish_kernel(int n, int nblk, const double *__restrict__
     }
     if (S) S[i] = acc;
     v[i] = acc + bi * tau_ext;
+    if (minr2_out) minr2_out[i] = smin;
     if (update_tol) {
         double t = __dmul_rn(__dmul_rn(smin, 0.25), 1e-2); // precision_handler.cpp:74
         double cur = tol[i];
@@ -284,7 +285,7 @@ void launch_speeds_finish(const Engine &e, const double *x, double tau_ext, doub
     const int nblk = (n + T - 1) / T;
     speeds_finish_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, nblk, e.d_part, x, e.d_y, e.d_b, e.p, e.d_pdx, e.d_pdy,
                                                          e.A, e.KASQR, tau_ext, S, v, e.d_minr2, e.d_tol,
-                                                         e.prec * e.prec, update_tol);
+                                                         e.prec * e.prec, update_tol, e.d_minr2_out);
 }
 
 void launch_add_stress(const Engine &e, const double *S, double tau_ext, double *v, cudaStream_t st)
@@ -306,7 +307,7 @@ void launch_speeds_raw(int n, const double *x, const double *y, const double *b,
     else
         pair_tiles_kernel<64, 0><<<(unsigned)tiles, 64, 0, st>>>(x, y, b, n, nblk, part, nullptr, 0.0);
     speeds_finish_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, nblk, part, x, y, b, 0, nullptr, nullptr, 0.0, 0.0,
-                                                         tau_ext, nullptr, v, nullptr, nullptr, 0.0, 0);
+                                                         tau_ext, nullptr, v, nullptr, nullptr, 0.0, 0, nullptr);
 }
 
 size_t pair_part_doubles(int n)
