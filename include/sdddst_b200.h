@@ -235,6 +235,29 @@ int sdddst_speeds_noalloc(int n, const double *x_device, const double *y_device,
  * total Krylov iterations. */
 int sdddst_solver_stats(void *ctx, long *solves, long *iterations);
 
+/* ---- Batches of independent systems (a population of random realisations).
+ * `count` systems of sizes[k] dislocations, concatenated in xyb (sum of sizes
+ * rows of {x, y, b}), share the parameters of `common` (n, p and the stress
+ * protocol are ignored: every system has no point defects and zero external
+ * stress).  Each system keeps its own cutoff (multiplier / sqrt(N_k)), step
+ * size, time, energy and counters and accepts or rejects its own steps
+ * (Simulation::step, simulation.cpp:435-650, per system); every phase of a
+ * step is one launch over all systems. */
+int sdddst_batch_create(const sdddst_params *common, int count, const int *sizes, const double *xyb, void **batch);
+int sdddst_batch_destroy(void *batch);
+/* One step attempt of every system; accepted[k] (optional, count ints)
+ * receives 1 where system k accepted. */
+int sdddst_batch_step(void *batch, int *accepted);
+/* count x 12 scalars, the layout of sdddst_get_scalars (entries without a
+ * batched counterpart are 0). */
+int sdddst_batch_get_scalars(void *batch, double *out);
+/* x coordinates of all systems (which: 0 accepted, 1 big step, 2 first small
+ * step, 3 second small step), sum of sizes doubles. */
+int sdddst_batch_get_positions(void *batch, int which, double *x);
+/* Pair-sum tile chosen by the autotuner, total dislocations, kernels launched
+ * so far and the batch's cudaStream_t (each pointer optional). */
+int sdddst_batch_info(void *batch, int *tile, long *total, long *launches, void **stream);
+
 /* Launch statistics: number of kernels this context has launched so far. */
 long sdddst_kernel_launches(void *ctx);
 

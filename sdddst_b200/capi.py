@@ -35,7 +35,8 @@ EXPORTS = [
     "sdddst_state_device", "sdddst_kernel_launches", "sdddst_upload_positions",
     "sdddst_download_positions", "sdddst_stream", "sdddst_vector_peaks", "sdddst_profile_pair_sum",
     "sdddst_speeds_noalloc", "sdddst_solver_stats", "sdddst_speeds_ext", "sdddst_set_scalars",
-    "sdddst_update_params", "sdddst_solve_csc",
+    "sdddst_update_params", "sdddst_solve_csc", "sdddst_batch_create", "sdddst_batch_destroy",
+    "sdddst_batch_step", "sdddst_batch_get_scalars", "sdddst_batch_get_positions", "sdddst_batch_info",
 ]
 
 
@@ -96,6 +97,13 @@ def load(path: str = LIB_PATH):
     lib.sdddst_set_scalars.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double]
     lib.sdddst_update_params.argtypes = [C.c_void_p, C.POINTER(Params)]
     lib.sdddst_solve_csc.argtypes = [C.c_void_p, _I, _I, _D, _D, _D, C.POINTER(C.c_int)]
+    lib.sdddst_batch_create.argtypes = [C.POINTER(Params), C.c_int, _I, _D, C.POINTER(C.c_void_p)]
+    lib.sdddst_batch_destroy.argtypes = [C.c_void_p]
+    lib.sdddst_batch_step.argtypes = [C.c_void_p, _I]
+    lib.sdddst_batch_get_scalars.argtypes = [C.c_void_p, _D]
+    lib.sdddst_batch_get_positions.argtypes = [C.c_void_p, C.c_int, _D]
+    lib.sdddst_batch_info.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_long), C.POINTER(C.c_long),
+                                      C.POINTER(C.c_void_p)]
     lib.sdddst_solver_stats.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long)]
     lib.sdddst_profile_pair_sum.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
     lib.sdddst_vector_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -283,3 +291,49 @@ class Engine:
 
     def launches(self) -> int:
         return int(self.lib.sdddst_kernel_launches(self.h))
+
+
+class Batch:
+    """Independent systems of uneven size stepped together on one GPU."""
+
+    def __init__(self, prm: Params, systems):
+        lib = load()
+        self.lib = lib
+        self.sizes = np.array([len(s) for s in systems], dtype=np.int32)
+        self.count = len(systems)
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)])
+        xyb = np.ascontiguousarray(np.concatenate([np.asarray(s, dtype=np.float64) for s in systems]).reshape(-1))
+        h = C.c_void_p()
+        _check(lib.sdddst_batch_create(C.byref(prm), self.count, self.sizes, xyb, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.sdddst_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self) -> np.ndarray:
+        acc = np.zeros(self.count, dtype=np.int32)
+        _check(self.lib.sdddst_batch_step(self.h, acc))
+        return acc.astype(bool)
+
+    def scalars(self) -> np.ndarray:
+        out = np.zeros(12 * self.count)
+        _check(self.lib.sdddst_batch_get_scalars(self.h, out))
+        return out.reshape(self.count, 12)
+
+    def positions(self, which: int = 0):
+        x = np.zeros(int(self.offsets[-1]))
+        _check(self.lib.sdddst_batch_get_positions(self.h, which, x))
+        return [x[self.offsets[k]:self.offsets[k + 1]] for k in range(self.count)]
+
+    def info(self):
+        t, n, l, s = C.c_int(0), C.c_long(0), C.c_long(0), C.c_void_p()
+        _check(self.lib.sdddst_batch_info(self.h, C.byref(t), C.byref(n), C.byref(l), C.byref(s)))
+        return {"tile": t.value, "total": n.value, "launches": l.value, "stream": s.value or 0}

@@ -58,6 +58,10 @@ struct ScratchConfig {
 
 } // namespace
 
+namespace sd {
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+} // namespace sd
+
 extern "C" {
 
 void sdddst_default_params(sdddst_params *p)

@@ -121,7 +121,7 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
                        &d_r, &d_ys, &d_bs, &d_xw, &d_gdiag};
     for (double **v : vecs) rc |= dalloc(v, n);
     rc |= dalloc(&d_minr2, n);
-    rc |= dalloc(&d_part, pair_part_doubles(n));
+    rc |= dalloc(&d_part, batch_backend ? 1 : pair_part_doubles(n));
     rc |= dalloc(&d_pdx, p);
     rc |= dalloc(&d_pdy, p);
     const int ncell = G * G;

@@ -49,6 +49,7 @@ struct Engine {
     float *d_valf = nullptr;   // FP32 values (mixed path)
     bool valf = false;         // which of the two holds G
     double *d_gdiag = nullptr; // G_ii in FP64 (both paths)
+    double *d_hrow = nullptr;  // per-row step size of a batch of systems (null: one system, scalar h)
     long nnz_cap = 0, nnz = 0;
     int *d_flag = nullptr; // device-side error flag of the assembly
     bool assembled_valid = false;
@@ -87,6 +88,7 @@ struct Engine {
 
     long launches = 0;
     std::string err;
+    bool batch_backend = false; // buffers for a batch of systems (batch.cu allocates its own pair-sum slabs)
 
     ~Engine();
     int init(const sdddst_params &prm, const double *xyb, const double *pd);
@@ -138,6 +140,7 @@ void launch_residual_g(const Engine &e, double h, const double *xn, const double
 void launch_axpy_update(const Engine &e, double *xn, const double *sol, cudaStream_t st);
 
 int reduce_sum(Engine &e, const double *a, const double *b, int n, int op, double *out);
+void set_last_error(const std::string &msg);
 
 int precond_alloc(Engine &e);
 void precond_free(Engine &e);

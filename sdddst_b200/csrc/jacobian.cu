@@ -241,11 +241,12 @@ __global__ void row_fill_kernel(int n, const double *__restrict__ x, const doubl
 }
 
 // d_i = (s / (1 + s))^2 for s = h G_ii > 0 (simulation.cpp:349-374).
-__global__ void make_dvec_kernel(int n, double h, const double *__restrict__ gdiag, double *__restrict__ dvec)
+__global__ void make_dvec_kernel(int n, double h, const double *__restrict__ hrow, const double *__restrict__ gdiag,
+                                 double *__restrict__ dvec)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double s = __dmul_rn(h, gdiag[i]);
+    double s = __dmul_rn(hrow ? hrow[i] : h, gdiag[i]);
     double d = 0.0;
     if (s > 0) {
         s = __drcp_rn(s);
@@ -353,7 +354,7 @@ int jacobian_assemble(Engine &e, const double *x)
 
 void launch_make_dvec(const Engine &e, double h, double *dvec, cudaStream_t st)
 {
-    make_dvec_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, h, e.d_gdiag, dvec);
+    make_dvec_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, h, e.d_hrow, e.d_gdiag, dvec);
 }
 
 void launch_export_jacobian(const Engine &e, double h, const double *dvec, double *val_out, cudaStream_t st)

@@ -18,10 +18,11 @@
 namespace sd {
 
 // y = J v  (warp per row; G values FP64 or FP32, arithmetic FP64)
+// hrow (optional): per-row step size, for block-diagonal batches of systems
 template <typename VT>
-__global__ void spmv_j_kernel(int n, double h, const int *__restrict__ rowptr, const int *__restrict__ col,
-                              const VT *__restrict__ val, const double *__restrict__ dvec,
-                              const double *__restrict__ v, double *__restrict__ y)
+__global__ void spmv_j_kernel(int n, double h, const double *__restrict__ hrow, const int *__restrict__ rowptr,
+                              const int *__restrict__ col, const VT *__restrict__ val,
+                              const double *__restrict__ dvec, const double *__restrict__ v, double *__restrict__ y)
 {
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -30,15 +31,16 @@ __global__ void spmv_j_kernel(int n, double h, const int *__restrict__ rowptr, c
     double acc = 0.0;
     for (int q = s + lane; q < e; q += 32) acc += (double)val[q] * v[col[q]];
     acc = warp_sum(acc);
-    if (lane == 0) y[row] = v[row] + (1.0 + dvec[row]) * 0.5 * h * acc;
+    const double hh = hrow ? hrow[row] : h;
+    if (lane == 0) y[row] = v[row] + (1.0 + dvec[row]) * 0.5 * hh * acc;
 }
 
 // diag(J)_i = 1 + (1 + d_i)/2 h G_ii
-__global__ void jdiag_inv_kernel(int n, double h, const double *__restrict__ gdiag, const double *__restrict__ dvec,
-                                 double *__restrict__ dinv)
+__global__ void jdiag_inv_kernel(int n, double h, const double *__restrict__ hrow, const double *__restrict__ gdiag,
+                                 const double *__restrict__ dvec, double *__restrict__ dinv)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dinv[i] = 1.0 / (1.0 + (1.0 + dvec[i]) * 0.5 * h * gdiag[i]);
+    if (i < n) dinv[i] = 1.0 / (1.0 + (1.0 + dvec[i]) * 0.5 * (hrow ? hrow[i] : h) * gdiag[i]);
 }
 
 __global__ void mul_kernel(int n, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ c)
@@ -132,12 +134,14 @@ __global__ void combine_kernel(int n, int kk, const double *__restrict__ V, size
 }
 
 // g_i = x_new - (1+d)/2 h v_new - x_old - (1-d)/2 h v_old (simulation.cpp:189-192)
-__global__ void residual_g_kernel(int n, double h, const double *__restrict__ xn, const double *__restrict__ xo,
-                                  const double *__restrict__ csp, const double *__restrict__ isp,
-                                  const double *__restrict__ dvec, double *__restrict__ g)
+__global__ void residual_g_kernel(int n, double h0, const double *__restrict__ hrow, const double *__restrict__ xn,
+                                  const double *__restrict__ xo, const double *__restrict__ csp,
+                                  const double *__restrict__ isp, const double *__restrict__ dvec,
+                                  double *__restrict__ g)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const double h = hrow ? hrow[i] : h0;
     const double d = dvec[i];
     const double a = __dmul_rn(__dmul_rn(__dmul_rn(__dadd_rn(1.0, d), 0.5), h), csp[i]);
     const double c = __dmul_rn(__dmul_rn(__dmul_rn(__dsub_rn(1.0, d), 0.5), h), isp[i]);
@@ -255,17 +259,17 @@ void launch_spmv_J(const Engine &e, double h, const double *dvec, const double *
 {
     const int wpb = 8;
     if (e.valf)
-        spmv_j_kernel<float><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_rowptr, e.d_col, e.d_valf, dvec,
-                                                                         v, y);
+        spmv_j_kernel<float><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_hrow, e.d_rowptr, e.d_col,
+                                                                         e.d_valf, dvec, v, y);
     else
-        spmv_j_kernel<double><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_rowptr, e.d_col, e.d_val, dvec,
-                                                                          v, y);
+        spmv_j_kernel<double><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_hrow, e.d_rowptr, e.d_col,
+                                                                          e.d_val, dvec, v, y);
 }
 
 void launch_residual_g(const Engine &e, double h, const double *xn, const double *xo, const double *csp,
                        const double *isp, const double *dvec, double *g, cudaStream_t st)
 {
-    residual_g_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, h, xn, xo, csp, isp, dvec, g);
+    residual_g_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, h, e.d_hrow, xn, xo, csp, isp, dvec, g);
 }
 
 void launch_axpy_update(const Engine &e, double *xn, const double *sol, cudaStream_t st)
@@ -374,7 +378,7 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
     cudaMemsetAsync(x, 0, sizeof(double) * n, st);
     if (precond == 1) {
         dinv = e.d_y_small; // n doubles reserved for the diagonal
-        jdiag_inv_kernel<<<nb, 256, 0, st>>>(n, h, e.d_gdiag, dvec, dinv);
+        jdiag_inv_kernel<<<nb, 256, 0, st>>>(n, h, e.d_hrow, e.d_gdiag, dvec, dinv);
         e.launches++;
     }
     auto apply_precond = [&](const double *in, double *out) -> const double * {

@@ -26,14 +26,15 @@ namespace sd {
 constexpr int kMaxBlock = 32;
 
 template <typename VT>
-__global__ void strongest_kernel(int n, double h, double theta, const int *__restrict__ rowptr,
-                                 const int *__restrict__ col, const VT *__restrict__ val,
-                                 const double *__restrict__ gdiag, const double *__restrict__ dvec,
-                                 int *__restrict__ ptr)
+__global__ void strongest_kernel(int n, double h0, const double *__restrict__ hrow, double theta,
+                                 const int *__restrict__ rowptr, const int *__restrict__ col,
+                                 const VT *__restrict__ val, const double *__restrict__ gdiag,
+                                 const double *__restrict__ dvec, int *__restrict__ ptr)
 {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (i >= n) return;
+    const double h = hrow ? hrow[i] : h0; // couplings never cross systems, so row i's h serves the pair
     const int s = rowptr[i], e = rowptr[i + 1];
     const double mii = 2.0 / (1.0 + dvec[i]) + h * gdiag[i];
     double best = -1.0;
@@ -152,7 +153,8 @@ __global__ void block_meta_kernel(int nb, const int *__restrict__ bstart, const 
 // One warp per block: dense J block, Gauss-Jordan inverse with partial
 // pivoting, written row-major at binv[off[b]].
 template <typename VT>
-__global__ void block_invert_kernel(int nb, double h, const int *__restrict__ bstart, const int *__restrict__ blen,
+__global__ void block_invert_kernel(int nb, double h0, const double *__restrict__ hrow, const int *__restrict__ bstart,
+                                    const int *__restrict__ blen,
                                     const int *__restrict__ members, const int *__restrict__ blk_of,
                                     const int *__restrict__ loc, const int *__restrict__ off,
                                     const int *__restrict__ rowptr, const int *__restrict__ col,
@@ -166,6 +168,7 @@ __global__ void block_invert_kernel(int nb, double h, const int *__restrict__ bs
     if (b >= nb) return;
     const int k = blen[b], s = bstart[b];
     double(*M)[2 * kMaxBlock + 1] = A[wib];
+    const double h = hrow ? hrow[members[s]] : h0; // a block lies inside one system
     if (k == 1) {
         if (lane == 0) {
             const int i = members[s];
@@ -269,11 +272,11 @@ int precond_build(Engine &e, double h, const double *dvec)
     const double theta = e.prm.precond_theta > 0 ? e.prm.precond_theta : 0.1;
     int *ptr = e.pc_ptr, *par = e.pc_parent, *par2 = e.pc_tmp;
     if (e.valf)
-        strongest_kernel<float><<<(n + 7) / 8, 256, 0, st>>>(n, h, theta, e.d_rowptr, e.d_col, e.d_valf, e.d_gdiag,
-                                                             dvec, ptr);
+        strongest_kernel<float><<<(n + 7) / 8, 256, 0, st>>>(n, h, e.d_hrow, theta, e.d_rowptr, e.d_col, e.d_valf,
+                                                             e.d_gdiag, dvec, ptr);
     else
-        strongest_kernel<double><<<(n + 7) / 8, 256, 0, st>>>(n, h, theta, e.d_rowptr, e.d_col, e.d_val, e.d_gdiag,
-                                                              dvec, ptr);
+        strongest_kernel<double><<<(n + 7) / 8, 256, 0, st>>>(n, h, e.d_hrow, theta, e.d_rowptr, e.d_col, e.d_val,
+                                                              e.d_gdiag, dvec, ptr);
     root_init_kernel<<<nb256, 256, 0, st>>>(n, ptr, par);
     for (int it = 0; it < 12; ++it) {
         jump_kernel<<<nb256, 256, 0, st>>>(n, par, par2);
@@ -314,11 +317,11 @@ int precond_build(Engine &e, double h, const double *dvec)
     }
     cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
     if (e.valf)
-        block_invert_kernel<float><<<(nb + 1) / 2, 64, 0, st>>>(nb, h, e.pc_bstart, e.pc_blen, e.pc_members,
+        block_invert_kernel<float><<<(nb + 1) / 2, 64, 0, st>>>(nb, h, e.d_hrow, e.pc_bstart, e.pc_blen, e.pc_members,
                                                                 e.pc_blk_of, e.pc_loc, e.pc_off, e.d_rowptr, e.d_col,
                                                                 e.d_valf, e.d_gdiag, dvec, e.pc_binv, e.d_flag);
     else
-        block_invert_kernel<double><<<(nb + 1) / 2, 64, 0, st>>>(nb, h, e.pc_bstart, e.pc_blen, e.pc_members,
+        block_invert_kernel<double><<<(nb + 1) / 2, 64, 0, st>>>(nb, h, e.d_hrow, e.pc_bstart, e.pc_blen, e.pc_members,
                                                                  e.pc_blk_of, e.pc_loc, e.pc_off, e.d_rowptr, e.d_col,
                                                                  e.d_val, e.d_gdiag, dvec, e.pc_binv, e.d_flag);
     e.launches += 1;
