@@ -91,7 +91,9 @@ typedef struct {
 
 /* Defaults of SimulationData() (simulation_data.cpp:43-109, constants.h):
  * cutoff multiplier 1, prec 1e-8, step 1, A = 1.6e-3, KASQR = 1.65^2*1e6/256,
- * ic = 2, zero stress, FP64 pair sum, cluster-preconditioned GMRES to 1e-13. */
+ * ic = 2, zero stress, FP64 pair sum, cluster-preconditioned GMRES (coupling
+ * threshold 0.05, at most 300 iterations, then retried with a rebuilt
+ * preconditioner) to 1e-13. */
 void sdddst_default_params(sdddst_params *prm);
 
 /* Creates a context and uploads the configuration.  Replaces constructing

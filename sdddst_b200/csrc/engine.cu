@@ -237,10 +237,31 @@ int Engine::assemble(const double *x)
     return rc;
 }
 
+// On a stall (no convergence within the iteration cap) the cluster
+// preconditioner is rebuilt with a five times lower coupling threshold --
+// larger clusters, more of the stiff couplings inverted exactly -- and the
+// solve repeated, at most twice; the threshold returns to its setting for the
+// next matrix.
 int Engine::solve(double h, const double *rhs, double *x_out)
 {
     int precond = prm.solver == SDDDST_SOLVER_GMRES_JACOBI ? 1 : prm.solver == SDDDST_SOLVER_GMRES_CLUSTER ? 2 : 0;
-    return gmres_solve(*this, h, d_dvec, rhs, x_out, precond);
+    int rc = gmres_solve(*this, h, d_dvec, rhs, x_out, precond);
+    if (rc != SDDDST_ERR_SOLVER || precond != 2) return rc;
+    const double theta0 = prm.precond_theta;
+    for (int attempt = 0; attempt < 2 && rc == SDDDST_ERR_SOLVER; ++attempt) {
+        prm.precond_theta = (prm.precond_theta > 0 ? prm.precond_theta : 0.05) / 5.0;
+        stalls++;
+        if (int rc2 = precond_build(*this, h, d_dvec)) {
+            prm.precond_theta = theta0;
+            return rc2;
+        }
+        rc = gmres_solve(*this, h, d_dvec, rhs, x_out, precond);
+    }
+    if (prm.precond_theta != theta0) {
+        prm.precond_theta = theta0;
+        if (int rc2 = precond_build(*this, h, d_dvec)) return rc2;
+    }
+    return rc;
 }
 
 int Engine::prepare_solver(double h)

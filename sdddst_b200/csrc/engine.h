@@ -64,6 +64,7 @@ struct Engine {
     int last_iters = 0;
     double last_resid = 0.0;
     long solves = 0, iterations = 0;      // solver statistics
+    long stalls = 0;                      // solves repeated with a rebuilt preconditioner
     double *d_hrec = nullptr;             // per-iteration Gram-Schmidt records
     double *h_hrec = nullptr;             // pinned copy
     unsigned int *d_counter = nullptr;    // last-block ticket of the fused reductions

@@ -37,6 +37,15 @@ constexpr float kA1 = 3.4938669795049805e-06f;                   // qn2 + qn3 + 
 constexpr float kB1 = 6.994256639099779e-06f;                    // 2 qn2 + 3 qn3 + 4 qn4
 constexpr float kQN2SQ = 1.2161556709409309e-11f;                // qn2^2 = qn4
 
+// Single-instruction approximate reciprocal (SFU, about 1 ulp); the FP32
+// path's accuracy target is set by its FP32 inputs, not by this rounding.
+__device__ __forceinline__ float rcp_fast(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 __device__ __forceinline__ float sinpi_poly(float y)
 {
     const float y2 = y * y;
@@ -69,17 +78,17 @@ __device__ __forceinline__ float tau_xy_f32(float dx, float dy)
     // k = 0
     const float D0 = 2.0f * (sh2 + sn2);
     const float N0 = fmaf(-4.0f * sh2, sn2, 2.0f * (sh2 - sn2));
-    const float r0 = __frcp_rn(D0);
+    const float r0 = rcp_fast(D0);
     float acc = dx * N0 * r0 * r0;
 
     // |k| = 1, exact
     {
         const float Cp = 0.5f * fmaf(E, kQP1, Ei * kQN1);
         const float Dp = Cp - cy;
-        const float rp = __frcp_rn(Dp * Dp);
+        const float rp = rcp_fast(Dp * Dp);
         const float Cm = 0.5f * fmaf(E, kQN1, Ei * kQP1);
         const float Dm = Cm - cy;
-        const float rm = __frcp_rn(Dm * Dm);
+        const float rm = rcp_fast(Dm * Dm);
         acc = fmaf((dx + 1.0f) * fmaf(Cp, cy, -1.0f), rp, acc);
         acc = fmaf((dx - 1.0f) * fmaf(Cm, cy, -1.0f), rm, acc);
     }
@@ -132,19 +141,19 @@ __device__ __forceinline__ float tau_xy_dx_f32(float dx, float dy)
     const float D0 = 2.0f * (sh2 + sn2);
     const float N0 = fmaf(-4.0f * sh2, sn2, 2.0f * (sh2 - sn2));
     const float S0 = 2.0f * sh * ch;
-    const float r0 = __frcp_rn(D0);
+    const float r0 = rcp_fast(D0);
     float acc = r0 * r0 * fmaf(twopi * dx * S0, fmaf(-2.0f * N0, r0, cy), N0);
     // |k| = 1
     {
         const float ap = E * kQP1, bp = Ei * kQN1;
         const float Cp = 0.5f * (ap + bp), Sp = 0.5f * (ap - bp);
         const float Dp = Cp - cy, Np = fmaf(Cp, cy, -1.0f);
-        const float rp = __frcp_rn(Dp);
+        const float rp = rcp_fast(Dp);
         acc = fmaf(rp * rp, fmaf(twopi * (dx + 1.0f) * Sp, fmaf(-2.0f * Np, rp, cy), Np), acc);
         const float am = E * kQN1, bm = Ei * kQP1;
         const float Cm = 0.5f * (am + bm), Sm = 0.5f * (am - bm);
         const float Dm = Cm - cy, Nm = fmaf(Cm, cy, -1.0f);
-        const float rm = __frcp_rn(Dm);
+        const float rm = rcp_fast(Dm);
         acc = fmaf(rm * rm, fmaf(twopi * (dx - 1.0f) * Sm, fmaf(-2.0f * Nm, rm, cy), Nm), acc);
     }
     // |k| = 2..4, first order, + side (E^-1) and - side (E)

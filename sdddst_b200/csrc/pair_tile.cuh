@@ -121,10 +121,15 @@ __device__ __forceinline__ void f32_tile_body(const double *sx, const double *sy
             tb[k][lane] = t;
         }
         __syncwarp();
-        double cs = 0.0;
+        // column partial of this 32-row chunk summed in FP32 (two halves),
+        // then carried in FP64
+        float c0s = 0.0f, c1s = 0.0f;
 #pragma unroll 8
-        for (int m = 0; m < 32; ++m) cs += (double)tb[lane][m];
-        colsum_w[c0 + lane] = cs;
+        for (int m = 0; m < 16; ++m) {
+            c0s += tb[lane][m];
+            c1s += tb[lane][m + 16];
+        }
+        colsum_w[c0 + lane] = (double)c0s + (double)c1s;
         __syncwarp();
     }
 }

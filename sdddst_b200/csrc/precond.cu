@@ -269,7 +269,7 @@ int precond_build(Engine &e, double h, const double *dvec)
     const int n = e.n;
     cudaStream_t st = e.st;
     const unsigned nb256 = (unsigned)((n + 255) / 256);
-    const double theta = e.prm.precond_theta > 0 ? e.prm.precond_theta : 0.1;
+    const double theta = e.prm.precond_theta > 0 ? e.prm.precond_theta : 0.05;
     int *ptr = e.pc_ptr, *par = e.pc_parent, *par2 = e.pc_tmp;
     if (e.valf)
         strongest_kernel<float><<<(n + 7) / 8, 256, 0, st>>>(n, h, e.d_hrow, theta, e.d_rowptr, e.d_col, e.d_valf,
