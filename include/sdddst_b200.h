@@ -56,7 +56,8 @@ enum {
 enum {
     SDDDST_SOLVER_GMRES = 0,         /* restarted GMRES, FP64, unpreconditioned */
     SDDDST_SOLVER_GMRES_JACOBI = 1,  /* restarted GMRES, FP64, diagonal preconditioner */
-    SDDDST_SOLVER_GMRES_CLUSTER = 2  /* restarted GMRES, FP64, block-Jacobi on strongly coupled clusters */
+    SDDDST_SOLVER_GMRES_CLUSTER = 2, /* restarted GMRES, FP64, block-Jacobi on strongly coupled clusters */
+    SDDDST_SOLVER_DIRECT = 3         /* sparse LU (multifrontal, nested dissection), FP64, refined to solver_tol */
 };
 
 /* Field kernels (Field plug-in): the analytic periodic field
@@ -236,6 +237,15 @@ int sdddst_speeds_noalloc(int n, const double *x_device, const double *y_device,
 /* Linear-solver statistics of this context: solves performed and their
  * total Krylov iterations. */
 int sdddst_solver_stats(void *ctx, long *solves, long *iterations);
+
+/* Sparse LU statistics of this context (SDDDST_SOLVER_DIRECT; zeros
+ * otherwise): factorizations performed, pivots perturbed, FP64 flops of one
+ * factorization of the last analysed pattern, doubles held by its fronts,
+ * number of fronts and tree depth (each pointer optional).  The reference
+ * reports nothing comparable: UMFPACK's statistics are not read
+ * (simulation.cpp:386-396). */
+int sdddst_direct_stats(void *ctx, long *factorizations, long *perturbed, double *flops, long *front_doubles,
+                        int *fronts, int *depth);
 
 /* ---- Batches of independent systems (a population of random realisations).
  * `count` systems of sizes[k] dislocations, concatenated in xyb (sum of sizes

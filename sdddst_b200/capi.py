@@ -25,7 +25,7 @@ ERR_NONFINITE = -6
 
 STRESS_ZERO, STRESS_FIXED_RATE, STRESS_SPRING, STRESS_CONSTANT = 0, 1, 2, 3
 PAIRSUM_FP64, PAIRSUM_FP32 = 0, 1
-SOLVER_GMRES, SOLVER_GMRES_JACOBI, SOLVER_GMRES_CLUSTER = 0, 1, 2
+SOLVER_GMRES, SOLVER_GMRES_JACOBI, SOLVER_GMRES_CLUSTER, SOLVER_DIRECT = 0, 1, 2, 3
 
 # Every extern "C" symbol of include/sdddst_b200.h.
 EXPORTS = [
@@ -37,6 +37,7 @@ EXPORTS = [
     "sdddst_speeds_noalloc", "sdddst_solver_stats", "sdddst_speeds_ext", "sdddst_set_scalars",
     "sdddst_update_params", "sdddst_solve_csc", "sdddst_batch_create", "sdddst_batch_destroy",
     "sdddst_batch_step", "sdddst_batch_get_scalars", "sdddst_batch_get_positions", "sdddst_batch_info",
+    "sdddst_direct_stats",
 ]
 
 
@@ -107,6 +108,9 @@ def load(path: str = LIB_PATH):
     lib.sdddst_solver_stats.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long)]
     lib.sdddst_profile_pair_sum.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
     lib.sdddst_vector_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.sdddst_direct_stats.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long),
+                                        C.POINTER(C.c_double), C.POINTER(C.c_long), C.POINTER(C.c_int),
+                                        C.POINTER(C.c_int)]
     lib.sdddst_kernel_launches.argtypes = [C.c_void_p]
     lib.sdddst_kernel_launches.restype = C.c_long
     _lib = lib
@@ -288,6 +292,15 @@ class Engine:
         a, b = C.c_long(0), C.c_long(0)
         _check(self.lib.sdddst_solver_stats(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def direct_stats(self) -> dict:
+        f, pp, fd = C.c_long(0), C.c_long(0), C.c_long(0)
+        fl = C.c_double(0.0)
+        nf, dp = C.c_int(0), C.c_int(0)
+        _check(self.lib.sdddst_direct_stats(self.h, C.byref(f), C.byref(pp), C.byref(fl), C.byref(fd),
+                                            C.byref(nf), C.byref(dp)))
+        return {"factorizations": f.value, "perturbed_pivots": pp.value, "lu_flops": fl.value,
+                "front_doubles": fd.value, "fronts": nf.value, "depth": dp.value}
 
     def launches(self) -> int:
         return int(self.lib.sdddst_kernel_launches(self.h))

@@ -582,6 +582,10 @@ static int batch_init(Batch &bt, const sdddst_params &common, int count, const i
         }
         bt.off[k + 1] = bt.off[k] + sizes[k];
     }
+    if (common.solver == SDDDST_SOLVER_DIRECT) {
+        bt.e.err = "batch: the sparse LU solver serves single systems; choose a GMRES solver";
+        return SDDDST_ERR_INVALID;
+    }
     bt.ntot = bt.off[count];
     if (bt.ntot > (1L << 30)) {
         bt.e.err = "batch too large";

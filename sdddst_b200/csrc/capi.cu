@@ -98,7 +98,7 @@ int sdddst_ctx_create(const sdddst_params *prm, const double *xyb, const double 
     if (prm->pairsum != SDDDST_PAIRSUM_FP64 && prm->pairsum != SDDDST_PAIRSUM_FP32)
         return fail(SDDDST_ERR_INVALID, "unsupported pair-sum mode");
     if (prm->solver != SDDDST_SOLVER_GMRES && prm->solver != SDDDST_SOLVER_GMRES_JACOBI &&
-        prm->solver != SDDDST_SOLVER_GMRES_CLUSTER)
+        prm->solver != SDDDST_SOLVER_GMRES_CLUSTER && prm->solver != SDDDST_SOLVER_DIRECT)
         return fail(SDDDST_ERR_INVALID, "unsupported solver");
     if (!(prm->prec > 0) || !(prm->step_size > 0) || !(prm->cutoff_multiplier > 0))
         return fail(SDDDST_ERR_INVALID, "prec, step size and cutoff multiplier must be positive");
@@ -498,6 +498,23 @@ int sdddst_solver_stats(void *ctx, long *solves, long *iterations)
     if (!ctx) return fail(SDDDST_ERR_INVALID, "null argument");
     if (solves) *solves = E(ctx)->solves;
     if (iterations) *iterations = E(ctx)->iterations;
+    return SDDDST_OK;
+}
+
+int sdddst_direct_stats(void *ctx, long *factorizations, long *perturbed, double *flops, long *front_doubles,
+                        int *fronts, int *depth)
+{
+    if (!ctx) return fail(SDDDST_ERR_INVALID, "null argument");
+    long f = 0, p = 0, fd = 0;
+    double fl = 0.0;
+    int nf = 0, dp = 0;
+    sd::direct_stats(*E(ctx), &f, &p, &fl, &fd, &nf, &dp);
+    if (factorizations) *factorizations = f;
+    if (perturbed) *perturbed = p;
+    if (flops) *flops = fl;
+    if (front_doubles) *front_doubles = fd;
+    if (fronts) *fronts = nf;
+    if (depth) *depth = dp;
     return SDDDST_OK;
 }
 

@@ -1,0 +1,1248 @@
+// Device sparse direct solve of J(h) x = rhs, the drop-in for the UMFPACK
+// factorization and solve of Simulation::calculateSparseFormForJacobian /
+// solveEQSys (simulation.cpp:386-396): a multifrontal LU over a geometric
+// nested dissection of the periodic unit cell.
+//
+// Ordering.  Two dislocations are coupled in J only when their periodic
+// distance is below the pattern radius r_p = (1 + sqrt(36.8)) c
+// (simulation.cpp:255-262), so a strip of width w > r_p separates the
+// dislocations on its two sides.  The tree splits the torus along x with two
+// strips (|x| < w/2 and |x| >= 1/2 - w/2), each half along y the same way,
+// then every rectangle across its longer side with one middle strip, down to
+// leaves with a side below 3w.  Strips and leaves are the fronts; their
+// dislocations are numbered in postorder (children before parents), in
+// ascending index inside a front.
+//
+// Symbolic structure.  What a subtree leaves behind in the Schur complement
+// couples ancestor-strip dislocations within r_p of the subtree's rectangle
+// (no coupling reaches farther), so each front holds its own dislocations
+// plus the ancestor-strip dislocations within w of its rectangle: a superset
+// of the exact structure, found by a distance test, exact zeros included.
+// A child's set lies inside its parent's front because the child's rectangle
+// lies inside the parent's.
+//
+// Numeric.  Each front is a dense FP64 row-major matrix assembled from the
+// rows and columns of J of its own dislocations plus its children's Schur
+// complements (extend-add, one child after the other), then partially
+// factored in blocks of 64 pivots: row pivoting inside the block, static
+// perturbation of pivots below sqrt(eps) of the block's largest entry, the
+// triangular inverses of each diagonal block kept for the solves, and an FP64
+// tiled update of the trailing matrix.  All fronts at one tree depth share the
+// launches.  Row swaps of a block are not applied to the columns left of it:
+// the forward solve applies each block's permutation when it reaches the
+// block.
+//
+// Solve.  The forward substitution, leaves to root, passes each front's update
+// part to its parent; the backward substitution, root to leaves, reads the
+// ancestors' solutions.  The caller refines against the unfactored J
+// (residual in FP64, refinement steps, GMRES preconditioned by the factors as
+// the last resort).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.h"
+
+namespace sd {
+
+namespace {
+
+constexpr int kNB = 64;          // pivot block
+constexpr int kMaxTree = 8191;   // tree nodes
+constexpr int kChunk = 256;      // dislocations per ranking chunk
+constexpr int kLeafMin = 96;     // expected dislocations below which a rectangle is not split
+
+struct TreeNode {
+    int axis;   // split axis (0: x, 1: y), -1: leaf
+    int torus;  // split of a periodic axis by two strips
+    double lo, hi, cut; // strip [lo, hi); torus: second strip |c| >= cut
+    double rx0, rx1, ry0, ry1; // rectangle of the subtree
+    int fullx, fully;          // the rectangle spans the period on that axis
+    int parent, child0, child1, depth;
+};
+
+struct FrontInfo {
+    long foff; // front matrix offset (doubles) in the pool
+    long ioff; // block inverses offset (doubles)
+    long woff; // solve vector offset (doubles)
+    int p, u, n, ld;
+    int start; // first elimination position of its own dislocations
+    int uoff;  // offset of its update list
+    int parent, child0, child1, depth;
+};
+
+struct Direct {
+    // tree (depends on the cutoff only)
+    double w = 0.0, built_for = -1.0;
+    int T = 0, maxdepth = 0;
+    std::vector<TreeNode> tree;
+    std::vector<int> postorder;
+    TreeNode *d_tree = nullptr;
+    // analysis of one Jacobian pattern
+    int nchunk = 0;
+    int *d_tn = nullptr, *d_lrank = nullptr, *d_ctab = nullptr, *d_cnt = nullptr, *d_pos = nullptr;
+    int *d_own = nullptr, *d_perm = nullptr, *d_ucnt = nullptr;
+    double *d_xw = nullptr, *d_yw = nullptr, *d_Y = nullptr;
+    int *d_upd = nullptr, *d_updpos = nullptr, *d_map = nullptr;
+    long upd_cap = 0, updpos_cap = 0, map_cap = 0;
+    std::vector<FrontInfo> fr;
+    FrontInfo *d_fr = nullptr;
+    std::vector<std::vector<int>> levels;
+    std::vector<int> level_off, level_pmax, level_nmax, level_umax;
+    int *d_levels = nullptr;
+    // numeric
+    double *d_F = nullptr, *d_inv = nullptr, *d_W = nullptr;
+    long F_cap = 0, inv_cap = 0, W_cap = 0, F_used = 0;
+    int *d_npert = nullptr;
+    bool analysed = false, factored = false;
+    double flops = 0.0; // LU flops of one factorization
+    long factorizations = 0, perturbed = 0;
+    int *h_buf = nullptr; // pinned
+    int h_buf_cap = 0;
+};
+
+Direct *D(Engine &e) { return static_cast<Direct *>(e.direct); }
+
+template <typename T> int grow(T *&p, long &cap, long need)
+{
+    if (need <= cap && p) return 0;
+    if (p) cudaFree(p);
+    p = nullptr;
+    long c = std::max(need, 1L);
+    c += c / 8;
+    if (cudaMalloc(&p, sizeof(T) * (size_t)c) != cudaSuccess) {
+        cap = 0;
+        return SDDDST_ERR_NOMEM;
+    }
+    cap = c;
+    return 0;
+}
+
+// ------------------------------------------------------------ device helpers
+
+__device__ __forceinline__ double wrap_unit(double v) { return v - rint(v); }
+
+__device__ int tree_assign(const TreeNode *__restrict__ T, double x, double y)
+{
+    int t = 0;
+    for (int guard = 0; guard < 64; ++guard) {
+        const TreeNode nd = T[t];
+        if (nd.axis < 0) return t;
+        const double c = nd.axis == 0 ? x : y;
+        if (c >= nd.lo && c < nd.hi) return t;
+        if (nd.torus) {
+            if (c >= nd.cut || c < -nd.cut) return t;
+            t = c < 0.0 ? nd.child0 : nd.child1;
+        } else {
+            t = c < nd.lo ? nd.child0 : nd.child1;
+        }
+    }
+    return t;
+}
+
+__device__ __forceinline__ double axis_gap(double c, double lo, double hi, int full)
+{
+    if (full || (c >= lo && c < hi)) return 0.0;
+    return fmin(fabs(wrap_unit(c - lo)), fabs(wrap_unit(c - hi)));
+}
+
+__device__ __forceinline__ bool near_rect(const TreeNode &t, double x, double y, double w)
+{
+    const double gx = axis_gap(x, t.rx0, t.rx1, t.fullx);
+    const double gy = axis_gap(y, t.ry0, t.ry1, t.fully);
+    return gx * gx + gy * gy < w * w;
+}
+
+// exclusive block scan of one int per thread (blockDim.x == 256)
+__device__ int block_scan_excl(int v, int *total)
+{
+    __shared__ int ws[8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    __syncthreads();
+    if (lane == 31) ws[wid] = incl;
+    __syncthreads();
+    int off = 0, tot = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        if (k < wid) off += ws[k];
+        tot += ws[k];
+    }
+    *total = tot;
+    return off + incl - v;
+}
+
+// ------------------------------------------------------------ symbolic kernels
+
+__global__ void assign_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
+                              const TreeNode *__restrict__ T, int *__restrict__ tn, double *__restrict__ xw,
+                              double *__restrict__ yw)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double a = wrap_unit(x[i]), b = wrap_unit(y[i]);
+    if (a >= 0.5) a -= 1.0;
+    if (b >= 0.5) b -= 1.0;
+    xw[i] = a;
+    yw[i] = b;
+    tn[i] = tree_assign(T, a, b);
+}
+
+// rank of each dislocation among the earlier ones of its chunk in the same
+// tree node; the last of a node in the chunk writes the chunk's count
+__global__ void chunk_rank_kernel(int n, int T, const int *__restrict__ tn, int *__restrict__ lrank,
+                                  int *__restrict__ ctab)
+{
+    __shared__ int s[kChunk];
+    const int i = blockIdx.x * kChunk + threadIdx.x;
+    s[threadIdx.x] = i < n ? tn[i] : -1;
+    __syncthreads();
+    if (i >= n) return;
+    const int me = s[threadIdx.x];
+    int before = 0, after = 0;
+    for (int k = 0; k < kChunk; ++k) {
+        const int eq = s[k] == me;
+        before += (k < (int)threadIdx.x) & eq;
+        after += (k > (int)threadIdx.x) & eq;
+    }
+    lrank[i] = before;
+    if (after == 0) ctab[(long)blockIdx.x * T + me] = before + 1;
+}
+
+__global__ void chunk_scan_kernel(int T, int nchunk, int *__restrict__ ctab, int *__restrict__ cnt)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    int run = 0;
+    for (int c = 0; c < nchunk; ++c) {
+        const int v = ctab[(long)c * T + t];
+        ctab[(long)c * T + t] = run;
+        run += v;
+    }
+    cnt[t] = run;
+}
+
+__global__ void place_kernel(int n, int T, const int *__restrict__ tn, const int *__restrict__ lrank,
+                             const int *__restrict__ ctab, const FrontInfo *__restrict__ fr, int *__restrict__ pos,
+                             int *__restrict__ own)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int t = tn[i];
+    const int q = fr[t].start + ctab[(long)(i / kChunk) * T + t] + lrank[i];
+    pos[i] = q;
+    own[q] = i;
+}
+
+// update sets: ancestor-strip dislocations within w of the node's rectangle,
+// nearest ancestor first (ascending elimination position)
+template <bool kFill>
+__global__ void update_set_kernel(const TreeNode *__restrict__ T, const FrontInfo *__restrict__ fr,
+                                  const int *__restrict__ own, const double *__restrict__ xw,
+                                  const double *__restrict__ yw, double w, int *__restrict__ ucnt,
+                                  int *__restrict__ upd, int *__restrict__ updpos)
+{
+    const int t = blockIdx.x;
+    const TreeNode me = T[t];
+    int count = 0;
+    int base = kFill ? fr[t].uoff : 0;
+    for (int a = me.parent; a >= 0; a = T[a].parent) {
+        const int s0 = fr[a].start, pa = fr[a].p;
+        for (int k0 = 0; k0 < pa; k0 += 256) {
+            const int k = k0 + threadIdx.x;
+            int j = -1, hit = 0;
+            if (k < pa) {
+                j = own[s0 + k];
+                hit = near_rect(me, xw[j], yw[j], w) ? 1 : 0;
+            }
+            int tot;
+            const int off = block_scan_excl(hit, &tot);
+            if (kFill && hit) {
+                upd[base + count + off] = j;
+                updpos[base + count + off] = s0 + k;
+            }
+            count += tot;
+        }
+    }
+    if (!kFill && threadIdx.x == 0) ucnt[t] = count;
+}
+
+__device__ __forceinline__ int find_sorted(const int *__restrict__ a, int len, int key)
+{
+    int lo = 0, hi = len;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < len && a[lo] == key) ? lo : -1;
+}
+
+// local index of elimination position q in front f (-1: not in the front)
+__device__ __forceinline__ int front_local(const FrontInfo &f, const int *__restrict__ updpos, int q)
+{
+    if (q >= f.start && q < f.start + f.p) return q - f.start;
+    const int k = find_sorted(updpos + f.uoff, f.u, q);
+    return k < 0 ? -1 : f.p + k;
+}
+
+__global__ void map_kernel(int T, const FrontInfo *__restrict__ fr, const int *__restrict__ updpos,
+                           int *__restrict__ map, int *__restrict__ flag)
+{
+    const int c = blockIdx.x;
+    const FrontInfo fc = fr[c];
+    if (fc.parent < 0) return;
+    const FrontInfo fp = fr[fc.parent];
+    for (int q = threadIdx.x; q < fc.u; q += blockDim.x) {
+        int l = front_local(fp, updpos, updpos[fc.uoff + q]);
+        if (l < 0) {
+            atomicExch(flag, 2);
+            l = 0;
+        }
+        map[fc.uoff + q] = l;
+    }
+}
+
+// ------------------------------------------------------------ numeric kernels
+
+// rows and columns of J of each front's own dislocations; one warp per row
+template <typename VT>
+__global__ void assemble_kernel(int n, double h, const int *__restrict__ rowptr, const int *__restrict__ col,
+                                const VT *__restrict__ val, const double *__restrict__ gdiag,
+                                const double *__restrict__ dvec, const int *__restrict__ tn,
+                                const int *__restrict__ pos, const FrontInfo *__restrict__ fr,
+                                const int *__restrict__ updpos, double *__restrict__ F, int *__restrict__ flag)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const FrontInfo f = fr[tn[i]];
+    double *Ff = F + f.foff;
+    const int li = pos[i] - f.start;
+    const double di = (1.0 + dvec[i]) * 0.5 * h;
+    const int s = rowptr[i], e = rowptr[i + 1];
+    for (int q = s + lane; q < e; q += 32) {
+        const int j = col[q];
+        if (j == i) {
+            Ff[(long)li * f.ld + li] = 1.0 + di * gdiag[i];
+            continue;
+        }
+        const int pj = pos[j];
+        if (pj < f.start) continue; // a descendant: assembled in its own front
+        const int lj = front_local(f, updpos, pj);
+        if (lj < 0) {
+            atomicExch(flag, 3);
+            continue;
+        }
+        const double g = (double)val[q];
+        Ff[(long)li * f.ld + lj] = di * g;
+        if (lj >= f.p) Ff[(long)lj * f.ld + li] = (1.0 + dvec[j]) * 0.5 * h * g;
+    }
+}
+
+// parent += child's Schur complement, for the child in one slot
+__global__ void extend_add_kernel(const FrontInfo *__restrict__ fr, const int *__restrict__ list, int slot,
+                                  double *__restrict__ F, const int *__restrict__ map)
+{
+    const FrontInfo ft = fr[list[blockIdx.y]];
+    const int c = slot ? ft.child1 : ft.child0;
+    if (c < 0) return;
+    const FrontInfo fc = fr[c];
+    const int tiles = (fc.u + 31) >> 5;
+    if ((int)blockIdx.x >= tiles * tiles) return;
+    const int a0 = (blockIdx.x / tiles) * 32, b0 = (blockIdx.x % tiles) * 32;
+    __shared__ int mr[32], mc[32];
+    if (threadIdx.x < 32) mr[threadIdx.x] = a0 + threadIdx.x < fc.u ? map[fc.uoff + a0 + threadIdx.x] : 0;
+    else if (threadIdx.x < 64) {
+        const int k = threadIdx.x - 32;
+        mc[k] = b0 + k < fc.u ? map[fc.uoff + b0 + k] : 0;
+    }
+    __syncthreads();
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const double *Fc = F + fc.foff;
+    double *Ft = F + ft.foff;
+    for (int r = ty; r < 32; r += 8) {
+        const int a = a0 + r, b = b0 + tx;
+        if (a < fc.u && b < fc.u)
+            Ft[(long)mr[r] * ft.ld + mc[tx]] += Fc[(long)(fc.p + a) * fc.ld + fc.p + b];
+    }
+}
+
+// LU of the diagonal block of pivot block j (row pivoting inside the block),
+// its triangular inverses, and the block-local row permutation
+__global__ void __launch_bounds__(256) diag_block_kernel(const FrontInfo *__restrict__ fr, const int *__restrict__ list,
+                                                         int j, double *__restrict__ F, double *__restrict__ inv,
+                                                         int *__restrict__ perm, int *__restrict__ npert)
+{
+    const FrontInfo f = fr[list[blockIdx.y]];
+    const int s = j * kNB;
+    if (s >= f.p) return;
+    const int b = min(kNB, f.p - s);
+    extern __shared__ double sm[];
+    double(*Dm)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
+    double(*Li)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm + kNB * (kNB + 1));
+    double(*Ui)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm + 2 * kNB * (kNB + 1));
+    __shared__ int pv[kNB];
+    __shared__ int piv;
+    __shared__ double red[8];
+    double *Ff = F + f.foff;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    double amax = 0.0;
+    for (int idx = tid; idx < b * b; idx += 256) {
+        const int r = idx / b, c = idx % b;
+        const double v = Ff[(long)(s + r) * f.ld + s + c];
+        Dm[r][c] = v;
+        amax = fmax(amax, fabs(v));
+    }
+    if (tid < kNB) pv[tid] = tid;
+    amax = warp_max(amax);
+    if (lane == 0) red[wid] = amax;
+    __syncthreads();
+    amax = red[0];
+    for (int k = 1; k < 8; ++k) amax = fmax(amax, red[k]);
+    const double thr = 1.4901161193847656e-08 * (amax > 0.0 ? amax : 1.0);
+    int pert = 0;
+    for (int c = 0; c < b; ++c) {
+        if (wid == 0) {
+            double best = -1.0;
+            int br = c;
+            for (int r = c + lane; r < b; r += 32) {
+                const double v = fabs(Dm[r][c]);
+                if (v > best) {
+                    best = v;
+                    br = r;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int orr = __shfl_xor_sync(0xffffffffu, br, o);
+                if (ob > best || (ob == best && orr < br)) {
+                    best = ob;
+                    br = orr;
+                }
+            }
+            if (lane == 0) piv = br;
+        }
+        __syncthreads();
+        const int pr = piv;
+        if (pr != c) {
+            if (tid < b) {
+                const double t = Dm[c][tid];
+                Dm[c][tid] = Dm[pr][tid];
+                Dm[pr][tid] = t;
+            }
+            if (tid == 0) {
+                const int t = pv[c];
+                pv[c] = pv[pr];
+                pv[pr] = t;
+            }
+        }
+        __syncthreads();
+        double d = Dm[c][c];
+        if (!(fabs(d) >= thr)) {
+            d = d < 0.0 ? -thr : thr;
+            pert = 1;
+        }
+        __syncthreads();
+        if (tid == 0) Dm[c][c] = d;
+        for (int r = c + 1 + tid; r < b; r += 256) Dm[r][c] /= d;
+        __syncthreads();
+        const int m = b - c - 1;
+        for (int idx = tid; idx < m * m; idx += 256) {
+            const int r = c + 1 + idx / m, cc = c + 1 + idx % m;
+            Dm[r][cc] -= Dm[r][c] * Dm[c][cc];
+        }
+        __syncthreads();
+        if (tid == 0 && pert) {
+            atomicAdd(npert, 1);
+            pert = 0;
+        }
+    }
+    // inverses: thread c < 64 owns column c of L^-1, thread 64 + c column c of U^-1
+    if (tid < kNB) {
+        const int c = tid;
+        for (int r = 0; r < kNB; ++r) Li[r][c] = r == c ? 1.0 : 0.0;
+        if (c < b)
+            for (int r = c + 1; r < b; ++r) {
+                double acc = Dm[r][c];
+                for (int k = c + 1; k < r; ++k) acc = fma(Dm[r][k], Li[k][c], acc);
+                Li[r][c] = -acc;
+            }
+    } else if (tid < 2 * kNB) {
+        const int c = tid - kNB;
+        for (int r = 0; r < kNB; ++r) Ui[r][c] = 0.0;
+        if (c < b) {
+            Ui[c][c] = 1.0 / Dm[c][c];
+            for (int r = c - 1; r >= 0; --r) {
+                double acc = 0.0;
+                for (int k = r + 1; k <= c; ++k) acc = fma(Dm[r][k], Ui[k][c], acc);
+                Ui[r][c] = -acc / Dm[r][r];
+            }
+        }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < b * b; idx += 256) {
+        const int r = idx / b, c = idx % b;
+        Ff[(long)(s + r) * f.ld + s + c] = Dm[r][c];
+    }
+    double *L = inv + f.ioff + (long)j * 2 * kNB * kNB;
+    double *U = L + kNB * kNB;
+    for (int idx = tid; idx < kNB * kNB; idx += 256) {
+        const int r = idx / kNB, c = idx % kNB;
+        L[idx] = Li[r][c];
+        U[idx] = Ui[r][c];
+    }
+    if (tid < b) perm[f.start + s + tid] = pv[tid];
+}
+
+// U12 = L11^-1 P A12 (first half of the grid) and L21 = A21 U11^-1 (second half)
+__global__ void __launch_bounds__(256) panel_kernel(const FrontInfo *__restrict__ fr, const int *__restrict__ list,
+                                                    int j, double *__restrict__ F, const double *__restrict__ inv,
+                                                    const int *__restrict__ perm, int half)
+{
+    const FrontInfo f = fr[list[blockIdx.y]];
+    const int s = j * kNB;
+    if (s >= f.p) return;
+    const int b = min(kNB, f.p - s), e = s + b, m = f.n - e;
+    if (m <= 0) return;
+    const bool upper = (int)blockIdx.x < half;
+    const int tile = upper ? blockIdx.x : blockIdx.x - half;
+    const int t0 = tile * kNB;
+    if (t0 >= m) return;
+    const int cnt = min(kNB, m - t0);
+    extern __shared__ double sm[];
+    double(*Xs)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
+    double(*As)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm + kNB * (kNB + 1));
+    double *Ff = F + f.foff;
+    const double *Lb = inv + f.ioff + (long)j * 2 * kNB * kNB;
+    const double *Xg = upper ? Lb : Lb + kNB * kNB;
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < kNB * kNB; idx += 256) Xs[idx / kNB][idx % kNB] = Xg[idx];
+    if (upper) {
+        for (int idx = tid; idx < kNB * kNB; idx += 256) {
+            const int k = idx / kNB, c = idx % kNB;
+            As[k][c] = (k < b && c < cnt) ? Ff[(long)(s + perm[f.start + s + k]) * f.ld + e + t0 + c] : 0.0;
+        }
+    } else {
+        for (int idx = tid; idx < kNB * kNB; idx += 256) {
+            const int r = idx / kNB, k = idx % kNB;
+            As[r][k] = (r < cnt && k < b) ? Ff[(long)(e + t0 + r) * f.ld + s + k] : 0.0;
+        }
+    }
+    __syncthreads();
+    const int tx = tid & 15, ty = tid >> 4;
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
+    if (upper) {
+        // R[i][c] = sum_k Linv[i][k] A[k][c]
+        for (int k = 0; k < b; ++k) {
+            double xv[4], av[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) xv[a] = Xs[ty * 4 + a][k];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) av[c] = As[k][tx + 16 * c];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[a][c] = fma(xv[a], av[c], acc[a][c]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int i = ty * 4 + a, cc = tx + 16 * c;
+                if (i < b && cc < cnt) Ff[(long)(s + i) * f.ld + e + t0 + cc] = acc[a][c];
+            }
+    } else {
+        // R[r][jj] = sum_k A[r][k] Uinv[k][jj]
+        for (int k = 0; k < b; ++k) {
+            double av[4], xv[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) av[a] = As[ty * 4 + a][k];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) xv[c] = Xs[k][tx + 16 * c];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[a][c] = fma(av[a], xv[c], acc[a][c]);
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int r = ty * 4 + a, jj = tx + 16 * c;
+                if (r < cnt && jj < b) Ff[(long)(e + t0 + r) * f.ld + s + jj] = acc[a][c];
+            }
+    }
+}
+
+// trailing update F[e:, e:] -= L21 U12: 128 x 128 tiles, 8 x 8 outputs per thread
+constexpr int kBM = 128, kBK = 16, kPad = 2;
+
+__global__ void __launch_bounds__(256, 1) update_kernel(const FrontInfo *__restrict__ fr, const int *__restrict__ list,
+                                                        int j, double *__restrict__ F)
+{
+    const FrontInfo f = fr[list[blockIdx.y]];
+    const int s = j * kNB;
+    if (s >= f.p) return;
+    const int b = min(kNB, f.p - s), e = s + b, m = f.n - e;
+    if (m <= 0) return;
+    const int tiles = (m + kBM - 1) / kBM;
+    if ((int)blockIdx.x >= tiles * tiles) return;
+    const int row0 = e + (blockIdx.x / tiles) * kBM, col0 = e + (blockIdx.x % tiles) * kBM;
+    __shared__ __align__(16) double As[kBK][kBM + kPad];
+    __shared__ __align__(16) double Bs[kBK][kBM + kPad];
+    double *Ff = F + f.foff;
+    const long ld = f.ld;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    double acc[8][8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[a][c] = 0.0;
+    double ra[8], rb[8];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = tid + 256 * q;
+            const int r = idx >> 4, k = idx & 15;
+            ra[q] = (row0 + r < f.n && k0 + k < b) ? Ff[(long)(row0 + r) * ld + s + k0 + k] : 0.0;
+            const int kb = idx >> 7, c = idx & 127;
+            rb[q] = (k0 + kb < b && col0 + c < f.n) ? Ff[(long)(s + k0 + kb) * ld + col0 + c] : 0.0;
+        }
+    };
+    const int nk = (b + kBK - 1) / kBK;
+    load(0);
+    for (int kc = 0; kc < nk; ++kc) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = tid + 256 * q;
+            As[idx & 15][idx >> 4] = ra[q];
+            Bs[idx >> 7][idx & 127] = rb[q];
+        }
+        __syncthreads();
+        if (kc + 1 < nk) load((kc + 1) * kBK);
+#pragma unroll
+        for (int k = 0; k < kBK; ++k) {
+            double av[8], bv[8];
+            const double2 a0 = *reinterpret_cast<const double2 *>(&As[k][ty * 4]);
+            const double2 a1 = *reinterpret_cast<const double2 *>(&As[k][ty * 4 + 2]);
+            const double2 a2 = *reinterpret_cast<const double2 *>(&As[k][64 + ty * 4]);
+            const double2 a3 = *reinterpret_cast<const double2 *>(&As[k][64 + ty * 4 + 2]);
+            const double2 b0 = *reinterpret_cast<const double2 *>(&Bs[k][tx * 4]);
+            const double2 b1 = *reinterpret_cast<const double2 *>(&Bs[k][tx * 4 + 2]);
+            const double2 b2 = *reinterpret_cast<const double2 *>(&Bs[k][64 + tx * 4]);
+            const double2 b3 = *reinterpret_cast<const double2 *>(&Bs[k][64 + tx * 4 + 2]);
+            av[0] = a0.x; av[1] = a0.y; av[2] = a1.x; av[3] = a1.y;
+            av[4] = a2.x; av[5] = a2.y; av[6] = a3.x; av[7] = a3.y;
+            bv[0] = b0.x; bv[1] = b0.y; bv[2] = b1.x; bv[3] = b1.y;
+            bv[4] = b2.x; bv[5] = b2.y; bv[6] = b3.x; bv[7] = b3.y;
+#pragma unroll
+            for (int a = 0; a < 8; ++a)
+#pragma unroll
+                for (int c = 0; c < 8; ++c) acc[a][c] = fma(av[a], bv[c], acc[a][c]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        const int r = row0 + (a < 4 ? ty * 4 + a : 64 + ty * 4 + a - 4);
+        if (r >= f.n) continue;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int cc = col0 + (c < 4 ? tx * 4 + c : 64 + tx * 4 + c - 4);
+            if (cc < f.n) Ff[(long)r * ld + cc] -= acc[a][c];
+        }
+    }
+}
+
+// ------------------------------------------------------------ solve kernels
+
+// forward, per front: own part from the right-hand side, update part zero,
+// plus the children's passed-up parts (child 0, then child 1)
+__global__ void fgather_kernel(const FrontInfo *__restrict__ fr, const int *__restrict__ list,
+                               const int *__restrict__ own, const int *__restrict__ map,
+                               const double *__restrict__ rhs, double *__restrict__ W)
+{
+    const FrontInfo f = fr[list[blockIdx.x]];
+    double *w = W + f.woff;
+    for (int k = threadIdx.x; k < f.n; k += blockDim.x) w[k] = k < f.p ? rhs[own[f.start + k]] : 0.0;
+    __syncthreads();
+    for (int slot = 0; slot < 2; ++slot) {
+        const int c = slot ? f.child1 : f.child0;
+        if (c < 0) continue;
+        const FrontInfo fc = fr[c];
+        const double *wc = W + fc.woff + fc.p;
+        for (int q = threadIdx.x; q < fc.u; q += blockDim.x) w[map[fc.uoff + q]] += wc[q];
+        __syncthreads();
+    }
+}
+
+constexpr int kRowsPerCta = 64;
+
+__device__ __forceinline__ void small_matvec(const double *__restrict__ M, const double *__restrict__ v, double *out,
+                                             int b)
+{
+    // out[i] = sum_k M[i][k] v[k] for i < b (M row-major 64 x 64, zeros outside its triangle)
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int i = wid; i < b; i += 8) {
+        double acc = 0.0;
+        if (lane < b) acc = M[i * kNB + lane] * v[lane];
+        if (lane + 32 < b) acc = fma(M[i * kNB + lane + 32], v[lane + 32], acc);
+        acc = warp_sum(acc);
+        if (lane == 0) out[i] = acc;
+    }
+}
+
+__global__ void fblock_kernel(const FrontInfo *__restrict__ fr, const int *__restrict__ list, int j,
+                              const double *__restrict__ F, const double *__restrict__ inv,
+                              const int *__restrict__ perm, double *__restrict__ W, double *__restrict__ Y)
+{
+    const FrontInfo f = fr[list[blockIdx.y]];
+    const int s = j * kNB;
+    if (s >= f.p) return;
+    const int b = min(kNB, f.p - s), e = s + b;
+    const int r0 = e + blockIdx.x * kRowsPerCta;
+    if (blockIdx.x > 0 && r0 >= f.n) return;
+    __shared__ double pw[kNB], yb[kNB];
+    double *w = W + f.woff;
+    if (threadIdx.x < kNB) pw[threadIdx.x] = threadIdx.x < b ? w[s + perm[f.start + s + threadIdx.x]] : 0.0;
+    __syncthreads();
+    small_matvec(inv + f.ioff + (long)j * 2 * kNB * kNB, pw, yb, b);
+    __syncthreads();
+    if (blockIdx.x == 0 && threadIdx.x < b) Y[f.start + s + threadIdx.x] = yb[threadIdx.x];
+    const double *Ff = F + f.foff;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int r = r0 + wid; r < min(f.n, r0 + kRowsPerCta); r += 8) {
+        const double *row = Ff + (long)r * f.ld + s;
+        double acc = 0.0;
+        if (lane < b) acc = row[lane] * yb[lane];
+        if (lane + 32 < b) acc = fma(row[lane + 32], yb[lane + 32], acc);
+        acc = warp_sum(acc);
+        if (lane == 0) w[r] -= acc;
+    }
+}
+
+// backward, per front: z = y - U12 x_update into the own part of W
+__global__ void bupdate_kernel(const FrontInfo *__restrict__ fr, const int *__restrict__ list,
+                               const double *__restrict__ F, const int *__restrict__ upd,
+                               const double *__restrict__ Y, const double *__restrict__ X, double *__restrict__ W)
+{
+    const FrontInfo f = fr[list[blockIdx.y]];
+    const int r0 = blockIdx.x * kRowsPerCta;
+    if (r0 >= f.p) return;
+    const double *Ff = F + f.foff;
+    double *w = W + f.woff;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int r = r0 + wid; r < min(f.p, r0 + kRowsPerCta); r += 8) {
+        const double *row = Ff + (long)r * f.ld + f.p;
+        double acc = 0.0;
+        for (int q = lane; q < f.u; q += 32) acc = fma(row[q], X[upd[f.uoff + q]], acc);
+        acc = warp_sum(acc);
+        if (lane == 0) w[r] = Y[f.start + r] - acc;
+    }
+}
+
+__global__ void bblock_kernel(const FrontInfo *__restrict__ fr, const int *__restrict__ list, int j,
+                              const double *__restrict__ F, const double *__restrict__ inv,
+                              const int *__restrict__ own, double *__restrict__ W, double *__restrict__ X)
+{
+    const FrontInfo f = fr[list[blockIdx.y]];
+    const int s = j * kNB;
+    if (s >= f.p) return;
+    const int b = min(kNB, f.p - s);
+    const int r0 = blockIdx.x * kRowsPerCta;
+    if (blockIdx.x > 0 && r0 >= s) return;
+    __shared__ double zb[kNB], xb[kNB];
+    double *w = W + f.woff;
+    if (threadIdx.x < kNB) zb[threadIdx.x] = threadIdx.x < b ? w[s + threadIdx.x] : 0.0;
+    __syncthreads();
+    small_matvec(inv + f.ioff + (long)j * 2 * kNB * kNB + kNB * kNB, zb, xb, b);
+    __syncthreads();
+    if (blockIdx.x == 0 && threadIdx.x < b) X[own[f.start + s + threadIdx.x]] = xb[threadIdx.x];
+    const double *Ff = F + f.foff;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int r = r0 + wid; r < min(s, r0 + kRowsPerCta); r += 8) {
+        const double *row = Ff + (long)r * f.ld + s;
+        double acc = 0.0;
+        if (lane < b) acc = row[lane] * xb[lane];
+        if (lane + 32 < b) acc = fma(row[lane + 32], xb[lane + 32], acc);
+        acc = warp_sum(acc);
+        if (lane == 0) w[r] -= acc;
+    }
+}
+
+__global__ void resid_kernel(int n, const double *__restrict__ rhs, const double *__restrict__ jx,
+                             double *__restrict__ r)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) r[i] = rhs[i] - jx[i];
+}
+
+__global__ void addto_kernel(int n, const double *__restrict__ z, double *__restrict__ x)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += z[i];
+}
+
+constexpr size_t kDiagSmem = 3 * kNB * (kNB + 1) * sizeof(double);
+constexpr size_t kPanelSmem = 2 * kNB * (kNB + 1) * sizeof(double);
+
+// ------------------------------------------------------------ host: tree
+
+void build_tree(Direct &d, const Engine &e)
+{
+    const double rp = e.cutoff * (1.0 + std::sqrt(36.8));
+    d.w = rp * (1.0 + 1e-6) + 1e-12;
+    const double w = d.w;
+    d.tree.clear();
+    TreeNode root{};
+    root.axis = -1;
+    root.fullx = root.fully = 1;
+    root.rx0 = root.ry0 = -0.5;
+    root.rx1 = root.ry1 = 0.5;
+    root.parent = root.child0 = root.child1 = -1;
+    d.tree.push_back(root);
+    std::vector<int> stack{0};
+    while (!stack.empty()) {
+        const int t = stack.back();
+        stack.pop_back();
+        TreeNode nd = d.tree[t];
+        if ((int)d.tree.size() + 2 > kMaxTree || nd.depth >= 40) continue;
+        int axis = -1, torus = 0;
+        if (nd.fullx || nd.fully) {
+            if (w < 0.4) {
+                axis = nd.fullx ? 0 : 1;
+                torus = 1;
+            }
+        } else {
+            const double lx = nd.rx1 - nd.rx0, ly = nd.ry1 - nd.ry0;
+            const double L = std::max(lx, ly);
+            if (L >= 3.0 * w && (double)e.n * lx * ly >= kLeafMin) axis = lx >= ly ? 0 : 1;
+        }
+        if (axis < 0) continue;
+        TreeNode c0 = nd, c1 = nd;
+        c0.axis = c1.axis = -1;
+        c0.torus = c1.torus = 0;
+        c0.parent = c1.parent = t;
+        c0.child0 = c0.child1 = c1.child0 = c1.child1 = -1;
+        c0.depth = c1.depth = nd.depth + 1;
+        nd.axis = axis;
+        nd.torus = torus;
+        if (torus) {
+            nd.lo = -0.5 * w;
+            nd.hi = 0.5 * w;
+            nd.cut = 0.5 - 0.5 * w;
+            if (axis == 0) {
+                c0.fullx = c1.fullx = 0;
+                c0.rx0 = -nd.cut; c0.rx1 = nd.lo;
+                c1.rx0 = nd.hi;   c1.rx1 = nd.cut;
+            } else {
+                c0.fully = c1.fully = 0;
+                c0.ry0 = -nd.cut; c0.ry1 = nd.lo;
+                c1.ry0 = nd.hi;   c1.ry1 = nd.cut;
+            }
+        } else {
+            const double a0 = axis == 0 ? nd.rx0 : nd.ry0, a1 = axis == 0 ? nd.rx1 : nd.ry1;
+            const double mid = 0.5 * (a0 + a1);
+            nd.lo = mid - 0.5 * w;
+            nd.hi = mid + 0.5 * w;
+            nd.cut = 0.0;
+            if (axis == 0) {
+                c0.rx1 = nd.lo;
+                c1.rx0 = nd.hi;
+            } else {
+                c0.ry1 = nd.lo;
+                c1.ry0 = nd.hi;
+            }
+        }
+        nd.child0 = (int)d.tree.size();
+        nd.child1 = nd.child0 + 1;
+        d.tree[t] = nd;
+        d.tree.push_back(c0);
+        d.tree.push_back(c1);
+        stack.push_back(nd.child0);
+        stack.push_back(nd.child1);
+    }
+    d.T = (int)d.tree.size();
+    // postorder
+    d.postorder.clear();
+    std::vector<std::pair<int, int>> st{{0, 0}};
+    while (!st.empty()) {
+        auto &top = st.back();
+        const TreeNode &nd = d.tree[top.first];
+        if (nd.axis >= 0 && top.second < 2) {
+            const int c = top.second == 0 ? nd.child0 : nd.child1;
+            top.second++;
+            st.push_back({c, 0});
+        } else {
+            d.postorder.push_back(top.first);
+            st.pop_back();
+        }
+    }
+    d.maxdepth = 0;
+    for (const auto &nd : d.tree) d.maxdepth = std::max(d.maxdepth, nd.depth);
+    d.levels.assign(d.maxdepth + 1, {});
+    for (int t = 0; t < d.T; ++t) d.levels[d.tree[t].depth].push_back(t);
+    d.level_off.assign(d.maxdepth + 2, 0);
+    std::vector<int> flat;
+    for (int l = 0; l <= d.maxdepth; ++l) {
+        d.level_off[l] = (int)flat.size();
+        flat.insert(flat.end(), d.levels[l].begin(), d.levels[l].end());
+    }
+    d.level_off[d.maxdepth + 1] = (int)flat.size();
+    if (d.d_tree) cudaFree(d.d_tree);
+    if (d.d_levels) cudaFree(d.d_levels);
+    cudaMalloc(&d.d_tree, sizeof(TreeNode) * d.T);
+    cudaMalloc(&d.d_levels, sizeof(int) * flat.size());
+    cudaMemcpy(d.d_tree, d.tree.data(), sizeof(TreeNode) * d.T, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.d_levels, flat.data(), sizeof(int) * flat.size(), cudaMemcpyHostToDevice);
+    if (d.d_fr) cudaFree(d.d_fr);
+    cudaMalloc(&d.d_fr, sizeof(FrontInfo) * d.T);
+    d.built_for = e.cutoff;
+}
+
+int ensure_host_buf(Direct &d, int count)
+{
+    if (count <= d.h_buf_cap) return 0;
+    if (d.h_buf) cudaFreeHost(d.h_buf);
+    d.h_buf = nullptr;
+    if (cudaMallocHost(&d.h_buf, sizeof(int) * count) != cudaSuccess) return SDDDST_ERR_NOMEM;
+    d.h_buf_cap = count;
+    return 0;
+}
+
+} // namespace
+
+// ------------------------------------------------------------ host entry points
+
+void direct_free(Engine &e)
+{
+    Direct *d = D(e);
+    if (!d) return;
+    void *bufs[] = {d->d_tree, d->d_tn, d->d_lrank, d->d_ctab, d->d_cnt, d->d_pos, d->d_own, d->d_perm, d->d_ucnt,
+                    d->d_xw, d->d_yw, d->d_Y, d->d_upd, d->d_updpos, d->d_map, d->d_fr, d->d_levels, d->d_F,
+                    d->d_inv, d->d_W, d->d_npert};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (d->h_buf) cudaFreeHost(d->h_buf);
+    delete d;
+    e.direct = nullptr;
+}
+
+// Symbolic phase for the Jacobian pattern assembled at positions x: the
+// elimination order and each front's index set.
+int direct_analyse(Engine &e, const double *x)
+{
+    if (!e.direct) {
+        Direct *d = new Direct();
+        e.direct = d;
+        const int n = e.n;
+        d->nchunk = (n + kChunk - 1) / kChunk;
+        bool ok = cudaMalloc(&d->d_tn, sizeof(int) * n) == cudaSuccess &&
+                  cudaMalloc(&d->d_lrank, sizeof(int) * n) == cudaSuccess &&
+                  cudaMalloc(&d->d_pos, sizeof(int) * n) == cudaSuccess &&
+                  cudaMalloc(&d->d_own, sizeof(int) * n) == cudaSuccess &&
+                  cudaMalloc(&d->d_perm, sizeof(int) * n) == cudaSuccess &&
+                  cudaMalloc(&d->d_xw, sizeof(double) * n) == cudaSuccess &&
+                  cudaMalloc(&d->d_yw, sizeof(double) * n) == cudaSuccess &&
+                  cudaMalloc(&d->d_Y, sizeof(double) * n) == cudaSuccess &&
+                  cudaMalloc(&d->d_npert, sizeof(int)) == cudaSuccess;
+        if (!ok) {
+            e.err = "direct solver: out of device memory";
+            return SDDDST_ERR_NOMEM;
+        }
+    }
+    Direct &d = *D(e);
+    const int n = e.n;
+    cudaStream_t st = e.st;
+    if (d.built_for != e.cutoff) {
+        build_tree(d, e);
+        if (d.d_ctab) cudaFree(d.d_ctab);
+        if (d.d_cnt) cudaFree(d.d_cnt);
+        if (d.d_ucnt) cudaFree(d.d_ucnt);
+        d.d_ctab = d.d_cnt = d.d_ucnt = nullptr;
+        if (cudaMalloc(&d.d_ctab, sizeof(int) * (size_t)d.nchunk * d.T) != cudaSuccess ||
+            cudaMalloc(&d.d_cnt, sizeof(int) * d.T) != cudaSuccess ||
+            cudaMalloc(&d.d_ucnt, sizeof(int) * d.T) != cudaSuccess) {
+            e.err = "direct solver: out of device memory";
+            return SDDDST_ERR_NOMEM;
+        }
+    }
+    d.analysed = d.factored = false;
+    const int T = d.T;
+    if (int rc = ensure_host_buf(d, 2 * T)) {
+        e.err = "direct solver: pinned buffer";
+        return rc;
+    }
+    // 1) tree node of every dislocation, its rank inside its node
+    assign_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, x, e.d_y, d.d_tree, d.d_tn, d.d_xw, d.d_yw);
+    cudaMemsetAsync(d.d_ctab, 0, sizeof(int) * (size_t)d.nchunk * T, st);
+    chunk_rank_kernel<<<d.nchunk, kChunk, 0, st>>>(n, T, d.d_tn, d.d_lrank, d.d_ctab);
+    chunk_scan_kernel<<<(T + 255) / 256, 256, 0, st>>>(T, d.nchunk, d.d_ctab, d.d_cnt);
+    cudaMemcpyAsync(d.h_buf, d.d_cnt, sizeof(int) * T, cudaMemcpyDeviceToHost, st);
+    e.launches += 3;
+    if (int rc = e.sync_check("direct analyse (counts)")) return rc;
+    d.fr.assign(T, FrontInfo{});
+    int start = 0;
+    for (int t : d.postorder) {
+        FrontInfo &f = d.fr[t];
+        f.p = d.h_buf[t];
+        f.start = start;
+        start += f.p;
+        f.parent = d.tree[t].parent;
+        f.child0 = d.tree[t].child0;
+        f.child1 = d.tree[t].child1;
+        f.depth = d.tree[t].depth;
+    }
+    cudaMemcpyAsync(d.d_fr, d.fr.data(), sizeof(FrontInfo) * T, cudaMemcpyHostToDevice, st);
+    place_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, T, d.d_tn, d.d_lrank, d.d_ctab, d.d_fr, d.d_pos, d.d_own);
+    // 2) update sets
+    update_set_kernel<false><<<T, 256, 0, st>>>(d.d_tree, d.d_fr, d.d_own, d.d_xw, d.d_yw, d.w, d.d_ucnt, nullptr,
+                                                nullptr);
+    cudaMemcpyAsync(d.h_buf, d.d_ucnt, sizeof(int) * T, cudaMemcpyDeviceToHost, st);
+    e.launches += 2;
+    if (int rc = e.sync_check("direct analyse (update sets)")) return rc;
+    long uoff = 0, foff = 0, ioff = 0, woff = 0;
+    double flops = 0.0;
+    for (int t = 0; t < T; ++t) {
+        FrontInfo &f = d.fr[t];
+        f.u = d.h_buf[t];
+        f.n = f.p + f.u;
+        f.ld = (f.n + 1) & ~1;
+        f.uoff = (int)uoff;
+        f.foff = foff;
+        f.ioff = ioff;
+        f.woff = woff;
+        uoff += f.u;
+        foff += (long)f.n * f.ld;
+        foff = (foff + 3) & ~3L;
+        ioff += (long)((f.p + kNB - 1) / kNB) * 2 * kNB * kNB;
+        woff += f.n;
+        for (int k = 0; k < f.p; ++k) {
+            const double r = (double)(f.n - k - 1);
+            flops += r + 2.0 * r * r;
+        }
+    }
+    if (uoff > 0x7fffffffL) {
+        e.err = "direct solver: update lists exceed 2^31 entries";
+        return SDDDST_ERR_CAPACITY;
+    }
+    d.flops = flops;
+    d.F_used = foff;
+    if (grow(d.d_upd, d.upd_cap, uoff) || grow(d.d_updpos, d.updpos_cap, uoff) || grow(d.d_map, d.map_cap, uoff)) {
+        e.err = "direct solver: out of device memory (update lists)";
+        return SDDDST_ERR_NOMEM;
+    }
+    if (grow(d.d_F, d.F_cap, foff) || grow(d.d_inv, d.inv_cap, ioff) || grow(d.d_W, d.W_cap, woff)) {
+        e.err = "direct solver: out of device memory (fronts)";
+        return SDDDST_ERR_NOMEM;
+    }
+    const int L = d.maxdepth + 1;
+    d.level_pmax.assign(L, 0);
+    d.level_nmax.assign(L, 0);
+    d.level_umax.assign(L, 0);
+    for (int l = 0; l < L; ++l)
+        for (int t : d.levels[l]) {
+            d.level_pmax[l] = std::max(d.level_pmax[l], d.fr[t].p);
+            d.level_nmax[l] = std::max(d.level_nmax[l], d.fr[t].n);
+            for (int c : {d.fr[t].child0, d.fr[t].child1})
+                if (c >= 0) d.level_umax[l] = std::max(d.level_umax[l], d.fr[c].u);
+        }
+    cudaMemcpyAsync(d.d_fr, d.fr.data(), sizeof(FrontInfo) * T, cudaMemcpyHostToDevice, st);
+    update_set_kernel<true><<<T, 256, 0, st>>>(d.d_tree, d.d_fr, d.d_own, d.d_xw, d.d_yw, d.w, nullptr, d.d_upd,
+                                               d.d_updpos);
+    cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
+    map_kernel<<<T, 256, 0, st>>>(T, d.d_fr, d.d_updpos, d.d_map, e.d_flag);
+    e.launches += 2;
+    cudaMemcpyAsync(&d.h_buf[0], e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (int rc = e.sync_check("direct analyse (maps)")) return rc;
+    if (d.h_buf[0]) {
+        e.err = "direct solver: a child's update set is not inside its parent's front";
+        return SDDDST_ERR_CAPACITY;
+    }
+    d.analysed = true;
+    return 0;
+}
+
+// Numeric factorization of J(h) = I + diag((1 + d)/2) h G on the analysed pattern.
+int direct_factor(Engine &e, double h, const double *dvec)
+{
+    Direct *dp = D(e);
+    if (!dp || !dp->analysed) {
+        e.err = "direct solver: factorization before analysis";
+        return SDDDST_ERR_INVALID;
+    }
+    Direct &d = *dp;
+    cudaStream_t st = e.st;
+    cudaFuncSetAttribute(diag_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem);
+    cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmem);
+    cudaMemsetAsync(d.d_F, 0, sizeof(double) * (size_t)d.F_used, st);
+    cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
+    cudaMemsetAsync(d.d_npert, 0, sizeof(int), st);
+    const int wpb = 8;
+    if (e.valf)
+        assemble_kernel<float><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(
+            e.n, h, e.d_rowptr, e.d_col, e.d_valf, e.d_gdiag, dvec, d.d_tn, d.d_pos, d.d_fr, d.d_updpos, d.d_F,
+            e.d_flag);
+    else
+        assemble_kernel<double><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(
+            e.n, h, e.d_rowptr, e.d_col, e.d_val, e.d_gdiag, dvec, d.d_tn, d.d_pos, d.d_fr, d.d_updpos, d.d_F,
+            e.d_flag);
+    e.launches++;
+    for (int l = d.maxdepth; l >= 0; --l) {
+        const int nf = (int)d.levels[l].size();
+        const int *list = d.d_levels + d.level_off[l];
+        if (d.level_umax[l] > 0) {
+            const int tiles = (d.level_umax[l] + 31) / 32;
+            for (int slot = 0; slot < 2; ++slot)
+                extend_add_kernel<<<dim3(tiles * tiles, nf), 256, 0, st>>>(d.d_fr, list, slot, d.d_F, d.d_map);
+            e.launches += 2;
+        }
+        const int nblk = (d.level_pmax[l] + kNB - 1) / kNB;
+        for (int j = 0; j < nblk; ++j) {
+            diag_block_kernel<<<dim3(1, nf), 256, kDiagSmem, st>>>(d.d_fr, list, j, d.d_F, d.d_inv, d.d_perm,
+                                                                   d.d_npert);
+            const int rest = d.level_nmax[l] - j * kNB;
+            const int half = (rest + kNB - 1) / kNB;
+            if (half > 0) {
+                panel_kernel<<<dim3(2 * half, nf), 256, kPanelSmem, st>>>(d.d_fr, list, j, d.d_F, d.d_inv, d.d_perm,
+                                                                          half);
+                const int tiles = (rest + kBM - 1) / kBM;
+                update_kernel<<<dim3(tiles * tiles, nf), 256, 0, st>>>(d.d_fr, list, j, d.d_F);
+                e.launches += 2;
+            }
+            e.launches++;
+        }
+    }
+    int hv[2];
+    cudaMemcpyAsync(&d.h_buf[0], e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&d.h_buf[1], d.d_npert, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (int rc = e.sync_check("direct factor")) return rc;
+    hv[0] = d.h_buf[0];
+    hv[1] = d.h_buf[1];
+    if (hv[0]) {
+        e.err = "direct solver: a Jacobian entry falls outside its front";
+        return SDDDST_ERR_CAPACITY;
+    }
+    d.perturbed += hv[1];
+    d.factorizations++;
+    d.factored = true;
+    return 0;
+}
+
+// x = (LU)^-1 b with the current factors; b and x may alias.
+int direct_apply(Engine &e, const double *b, double *x)
+{
+    Direct *dp = D(e);
+    if (!dp || !dp->factored) {
+        e.err = "direct solver: solve before factorization";
+        return SDDDST_ERR_INVALID;
+    }
+    Direct &d = *dp;
+    cudaStream_t st = e.st;
+    for (int l = d.maxdepth; l >= 0; --l) {
+        const int nf = (int)d.levels[l].size();
+        const int *list = d.d_levels + d.level_off[l];
+        fgather_kernel<<<nf, 256, 0, st>>>(d.d_fr, list, d.d_own, d.d_map, b, d.d_W);
+        const int nblk = (d.level_pmax[l] + kNB - 1) / kNB;
+        for (int j = 0; j < nblk; ++j) {
+            const int rest = std::max(1, d.level_nmax[l] - j * kNB);
+            fblock_kernel<<<dim3((rest + kRowsPerCta - 1) / kRowsPerCta, nf), 256, 0, st>>>(
+                d.d_fr, list, j, d.d_F, d.d_inv, d.d_perm, d.d_W, d.d_Y);
+        }
+        e.launches += 1 + nblk;
+    }
+    for (int l = 0; l <= d.maxdepth; ++l) {
+        const int nf = (int)d.levels[l].size();
+        const int *list = d.d_levels + d.level_off[l];
+        const int pm = d.level_pmax[l];
+        if (pm == 0) continue;
+        bupdate_kernel<<<dim3((pm + kRowsPerCta - 1) / kRowsPerCta, nf), 256, 0, st>>>(d.d_fr, list, d.d_F, d.d_upd,
+                                                                                    d.d_Y, x, d.d_W);
+        const int nblk = (pm + kNB - 1) / kNB;
+        for (int j = nblk - 1; j >= 0; --j) {
+            const int rows = std::max(1, j * kNB);
+            bblock_kernel<<<dim3((rows + kRowsPerCta - 1) / kRowsPerCta, nf), 256, 0, st>>>(
+                d.d_fr, list, j, d.d_F, d.d_inv, d.d_own, d.d_W, x);
+        }
+        e.launches += 1 + nblk;
+    }
+    return 0;
+}
+
+// Direct solve refined against the unfactored J: up to three refinement
+// steps on the FP64 residual, then GMRES preconditioned by the factors.
+int direct_solve(Engine &e, double h, const double *dvec, const double *rhs, double *x)
+{
+    const int n = e.n;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    const double tol = e.prm.solver_tol > 0 ? e.prm.solver_tol : 1e-13;
+    double bn2 = 0.0;
+    if (int rc = e.sum_sq(rhs, &bn2)) return rc;
+    if (!std::isfinite(bn2)) {
+        e.err = "solve: non-finite right-hand side";
+        return SDDDST_ERR_NONFINITE;
+    }
+    e.solves++;
+    if (bn2 == 0.0) {
+        cudaMemsetAsync(x, 0, sizeof(double) * n, e.st);
+        e.last_iters = 0;
+        return 0;
+    }
+    if (int rc = direct_apply(e, rhs, x)) return rc;
+    for (int it = 0; it <= 3; ++it) {
+        launch_spmv_J(e, h, dvec, x, e.d_w, e.st);
+        resid_kernel<<<nb, 256, 0, e.st>>>(n, rhs, e.d_w, e.d_r);
+        e.launches += 2;
+        double rn2 = 0.0;
+        if (int rc = e.sum_sq(e.d_r, &rn2)) return rc;
+        if (!std::isfinite(rn2)) break;
+        e.last_resid = std::sqrt(rn2 / bn2);
+        if (rn2 <= tol * tol * bn2) {
+            e.last_iters = it;
+            e.iterations += it;
+            return 0;
+        }
+        if (it == 3) break;
+        if (int rc = direct_apply(e, e.d_r, e.d_z)) return rc;
+        addto_kernel<<<nb, 256, 0, e.st>>>(n, e.d_z, x);
+        e.launches++;
+    }
+    e.stalls++;
+    e.solves--; // counted again by GMRES
+    return gmres_solve(e, h, dvec, rhs, x, 3);
+}
+
+int direct_stats(const Engine &e, long *factorizations, long *perturbed, double *flops, long *front_doubles,
+                 int *fronts, int *depth)
+{
+    const Direct *d = static_cast<const Direct *>(e.direct);
+    if (!d) {
+        *factorizations = *perturbed = *front_doubles = 0;
+        *flops = 0.0;
+        *fronts = *depth = 0;
+        return 0;
+    }
+    *factorizations = d->factorizations;
+    *perturbed = d->perturbed;
+    *flops = d->flops;
+    *front_doubles = d->F_used;
+    *fronts = d->T;
+    *depth = d->maxdepth + 1;
+    return 0;
+}
+
+} // namespace sd

@@ -45,6 +45,7 @@ Engine::~Engine()
     if (d_hrec) cudaFree(d_hrec);
     if (d_counter) cudaFree(d_counter);
     precond_free(*this);
+    direct_free(*this);
     if (st) cudaStreamDestroy(st);
 }
 
@@ -234,6 +235,7 @@ int Engine::speeds(const double *x, double *v_out, double *S_out, int stress_typ
 int Engine::assemble(const double *x)
 {
     int rc = jacobian_assemble(*this, x);
+    if (rc == 0 && prm.solver == SDDDST_SOLVER_DIRECT) rc = direct_analyse(*this, x);
     return rc;
 }
 
@@ -244,6 +246,7 @@ int Engine::assemble(const double *x)
 // next matrix.
 int Engine::solve(double h, const double *rhs, double *x_out)
 {
+    if (prm.solver == SDDDST_SOLVER_DIRECT) return direct_solve(*this, h, d_dvec, rhs, x_out);
     int precond = prm.solver == SDDDST_SOLVER_GMRES_JACOBI ? 1 : prm.solver == SDDDST_SOLVER_GMRES_CLUSTER ? 2 : 0;
     int rc = gmres_solve(*this, h, d_dvec, rhs, x_out, precond);
     if (rc != SDDDST_ERR_SOLVER || precond != 2) return rc;
@@ -267,6 +270,7 @@ int Engine::solve(double h, const double *rhs, double *x_out)
 int Engine::prepare_solver(double h)
 {
     if (prm.solver == SDDDST_SOLVER_GMRES_CLUSTER) return precond_build(*this, h, d_dvec);
+    if (prm.solver == SDDDST_SOLVER_DIRECT) return direct_factor(*this, h, d_dvec);
     return 0;
 }
 

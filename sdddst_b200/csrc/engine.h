@@ -78,6 +78,9 @@ struct Engine {
     long pc_binv_cap = 0;
     int pc_nb = 0;
 
+    // ---- sparse LU (direct.cu)
+    void *direct = nullptr;
+
     // ---- host scalars (SimulationData / Simulation members)
     double step_size = 1.0, sim_time = 0.0, strain = 0.0;
     double energy = 0.0, energy_accum = 0.0, vsquare = 0.0, vsquare1 = 0.0, vsquare2 = 0.0;
@@ -147,5 +150,13 @@ int precond_alloc(Engine &e);
 void precond_free(Engine &e);
 int precond_build(Engine &e, double h, const double *dvec);
 void precond_apply(Engine &e, const double *v, double *z);
+
+int direct_analyse(Engine &e, const double *x);
+int direct_factor(Engine &e, double h, const double *dvec);
+int direct_apply(Engine &e, const double *b, double *x);
+int direct_solve(Engine &e, double h, const double *dvec, const double *rhs, double *x);
+int direct_stats(const Engine &e, long *factorizations, long *perturbed, double *flops, long *front_doubles,
+                 int *fronts, int *depth);
+void direct_free(Engine &e);
 
 } // namespace sd

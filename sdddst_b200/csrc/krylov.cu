@@ -357,7 +357,7 @@ __global__ void normalize_kernel(int n, const double *__restrict__ w, const doub
 }
 
 // Restarted GMRES(m) on J(h) x = rhs, x0 = 0, right preconditioned
-// (precond 0: none, 1: diagonal, 2: cluster blocks).  Iterations run without
+// (precond 0: none, 1: diagonal, 2: cluster blocks, 3: sparse LU factors).  Iterations run without
 // host synchronisation; every `chk` iterations the Hessenberg columns come
 // back in one copy, the host applies the Givens rotations and tests
 // convergence (so at most chk-1 iterations past convergence are computed).
@@ -389,6 +389,10 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
         }
         if (precond == 2) {
             precond_apply(e, in, out);
+            return out;
+        }
+        if (precond == 3) {
+            direct_apply(e, in, out);
             return out;
         }
         return in;
@@ -479,10 +483,11 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
             yv[i] = s / H[(size_t)i * m + i];
         }
         cudaMemcpyAsync(e.d_y_small + n, yv.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st);
-        if (precond == 2) {
+        if (precond >= 2) {
             cudaMemsetAsync(r, 0, sizeof(double) * n, st);
             combine_kernel<<<nb, 256, 0, st>>>(n, k, V, ldv, e.d_y_small + n, nullptr, r);
-            precond_apply(e, r, z);
+            if (precond == 2) precond_apply(e, r, z);
+            else direct_apply(e, r, z);
             add_kernel<<<nb, 256, 0, st>>>(n, z, x);
             e.launches += 2;
         } else {
