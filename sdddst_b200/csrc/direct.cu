@@ -101,6 +101,11 @@ struct Direct {
     long factorizations = 0, perturbed = 0;
     int *h_buf = nullptr; // pinned
     int h_buf_cap = 0;
+    // lookahead: the pivot blocks of outer block J+1 are factored on a
+    // high-priority side stream while the main stream updates the rest of
+    // the trailing matrix of outer block J
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_side = nullptr, ev_next = nullptr, ev_level = nullptr;
 };
 
 Direct *D(Engine &e) { return static_cast<Direct *>(e.direct); }
@@ -377,7 +382,9 @@ __global__ void extend_add_kernel(const FrontInfo *__restrict__ fr, const int *_
 
 // LU of the diagonal block of pivot block j (row pivoting inside the block),
 // its triangular inverses, and the block-local row permutation
-__global__ void __launch_bounds__(256) diag_block_kernel(const FrontInfo *__restrict__ fr, const int *__restrict__ list,
+constexpr int kDiagThreads = 256;
+
+__global__ void __launch_bounds__(kDiagThreads) diag_block_kernel(const FrontInfo *__restrict__ fr, const int *__restrict__ list,
                                                          int j, double *__restrict__ F, double *__restrict__ inv,
                                                          int *__restrict__ perm, int *__restrict__ npert)
 {
@@ -395,9 +402,9 @@ __global__ void __launch_bounds__(256) diag_block_kernel(const FrontInfo *__rest
     double *Ff = F + f.foff;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     double amax = 0.0;
-    for (int idx = tid; idx < b * b; idx += 256) {
-        const int r = idx / b, c = idx % b;
-        const double v = Ff[(long)(s + r) * f.ld + s + c];
+    for (int idx = tid; idx < kNB * kNB; idx += 256) {
+        const int r = idx >> 6, c = idx & 63;
+        const double v = (r < b && c < b) ? Ff[(long)(s + r) * f.ld + s + c] : 0.0;
         Dm[r][c] = v;
         amax = fmax(amax, fabs(v));
     }
@@ -455,10 +462,10 @@ __global__ void __launch_bounds__(256) diag_block_kernel(const FrontInfo *__rest
         if (tid == 0) Dm[c][c] = d;
         for (int r = c + 1 + tid; r < b; r += 256) Dm[r][c] /= d;
         __syncthreads();
-        const int m = b - c - 1;
-        for (int idx = tid; idx < m * m; idx += 256) {
-            const int r = c + 1 + idx / m, cc = c + 1 + idx % m;
-            Dm[r][cc] -= Dm[r][c] * Dm[c][cc];
+        // rank-1 update on a 16 x 16 thread grid (no index division)
+        for (int r = c + 1 + (tid >> 4); r < b; r += 16) {
+            const double l = Dm[r][c];
+            for (int cc = c + 1 + (tid & 15); cc < b; cc += 16) Dm[r][cc] = fma(-l, Dm[c][cc], Dm[r][cc]);
         }
         __syncthreads();
         if (tid == 0 && pert) {
@@ -489,9 +496,9 @@ __global__ void __launch_bounds__(256) diag_block_kernel(const FrontInfo *__rest
         }
     }
     __syncthreads();
-    for (int idx = tid; idx < b * b; idx += 256) {
-        const int r = idx / b, c = idx % b;
-        Ff[(long)(s + r) * f.ld + s + c] = Dm[r][c];
+    for (int idx = tid; idx < kNB * kNB; idx += 256) {
+        const int r = idx >> 6, c = idx & 63;
+        if (r < b && c < b) Ff[(long)(s + r) * f.ld + s + c] = Dm[r][c];
     }
     double *L = inv + f.ioff + (long)j * 2 * kNB * kNB;
     double *U = L + kNB * kNB;
@@ -503,21 +510,35 @@ __global__ void __launch_bounds__(256) diag_block_kernel(const FrontInfo *__rest
     if (tid < b) perm[f.start + s + tid] = pv[tid];
 }
 
-// U12 = L11^-1 P A12 (first half of the grid) and L21 = A21 U11^-1 (second half)
+// Pivot block j's row panel U12 = L11^-1 P A12 over a column range (the first
+// `uhalf` CTAs of the grid, 64 columns each) and its column panel
+// L21 = A21 U11^-1 for rows e..n (the other CTAs, when `lrows` is set).
+// Column ranges of the U12 part: umode 1: [e, e1), up to the end of the
+// 128-pivot outer block; umode 2: [e1, n), deferred until the outer block's
+// second pivot block is factored; umode 3: [e, n).
 __global__ void __launch_bounds__(256) panel_kernel(const FrontInfo *__restrict__ fr, const int *__restrict__ list,
                                                     int j, double *__restrict__ F, const double *__restrict__ inv,
-                                                    const int *__restrict__ perm, int half)
+                                                    const int *__restrict__ perm, int umode, int uhalf, int lrows)
 {
     const FrontInfo f = fr[list[blockIdx.y]];
     const int s = j * kNB;
     if (s >= f.p) return;
-    const int b = min(kNB, f.p - s), e = s + b, m = f.n - e;
-    if (m <= 0) return;
-    const bool upper = (int)blockIdx.x < half;
-    const int tile = upper ? blockIdx.x : blockIdx.x - half;
+    const int b = min(kNB, f.p - s), e = s + b;
+    const int e1 = min(f.p, (j >> 1) * 2 * kNB + 2 * kNB);
+    const bool upper = (int)blockIdx.x < uhalf;
+    int lo, hi;
+    if (upper) {
+        lo = umode == 2 ? e1 : e;
+        hi = umode == 1 ? e1 : f.n;
+    } else {
+        if (!lrows) return;
+        lo = e;
+        hi = f.n;
+    }
+    const int tile = upper ? blockIdx.x : blockIdx.x - uhalf;
     const int t0 = tile * kNB;
-    if (t0 >= m) return;
-    const int cnt = min(kNB, m - t0);
+    if (lo + t0 >= hi) return;
+    const int cnt = min(kNB, hi - lo - t0);
     extern __shared__ double sm[];
     double(*Xs)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
     double(*As)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm + kNB * (kNB + 1));
@@ -529,12 +550,12 @@ __global__ void __launch_bounds__(256) panel_kernel(const FrontInfo *__restrict_
     if (upper) {
         for (int idx = tid; idx < kNB * kNB; idx += 256) {
             const int k = idx / kNB, c = idx % kNB;
-            As[k][c] = (k < b && c < cnt) ? Ff[(long)(s + perm[f.start + s + k]) * f.ld + e + t0 + c] : 0.0;
+            As[k][c] = (k < b && c < cnt) ? Ff[(long)(s + perm[f.start + s + k]) * f.ld + lo + t0 + c] : 0.0;
         }
     } else {
         for (int idx = tid; idx < kNB * kNB; idx += 256) {
             const int r = idx / kNB, k = idx % kNB;
-            As[r][k] = (r < cnt && k < b) ? Ff[(long)(e + t0 + r) * f.ld + s + k] : 0.0;
+            As[r][k] = (r < cnt && k < b) ? Ff[(long)(lo + t0 + r) * f.ld + s + k] : 0.0;
         }
     }
     __syncthreads();
@@ -563,7 +584,7 @@ __global__ void __launch_bounds__(256) panel_kernel(const FrontInfo *__restrict_
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const int i = ty * 4 + a, cc = tx + 16 * c;
-                if (i < b && cc < cnt) Ff[(long)(s + i) * f.ld + e + t0 + cc] = acc[a][c];
+                if (i < b && cc < cnt) Ff[(long)(s + i) * f.ld + lo + t0 + cc] = acc[a][c];
             }
     } else {
         // R[r][jj] = sum_k A[r][k] Uinv[k][jj]
@@ -583,68 +604,112 @@ __global__ void __launch_bounds__(256) panel_kernel(const FrontInfo *__restrict_
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const int r = ty * 4 + a, jj = tx + 16 * c;
-                if (r < cnt && jj < b) Ff[(long)(e + t0 + r) * f.ld + s + jj] = acc[a][c];
+                if (r < cnt && jj < b) Ff[(long)(lo + t0 + r) * f.ld + s + jj] = acc[a][c];
             }
     }
 }
 
-// trailing update F[e:, e:] -= L21 U12: 128 x 128 tiles, 8 x 8 outputs per thread
+// Updates of the trailing matrix by outer block J (pivot blocks 2J and 2J+1,
+// columns [s0, e0) and [e0, e1)):
+//   mode 0: rows [e0, n) x columns [e0, e1), K = [s0, e0)  (second pivot block's columns);
+//   mode 1: rows [e0, e1) x columns [e1, n), K = [s0, e0)  (second pivot block's rows);
+//   mode 2: rows [e1, n) x columns [e1, s0 + 256), K = [s0, e1)  (the next outer block's columns);
+//   mode 3: rows [e1, n) x columns [s0 + 256, n), K = [s0, e1)  (the rest of the trailing matrix).
+// 128 x 128 tiles, 8 x 8 outputs per thread; K in chunks of 16 double-buffered
+// in shared memory by cp.async (8-byte copies, zero-filled outside the
+// ranges); the accumulators start from C (independent loads in flight with
+// the first copy), so C is read and written once per outer block.
 constexpr int kBM = 128, kBK = 16, kPad = 2;
+constexpr size_t kUpdateSmem = 2 * 2 * kBK * (kBM + kPad) * sizeof(double);
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool pred)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    const int sz = pred ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 __global__ void __launch_bounds__(256, 1) update_kernel(const FrontInfo *__restrict__ fr, const int *__restrict__ list,
-                                                        int j, double *__restrict__ F)
+                                                        int J, int mode, double *__restrict__ F)
 {
     const FrontInfo f = fr[list[blockIdx.y]];
-    const int s = j * kNB;
+    const int s = J * 2 * kNB;
     if (s >= f.p) return;
-    const int b = min(kNB, f.p - s), e = s + b, m = f.n - e;
-    if (m <= 0) return;
-    const int tiles = (m + kBM - 1) / kBM;
-    if ((int)blockIdx.x >= tiles * tiles) return;
-    const int row0 = e + (blockIdx.x / tiles) * kBM, col0 = e + (blockIdx.x % tiles) * kBM;
-    __shared__ __align__(16) double As[kBK][kBM + kPad];
-    __shared__ __align__(16) double Bs[kBK][kBM + kPad];
+    const int e0 = s + min(kNB, f.p - s), e1 = min(f.p, s + 2 * kNB);
+    int rlo, rhi, clo, chi, kend;
+    if (mode == 0) {
+        rlo = e0; rhi = f.n; clo = e0; chi = e1; kend = e0;
+    } else if (mode == 1) {
+        rlo = e0; rhi = e1; clo = e1; chi = f.n; kend = e0;
+    } else if (mode == 2) {
+        rlo = e1; rhi = f.n; clo = e1; chi = min(f.n, s + 4 * kNB); kend = e1;
+    } else {
+        rlo = e1; rhi = f.n; clo = s + 4 * kNB; chi = f.n; kend = e1;
+    }
+    if (rlo >= rhi || clo >= chi) return;
+    const int b = kend - s;
+    const int tm = (rhi - rlo + kBM - 1) / kBM, tn = (chi - clo + kBM - 1) / kBM;
+    if ((int)blockIdx.x >= tm * tn) return;
+    const int row0 = rlo + (blockIdx.x / tn) * kBM, col0 = clo + (blockIdx.x % tn) * kBM;
+    extern __shared__ __align__(16) double smu[];
+    typedef double Tile[kBK][kBM + kPad];
+    Tile *As = reinterpret_cast<Tile *>(smu);
+    Tile *Bs = reinterpret_cast<Tile *>(smu + 2 * kBK * (kBM + kPad));
     double *Ff = F + f.foff;
     const long ld = f.ld;
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    double acc[8][8];
-#pragma unroll
-    for (int a = 0; a < 8; ++a)
-#pragma unroll
-        for (int c = 0; c < 8; ++c) acc[a][c] = 0.0;
-    double ra[8], rb[8];
-    auto load = [&](int k0) {
+    // thread tid copies A rows (tid >> 4) + 16 q, column tid & 15, and B rows
+    // (tid >> 7) + 2 q, column tid & 127, of each chunk (q = 0..7)
+    const int ar = tid >> 4, ak = tid & 15, bk = tid >> 7, bc = tid & 127;
+    const double *gA = Ff + (long)(row0 + ar) * ld + s + ak;
+    const double *gB = Ff + (long)(s + bk) * ld + col0 + bc;
+    const bool colB_ok = col0 + bc < chi;
+    auto issue = [&](int buf, int k0) {
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            const int idx = tid + 256 * q;
-            const int r = idx >> 4, k = idx & 15;
-            ra[q] = (row0 + r < f.n && k0 + k < b) ? Ff[(long)(row0 + r) * ld + s + k0 + k] : 0.0;
-            const int kb = idx >> 7, c = idx & 127;
-            rb[q] = (k0 + kb < b && col0 + c < f.n) ? Ff[(long)(s + k0 + kb) * ld + col0 + c] : 0.0;
+            const bool pa = row0 + ar + 16 * q < rhi && k0 + ak < b;
+            cp_async8(&As[buf][ak][ar + 16 * q], pa ? gA + (long)16 * q * ld + k0 : Ff, pa);
+            const bool pb = k0 + bk + 2 * q < b && colB_ok;
+            cp_async8(&Bs[buf][bk + 2 * q][bc], pb ? gB + (long)(k0 + 2 * q) * ld : Ff, pb);
         }
+        cp_async_commit();
     };
     const int nk = (b + kBK - 1) / kBK;
-    load(0);
-    for (int kc = 0; kc < nk; ++kc) {
+    issue(0, 0);
+    double acc[8][8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int idx = tid + 256 * q;
-            As[idx & 15][idx >> 4] = ra[q];
-            Bs[idx >> 7][idx & 127] = rb[q];
+    for (int a = 0; a < 8; ++a) {
+        const int r = row0 + (a < 4 ? ty * 4 + a : 64 + ty * 4 + a - 4);
+        const double *row = Ff + (long)min(r, rhi - 1) * ld;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int cc = col0 + (c < 4 ? tx * 4 + c : 64 + tx * 4 + c - 4);
+            acc[a][c] = (r < rhi && cc < chi) ? row[cc] : 0.0;
+        }
+    }
+    for (int kc = 0; kc < nk; ++kc) {
+        if (kc + 1 < nk) {
+            issue((kc + 1) & 1, (kc + 1) * kBK);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
-        if (kc + 1 < nk) load((kc + 1) * kBK);
+        const Tile &A = As[kc & 1];
+        const Tile &B = Bs[kc & 1];
 #pragma unroll
         for (int k = 0; k < kBK; ++k) {
             double av[8], bv[8];
-            const double2 a0 = *reinterpret_cast<const double2 *>(&As[k][ty * 4]);
-            const double2 a1 = *reinterpret_cast<const double2 *>(&As[k][ty * 4 + 2]);
-            const double2 a2 = *reinterpret_cast<const double2 *>(&As[k][64 + ty * 4]);
-            const double2 a3 = *reinterpret_cast<const double2 *>(&As[k][64 + ty * 4 + 2]);
-            const double2 b0 = *reinterpret_cast<const double2 *>(&Bs[k][tx * 4]);
-            const double2 b1 = *reinterpret_cast<const double2 *>(&Bs[k][tx * 4 + 2]);
-            const double2 b2 = *reinterpret_cast<const double2 *>(&Bs[k][64 + tx * 4]);
-            const double2 b3 = *reinterpret_cast<const double2 *>(&Bs[k][64 + tx * 4 + 2]);
+            const double2 a0 = *reinterpret_cast<const double2 *>(&A[k][ty * 4]);
+            const double2 a1 = *reinterpret_cast<const double2 *>(&A[k][ty * 4 + 2]);
+            const double2 a2 = *reinterpret_cast<const double2 *>(&A[k][64 + ty * 4]);
+            const double2 a3 = *reinterpret_cast<const double2 *>(&A[k][64 + ty * 4 + 2]);
+            const double2 b0 = *reinterpret_cast<const double2 *>(&B[k][tx * 4]);
+            const double2 b1 = *reinterpret_cast<const double2 *>(&B[k][tx * 4 + 2]);
+            const double2 b2 = *reinterpret_cast<const double2 *>(&B[k][64 + tx * 4]);
+            const double2 b3 = *reinterpret_cast<const double2 *>(&B[k][64 + tx * 4 + 2]);
             av[0] = a0.x; av[1] = a0.y; av[2] = a1.x; av[3] = a1.y;
             av[4] = a2.x; av[5] = a2.y; av[6] = a3.x; av[7] = a3.y;
             bv[0] = b0.x; bv[1] = b0.y; bv[2] = b1.x; bv[3] = b1.y;
@@ -652,18 +717,19 @@ __global__ void __launch_bounds__(256, 1) update_kernel(const FrontInfo *__restr
 #pragma unroll
             for (int a = 0; a < 8; ++a)
 #pragma unroll
-                for (int c = 0; c < 8; ++c) acc[a][c] = fma(av[a], bv[c], acc[a][c]);
+                for (int c = 0; c < 8; ++c) acc[a][c] = fma(-av[a], bv[c], acc[a][c]);
         }
         __syncthreads();
     }
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
         const int r = row0 + (a < 4 ? ty * 4 + a : 64 + ty * 4 + a - 4);
-        if (r >= f.n) continue;
+        if (r >= rhi) continue;
+        double *row = Ff + (long)r * ld;
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
             const int cc = col0 + (c < 4 ? tx * 4 + c : 64 + tx * 4 + c - 4);
-            if (cc < f.n) Ff[(long)r * ld + cc] -= acc[a][c];
+            if (cc < chi) row[cc] = acc[a][c];
         }
     }
 }
@@ -938,6 +1004,12 @@ void direct_free(Engine &e)
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (d->h_buf) cudaFreeHost(d->h_buf);
+    if (d->side) {
+        cudaStreamSynchronize(d->side);
+        cudaStreamDestroy(d->side);
+    }
+    for (cudaEvent_t ev : {d->ev_side, d->ev_next, d->ev_level})
+        if (ev) cudaEventDestroy(ev);
     delete d;
     e.direct = nullptr;
 }
@@ -1089,6 +1161,18 @@ int direct_factor(Engine &e, double h, const double *dvec)
     cudaStream_t st = e.st;
     cudaFuncSetAttribute(diag_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem);
     cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmem);
+    cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmem);
+    if (!d.side) {
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        if (cudaStreamCreateWithPriority(&d.side, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+            cudaEventCreateWithFlags(&d.ev_side, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&d.ev_next, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&d.ev_level, cudaEventDisableTiming) != cudaSuccess) {
+            e.err = "direct solver: stream or event creation failed";
+            return SDDDST_ERR_CUDA;
+        }
+    }
     cudaMemsetAsync(d.d_F, 0, sizeof(double) * (size_t)d.F_used, st);
     cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
     cudaMemsetAsync(d.d_npert, 0, sizeof(int), st);
@@ -1111,20 +1195,38 @@ int direct_factor(Engine &e, double h, const double *dvec)
                 extend_add_kernel<<<dim3(tiles * tiles, nf), 256, 0, st>>>(d.d_fr, list, slot, d.d_F, d.d_map);
             e.launches += 2;
         }
-        const int nblk = (d.level_pmax[l] + kNB - 1) / kNB;
-        for (int j = 0; j < nblk; ++j) {
-            diag_block_kernel<<<dim3(1, nf), 256, kDiagSmem, st>>>(d.d_fr, list, j, d.d_F, d.d_inv, d.d_perm,
-                                                                   d.d_npert);
-            const int rest = d.level_nmax[l] - j * kNB;
+        // outer blocks of 128 pivots: two pivot blocks of 64, the trailing
+        // update once per outer block (K = 128).  The side stream factors
+        // outer block J's pivot blocks (they need only the columns of J that
+        // outer block J-1's mode-2 update produced) while the main stream
+        // still updates the rest of the trailing matrix (mode 3 of J-1).
+        cudaEventRecord(d.ev_level, st);
+        cudaStreamWaitEvent(d.side, d.ev_level, 0);
+        const int nouter = (d.level_pmax[l] + 2 * kNB - 1) / (2 * kNB);
+        for (int J = 0; J < nouter; ++J) {
+            const int j0 = 2 * J, j1 = j0 + 1;
+            const int rest = std::max(1, d.level_nmax[l] - J * 2 * kNB); // bounds every row / column count below
             const int half = (rest + kNB - 1) / kNB;
-            if (half > 0) {
-                panel_kernel<<<dim3(2 * half, nf), 256, kPanelSmem, st>>>(d.d_fr, list, j, d.d_F, d.d_inv, d.d_perm,
-                                                                          half);
-                const int tiles = (rest + kBM - 1) / kBM;
-                update_kernel<<<dim3(tiles * tiles, nf), 256, 0, st>>>(d.d_fr, list, j, d.d_F);
-                e.launches += 2;
-            }
-            e.launches++;
+            const int tiles = (rest + kBM - 1) / kBM;
+            if (J > 0) cudaStreamWaitEvent(d.side, d.ev_next, 0);
+            diag_block_kernel<<<dim3(1, nf), kDiagThreads, kDiagSmem, d.side>>>(d.d_fr, list, j0, d.d_F, d.d_inv,
+                                                                                d.d_perm, d.d_npert);
+            panel_kernel<<<dim3(1 + half, nf), 256, kPanelSmem, d.side>>>(d.d_fr, list, j0, d.d_F, d.d_inv,
+                                                                         d.d_perm, 1, 1, 1);
+            update_kernel<<<dim3(tiles, nf), 256, kUpdateSmem, d.side>>>(d.d_fr, list, J, 0, d.d_F);
+            diag_block_kernel<<<dim3(1, nf), kDiagThreads, kDiagSmem, d.side>>>(d.d_fr, list, j1, d.d_F, d.d_inv,
+                                                                                d.d_perm, d.d_npert);
+            cudaEventRecord(d.ev_side, d.side);
+            cudaStreamWaitEvent(st, d.ev_side, 0);
+            panel_kernel<<<dim3(half, nf), 256, kPanelSmem, st>>>(d.d_fr, list, j0, d.d_F, d.d_inv, d.d_perm, 2,
+                                                                 half, 0);
+            update_kernel<<<dim3(tiles, nf), 256, kUpdateSmem, st>>>(d.d_fr, list, J, 1, d.d_F);
+            panel_kernel<<<dim3(2 * half, nf), 256, kPanelSmem, st>>>(d.d_fr, list, j1, d.d_F, d.d_inv, d.d_perm,
+                                                                     3, half, 1);
+            update_kernel<<<dim3(2 * tiles, nf), 256, kUpdateSmem, st>>>(d.d_fr, list, J, 2, d.d_F);
+            cudaEventRecord(d.ev_next, st);
+            update_kernel<<<dim3(tiles * tiles, nf), 256, kUpdateSmem, st>>>(d.d_fr, list, J, 3, d.d_F);
+            e.launches += 9;
         }
     }
     int hv[2];
