@@ -11,10 +11,12 @@ step and two half steps, each with a Jacobian solve, the error estimate and
 accept/reject; value = accepted steps / device time of the K timed attempts.
 
 The main line is the mixed-precision path (FP32 pair terms with FP64
-accumulation, FP64 positions, Jacobian, error ratio and GMRES solve); the
-plain FP64 path is timed beside it (``plain_fp64``) and its position
-difference after one step from the same state is reported
-(``position_error_vs_fp64``).  Inputs are device-resident when the timed
+accumulation, FP64 positions, error ratio and GMRES solve preconditioned by
+cluster block-Jacobi); the plain FP64 drop-in (FP64 pair sum, FP64 Jacobian,
+device sparse LU in place of UMFPACK) is timed beside it (``plain_fp64``,
+with the LU's factorization time and FP64 flop rate under ``lu``) and the
+mixed path's position difference after one step from the same state is
+reported (``position_error_vs_fp64``).  Inputs are device-resident when the timed
 region starts; between timed steps a 256 MiB buffer is written to flush L2.
 ``e2e`` repeats the measurement through the C ABI with the state crossing
 host<->device every step (pinned host buffers).
@@ -135,11 +137,12 @@ def _vector_peaks(device):
         return {}
 
 
-def make_engine(n, pairsum, device):
+def make_engine(n, pairsum, device, solver=None):
     from sdddst_b200 import capi, workloads
     xyb, _ = workloads.dislocations(n, SEED)
+    extra = {} if solver is None else {"solver": solver}
     prm = capi.cli_params(n, CUTOFF_M, PREC, step_size=H0, device=device,
-                          pairsum=capi.PAIRSUM_FP32 if pairsum == "fp32" else capi.PAIRSUM_FP64)
+                          pairsum=capi.PAIRSUM_FP32 if pairsum == "fp32" else capi.PAIRSUM_FP64, **extra)
     return capi.Engine(prm, xyb), xyb
 
 
@@ -410,10 +413,26 @@ def main():
     plain = None
     pos_err = None
     if not args.no_plain:
-        eng_p, _ = make_engine(args.n, "fp64", local)
-        p_ms, p_acc, _ = time_steps(torch, eng_p, max(2, args.steps // 2), max(1, args.warmup - 1), flush)
+        # the plain drop-in: FP64 pair sum, FP64 Jacobian, device sparse LU
+        from sdddst_b200 import capi
+        eng_p, _ = make_engine(args.n, "fp64", local, solver=capi.SOLVER_DIRECT)
+        p_steps = max(3, args.steps // 2)
+        p_ms, p_acc, p_launch = time_steps(torch, eng_p, p_steps, 3, flush)
         plain = {"value": p_acc / (p_ms * 1e-3) if p_ms > 0 else 0.0, "unit": UNIT,
-                 "ms_per_step": p_ms / max(2, args.steps // 2), "steps": max(2, args.steps // 2)}
+                 "ms_per_step": p_ms / p_steps, "steps": p_steps, "accepted": p_acc, "gpu_launches": p_launch,
+                 "pairsum": "fp64", "solver": "sparse LU fp64 (multifrontal, nested dissection), refined to 1e-13"}
+        try:
+            h_now = eng_p.scalars()["step_size"]
+            f_ms, s_ms = eng_p.profile_direct(h_now, 2)
+            st = eng_p.direct_stats()
+            f64 = vp.get("fp64_tflops") or 40.0
+            ach = st["lu_flops"] / (f_ms * 1e-3) / 1e12 if f_ms > 0 else 0.0
+            plain["lu"] = {"bound": "fp64", "flops_per_factorization": st["lu_flops"], "factor_ms": f_ms,
+                           "solve_ms": s_ms, "achieved": ach, "peak": f64, "unit": "TFLOP/s", "frac": ach / f64,
+                           "fronts": st["fronts"], "tree_depth": st["depth"],
+                           "front_gb": st["front_doubles"] * 8 / 1e9, "perturbed_pivots": st["perturbed_pivots"]}
+        except Exception as ex:
+            plain["lu"] = {"error": str(ex)[:200]}
         if args.pairsum == "fp32":
             err, same = position_error(eng, eng_p)
             pos_err = {"max_abs": err, "same_decision": same}
@@ -440,7 +459,8 @@ def main():
         "ms_per_step": total_ms / max(1, args.steps), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64" if args.pairsum == "fp32" else "f64", "data": "synthetic",
         "config": {"workload": f"n{args.n}_m{CUTOFF_M}_seed{SEED}", "N": args.n, "cutoff_multiplier": CUTOFF_M,
-                   "prec": PREC, "initial_step": H0, "pairsum": args.pairsum, "solver": "gmres(30) fp64",
+                   "prec": PREC, "initial_step": H0, "pairsum": args.pairsum,
+                   "solver": "gmres(30) fp64, cluster block-Jacobi preconditioner",
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas" if ws > 1 else "none",
                    "accepted": accepted, "attempts": args.steps, "final_step_size": sc["step_size"],
                    "solver_stats": solver_stats},

@@ -247,6 +247,15 @@ int sdddst_solver_stats(void *ctx, long *solves, long *iterations);
 int sdddst_direct_stats(void *ctx, long *factorizations, long *perturbed, double *flops, long *front_doubles,
                         int *fronts, int *depth);
 
+/* Diagnostic timing of the sparse LU (SDDDST_SOLVER_DIRECT contexts): the
+ * Jacobian J(h) at the accepted configuration is assembled and analysed,
+ * factored once untimed, then factored `reps` times and solved `reps` times
+ * with CUDA events on the context's stream; writes the mean device
+ * milliseconds of one factorization and of one forward/backward solve.
+ * Stands in for timing UMFPACK's numeric factorization and solve
+ * (simulation.cpp:386-396). */
+int sdddst_profile_direct(void *ctx, double h, int reps, double *factor_ms, double *solve_ms);
+
 /* ---- Batches of independent systems (a population of random realisations).
  * `count` systems of sizes[k] dislocations, concatenated in xyb (sum of sizes
  * rows of {x, y, b}), share the parameters of `common` (n, p and the stress

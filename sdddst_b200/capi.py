@@ -37,7 +37,7 @@ EXPORTS = [
     "sdddst_speeds_noalloc", "sdddst_solver_stats", "sdddst_speeds_ext", "sdddst_set_scalars",
     "sdddst_update_params", "sdddst_solve_csc", "sdddst_batch_create", "sdddst_batch_destroy",
     "sdddst_batch_step", "sdddst_batch_get_scalars", "sdddst_batch_get_positions", "sdddst_batch_info",
-    "sdddst_direct_stats",
+    "sdddst_direct_stats", "sdddst_profile_direct",
 ]
 
 
@@ -111,6 +111,8 @@ def load(path: str = LIB_PATH):
     lib.sdddst_direct_stats.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long),
                                         C.POINTER(C.c_double), C.POINTER(C.c_long), C.POINTER(C.c_int),
                                         C.POINTER(C.c_int)]
+    lib.sdddst_profile_direct.argtypes = [C.c_void_p, C.c_double, C.c_int, C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double)]
     lib.sdddst_kernel_launches.argtypes = [C.c_void_p]
     lib.sdddst_kernel_launches.restype = C.c_long
     _lib = lib
@@ -301,6 +303,13 @@ class Engine:
                                             C.byref(nf), C.byref(dp)))
         return {"factorizations": f.value, "perturbed_pivots": pp.value, "lu_flops": fl.value,
                 "front_doubles": fd.value, "fronts": nf.value, "depth": dp.value}
+
+    def profile_direct(self, h: float, reps: int = 2):
+        """Mean device milliseconds of one sparse-LU factorization of J(h)
+        at the accepted configuration and of one solve with it."""
+        f, s = C.c_double(0.0), C.c_double(0.0)
+        _check(self.lib.sdddst_profile_direct(self.h, float(h), int(reps), C.byref(f), C.byref(s)))
+        return f.value, s.value
 
     def launches(self) -> int:
         return int(self.lib.sdddst_kernel_launches(self.h))

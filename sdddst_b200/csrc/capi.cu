@@ -493,6 +493,43 @@ int sdddst_profile_pair_sum(void *ctx, int reps, double *ms_per_launch)
     return from_engine(e, rc);
 }
 
+int sdddst_profile_direct(void *ctx, double h, int reps, double *factor_ms, double *solve_ms)
+{
+    if (!ctx || !factor_ms || !solve_ms || reps < 1 || !(h > 0)) return fail(SDDDST_ERR_INVALID, "bad argument");
+    sd::Engine *e = E(ctx);
+    if (e->prm.solver != SDDDST_SOLVER_DIRECT) return fail(SDDDST_ERR_INVALID, "the context's solver is not the sparse LU");
+    cudaSetDevice(e->device);
+    try {
+        if (int rc = e->assemble(e->d_x0)) return from_engine(e, rc);
+        sd::launch_make_dvec(*e, h, e->d_dvec, e->st);
+        if (int rc = sd::direct_factor(*e, h, e->d_dvec)) return from_engine(e, rc); // warm-up
+        cudaEvent_t a, b, c;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventCreate(&c);
+        cudaEventRecord(a, e->st);
+        int rc = 0;
+        for (int r = 0; r < reps && !rc; ++r) rc = sd::direct_factor(*e, h, e->d_dvec);
+        cudaEventRecord(b, e->st);
+        for (int r = 0; r < reps && !rc; ++r) rc = sd::direct_apply(*e, e->d_v0, e->d_sol);
+        cudaEventRecord(c, e->st);
+        if (!rc) rc = e->sync_check("profile direct");
+        float m1 = 0.f, m2 = 0.f;
+        if (!rc) {
+            cudaEventElapsedTime(&m1, a, b);
+            cudaEventElapsedTime(&m2, b, c);
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        cudaEventDestroy(c);
+        *factor_ms = m1 / reps;
+        *solve_ms = m2 / reps;
+        return from_engine(e, rc);
+    } catch (const std::exception &ex) {
+        return fail(SDDDST_ERR_NOMEM, ex.what());
+    }
+}
+
 int sdddst_solver_stats(void *ctx, long *solves, long *iterations)
 {
     if (!ctx) return fail(SDDDST_ERR_INVALID, "null argument");
