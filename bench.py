@@ -18,6 +18,10 @@ with the LU's factorization time and FP64 flop rate under ``lu``) and the
 mixed path's position difference after one step from the same state is
 reported (``position_error_vs_fp64``).  Inputs are device-resident when the timed
 region starts; between timed steps a 256 MiB buffer is written to flush L2.
+``learned_precond`` and ``neumann_precond`` time the same mixed path with
+the GMRES preconditioner extended by the learned correction C (the
+message-passing network of sdddst_b200/learned.py, inferred on the device)
+and by its analytic first-order part alone.
 ``e2e`` repeats the measurement through the C ABI with the state crossing
 host<->device every step (pinned host buffers).
 
@@ -346,6 +350,7 @@ def main():
                     help="profiling target: launch only the pair-sum kernels (or only steps) and exit")
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-realisations measurement")
+    ap.add_argument("--no-variants", action="store_true", help="skip the preconditioner variants")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
@@ -438,6 +443,28 @@ def main():
             pos_err = {"max_abs": err, "same_decision": same}
         eng_p.close()
 
+    # the preconditioner variants of the same mixed path: cluster blocks plus
+    # the learned correction, and plus its analytic first-order part alone
+    variants = {}
+    if not args.no_variants:
+        from sdddst_b200 import capi
+        for name, solver in (("learned_precond", capi.SOLVER_GMRES_LEARNED),
+                             ("neumann_precond", capi.SOLVER_GMRES_NEUMANN)):
+            try:
+                ev, _ = make_engine(args.n, args.pairsum, local, solver=solver)
+                if solver == capi.SOLVER_GMRES_LEARNED:
+                    ev.set_preconditioner_weights()
+                v_steps = max(3, args.steps // 2)
+                v_ms, v_acc, v_launch = time_steps(torch, ev, v_steps, 3, flush)
+                st = time_steps.last_solver
+                variants[name] = {"value": v_acc / (v_ms * 1e-3) if v_ms > 0 else 0.0, "unit": UNIT,
+                                  "ms_per_step": v_ms / v_steps, "steps": v_steps, "accepted": v_acc,
+                                  "gpu_launches": v_launch,
+                                  "gmres_iterations_per_solve": st["iterations"] / max(1, st["solves"])}
+                ev.close()
+            except Exception as ex:
+                variants[name] = {"error": str(ex)[:200]}
+
     batch = None
     if not args.no_batch:
         try:
@@ -463,12 +490,14 @@ def main():
                    "solver": "gmres(30) fp64, cluster block-Jacobi preconditioner",
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas" if ws > 1 else "none",
                    "accepted": accepted, "attempts": args.steps, "final_step_size": sc["step_size"],
-                   "solver_stats": solver_stats},
+                   "solver_stats": solver_stats,
+                   "gmres_iterations_per_solve": solver_stats["iterations"] / max(1, solver_stats["solves"])},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "roofline": roof,
         "clocks": clk,
         "plain_fp64": plain,
+        **variants,
         "position_error_vs_fp64": pos_err,
         "batch_512": batch,
         "cpu_baseline": cpu,

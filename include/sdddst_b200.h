@@ -57,7 +57,12 @@ enum {
     SDDDST_SOLVER_GMRES = 0,         /* restarted GMRES, FP64, unpreconditioned */
     SDDDST_SOLVER_GMRES_JACOBI = 1,  /* restarted GMRES, FP64, diagonal preconditioner */
     SDDDST_SOLVER_GMRES_CLUSTER = 2, /* restarted GMRES, FP64, block-Jacobi on strongly coupled clusters */
-    SDDDST_SOLVER_DIRECT = 3         /* sparse LU (multifrontal, nested dissection), FP64, refined to solver_tol */
+    SDDDST_SOLVER_DIRECT = 3,        /* sparse LU (multifrontal, nested dissection), FP64, refined to solver_tol */
+    SDDDST_SOLVER_GMRES_LEARNED = 4, /* restarted GMRES, FP64, cluster block-Jacobi plus a learned correction on
+                                        J's pattern (weights: sdddst_set_preconditioner_weights); falls back to
+                                        the sparse LU when GMRES stalls */
+    SDDDST_SOLVER_GMRES_NEUMANN = 5  /* as SDDDST_SOLVER_GMRES_LEARNED with the analytic first-order
+                                        block-Neumann correction in place of the network */
 };
 
 /* Field kernels (Field plug-in): the analytic periodic field
@@ -255,6 +260,25 @@ int sdddst_direct_stats(void *ctx, long *factorizations, long *perturbed, double
  * Stands in for timing UMFPACK's numeric factorization and solve
  * (simulation.cpp:386-396). */
 int sdddst_profile_direct(void *ctx, double h, int reps, double *factor_ms, double *solve_ms);
+
+/* Applies the cluster block-Jacobi preconditioner of J(h) at the accepted
+ * configuration to k device vectors (in_device, out_device: k x n doubles,
+ * vector q at offset q n) and, when block_of_device is not null, writes each
+ * dislocation's block index (n ints, device).  Produces the training data of
+ * the learned preconditioner; no counterpart in the reference. */
+int sdddst_precond_apply(void *ctx, double h, int k, const double *in_device, double *out_device,
+                         int *block_of_device);
+
+/* Weights of the learned preconditioner correction (SDDDST_SOLVER_GMRES_LEARNED):
+ * `count` BF16 bit patterns in the flat order of sdddst_b200/learned.py
+ * (59522 for the shipped network); SDDDST_ERR_INVALID on another count.  No
+ * counterpart in the reference. */
+int sdddst_set_preconditioner_weights(void *ctx, const unsigned short *bf16, long count);
+
+/* The learned correction C for J(h) at the accepted configuration: `nnz`
+ * floats aligned with the CSR of sdddst_jacobian (diagonal in each row's
+ * first slot).  Requires loaded weights; no counterpart in the reference. */
+int sdddst_learned_correction(void *ctx, double h, float *values, long cap, long *nnz);
 
 /* ---- Batches of independent systems (a population of random realisations).
  * `count` systems of sizes[k] dislocations, concatenated in xyb (sum of sizes

@@ -26,6 +26,7 @@ ERR_NONFINITE = -6
 STRESS_ZERO, STRESS_FIXED_RATE, STRESS_SPRING, STRESS_CONSTANT = 0, 1, 2, 3
 PAIRSUM_FP64, PAIRSUM_FP32 = 0, 1
 SOLVER_GMRES, SOLVER_GMRES_JACOBI, SOLVER_GMRES_CLUSTER, SOLVER_DIRECT = 0, 1, 2, 3
+SOLVER_GMRES_LEARNED, SOLVER_GMRES_NEUMANN = 4, 5
 
 # Every extern "C" symbol of include/sdddst_b200.h.
 EXPORTS = [
@@ -37,7 +38,8 @@ EXPORTS = [
     "sdddst_speeds_noalloc", "sdddst_solver_stats", "sdddst_speeds_ext", "sdddst_set_scalars",
     "sdddst_update_params", "sdddst_solve_csc", "sdddst_batch_create", "sdddst_batch_destroy",
     "sdddst_batch_step", "sdddst_batch_get_scalars", "sdddst_batch_get_positions", "sdddst_batch_info",
-    "sdddst_direct_stats", "sdddst_profile_direct",
+    "sdddst_direct_stats", "sdddst_profile_direct", "sdddst_precond_apply", "sdddst_set_preconditioner_weights",
+    "sdddst_learned_correction",
 ]
 
 
@@ -113,6 +115,9 @@ def load(path: str = LIB_PATH):
                                         C.POINTER(C.c_int)]
     lib.sdddst_profile_direct.argtypes = [C.c_void_p, C.c_double, C.c_int, C.POINTER(C.c_double),
                                           C.POINTER(C.c_double)]
+    lib.sdddst_precond_apply.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.sdddst_set_preconditioner_weights.argtypes = [C.c_void_p, C.c_void_p, C.c_long]
+    lib.sdddst_learned_correction.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_long, C.POINTER(C.c_long)]
     lib.sdddst_kernel_launches.argtypes = [C.c_void_p]
     lib.sdddst_kernel_launches.restype = C.c_long
     _lib = lib
@@ -310,6 +315,33 @@ class Engine:
         f, s = C.c_double(0.0), C.c_double(0.0)
         _check(self.lib.sdddst_profile_direct(self.h, float(h), int(reps), C.byref(f), C.byref(s)))
         return f.value, s.value
+
+    def precond_apply(self, h: float, k: int, in_ptr: int, out_ptr: int, block_ptr: int = 0):
+        """Cluster preconditioner of J(h) at the accepted configuration applied
+        to k device vectors (raw device pointers, k x n doubles)."""
+        _check(self.lib.sdddst_precond_apply(self.h, float(h), int(k), C.c_void_p(in_ptr), C.c_void_p(out_ptr),
+                                             C.c_void_p(block_ptr) if block_ptr else None))
+
+    def set_preconditioner_weights(self, bf16=None):
+        """Loads the learned preconditioner's BF16 weights (uint16 bit
+        patterns; default: the shipped sdddst_b200/learned_weights.npz)."""
+        if bf16 is None:
+            from sdddst_b200 import learned
+            bf16 = learned.load_weights()
+        w = np.ascontiguousarray(bf16, dtype=np.uint16)
+        _check(self.lib.sdddst_set_preconditioner_weights(self.h, w.ctypes.data, int(w.size)))
+
+    def learned_correction(self, h: float) -> np.ndarray:
+        """Values of the learned correction C for J(h) at the accepted
+        configuration, aligned with the CSR of jacobian()."""
+        cap = C.c_long(0)
+        probe = np.zeros(1, dtype=np.float32)
+        rc = self.lib.sdddst_learned_correction(self.h, float(h), probe.ctypes.data, 0, C.byref(cap))
+        if rc not in (OK, ERR_CAPACITY):
+            _check(rc)
+        out = np.zeros(max(1, cap.value), dtype=np.float32)
+        _check(self.lib.sdddst_learned_correction(self.h, float(h), out.ctypes.data, out.size, C.byref(cap)))
+        return out[:cap.value]
 
     def launches(self) -> int:
         return int(self.lib.sdddst_kernel_launches(self.h))

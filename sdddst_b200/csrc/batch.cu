@@ -582,8 +582,9 @@ static int batch_init(Batch &bt, const sdddst_params &common, int count, const i
         }
         bt.off[k + 1] = bt.off[k] + sizes[k];
     }
-    if (common.solver == SDDDST_SOLVER_DIRECT) {
-        bt.e.err = "batch: the sparse LU solver serves single systems; choose a GMRES solver";
+    if (common.solver == SDDDST_SOLVER_DIRECT || common.solver == SDDDST_SOLVER_GMRES_LEARNED ||
+        common.solver == SDDDST_SOLVER_GMRES_NEUMANN) {
+        bt.e.err = "batch: the sparse LU and learned solvers serve single systems; choose another GMRES solver";
         return SDDDST_ERR_INVALID;
     }
     bt.ntot = bt.off[count];

@@ -98,7 +98,8 @@ int sdddst_ctx_create(const sdddst_params *prm, const double *xyb, const double 
     if (prm->pairsum != SDDDST_PAIRSUM_FP64 && prm->pairsum != SDDDST_PAIRSUM_FP32)
         return fail(SDDDST_ERR_INVALID, "unsupported pair-sum mode");
     if (prm->solver != SDDDST_SOLVER_GMRES && prm->solver != SDDDST_SOLVER_GMRES_JACOBI &&
-        prm->solver != SDDDST_SOLVER_GMRES_CLUSTER && prm->solver != SDDDST_SOLVER_DIRECT)
+        prm->solver != SDDDST_SOLVER_GMRES_CLUSTER && prm->solver != SDDDST_SOLVER_DIRECT &&
+        prm->solver != SDDDST_SOLVER_GMRES_LEARNED && prm->solver != SDDDST_SOLVER_GMRES_NEUMANN)
         return fail(SDDDST_ERR_INVALID, "unsupported solver");
     if (!(prm->prec > 0) || !(prm->step_size > 0) || !(prm->cutoff_multiplier > 0))
         return fail(SDDDST_ERR_INVALID, "prec, step size and cutoff multiplier must be positive");
@@ -525,6 +526,54 @@ int sdddst_profile_direct(void *ctx, double h, int reps, double *factor_ms, doub
         *factor_ms = m1 / reps;
         *solve_ms = m2 / reps;
         return from_engine(e, rc);
+    } catch (const std::exception &ex) {
+        return fail(SDDDST_ERR_NOMEM, ex.what());
+    }
+}
+
+int sdddst_precond_apply(void *ctx, double h, int k, const double *in_device, double *out_device,
+                         int *block_of_device)
+{
+    if (!ctx || !in_device || !out_device || k < 1 || !(h > 0)) return fail(SDDDST_ERR_INVALID, "bad argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    try {
+        if (int rc = e->assemble(e->d_x0)) return from_engine(e, rc);
+        sd::launch_make_dvec(*e, h, e->d_dvec, e->st);
+        if (int rc = sd::precond_build(*e, h, e->d_dvec)) return from_engine(e, rc);
+        for (int q = 0; q < k; ++q) sd::precond_apply(*e, in_device + (size_t)q * e->n, out_device + (size_t)q * e->n);
+        if (block_of_device)
+            cudaMemcpyAsync(block_of_device, e->pc_blk_of, sizeof(int) * e->n, cudaMemcpyDeviceToDevice, e->st);
+        return from_engine(e, e->sync_check("precond apply"));
+    } catch (const std::exception &ex) {
+        return fail(SDDDST_ERR_NOMEM, ex.what());
+    }
+}
+
+int sdddst_set_preconditioner_weights(void *ctx, const unsigned short *bf16, long count)
+{
+    if (!ctx || !bf16) return fail(SDDDST_ERR_INVALID, "null argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    return from_engine(e, sd::learned_set_weights(*e, bf16, count));
+}
+
+int sdddst_learned_correction(void *ctx, double h, float *values, long cap, long *nnz)
+{
+    if (!ctx || !values || !nnz || !(h > 0)) return fail(SDDDST_ERR_INVALID, "bad argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    try {
+        if (!e->learned) return fail(SDDDST_ERR_INVALID, "no learned preconditioner weights loaded");
+        if (!e->d_xasm && cudaMalloc(&e->d_xasm, sizeof(double) * e->n) != cudaSuccess)
+            return fail(SDDDST_ERR_NOMEM, "positions buffer");
+        if (int rc = e->assemble(e->d_x0)) return from_engine(e, rc);
+        cudaMemcpyAsync(e->d_xasm, e->d_x0, sizeof(double) * e->n, cudaMemcpyDeviceToDevice, e->st);
+        sd::launch_make_dvec(*e, h, e->d_dvec, e->st);
+        if (int rc = sd::precond_build(*e, h, e->d_dvec)) return from_engine(e, rc);
+        if (int rc = sd::learned_build(*e, h, e->d_dvec, e->d_xasm, false)) return from_engine(e, rc);
+        *nnz = e->nnz;
+        return from_engine(e, sd::learned_export(*e, values, cap));
     } catch (const std::exception &ex) {
         return fail(SDDDST_ERR_NOMEM, ex.what());
     }

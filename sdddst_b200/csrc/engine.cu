@@ -46,6 +46,8 @@ Engine::~Engine()
     if (d_counter) cudaFree(d_counter);
     precond_free(*this);
     direct_free(*this);
+    learned_free(*this);
+    if (d_xasm) cudaFree(d_xasm);
     if (st) cudaStreamDestroy(st);
 }
 
@@ -236,6 +238,13 @@ int Engine::assemble(const double *x)
 {
     int rc = jacobian_assemble(*this, x);
     if (rc == 0 && prm.solver == SDDDST_SOLVER_DIRECT) rc = direct_analyse(*this, x);
+    if (rc == 0 && (prm.solver == SDDDST_SOLVER_GMRES_LEARNED || prm.solver == SDDDST_SOLVER_GMRES_NEUMANN)) {
+        if (!d_xasm && cudaMalloc(&d_xasm, sizeof(double) * n) != cudaSuccess) {
+            err = "out of device memory";
+            return SDDDST_ERR_NOMEM;
+        }
+        cudaMemcpyAsync(d_xasm, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
+    }
     return rc;
 }
 
@@ -247,6 +256,16 @@ int Engine::assemble(const double *x)
 int Engine::solve(double h, const double *rhs, double *x_out)
 {
     if (prm.solver == SDDDST_SOLVER_DIRECT) return direct_solve(*this, h, d_dvec, rhs, x_out);
+    if (prm.solver == SDDDST_SOLVER_GMRES_LEARNED || prm.solver == SDDDST_SOLVER_GMRES_NEUMANN) {
+        // GMRES preconditioned by B + C; on a stall, the device sparse LU of
+        // the same matrix (analysed at the assembly positions)
+        int rc = gmres_solve(*this, h, d_dvec, rhs, x_out, 4);
+        if (rc != SDDDST_ERR_SOLVER) return rc;
+        stalls++;
+        if (int rc2 = direct_analyse(*this, d_xasm)) return rc2;
+        if (int rc2 = direct_factor(*this, h, d_dvec)) return rc2;
+        return direct_solve(*this, h, d_dvec, rhs, x_out);
+    }
     int precond = prm.solver == SDDDST_SOLVER_GMRES_JACOBI ? 1 : prm.solver == SDDDST_SOLVER_GMRES_CLUSTER ? 2 : 0;
     int rc = gmres_solve(*this, h, d_dvec, rhs, x_out, precond);
     if (rc != SDDDST_ERR_SOLVER || precond != 2) return rc;
@@ -271,6 +290,10 @@ int Engine::prepare_solver(double h)
 {
     if (prm.solver == SDDDST_SOLVER_GMRES_CLUSTER) return precond_build(*this, h, d_dvec);
     if (prm.solver == SDDDST_SOLVER_DIRECT) return direct_factor(*this, h, d_dvec);
+    if (prm.solver == SDDDST_SOLVER_GMRES_LEARNED || prm.solver == SDDDST_SOLVER_GMRES_NEUMANN) {
+        if (int rc = precond_build(*this, h, d_dvec)) return rc;
+        return learned_build(*this, h, d_dvec, d_xasm, prm.solver == SDDDST_SOLVER_GMRES_NEUMANN);
+    }
     return 0;
 }
 

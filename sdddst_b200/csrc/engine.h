@@ -81,6 +81,10 @@ struct Engine {
     // ---- sparse LU (direct.cu)
     void *direct = nullptr;
 
+    // ---- learned preconditioner correction (learned.cu)
+    void *learned = nullptr;
+    double *d_xasm = nullptr; // positions of the last assembly (learned features, LU fallback)
+
     // ---- host scalars (SimulationData / Simulation members)
     double step_size = 1.0, sim_time = 0.0, strain = 0.0;
     double energy = 0.0, energy_accum = 0.0, vsquare = 0.0, vsquare1 = 0.0, vsquare2 = 0.0;
@@ -158,5 +162,12 @@ int direct_solve(Engine &e, double h, const double *dvec, const double *rhs, dou
 int direct_stats(const Engine &e, long *factorizations, long *perturbed, double *flops, long *front_doubles,
                  int *fronts, int *depth);
 void direct_free(Engine &e);
+
+int learned_set_weights(Engine &e, const unsigned short *bf16, long count);
+int learned_build(Engine &e, double h, const double *dvec, const double *x, bool analytic);
+void learned_apply_add(Engine &e, const double *v, double *z);
+int learned_export(Engine &e, float *host, long cap);
+void learned_free(Engine &e);
+long learned_weight_count();
 
 } // namespace sd

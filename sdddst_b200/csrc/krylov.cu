@@ -357,7 +357,8 @@ __global__ void normalize_kernel(int n, const double *__restrict__ w, const doub
 }
 
 // Restarted GMRES(m) on J(h) x = rhs, x0 = 0, right preconditioned
-// (precond 0: none, 1: diagonal, 2: cluster blocks, 3: sparse LU factors).  Iterations run without
+// (precond 0: none, 1: diagonal, 2: cluster blocks, 3: sparse LU factors, 4: cluster
+// blocks plus the learned correction).  Iterations run without
 // host synchronisation; every `chk` iterations the Hessenberg columns come
 // back in one copy, the host applies the Givens rotations and tests
 // convergence (so at most chk-1 iterations past convergence are computed).
@@ -393,6 +394,11 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
         }
         if (precond == 3) {
             direct_apply(e, in, out);
+            return out;
+        }
+        if (precond == 4) {
+            precond_apply(e, in, out);
+            learned_apply_add(e, in, out);
             return out;
         }
         return in;
@@ -487,7 +493,11 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
             cudaMemsetAsync(r, 0, sizeof(double) * n, st);
             combine_kernel<<<nb, 256, 0, st>>>(n, k, V, ldv, e.d_y_small + n, nullptr, r);
             if (precond == 2) precond_apply(e, r, z);
-            else direct_apply(e, r, z);
+            else if (precond == 3) direct_apply(e, r, z);
+            else {
+                precond_apply(e, r, z);
+                learned_apply_add(e, r, z);
+            }
             add_kernel<<<nb, 256, 0, st>>>(n, z, x);
             e.launches += 2;
         } else {

@@ -1,0 +1,488 @@
+// Learned correction C of the cluster block-Jacobi preconditioner B: the
+// GMRES preconditioner of SDDDST_SOLVER_GMRES_LEARNED is M = B + C, C on the
+// sparsity pattern of J, its values from a message-passing network over the
+// cutoff-neighbour graph (hidden width 64, three rounds, ReLU).  Weights are
+// held in BF16 and converted on load; all arithmetic is FP32.
+//
+//   h_i  = relu(W_in f_i + b_in)
+//   3 x: m_ij = relu(P h_i + b_P + Q h_j + R e_ij), a_i = mean_j m_ij,
+//        h_i += relu(U [h_i; a_i] + b_U)
+//   c_ij = w_o . relu(P_o h_i + b_Po + Q_o h_j + R_o e_ij) + b_o - (1 - s_ij),  c_ii = w_d . h_i + b_d
+//   C_ij = c_ij A_ij / (J_ii J_jj),  C_ii = c_ii / J_ii,   J = I + A, A = diag((1+d)/2) h G
+// (s_ij = 1 when i and j share a cluster block; with zero output layers C is
+// the analytic first-order block-Neumann correction, which
+// SDDDST_SOLVER_GMRES_NEUMANN uses without the network)
+//
+// Features (t(v) = sign(v) log(1 + |v|)): node [t(A_ii), t(sum_j |A_ij|),
+// t(sum_j |A_ji|), deg / 627]; edge [t(A_ij), t(A_ji), dx / 7c, dy / 7c,
+// same cluster block].  The message function is linear in [h_i; h_j; e_ij]
+// before its activation, so it splits into per-node projections (P h, Q h:
+// N x 64 x 64 products, shared-memory tiled) and a per-edge sum over the
+// CSR rows (one warp per row, one or two channels per lane); no edge-sized
+// matrix product exists.  The flat weight order and the features follow
+// sdddst_b200/learned.py, the PyTorch definition the network was trained in.
+#include <cuda_bf16.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "engine.h"
+
+namespace sd {
+
+namespace {
+
+constexpr int kH = 64, kNF = 4, kEF = 5, kLayers = 3;
+constexpr float kDegScale = 627.0f, kPosScale = 7.0f;
+
+struct WeightOffsets {
+    long in_w, in_b;
+    long P[kLayers], Pb[kLayers], Q[kLayers], R[kLayers], U[kLayers], Ub[kLayers];
+    long Po, Pob, Qo, Ro, wo, wob, wd, wdb, total;
+};
+
+WeightOffsets offsets()
+{
+    WeightOffsets o{};
+    long p = 0;
+    auto take = [&](long k) {
+        const long at = p;
+        p += k;
+        return at;
+    };
+    o.in_w = take(kH * kNF);
+    o.in_b = take(kH);
+    for (int l = 0; l < kLayers; ++l) {
+        o.P[l] = take(kH * kH);
+        o.Pb[l] = take(kH);
+        o.Q[l] = take(kH * kH);
+        o.R[l] = take(kH * kEF);
+        o.U[l] = take(kH * 2 * kH);
+        o.Ub[l] = take(kH);
+    }
+    o.Po = take(kH * kH);
+    o.Pob = take(kH);
+    o.Qo = take(kH * kH);
+    o.Ro = take(kH * kEF);
+    o.wo = take(kH);
+    o.wob = take(1);
+    o.wd = take(kH);
+    o.wdb = take(1);
+    o.total = p;
+    return o;
+}
+
+struct Learned {
+    bool has_weights = false;
+    __nv_bfloat16 *d_w = nullptr;
+    WeightOffsets off{};
+    float *d_nf = nullptr, *d_h = nullptr, *d_ph = nullptr, *d_qh = nullptr, *d_agg = nullptr;
+    double *d_jii = nullptr;
+    float *d_cval = nullptr;
+    long cval_cap = 0;
+    long builds = 0;
+};
+
+Learned *LN(Engine &e) { return static_cast<Learned *>(e.learned); }
+
+__device__ __forceinline__ float bf(const __nv_bfloat16 *w, long i) { return __bfloat162float(w[i]); }
+__device__ __forceinline__ float tlogf(float v) { return copysignf(log1pf(fabsf(v)), v); }
+
+// node features and J_ii; one warp per row
+template <typename VT>
+__global__ void feat_kernel(int n, double h, const int *__restrict__ rowptr, const int *__restrict__ col,
+                            const VT *__restrict__ val, const double *__restrict__ gdiag,
+                            const double *__restrict__ dvec, float *__restrict__ nf, double *__restrict__ jii)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const double di = (1.0 + dvec[i]) * 0.5 * h;
+    double rs = 0.0, cs = 0.0;
+    int deg = 0;
+    for (int q = rowptr[i] + lane; q < rowptr[i + 1]; q += 32) {
+        const int j = col[q];
+        if (j == i) continue;
+        const double g = (double)val[q];
+        rs += fabs(di * g);
+        cs += fabs((1.0 + dvec[j]) * 0.5 * h * g);
+        ++deg;
+    }
+    rs = warp_sum(rs);
+    cs = warp_sum(cs);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) deg += __shfl_xor_sync(0xffffffffu, deg, o);
+    if (lane == 0) {
+        const double aii = di * gdiag[i];
+        jii[i] = 1.0 + aii;
+        nf[4 * i + 0] = tlogf((float)aii);
+        nf[4 * i + 1] = tlogf((float)rs);
+        nf[4 * i + 2] = tlogf((float)cs);
+        nf[4 * i + 3] = (float)deg / kDegScale;
+    }
+}
+
+__global__ void node_in_kernel(int n, const float *__restrict__ nf, const __nv_bfloat16 *__restrict__ w, long ow,
+                               long ob, float *__restrict__ hout)
+{
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long)n * kH) return;
+    const int i = (int)(idx >> 6), c = (int)(idx & 63);
+    float acc = bf(w, ob + c);
+#pragma unroll
+    for (int f = 0; f < kNF; ++f) acc = fmaf(bf(w, ow + c * kNF + f), nf[4 * i + f], acc);
+    hout[idx] = fmaxf(acc, 0.0f);
+}
+
+// ph = P h + b_P and qh = Q h for 32 nodes per CTA (weights transposed in
+// shared memory so that a warp reads consecutive output channels)
+constexpr int kProjNodes = 32;
+
+__global__ void __launch_bounds__(256) proj_kernel(int n, const float *__restrict__ hin,
+                                                   const __nv_bfloat16 *__restrict__ w, long oP, long oPb, long oQ,
+                                                   float *__restrict__ ph, float *__restrict__ qh)
+{
+    __shared__ float PT[kH][kH], QT[kH][kH], hs[kProjNodes][kH + 1];
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < kH * kH; idx += 256) {
+        const int c = idx >> 6, k = idx & 63;
+        PT[k][c] = bf(w, oP + idx);
+        QT[k][c] = bf(w, oQ + idx);
+    }
+    const int i0 = blockIdx.x * kProjNodes;
+    for (int idx = tid; idx < kProjNodes * kH; idx += 256) {
+        const int r = idx >> 6, k = idx & 63;
+        hs[r][k] = i0 + r < n ? hin[(long)(i0 + r) * kH + k] : 0.0f;
+    }
+    __syncthreads();
+    const int c = tid & 63, g = tid >> 6;
+    const float bp = bf(w, oPb + c);
+    for (int r = g; r < kProjNodes; r += 4) {
+        if (i0 + r >= n) break;
+        float a = bp, b = 0.0f;
+#pragma unroll 16
+        for (int k = 0; k < kH; ++k) {
+            const float hv = hs[r][k];
+            a = fmaf(PT[k][c], hv, a);
+            b = fmaf(QT[k][c], hv, b);
+        }
+        ph[(long)(i0 + r) * kH + c] = a;
+        qh[(long)(i0 + r) * kH + c] = b;
+    }
+}
+
+// per-edge pass, one warp per row: lane l holds channels l and l + 32.
+// kOut = false: agg_i = mean_j relu(ph_i + qh_j + R e_ij);
+// kOut = true:  C_ij = (w_o . relu(ph_i + qh_j + R e_ij) + b_o) A_ij / (J_ii J_jj)
+template <typename VT, bool kOut>
+__global__ void edge_kernel(int n, double h, const int *__restrict__ rowptr, const int *__restrict__ col,
+                            const VT *__restrict__ val, const double *__restrict__ dvec,
+                            const double *__restrict__ jii, const double *__restrict__ x,
+                            const double *__restrict__ y, const int *__restrict__ blk, double cutoff,
+                            const float *__restrict__ ph, const float *__restrict__ qh,
+                            const __nv_bfloat16 *__restrict__ w, long oR, long owo, long owob,
+                            float *__restrict__ agg, float *__restrict__ cval)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const int c0 = lane, c1 = lane + 32;
+    float r0[kEF], r1[kEF];
+#pragma unroll
+    for (int f = 0; f < kEF; ++f) {
+        r0[f] = bf(w, oR + c0 * kEF + f);
+        r1[f] = bf(w, oR + c1 * kEF + f);
+    }
+    float wo0 = 0.0f, wo1 = 0.0f, bo = 0.0f;
+    if (kOut) {
+        wo0 = bf(w, owo + c0);
+        wo1 = bf(w, owo + c1);
+        bo = bf(w, owob);
+    }
+    const float p0 = ph[(long)i * kH + c0], p1 = ph[(long)i * kH + c1];
+    const double di = (1.0 + dvec[i]) * 0.5 * h;
+    const double ji = jii[i];
+    const double xi = x[i], yi = y[i];
+    const int bi = blk[i];
+    const float inv_pos = (float)(1.0 / (kPosScale * cutoff));
+    float s0 = 0.0f, s1 = 0.0f;
+    int cnt = 0;
+    const int qs = rowptr[i], qe = rowptr[i + 1];
+    for (int q0 = qs; q0 < qe; q0 += 32) {
+        const int q = q0 + lane;
+        int j = -1;
+        float e0 = 0.f, e1 = 0.f, e2 = 0.f, e3 = 0.f, e4 = 0.f, sc = 0.f;
+        if (q < qe) {
+            j = col[q];
+            if (j != i) {
+                const double g = (double)val[q];
+                const double aij = di * g, aji = (1.0 + dvec[j]) * 0.5 * h * g;
+                double dx = x[j] - xi, dy = y[j] - yi;
+                dx -= rint(dx);
+                dy -= rint(dy);
+                e0 = tlogf((float)aij);
+                e1 = tlogf((float)aji);
+                e2 = (float)dx * inv_pos;
+                e3 = (float)dy * inv_pos;
+                e4 = blk[j] == bi ? 1.0f : 0.0f;
+                sc = (float)(aij / (ji * jii[j]));
+            } else if (kOut) {
+                j = -2; // the diagonal slot is written by the diagonal output
+            }
+        }
+        unsigned m = __ballot_sync(0xffffffffu, j >= 0);
+        cnt += __popc(m);
+        while (m) {
+            const int t = __ffs(m) - 1;
+            m &= m - 1;
+            const int jt = __shfl_sync(0xffffffffu, j, t);
+            const float f0 = __shfl_sync(0xffffffffu, e0, t), f1 = __shfl_sync(0xffffffffu, e1, t);
+            const float f2 = __shfl_sync(0xffffffffu, e2, t), f3 = __shfl_sync(0xffffffffu, e3, t);
+            const float f4 = __shfl_sync(0xffffffffu, e4, t);
+            float a = p0 + qh[(long)jt * kH + c0];
+            float b = p1 + qh[(long)jt * kH + c1];
+            a = fmaf(r0[0], f0, a); a = fmaf(r0[1], f1, a); a = fmaf(r0[2], f2, a);
+            a = fmaf(r0[3], f3, a); a = fmaf(r0[4], f4, a);
+            b = fmaf(r1[0], f0, b); b = fmaf(r1[1], f1, b); b = fmaf(r1[2], f2, b);
+            b = fmaf(r1[3], f3, b); b = fmaf(r1[4], f4, b);
+            a = fmaxf(a, 0.0f);
+            b = fmaxf(b, 0.0f);
+            if (kOut) {
+                float v = fmaf(wo0, a, wo1 * b);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == t) cval[q] = (v + bo - (1.0f - f4)) * sc;
+            } else {
+                s0 += a;
+                s1 += b;
+            }
+        }
+    }
+    if (!kOut) {
+        const float inv = 1.0f / (float)max(cnt, 1);
+        agg[(long)i * kH + c0] = s0 * inv;
+        agg[(long)i * kH + c1] = s1 * inv;
+    }
+}
+
+// h_i += relu(U [h_i; a_i] + b_U), 16 nodes per CTA
+constexpr int kUpdNodes = 16;
+
+__global__ void __launch_bounds__(256) update_kernel(int n, float *__restrict__ hio, const float *__restrict__ agg,
+                                                     const __nv_bfloat16 *__restrict__ w, long oU, long oUb)
+{
+    __shared__ float UT[2 * kH][kH];
+    __shared__ float xs[kUpdNodes][2 * kH + 1];
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < kH * 2 * kH; idx += 256) {
+        const int c = idx / (2 * kH), k = idx % (2 * kH);
+        UT[k][c] = bf(w, oU + idx);
+    }
+    const int i0 = blockIdx.x * kUpdNodes;
+    for (int idx = tid; idx < kUpdNodes * 2 * kH; idx += 256) {
+        const int r = idx / (2 * kH), k = idx % (2 * kH);
+        float v = 0.0f;
+        if (i0 + r < n) v = k < kH ? hio[(long)(i0 + r) * kH + k] : agg[(long)(i0 + r) * kH + k - kH];
+        xs[r][k] = v;
+    }
+    __syncthreads();
+    const int c = tid & 63, g = tid >> 6;
+    const float bu = bf(w, oUb + c);
+    for (int r = g; r < kUpdNodes; r += 4) {
+        if (i0 + r >= n) break;
+        float a = bu;
+#pragma unroll 16
+        for (int k = 0; k < 2 * kH; ++k) a = fmaf(UT[k][c], xs[r][k], a);
+        hio[(long)(i0 + r) * kH + c] = xs[r][c] + fmaxf(a, 0.0f);
+    }
+}
+
+// analytic first-order block-Neumann correction: C_ij = -A_ij / (J_ii J_jj)
+// across cluster blocks, 0 inside them and on the diagonal
+template <typename VT>
+__global__ void first_order_kernel(int n, double h, const int *__restrict__ rowptr, const int *__restrict__ col,
+                                   const VT *__restrict__ val, const double *__restrict__ dvec,
+                                   const double *__restrict__ jii, const int *__restrict__ blk,
+                                   float *__restrict__ cval)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const double di = (1.0 + dvec[i]) * 0.5 * h, ji = jii[i];
+    const int bi = blk[i];
+    for (int q = rowptr[i] + lane; q < rowptr[i + 1]; q += 32) {
+        const int j = col[q];
+        float v = 0.0f;
+        if (j != i && blk[j] != bi) v = (float)(-(di * (double)val[q]) / (ji * jii[j]));
+        cval[q] = v;
+    }
+}
+
+// C_ii = (w_d . h_i + b_d) / J_ii into each row's diagonal slot (slot 0)
+__global__ void diag_out_kernel(int n, const float *__restrict__ hin, const __nv_bfloat16 *__restrict__ w, long owd,
+                                long owdb, const double *__restrict__ jii, const int *__restrict__ rowptr,
+                                float *__restrict__ cval)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    float v = bf(w, owd + lane) * hin[(long)i * kH + lane] + bf(w, owd + lane + 32) * hin[(long)i * kH + lane + 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) cval[rowptr[i]] = (float)((v + bf(w, owdb)) / jii[i]);
+}
+
+// z += C v, one warp per row
+__global__ void apply_kernel(int n, const int *__restrict__ rowptr, const int *__restrict__ col,
+                             const float *__restrict__ cval, const double *__restrict__ v, double *__restrict__ z)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    double acc = 0.0;
+    for (int q = rowptr[i] + lane; q < rowptr[i + 1]; q += 32) acc += (double)cval[q] * v[col[q]];
+    acc = warp_sum(acc);
+    if (lane == 0) z[i] += acc;
+}
+
+} // namespace
+
+static int learned_ensure(Engine &e)
+{
+    if (e.learned) return 0;
+    Learned *L = new Learned();
+    e.learned = L;
+    const size_t nh = (size_t)e.n * kH;
+    const bool ok = cudaMalloc(&L->d_w, sizeof(__nv_bfloat16) * offsets().total) == cudaSuccess &&
+                    cudaMalloc(&L->d_nf, sizeof(float) * 4 * e.n) == cudaSuccess &&
+                    cudaMalloc(&L->d_h, sizeof(float) * nh) == cudaSuccess &&
+                    cudaMalloc(&L->d_ph, sizeof(float) * nh) == cudaSuccess &&
+                    cudaMalloc(&L->d_qh, sizeof(float) * nh) == cudaSuccess &&
+                    cudaMalloc(&L->d_agg, sizeof(float) * nh) == cudaSuccess &&
+                    cudaMalloc(&L->d_jii, sizeof(double) * e.n) == cudaSuccess;
+    if (!ok) {
+        e.err = "learned preconditioner: out of device memory";
+        return SDDDST_ERR_NOMEM;
+    }
+    return 0;
+}
+
+int learned_set_weights(Engine &e, const unsigned short *bf16, long count)
+{
+    const WeightOffsets o = offsets();
+    if (count != o.total) {
+        e.err = "learned preconditioner: expected " + std::to_string(o.total) + " weights, got " +
+                std::to_string(count);
+        return SDDDST_ERR_INVALID;
+    }
+    if (int rc = learned_ensure(e)) return rc;
+    Learned &L = *LN(e);
+    L.off = o;
+    cudaMemcpyAsync(L.d_w, bf16, sizeof(unsigned short) * o.total, cudaMemcpyHostToDevice, e.st);
+    L.has_weights = true;
+    return e.sync_check("learned weights");
+}
+
+// C for the assembled J(h); the cluster preconditioner must be built (its
+// block indices are an edge feature).  analytic: the first-order
+// block-Neumann correction without the network.
+int learned_build(Engine &e, double h, const double *dvec, const double *x, bool analytic)
+{
+    if (!analytic && !(e.learned && LN(e)->has_weights)) {
+        e.err = "learned preconditioner: no weights loaded (sdddst_set_preconditioner_weights)";
+        return SDDDST_ERR_INVALID;
+    }
+    if (int rc = learned_ensure(e)) return rc;
+    Learned &L = *LN(e);
+    if (e.nnz > L.cval_cap) {
+        if (L.d_cval) cudaFree(L.d_cval);
+        L.d_cval = nullptr;
+        L.cval_cap = 0;
+        const long cap = e.nnz + e.nnz / 8;
+        if (cudaMalloc(&L.d_cval, sizeof(float) * cap) != cudaSuccess) {
+            e.err = "learned preconditioner: out of device memory";
+            return SDDDST_ERR_NOMEM;
+        }
+        L.cval_cap = cap;
+    }
+    const WeightOffsets &o = L.off;
+    const int n = e.n;
+    cudaStream_t st = e.st;
+    const unsigned wrows = (unsigned)((n + 7) / 8); // 8 warps per CTA, one row each
+    if (e.valf)
+        feat_kernel<float><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_valf, e.d_gdiag, dvec, L.d_nf,
+                                                  L.d_jii);
+    else
+        feat_kernel<double><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, e.d_gdiag, dvec, L.d_nf,
+                                                   L.d_jii);
+    if (analytic) {
+        if (e.valf)
+            first_order_kernel<float><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_valf, dvec, L.d_jii,
+                                                             e.pc_blk_of, L.d_cval);
+        else
+            first_order_kernel<double><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, L.d_jii,
+                                                              e.pc_blk_of, L.d_cval);
+        e.launches += 2;
+        L.builds++;
+        return 0;
+    }
+    node_in_kernel<<<(unsigned)(((long)n * kH + 255) / 256), 256, 0, st>>>(n, L.d_nf, L.d_w, o.in_w, o.in_b, L.d_h);
+    const unsigned pgrid = (unsigned)((n + kProjNodes - 1) / kProjNodes);
+    const unsigned ugrid = (unsigned)((n + kUpdNodes - 1) / kUpdNodes);
+    for (int l = 0; l < kLayers; ++l) {
+        proj_kernel<<<pgrid, 256, 0, st>>>(n, L.d_h, L.d_w, o.P[l], o.Pb[l], o.Q[l], L.d_ph, L.d_qh);
+        if (e.valf)
+            edge_kernel<float, false><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_valf, dvec, L.d_jii, x,
+                                                             e.d_y, e.pc_blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w,
+                                                             o.R[l], 0, 0, L.d_agg, nullptr);
+        else
+            edge_kernel<double, false><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, L.d_jii, x,
+                                                              e.d_y, e.pc_blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w,
+                                                              o.R[l], 0, 0, L.d_agg, nullptr);
+        update_kernel<<<ugrid, 256, 0, st>>>(n, L.d_h, L.d_agg, L.d_w, o.U[l], o.Ub[l]);
+    }
+    proj_kernel<<<pgrid, 256, 0, st>>>(n, L.d_h, L.d_w, o.Po, o.Pob, o.Qo, L.d_ph, L.d_qh);
+    if (e.valf)
+        edge_kernel<float, true><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_valf, dvec, L.d_jii, x, e.d_y,
+                                                        e.pc_blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w, o.Ro, o.wo,
+                                                        o.wob, nullptr, L.d_cval);
+    else
+        edge_kernel<double, true><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, L.d_jii, x,
+                                                         e.d_y, e.pc_blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w, o.Ro,
+                                                         o.wo, o.wob, nullptr, L.d_cval);
+    diag_out_kernel<<<wrows, 256, 0, st>>>(n, L.d_h, L.d_w, o.wd, o.wdb, L.d_jii, e.d_rowptr, L.d_cval);
+    e.launches += 4 + 3 * kLayers + 2;
+    L.builds++;
+    return 0;
+}
+
+void learned_apply_add(Engine &e, const double *v, double *z)
+{
+    Learned &L = *LN(e);
+    apply_kernel<<<(unsigned)((e.n + 7) / 8), 256, 0, e.st>>>(e.n, e.d_rowptr, e.d_col, L.d_cval, v, z);
+    e.launches++;
+}
+
+int learned_export(Engine &e, float *host, long cap)
+{
+    Learned *Lp = LN(e);
+    if (!Lp || !Lp->d_cval) return SDDDST_ERR_INVALID;
+    if (cap < e.nnz) return SDDDST_ERR_CAPACITY;
+    cudaMemcpyAsync(host, Lp->d_cval, sizeof(float) * e.nnz, cudaMemcpyDeviceToHost, e.st);
+    return e.sync_check("learned export");
+}
+
+void learned_free(Engine &e)
+{
+    Learned *L = LN(e);
+    if (!L) return;
+    void *bufs[] = {L->d_w, L->d_nf, L->d_h, L->d_ph, L->d_qh, L->d_agg, L->d_jii, L->d_cval};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    delete L;
+    e.learned = nullptr;
+}
+
+long learned_weight_count() { return offsets().total; }
+
+} // namespace sd
