@@ -226,36 +226,52 @@ __global__ void edge_kernel(int n, double h, const int *__restrict__ rowptr, con
                 e3 = (float)dy * inv_pos;
                 e4 = blk[j] == bi ? 1.0f : 0.0f;
                 sc = (float)(aij / (ji * jii[j]));
-            } else if (kOut) {
-                j = -2; // the diagonal slot is written by the diagonal output
+            } else {
+                j = -2; // the diagonal slot is no edge (its C value comes from the diagonal output)
             }
         }
-        unsigned m = __ballot_sync(0xffffffffu, j >= 0);
-        cnt += __popc(m);
-        while (m) {
-            const int t = __ffs(m) - 1;
-            m &= m - 1;
+        cnt += __popc(__ballot_sync(0xffffffffu, j >= 0));
+        // the chunk's 32 edges unrolled: independent gathers of qh_j; the
+        // output pass leaves lane t's two-channel partial of edge t in v[t]
+        float v[32];
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
             const int jt = __shfl_sync(0xffffffffu, j, t);
             const float f0 = __shfl_sync(0xffffffffu, e0, t), f1 = __shfl_sync(0xffffffffu, e1, t);
             const float f2 = __shfl_sync(0xffffffffu, e2, t), f3 = __shfl_sync(0xffffffffu, e3, t);
             const float f4 = __shfl_sync(0xffffffffu, e4, t);
-            float a = p0 + qh[(long)jt * kH + c0];
-            float b = p1 + qh[(long)jt * kH + c1];
-            a = fmaf(r0[0], f0, a); a = fmaf(r0[1], f1, a); a = fmaf(r0[2], f2, a);
-            a = fmaf(r0[3], f3, a); a = fmaf(r0[4], f4, a);
-            b = fmaf(r1[0], f0, b); b = fmaf(r1[1], f1, b); b = fmaf(r1[2], f2, b);
-            b = fmaf(r1[3], f3, b); b = fmaf(r1[4], f4, b);
-            a = fmaxf(a, 0.0f);
-            b = fmaxf(b, 0.0f);
+            float a = 0.0f, b = 0.0f;
+            if (jt >= 0) {
+                a = p0 + qh[(long)jt * kH + c0];
+                b = p1 + qh[(long)jt * kH + c1];
+                a = fmaf(r0[0], f0, a); a = fmaf(r0[1], f1, a); a = fmaf(r0[2], f2, a);
+                a = fmaf(r0[3], f3, a); a = fmaf(r0[4], f4, a);
+                b = fmaf(r1[0], f0, b); b = fmaf(r1[1], f1, b); b = fmaf(r1[2], f2, b);
+                b = fmaf(r1[3], f3, b); b = fmaf(r1[4], f4, b);
+                a = fmaxf(a, 0.0f);
+                b = fmaxf(b, 0.0f);
+            }
             if (kOut) {
-                float v = fmaf(wo0, a, wo1 * b);
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == t) cval[q] = (v + bo - (1.0f - f4)) * sc;
+                v[t] = fmaf(wo0, a, wo1 * b);
             } else {
                 s0 += a;
                 s1 += b;
             }
+        }
+        if (kOut) {
+            // reduce-scatter over the warp: afterwards lane l holds the sum
+            // over all lanes of v[l] in v[0] (31 shuffles for 32 edges)
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) {
+                const bool up = (lane & o) != 0;
+#pragma unroll
+                for (int k = 0; k < o; ++k) {
+                    const float send = up ? v[k] : v[k + o];
+                    const float keep = up ? v[k + o] : v[k];
+                    v[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+                }
+            }
+            if (j >= 0) cval[q] = (v[0] + bo - (1.0f - e4)) * sc;
         }
     }
     if (!kOut) {
@@ -268,7 +284,7 @@ __global__ void edge_kernel(int n, double h, const int *__restrict__ rowptr, con
 // h_i += relu(U [h_i; a_i] + b_U), 16 nodes per CTA
 constexpr int kUpdNodes = 16;
 
-__global__ void __launch_bounds__(256) update_kernel(int n, float *__restrict__ hio, const float *__restrict__ agg,
+__global__ void __launch_bounds__(256) node_update_kernel(int n, float *__restrict__ hio, const float *__restrict__ agg,
                                                      const __nv_bfloat16 *__restrict__ w, long oU, long oUb)
 {
     __shared__ float UT[2 * kH][kH];
@@ -439,7 +455,7 @@ int learned_build(Engine &e, double h, const double *dvec, const double *x, bool
             edge_kernel<double, false><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, L.d_jii, x,
                                                               e.d_y, e.pc_blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w,
                                                               o.R[l], 0, 0, L.d_agg, nullptr);
-        update_kernel<<<ugrid, 256, 0, st>>>(n, L.d_h, L.d_agg, L.d_w, o.U[l], o.Ub[l]);
+        node_update_kernel<<<ugrid, 256, 0, st>>>(n, L.d_h, L.d_agg, L.d_w, o.U[l], o.Ub[l]);
     }
     proj_kernel<<<pgrid, 256, 0, st>>>(n, L.d_h, L.d_w, o.Po, o.Pob, o.Qo, L.d_ph, L.d_qh);
     if (e.valf)

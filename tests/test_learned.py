@@ -5,7 +5,7 @@
 * GPU: the CUDA inference (csrc/learned.cu) against the PyTorch FP32
   definition of the same network (sdddst_b200/learned.py) with the same BF16
   weights, on the same Jacobian and cluster blocks (FP32 arithmetic in both,
-  different summation orders: 1e-4 of the largest |C| plus 1e-4 relative);
+  different summation orders: 2e-5 of the largest |C| plus 1e-4 relative);
   the learned solver's trajectory against the cluster-preconditioned one
   (both solve to a 1e-13 residual: same decisions, positions within 1e-9).
 """
@@ -66,7 +66,7 @@ def test_learned_inference_matches_torch(engine_lib):
     scale = np.abs(ref).max()
     assert scale > 0
     err = np.abs(cval.astype(np.float64) - ref)
-    assert np.all(err <= 1e-4 * scale + 1e-4 * np.abs(ref)), (err.max(), scale)
+    assert np.all(err <= 2e-5 * scale + 1e-4 * np.abs(ref)), (err.max(), scale)
 
 
 @pytest.mark.gpu
