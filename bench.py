@@ -283,7 +283,24 @@ def reference_arm(args):
 
 def profile_target(args):
     """Small, self-contained launches for ncu captures: the pair-sum kernels
-    `reps` times on the workload's configuration, or `steps` step attempts."""
+    `reps` times on the workload's configuration, `steps` step attempts, one
+    sparse-LU solve (plain FP64 engine, h = 1e-6), or one inference of the
+    learned preconditioner correction (h = 1e-7)."""
+    from sdddst_b200 import capi
+    if args.only == "direct":
+        eng, xyb = make_engine(args.n, "fp64", 0, solver=capi.SOLVER_DIRECT)
+        rhs = np.random.default_rng(0).standard_normal(args.n)
+        x, refinements = eng.solve(1e-6, xyb, rhs)
+        print(json.dumps({"target": "direct", "n": args.n, "refinements": refinements, **eng.direct_stats()}))
+        eng.close()
+        return
+    if args.only == "learned":
+        eng, _ = make_engine(args.n, args.pairsum, 0, solver=capi.SOLVER_GMRES_LEARNED)
+        eng.set_preconditioner_weights()
+        c = eng.learned_correction(1e-7)
+        print(json.dumps({"target": "learned", "n": args.n, "nnz": int(c.size)}))
+        eng.close()
+        return
     eng, _ = make_engine(args.n, args.pairsum, 0)
     if args.only == "pairsum":
         ms = eng.profile_pair_sum(args.reps)
@@ -346,7 +363,7 @@ def main():
     ap.add_argument("--n", type=int, default=N_FULL)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--only", default=None, choices=["pairsum", "step"],
+    ap.add_argument("--only", default=None, choices=["pairsum", "step", "direct", "learned"],
                     help="profiling target: launch only the pair-sum kernels (or only steps) and exit")
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-realisations measurement")
