@@ -67,7 +67,12 @@ enum {
 
 /* Field kernels (Field plug-in): the analytic periodic field
  * (Fields/AnalyticField.cpp). */
-enum { SDDDST_FIELD_ANALYTIC = 0 };
+enum {
+    SDDDST_FIELD_ANALYTIC = 0,  /* AnalyticField (AnalyticField.cpp:145-181) */
+    SDDDST_FIELD_TABULATED = 1  /* tabulated 1024 x 1024 field with bicubic interpolation, the counterpart of
+                                   PeriodicShearStressELTE (python/src/periodic_shear_stress_ELTE_wrapper.cpp:40-46);
+                                   tables built on the device from the analytic field; FP64 pair sum */
+};
 
 typedef struct {
     int n;                    /* dislocation count (SimulationData::dc) */

@@ -587,6 +587,10 @@ static int batch_init(Batch &bt, const sdddst_params &common, int count, const i
         bt.e.err = "batch: the sparse LU and learned solvers serve single systems; choose another GMRES solver";
         return SDDDST_ERR_INVALID;
     }
+    if (common.field != SDDDST_FIELD_ANALYTIC) {
+        bt.e.err = "batch: only the analytic field is supported";
+        return SDDDST_ERR_INVALID;
+    }
     bt.ntot = bt.off[count];
     if (bt.ntot > (1L << 30)) {
         bt.e.err = "batch too large";

@@ -94,7 +94,8 @@ int sdddst_ctx_create(const sdddst_params *prm, const double *xyb, const double 
 {
     if (!prm || !ctx) return fail(SDDDST_ERR_INVALID, "null argument");
     *ctx = nullptr;
-    if (prm->field != SDDDST_FIELD_ANALYTIC) return fail(SDDDST_ERR_INVALID, "unsupported field kind");
+    if (prm->field != SDDDST_FIELD_ANALYTIC && prm->field != SDDDST_FIELD_TABULATED)
+        return fail(SDDDST_ERR_INVALID, "unsupported field kind");
     if (prm->pairsum != SDDDST_PAIRSUM_FP64 && prm->pairsum != SDDDST_PAIRSUM_FP32)
         return fail(SDDDST_ERR_INVALID, "unsupported pair-sum mode");
     if (prm->solver != SDDDST_SOLVER_GMRES && prm->solver != SDDDST_SOLVER_GMRES_JACOBI &&

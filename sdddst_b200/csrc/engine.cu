@@ -48,6 +48,8 @@ Engine::~Engine()
     direct_free(*this);
     learned_free(*this);
     if (d_xasm) cudaFree(d_xasm);
+    if (d_tab_xy) cudaFree(d_tab_xy);
+    if (d_tab_dx) cudaFree(d_tab_dx);
     if (st) cudaStreamDestroy(st);
 }
 
@@ -190,7 +192,9 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     cudaMemcpyAsync(d_tol_last, t0.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(d_dvec, 0, sizeof(double) * n, st);
     cudaMemsetAsync(d_counter, 0, sizeof(unsigned int), st);
-    return sync_check("init");
+    if (int rc = sync_check("init")) return rc;
+    if (prm.field == SDDDST_FIELD_TABULATED) return tabulated_build(*this);
+    return 0;
 }
 
 // ---------------------------------------------------------------- stress

@@ -35,6 +35,7 @@ struct Engine {
     double *d_pdx = nullptr, *d_pdy = nullptr;
     double *d_ys = nullptr, *d_bs = nullptr; // scratch y, b of caller-supplied configurations
     double *d_xw = nullptr;                  // positions wrapped into [-0.5, 0.5) (mixed pair sum)
+    double *d_tab_xy = nullptr, *d_tab_dx = nullptr; // tabulated field: remainder tables (null: analytic)
     double *d_minr2_out = nullptr;           // optional per-dislocation min distance output
 
     // ---- cell list of the cutoff-neighbour search
@@ -136,6 +137,7 @@ void launch_speeds_raw(int n, const double *x, const double *y, const double *b,
                        double *v, cudaStream_t st);
 
 int jacobian_assemble(Engine &e, const double *x);
+int tabulated_build(Engine &e);
 int alloc_csr_values(Engine &e, long cap);
 void launch_make_dvec(const Engine &e, double h, double *dvec, cudaStream_t st);
 void launch_export_jacobian(const Engine &e, double h, const double *dvec, double *val_out, cudaStream_t st);

@@ -17,6 +17,7 @@
 #include "engine.h"
 #include "field_f64.cuh"
 #include "field_f32.cuh"
+#include "tabulated_field.cuh"
 
 namespace sd {
 
@@ -168,7 +169,8 @@ __global__ void row_fill_kernel(int n, const double *__restrict__ x, const doubl
                                 const double *__restrict__ b, CellScan cs, double c, double c2, double ic2,
                                 const int *__restrict__ rowptr, int *__restrict__ col, VT *__restrict__ val,
                                 double *__restrict__ gdiag, int p, const double *__restrict__ pdx,
-                                const double *__restrict__ pdy, double A, double K, int *__restrict__ flag)
+                                const double *__restrict__ pdy, double A, double K, int *__restrict__ flag,
+                                const double *__restrict__ tab_dx)
 {
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -217,7 +219,8 @@ __global__ void row_fill_kernel(int n, const double *__restrict__ x, const doubl
         double w;
         pair_kept(r2_exact(dx, dy), c, c2, ic2, &w);
         double tdx;
-        if (sizeof(VT) == sizeof(double)) tdx = tau_xy_dx_f64(dx, dy);
+        if (tab_dx) tdx = tau0_xy_dx(dx, dy) + tab_interp(tab_dx, dx, dy); // tabulated field
+        else if (sizeof(VT) == sizeof(double)) tdx = tau_xy_dx_f64(dx, dy);
         else tdx = (double)tau_xy_dx_f32(__double2float_rn(dx), __double2float_rn(dy));
         const VT v = (VT)(bi * b[j] * tdx * w);
         val[q] = v;
@@ -336,11 +339,13 @@ int jacobian_assemble(Engine &e, const double *x)
     if (e.valf)
         row_fill_kernel<float><<<rb, 32 * wpb, 0, st>>>(n, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr,
                                                        e.one_per_cutoff_sqr, e.d_rowptr, e.d_col, e.d_valf,
-                                                       e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag);
+                                                       e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag,
+                                                       e.d_tab_dx);
     else
         row_fill_kernel<double><<<rb, 32 * wpb, 0, st>>>(n, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr,
                                                         e.one_per_cutoff_sqr, e.d_rowptr, e.d_col, e.d_val,
-                                                        e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag);
+                                                        e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag,
+                                                        e.d_tab_dx);
     e.launches += 1;
     int flag = 0;
     cudaMemcpyAsync(&flag, e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);

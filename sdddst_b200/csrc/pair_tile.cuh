@@ -6,16 +6,30 @@
 #include "common.cuh"
 #include "field_f32.cuh"
 #include "field_f64.cuh"
+#include "tabulated_field.cuh"
 
 namespace sd {
 
+// Field of the FP64 tile: the analytic periodic sum, or the tabulated field
+// (closed-form image-free term plus the interpolated smooth remainder).
+struct AnalyticField64 {
+    __device__ __forceinline__ double xy(double dx, double dy) const { return tau_xy_f64(dx, dy); }
+};
+struct TabulatedField64 {
+    const double *rem; // remainder table of tau_xy
+    __device__ __forceinline__ double xy(double dx, double dy) const
+    {
+        return tau0_xy(dx, dy) + tab_interp(rem, dx, dy);
+    }
+};
+
 // One T x T tile (I, J), I <= J, of the FP64 pair sum over a system of n
 // dislocations at x, y, b (see the file comment for the partial-sum layout).
-template <int T>
+template <int T, class Field = AnalyticField64>
 __device__ __forceinline__ void pair_tile_f64(const double *__restrict__ x, const double *__restrict__ y,
                                               const double *__restrict__ b, int n, int I, int J,
                                               double *__restrict__ part, unsigned long long *__restrict__ minr2,
-                                              double r2_track)
+                                              double r2_track, const Field fld = Field())
 {
     constexpr int W = T / 32;
     __shared__ double sx[T], sy[T], sb[T];
@@ -52,7 +66,7 @@ __device__ __forceinline__ void pair_tile_f64(const double *__restrict__ x, cons
                 dx = 0.25;
                 dy = 0.25;
             }
-            double t = bi * sb[jj] * tau_xy_f64(dx, dy);
+            double t = bi * sb[jj] * fld.xy(dx, dy);
             t = valid ? t : 0.0;
             acc += t;
             if (valid && r2 < r2_track) { // rare: only pairs that can set a tolerance

@@ -42,6 +42,18 @@ __global__ void __launch_bounds__(T) pair_tiles_kernel(const double *__restrict_
 }
 
 template <int T>
+__global__ void __launch_bounds__(T) pair_tiles_tab_kernel(const double *__restrict__ x, const double *__restrict__ y,
+                                                           const double *__restrict__ b, int n, int nblk,
+                                                           double *__restrict__ part,
+                                                           unsigned long long *__restrict__ minr2, double r2_track,
+                                                           const double *__restrict__ rem)
+{
+    int I, J;
+    tile_coords((long)blockIdx.x, I, J);
+    pair_tile_f64<T, TabulatedField64>(x, y, b, n, I, J, part, minr2, r2_track, TabulatedField64{rem});
+}
+
+template <int T>
 __global__ void __launch_bounds__(T) pair_tiles_f32_kernel(const double *__restrict__ xw, const double *__restrict__ y,
                                                            const double *__restrict__ b, int n, int nblk,
                                                            double *__restrict__ part,
@@ -70,8 +82,17 @@ __global__ void speeds_finish_kernel(int n, int nblk, const double *__restrict__
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double acc = 0.0;
-    for (int L = 0; L < nblk; ++L) acc += part[(size_t)L * n + i];
+    // compensated (Neumaier) FP64 sum of the per-tile partials, in a fixed
+    // order: the tile partials themselves are FP64 sums of at most one
+    // tile's pairs, so the long reduction is this one
+    double acc = 0.0, comp = 0.0;
+    for (int L = 0; L < nblk; ++L) {
+        const double v = part[(size_t)L * n + i];
+        const double t = acc + v;
+        comp += fabs(acc) >= fabs(v) ? (acc - t) + v : (v - t) + acc;
+        acc = t;
+    }
+    acc += comp;
     double smin = update_tol ? __longlong_as_double((long long)minr2[i]) : 0.0;
     const double xi = x[i], yi = y[i], bi = b[i];
     for (int q = 0; q < p; ++q) {
@@ -114,6 +135,15 @@ void launch_pair_sum(const Engine &e, const double *x, cudaStream_t st, int mode
     const int nblk = (n + T - 1) / T;
     const long tiles = (long)nblk * (nblk + 1) / 2;
     fill_u64_kernel<<<(n + 255) / 256, 256, 0, st>>>(e.d_minr2, 0x7FF0000000000000ull, n);
+    if (e.d_tab_xy) { // tabulated field: FP64 tiles whatever the pair-sum mode
+        if (T == 128)
+            pair_tiles_tab_kernel<128><<<(unsigned)tiles, 128, 0, st>>>(x, e.d_y, e.d_b, n, nblk, e.d_part, e.d_minr2,
+                                                                        r2_track, e.d_tab_xy);
+        else
+            pair_tiles_tab_kernel<64><<<(unsigned)tiles, 64, 0, st>>>(x, e.d_y, e.d_b, n, nblk, e.d_part, e.d_minr2,
+                                                                      r2_track, e.d_tab_xy);
+        return;
+    }
     if (mode == 0) {
         if (T == 128)
             pair_tiles_kernel<128, 0><<<(unsigned)tiles, 128, 0, st>>>(x, e.d_y, e.d_b, n, nblk, e.d_part, e.d_minr2, r2_track);

@@ -9,6 +9,10 @@
 #include "simulation.h"
 
 #include "Fields/AnalyticField.h"
+#include "Fields/PeriodicShearStressELTE.h"
+#include "../../csrc/tabulated_field.cuh"
+#include "Fields/PeriodicShearStressELTE.h"
+#include "../../csrc/tabulated_field.cuh"
 #include "StressProtocols/fixed_rate_protocol.h"
 #include "StressProtocols/spring_protocol.h"
 #include "constants.h"
@@ -782,3 +786,67 @@ double Simulation::getElement(int j, int si, int ei)
 }
 
 } // namespace sdddstCore
+
+// ---------------------------------------------------------------- tabulated field
+// Host tables of PeriodicShearStressELTE (the engine builds its own on the
+// device): remainder of the analytic field after its image-free term.
+
+namespace {
+
+std::vector<double> build_remainder(bool dx_table)
+{
+    sdddstCore::AnalyticField af;
+    auto rem = [&](double x, double y) {
+        return dx_table ? af.xy_diff_x(x, y) - sd::tau0_xy_dx(x, y) : af.xy(x, y) - sd::tau0_xy(x, y);
+    };
+    std::vector<double> t((size_t)sd::kTabS * sd::kTabS);
+    for (int ky = 0; ky < sd::kTabS; ++ky)
+        for (int kx = 0; kx < sd::kTabS; ++kx) {
+            const double x = sd::tab_coord(kx), y = sd::tab_coord(ky);
+            double v;
+            if (x == 0.0 && y == 0.0) { // limit at the origin: Richardson on symmetric averages
+                auto avg = [&](double d) { return 0.25 * (rem(d, 0) + rem(-d, 0) + rem(0, d) + rem(0, -d)); };
+                v = (4.0 * avg(1e-3) - avg(2e-3)) / 3.0;
+            } else {
+                v = rem(x, y);
+            }
+            t[(size_t)ky * sd::kTabS + kx] = v;
+        }
+    return t;
+}
+
+} // namespace
+
+namespace sdddstCoreELTE {
+
+PeriodicShearStressELTE::PeriodicShearStressELTE() : Field() {}
+PeriodicShearStressELTE::~PeriodicShearStressELTE() {}
+int PeriodicShearStressELTE::deviceKind() const { return SDDDST_FIELD_TABULATED; }
+
+void PeriodicShearStressELTE::loadStress(std::string path, std::string type, int size)
+{
+    (void)path;
+    if (size != sd::kTabG) throw std::invalid_argument("PeriodicShearStressELTE: tables are 1024 x 1024");
+    if (type == "xy") remXY = build_remainder(false);
+    else if (type == "xy_diff_x") remDX = build_remainder(true);
+    else throw std::invalid_argument("PeriodicShearStressELTE: unknown table type " + type);
+}
+
+double PeriodicShearStressELTE::xy(double dx, double dy)
+{
+    if (remXY.empty()) throw std::logic_error("PeriodicShearStressELTE: call loadStress(path, \"xy\", 1024) first");
+    normalize(dx);
+    normalize(dy);
+    return sd::tau0_xy(dx, dy) + sd::tab_interp(remXY.data(), dx, dy);
+}
+
+double PeriodicShearStressELTE::xy_diff_x(double dx, double dy)
+{
+    if (remDX.empty())
+        throw std::logic_error("PeriodicShearStressELTE: call loadStress(path, \"xy_diff_x\", 1024) first");
+    normalize(dx);
+    normalize(dy);
+    return sd::tau0_xy_dx(dx, dy) + sd::tab_interp(remDX.data(), dx, dy);
+}
+
+} // namespace sdddstCoreELTE

@@ -7,6 +7,7 @@
 #include <pybind11/stl_bind.h>
 
 #include "Fields/AnalyticField.h"
+#include "Fields/PeriodicShearStressELTE.h"
 #include "StressProtocols/fixed_rate_protocol.h"
 #include "StressProtocols/spring_protocol.h"
 #include "simulation.h"
@@ -38,6 +39,19 @@ struct PyField {
 struct PyAnalyticField : PyField {
     void init() override { field.reset(new AnalyticField); }
     std::string name() const override { return "AnalyticField"; }
+};
+// python/src/periodic_shear_stress_ELTE_wrapper.cpp:34-51
+struct PyPeriodicShearStressFieldELTE : PyField {
+    std::string pwd;
+    void setPWD(std::string path) { pwd = path; }
+    void init() override
+    {
+        std::unique_ptr<sdddstCoreELTE::PeriodicShearStressELTE> t(new sdddstCoreELTE::PeriodicShearStressELTE);
+        t->loadStress(pwd, "xy", 1024);
+        t->loadStress(pwd, "xy_diff_x", 1024);
+        field.reset(t.release());
+    }
+    std::string name() const override { return "Periodic Shear Stress Field ELTE"; }
 };
 struct PyStressProtocol {
     std::unique_ptr<StressProtocol> protocol;
@@ -152,6 +166,9 @@ PYBIND11_MODULE(PySdddstCore, m)
         .def("__str__", &PyField::str)
         .def("__repr__", &PyField::str);
     py::class_<PyAnalyticField, PyField>(m, "AnalyticFieldObject").def(py::init<>());
+    py::class_<PyPeriodicShearStressFieldELTE, PyField>(m, "PeriodicShearStressFieldELTEObject")
+        .def(py::init<>())
+        .def("setPWD", &PyPeriodicShearStressFieldELTE::setPWD);
 
     py::enum_<StressProtocolStepType>(m, "StepType")
         .value("Original", Original)
