@@ -216,6 +216,42 @@ def position_error(eng_mixed, eng_plain):
     return max(errs), am == ap
 
 
+def measure_precision(torch, steps, flush, device):
+    """The precision workload: N=16384 (seed 2), cutoff multiplier 1, FP32
+    pair terms with compensated FP64 accumulation, FP32 Jacobian values, FP32
+    sparse LU refined in FP64 to a 1e-12 relative residual, against the plain
+    FP64 path (FP64 pair sum, FP64 LU); velocity error on the initial
+    configuration and position error one accepted step from the same state."""
+    from sdddst_b200 import capi, workloads
+    n = 16384
+    xyb, _ = workloads.dislocations(n, 2)
+    mk = lambda ps, sv: capi.Engine(capi.cli_params(n, 1.0, PREC, step_size=H0, device=device, pairsum=ps,
+                                                    solver=sv, solver_tol=1e-12), xyb)
+    e32 = mk(capi.PAIRSUM_FP32, capi.SOLVER_DIRECT_MIXED)
+    e64 = mk(capi.PAIRSUM_FP64, capi.SOLVER_DIRECT)
+    v32, _ = e32.speeds(xyb)
+    v64, _ = e64.speeds(xyb)
+    out = {"config": "N=16384 seed 2, cutoff multiplier 1, prec 1e-5, solves refined to 1e-12",
+           "velocity_error_rel": float(np.abs(v32 - v64).max() / np.abs(v64).max())}
+    for name, e in (("fp32_lu_refined", e32), ("fp64_lu", e64)):
+        ms, acc, _ = time_steps(torch, e, steps, 3, flush)
+        out[name] = {"value": acc / (ms * 1e-3) if ms > 0 else 0.0, "unit": UNIT, "ms_per_step": ms / steps,
+                     "accepted": acc}
+    err = None
+    for _ in range(10):
+        x, sc = e64.config(0), e64.scalars()
+        for e in (e32, e64):
+            e.set_state(x, sc["step_size"], sc["sim_time"], sc["energy"], sc["strain"], False)
+        a32, a64 = e32.step(), e64.step()
+        if a64 and a32:
+            err = max(float(np.abs(e32.config(w)[:, 0] - e64.config(w)[:, 0]).max()) for w in (1, 2, 3))
+            break
+    out["position_error_one_step"] = err
+    e32.close()
+    e64.close()
+    return out
+
+
 def cpu_baseline_sample(n_full, sample_n=4096, reps=1):
     """The reference hot path (compiled in place) on a bounded sample: the
     first `sample_n` dislocations of the workload with the same cutoff radius
@@ -482,6 +518,13 @@ def main():
             except Exception as ex:
                 variants[name] = {"error": str(ex)[:200]}
 
+    precision = None
+    if not args.no_variants:
+        try:
+            precision = measure_precision(torch, max(3, args.steps // 2), flush, local)
+        except Exception as ex:
+            precision = {"error": str(ex)[:200]}
+
     batch = None
     if not args.no_batch:
         try:
@@ -516,6 +559,7 @@ def main():
         "plain_fp64": plain,
         **variants,
         "position_error_vs_fp64": pos_err,
+        "precision_16384": precision,
         "batch_512": batch,
         "cpu_baseline": cpu,
     }

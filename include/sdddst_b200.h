@@ -61,8 +61,9 @@ enum {
     SDDDST_SOLVER_GMRES_LEARNED = 4, /* restarted GMRES, FP64, cluster block-Jacobi plus a learned correction on
                                         J's pattern (weights: sdddst_set_preconditioner_weights); falls back to
                                         the sparse LU when GMRES stalls */
-    SDDDST_SOLVER_GMRES_NEUMANN = 5  /* as SDDDST_SOLVER_GMRES_LEARNED with the analytic first-order
+    SDDDST_SOLVER_GMRES_NEUMANN = 5, /* as SDDDST_SOLVER_GMRES_LEARNED with the analytic first-order
                                         block-Neumann correction in place of the network */
+    SDDDST_SOLVER_DIRECT_MIXED = 6   /* sparse LU with FP32 fronts, FP64 iterative refinement to solver_tol */
 };
 
 /* Field kernels (Field plug-in): the analytic periodic field

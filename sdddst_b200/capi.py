@@ -27,7 +27,7 @@ STRESS_ZERO, STRESS_FIXED_RATE, STRESS_SPRING, STRESS_CONSTANT = 0, 1, 2, 3
 PAIRSUM_FP64, PAIRSUM_FP32 = 0, 1
 FIELD_ANALYTIC, FIELD_TABULATED = 0, 1
 SOLVER_GMRES, SOLVER_GMRES_JACOBI, SOLVER_GMRES_CLUSTER, SOLVER_DIRECT = 0, 1, 2, 3
-SOLVER_GMRES_LEARNED, SOLVER_GMRES_NEUMANN = 4, 5
+SOLVER_GMRES_LEARNED, SOLVER_GMRES_NEUMANN, SOLVER_DIRECT_MIXED = 4, 5, 6
 
 # Every extern "C" symbol of include/sdddst_b200.h.
 EXPORTS = [

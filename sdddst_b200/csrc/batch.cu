@@ -582,7 +582,8 @@ static int batch_init(Batch &bt, const sdddst_params &common, int count, const i
         }
         bt.off[k + 1] = bt.off[k] + sizes[k];
     }
-    if (common.solver == SDDDST_SOLVER_DIRECT || common.solver == SDDDST_SOLVER_GMRES_LEARNED ||
+    if (common.solver == SDDDST_SOLVER_DIRECT || common.solver == SDDDST_SOLVER_DIRECT_MIXED ||
+        common.solver == SDDDST_SOLVER_GMRES_LEARNED ||
         common.solver == SDDDST_SOLVER_GMRES_NEUMANN) {
         bt.e.err = "batch: the sparse LU and learned solvers serve single systems; choose another GMRES solver";
         return SDDDST_ERR_INVALID;

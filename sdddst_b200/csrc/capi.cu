@@ -100,7 +100,8 @@ int sdddst_ctx_create(const sdddst_params *prm, const double *xyb, const double 
         return fail(SDDDST_ERR_INVALID, "unsupported pair-sum mode");
     if (prm->solver != SDDDST_SOLVER_GMRES && prm->solver != SDDDST_SOLVER_GMRES_JACOBI &&
         prm->solver != SDDDST_SOLVER_GMRES_CLUSTER && prm->solver != SDDDST_SOLVER_DIRECT &&
-        prm->solver != SDDDST_SOLVER_GMRES_LEARNED && prm->solver != SDDDST_SOLVER_GMRES_NEUMANN)
+        prm->solver != SDDDST_SOLVER_GMRES_LEARNED && prm->solver != SDDDST_SOLVER_GMRES_NEUMANN &&
+        prm->solver != SDDDST_SOLVER_DIRECT_MIXED)
         return fail(SDDDST_ERR_INVALID, "unsupported solver");
     if (!(prm->prec > 0) || !(prm->step_size > 0) || !(prm->cutoff_multiplier > 0))
         return fail(SDDDST_ERR_INVALID, "prec, step size and cutoff multiplier must be positive");
@@ -499,7 +500,8 @@ int sdddst_profile_direct(void *ctx, double h, int reps, double *factor_ms, doub
 {
     if (!ctx || !factor_ms || !solve_ms || reps < 1 || !(h > 0)) return fail(SDDDST_ERR_INVALID, "bad argument");
     sd::Engine *e = E(ctx);
-    if (e->prm.solver != SDDDST_SOLVER_DIRECT) return fail(SDDDST_ERR_INVALID, "the context's solver is not the sparse LU");
+    if (e->prm.solver != SDDDST_SOLVER_DIRECT && e->prm.solver != SDDDST_SOLVER_DIRECT_MIXED)
+        return fail(SDDDST_ERR_INVALID, "the context's solver is not the sparse LU");
     cudaSetDevice(e->device);
     try {
         if (int rc = e->assemble(e->d_x0)) return from_engine(e, rc);

@@ -241,7 +241,8 @@ int Engine::speeds(const double *x, double *v_out, double *S_out, int stress_typ
 int Engine::assemble(const double *x)
 {
     int rc = jacobian_assemble(*this, x);
-    if (rc == 0 && prm.solver == SDDDST_SOLVER_DIRECT) rc = direct_analyse(*this, x);
+    if (rc == 0 && (prm.solver == SDDDST_SOLVER_DIRECT || prm.solver == SDDDST_SOLVER_DIRECT_MIXED))
+        rc = direct_analyse(*this, x);
     if (rc == 0 && (prm.solver == SDDDST_SOLVER_GMRES_LEARNED || prm.solver == SDDDST_SOLVER_GMRES_NEUMANN)) {
         if (!d_xasm && cudaMalloc(&d_xasm, sizeof(double) * n) != cudaSuccess) {
             err = "out of device memory";
@@ -259,7 +260,8 @@ int Engine::assemble(const double *x)
 // next matrix.
 int Engine::solve(double h, const double *rhs, double *x_out)
 {
-    if (prm.solver == SDDDST_SOLVER_DIRECT) return direct_solve(*this, h, d_dvec, rhs, x_out);
+    if (prm.solver == SDDDST_SOLVER_DIRECT || prm.solver == SDDDST_SOLVER_DIRECT_MIXED)
+        return direct_solve(*this, h, d_dvec, rhs, x_out);
     if (prm.solver == SDDDST_SOLVER_GMRES_LEARNED || prm.solver == SDDDST_SOLVER_GMRES_NEUMANN) {
         // GMRES preconditioned by B + C; on a stall, the device sparse LU of
         // the same matrix (analysed at the assembly positions)
@@ -293,7 +295,8 @@ int Engine::solve(double h, const double *rhs, double *x_out)
 int Engine::prepare_solver(double h)
 {
     if (prm.solver == SDDDST_SOLVER_GMRES_CLUSTER) return precond_build(*this, h, d_dvec);
-    if (prm.solver == SDDDST_SOLVER_DIRECT) return direct_factor(*this, h, d_dvec);
+    if (prm.solver == SDDDST_SOLVER_DIRECT || prm.solver == SDDDST_SOLVER_DIRECT_MIXED)
+        return direct_factor(*this, h, d_dvec);
     if (prm.solver == SDDDST_SOLVER_GMRES_LEARNED || prm.solver == SDDDST_SOLVER_GMRES_NEUMANN) {
         if (int rc = precond_build(*this, h, d_dvec)) return rc;
         return learned_build(*this, h, d_dvec, d_xasm, prm.solver == SDDDST_SOLVER_GMRES_NEUMANN);

@@ -73,5 +73,6 @@ def test_header_enums_match_binding(engine_lib):
     txt = open(HEADER).read()
     enums = dict((k, int(v)) for k, v in re.findall(r"SDDDST_((?:SOLVER|FIELD)_\w+) = (\d+)", txt))
     for name in ("SOLVER_GMRES", "SOLVER_GMRES_JACOBI", "SOLVER_GMRES_CLUSTER", "SOLVER_DIRECT",
-                 "SOLVER_GMRES_LEARNED", "SOLVER_GMRES_NEUMANN", "FIELD_ANALYTIC", "FIELD_TABULATED"):
+                 "SOLVER_GMRES_LEARNED", "SOLVER_GMRES_NEUMANN", "SOLVER_DIRECT_MIXED", "FIELD_ANALYTIC",
+                 "FIELD_TABULATED"):
         assert enums[name] == getattr(engine_lib, name), name

@@ -134,3 +134,60 @@ def test_direct_matches_gmres_trajectory_config2(engine_lib):
         assert a[0] == a[1], k
         x0, x1 = engines[0].config(0)[:, 0], engines[1].config(0)[:, 0]
         assert np.abs(x0 - x1).max() <= 1e-9, k
+
+
+def test_direct_mixed_solve_residual(engine_lib):
+    """SDDDST_SOLVER_DIRECT_MIXED: FP32 fronts, FP64 refinement to the solver
+    tolerance (relative residual 1e-12 against the device's own J)."""
+    import scipy.sparse as sp
+    from sdddst_b200 import capi
+    n, p = 4096, 256
+    xyb, pd = workloads.dislocations(n, 1, p)
+    prm = capi.cli_params(n, 1.0, 1e-7, p=p, pd_scaling=True, stress_kind=capi.STRESS_CONSTANT, stress_value=0.01,
+                          solver=capi.SOLVER_DIRECT_MIXED)
+    e = capi.Engine(prm, xyb, pd)
+    for h in (1e-6, 1e-4):
+        rp, col, val, d = e.jacobian(h, xyb)
+        J = sp.csr_matrix((val, col, rp), shape=(n, n))
+        b = np.random.default_rng(2).standard_normal(n)
+        x, refinements = e.solve(h, xyb, b)
+        assert refinements <= 10
+        assert np.linalg.norm(J @ x - b) <= 1e-12 * np.linalg.norm(b)
+
+
+def test_precision_workload_one_step_against_fp64(engine_lib):
+    """The precision workload (N=16384, seed 2, cutoff multiplier 1): FP32 pair
+    terms with FP64 accumulation, FP32 Jacobian values, FP32 LU with FP64
+    refinement, against the plain FP64 path (FP64 pair sum, FP64 LU) one
+    step from the same state: velocities within 1e-5 relative, positions
+    within 1e-8 (the bar of the precision forms)."""
+    from sdddst_b200 import capi
+    n = 16384
+    xyb, _ = workloads.dislocations(n, 2)
+    common = dict(step_size=1e-6)
+    e32 = capi.Engine(capi.cli_params(n, 1.0, 1e-5, pairsum=capi.PAIRSUM_FP32, solver=capi.SOLVER_DIRECT_MIXED,
+                                      **common), xyb)
+    e64 = capi.Engine(capi.cli_params(n, 1.0, 1e-5, pairsum=capi.PAIRSUM_FP64, solver=capi.SOLVER_DIRECT, **common),
+                      xyb)
+    v32, _ = e32.speeds(xyb)
+    v64, _ = e64.speeds(xyb)
+    assert np.abs(v32 - v64).max() <= 1e-5 * np.abs(v64).max()
+    # the step size adapts first (the initial 1e-6 is rejected for close
+    # pairs); then one step from the same accepted state on both paths
+    accepted = 0
+    for _ in range(12):
+        accepted += e64.step()
+        if accepted >= 3:
+            break
+    assert accepted >= 3
+    for attempt in range(10):
+        x, sc = e64.config(0), e64.scalars()
+        for e in (e32, e64):
+            e.set_state(x, sc["step_size"], sc["sim_time"], sc["energy"], sc["strain"], False)
+        a32, a64 = e32.step(), e64.step()
+        assert a32 == a64, (attempt, sc["step_size"], e32.scalars(), e64.scalars())
+        if a64:
+            for which in (1, 2, 3):
+                assert np.abs(e32.config(which)[:, 0] - e64.config(which)[:, 0]).max() <= 1e-8, which
+            return
+    pytest.fail("no accepted step in 10 attempts")
