@@ -54,6 +54,7 @@ UNIT = "steps/s"
 N_FULL = 32768
 SEED = 4
 CUTOFF_M = 2.0
+PAIR_F32_DRAM_BYTES_N32768 = 812544 + 8764672  # measured, see the roofline note in main()
 PREC = 1e-5
 H0 = 1e-6
 # Pair-sum FLOP convention: tau_xy = 130 FP operations per unique pair.
@@ -342,8 +343,18 @@ def profile_target(args):
         ms = eng.profile_pair_sum(args.reps)
         print(json.dumps({"target": "pairsum", "n": args.n, "pairsum": args.pairsum, "ms_per_launch": ms}))
     else:
+        # `warmup` untimed attempts (the step size adapts), then `steps`
+        # attempts inside the NVTX range "steps" (ncu --nvtx --nvtx-include steps/)
+        import torch
+        for _ in range(args.warmup):
+            eng.step()
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("steps")
         acc = sum(eng.step() for _ in range(args.steps))
-        print(json.dumps({"target": "step", "n": args.n, "accepted": acc, "steps": args.steps}))
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        print(json.dumps({"target": "step", "n": args.n, "accepted": acc, "steps": args.steps,
+                          "warmup": args.warmup}))
     eng.close()
 
 
@@ -463,8 +474,11 @@ def main():
     peak_src = "measured (FMA chain microbenchmark, sdddst_vector_peaks)" if peak else "nominal"
     if not peak:
         peak = 80.0 if args.pairsum == "fp32" else 40.0
+    # DRAM traffic of one full-size launch (dram__bytes_read.sum + dram__bytes_write.sum, one ncu
+    # capture at N=32768, profiles/pair_tiles_f32_n16384.md): positions read, partials mostly in L2
+    traffic = PAIR_F32_DRAM_BYTES_N32768 if (args.pairsum == "fp32" and args.n == N_FULL) else None
     roof = {"bound": args.pairsum, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+            "frac": achieved / peak, "traffic": traffic, "traffic_unit": "bytes per launch", "peak_source": peak_src,
             "kernel": "pair_tiles_kernel (one velocity evaluation)",
             "work": f"{FLOP_PER_PAIR:.0f} FLOP x N(N-1)/2 unique pairs", "ms": t_pair_ms}
 

@@ -16,7 +16,10 @@
 //    t = 2 E^{-+1} e^{-2 pi k} the sums over k = 2..4 collapse to
 //    polynomials in dx with constant coefficients (the t^2 part is kept for
 //    k = 2 only; for k >= 3 it is below 3e-7 of a term that is itself below
-//    1e-7 of tau).
+//    1e-7 of tau);
+//  * the reference's end image (weight |dx|, at |u| >= 4.5: below 5e-11 in
+//    tau_xy) and the partial weight of the k = 4 image (below 1e-9) are left
+//    out: both are far below the FP32 resolution of the sum.
 #pragma once
 
 #include "common.cuh"
@@ -31,8 +34,6 @@ constexpr float kQP1 = 535.4916555247647f;                       // e^{2 pi}
 constexpr float kQN1 = 1.8674427317079889e-03f;                  // e^{-2 pi}
 constexpr float kQN2 = 3.4873423562089956e-06f;
 constexpr float kQN3 = 6.512412136079901e-09f;
-constexpr float kQN4 = 1.2161556709409309e-11f;
-constexpr float kQN5 = 2.2711010683240937e-14f;
 constexpr float kA1 = 3.4938669795049805e-06f;                   // qn2 + qn3 + qn4
 constexpr float kB1 = 6.994256639099779e-06f;                    // 2 qn2 + 3 qn3 + 4 qn4
 constexpr float kQN2SQ = 1.2161556709409309e-11f;                // qn2^2 = qn4
@@ -73,7 +74,6 @@ __device__ __forceinline__ float tau_xy_f32(float dx, float dy)
     const float sh = fabsf(a) < 0.5f ? poly : 0.5f * (ep - epi);
     const float sh2 = sh * sh;
     const float E = ep * ep, Ei = epi * epi;
-    const bool pos = dx >= 0.0f;
 
     // k = 0
     const float D0 = 2.0f * (sh2 + sn2);
@@ -95,15 +95,8 @@ __device__ __forceinline__ float tau_xy_f32(float dx, float dy)
     // |u| >= 1.5: first-order sums over k = 2..4 (+k side uses E^-1, -k side E)
     const float c2 = fmaf(2.0f * cy, cy, -1.0f);
     const float base = dx * kA1;
-    const float w4 = pos ? -dx * (dx + 4.0f) * kQN4 : dx * (dx - 4.0f) * kQN4;
-    const float S1p = base + kB1 + (pos ? w4 : 0.0f);
-    const float S1m = base - kB1 + (pos ? 0.0f : w4);
-    float far = 2.0f * cy * fmaf(Ei, S1p, E * S1m);
+    float far = 2.0f * cy * fmaf(Ei, base + kB1, E * (base - kB1));
     far = fmaf(4.0f * c2 * kQN2SQ, fmaf(Ei * Ei, dx + 2.0f, E * E * (dx - 2.0f)), far);
-    // end image: -5 (dx >= 0) or +5 (dx < 0), weight |dx|
-    const float t5 = 2.0f * (pos ? E : Ei) * kQN5;
-    const float u5 = pos ? dx - 5.0f : dx + 5.0f;
-    far = fmaf(fabsf(dx) * u5 * t5, fmaf(c2, t5, cy), far);
     return (acc + far) * kTwoPiSqF;
 }
 
@@ -119,7 +112,10 @@ namespace sd {
 //                   + ((2 cy^2 - 1) + 2 pi |u| (2 - 4 cy^2)) t^2 ] + O(t^3),
 //   f(u)  = 2 pi^2 u cy t + O(t^2),
 // with the second order kept for k = 2 only and the k = 2..4 first-order sums
-// collapsed to polynomials in dx.
+// collapsed to polynomials in dx.  The end image, the partial weight of the
+// k = 4 image and the end/edge difference of the reference's weighting are
+// left out (each below 1.2e-6 absolute, while |d tau / dx| >= 4 over the
+// cell: below the FP32 resolution of the value).
 __device__ __forceinline__ float tau_xy_dx_f32(float dx, float dy)
 {
     const float twopi = 6.28318530717959f;
@@ -135,7 +131,6 @@ __device__ __forceinline__ float tau_xy_dx_f32(float dx, float dy)
     const float ch = 0.5f * (ep + epi);
     const float sh2 = sh * sh;
     const float E = ep * ep, Ei = epi * epi;
-    const bool pos = dx >= 0.0f;
 
     // k = 0
     const float D0 = 2.0f * (sh2 + sn2);
@@ -157,10 +152,8 @@ __device__ __forceinline__ float tau_xy_dx_f32(float dx, float dy)
         acc = fmaf(rm * rm, fmaf(twopi * (dx - 1.0f) * Sm, fmaf(-2.0f * Nm, rm, cy), Nm), acc);
     }
     // |k| = 2..4, first order, + side (E^-1) and - side (E)
-    const float sp = fmaf(1.0f - twopi * dx, kA1, -twopi * kB1) -
-                     (pos ? dx * kQN4 * (1.0f - twopi * (dx + 4.0f)) : 0.0f);
-    const float sm = fmaf(1.0f + twopi * dx, kA1, -twopi * kB1) +
-                     (pos ? 0.0f : dx * kQN4 * (1.0f - twopi * (4.0f - dx)));
+    const float sp = fmaf(1.0f - twopi * dx, kA1, -twopi * kB1);
+    const float sm = fmaf(1.0f + twopi * dx, kA1, -twopi * kB1);
     float far = 2.0f * cy * fmaf(Ei, sp, E * sm);
     // second order, k = 2
     {
@@ -169,13 +162,6 @@ __device__ __forceinline__ float tau_xy_dx_f32(float dx, float dy)
         far = fmaf(tp * tp, fmaf(twopi * (dx + 2.0f), c4, c2), far);
         far = fmaf(tm * tm, fmaf(twopi * (2.0f - dx), c4, c2), far);
     }
-    // end image (weight |dx|) and sigma (f(u_end) - f(u_edge))
-    const float te = 2.0f * (pos ? E : Ei) * kQN5;
-    const float ue_abs = pos ? 5.0f - dx : 5.0f + dx;
-    far = fmaf(fabsf(dx) * cy * te, fmaf(-twopi, ue_abs, 1.0f), far);
-    const float fe = (pos ? dx - 5.0f : dx + 5.0f) * te * cy;
-    const float fg = (pos ? (dx + 4.0f) * 2.0f * Ei * kQN4 : (dx - 4.0f) * 2.0f * E * kQN4) * cy;
-    far += pos ? fe - fg : fg - fe;
     return (acc + far) * kTwoPiSqF;
 }
 

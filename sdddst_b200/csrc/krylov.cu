@@ -375,7 +375,6 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
     const int stride = 2 * (m + 1) + 1; // per-iteration record: c1[m+1], c2[m+1], nrm2
     double *V = e.d_V, *w = e.d_w, *z = e.d_z, *r = e.d_r;
     double *dinv = nullptr;
-    const int wpb = 8;
     cudaMemsetAsync(x, 0, sizeof(double) * n, st);
     if (precond == 1) {
         dinv = e.d_y_small; // n doubles reserved for the diagonal
