@@ -1341,7 +1341,7 @@ int direct_solve(Engine &e, double h, const double *dvec, const double *rhs, dou
     for (int it = 0; it <= max_ref; ++it) {
         launch_spmv_J(e, h, dvec, x, e.d_w, e.st);
         resid_kernel<<<nb, 256, 0, e.st>>>(n, rhs, e.d_w, e.d_r);
-        e.launches += 2;
+        e.launches++;
         double rn2 = 0.0;
         if (int rc = e.sum_sq(e.d_r, &rn2)) return rc;
         if (!std::isfinite(rn2)) break;

@@ -50,6 +50,9 @@ struct Engine {
     float *d_valf = nullptr;   // FP32 values (mixed path)
     bool valf = false;         // which of the two holds G
     double *d_gdiag = nullptr; // G_ii in FP64 (both paths)
+    int *d_col_s = nullptr;    // column positions in the cell-sorted order (SpMV gathers; diagonal slot unused)
+    double *d_vsort = nullptr; // SpMV input gathered into the cell-sorted order
+    bool col_s_valid = false;  // d_col_s matches the assembled CSR
     double *d_hrow = nullptr;  // per-row step size of a batch of systems (null: one system, scalar h)
     long nnz_cap = 0, nnz = 0;
     int *d_flag = nullptr; // device-side error flag of the assembly
@@ -142,7 +145,7 @@ int alloc_csr_values(Engine &e, long cap);
 void launch_make_dvec(const Engine &e, double h, double *dvec, cudaStream_t st);
 void launch_export_jacobian(const Engine &e, double h, const double *dvec, double *val_out, cudaStream_t st);
 
-void launch_spmv_J(const Engine &e, double h, const double *dvec, const double *v, double *y, cudaStream_t st);
+void launch_spmv_J(Engine &e, double h, const double *dvec, const double *v, double *y, cudaStream_t st);
 int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, double *x, int precond);
 
 void launch_residual_g(const Engine &e, double h, const double *xn, const double *xo, const double *csp,

@@ -170,7 +170,7 @@ __global__ void row_fill_kernel(int n, const double *__restrict__ x, const doubl
                                 const int *__restrict__ rowptr, int *__restrict__ col, VT *__restrict__ val,
                                 double *__restrict__ gdiag, int p, const double *__restrict__ pdx,
                                 const double *__restrict__ pdy, double A, double K, int *__restrict__ flag,
-                                const double *__restrict__ tab_dx)
+                                const double *__restrict__ tab_dx, int *__restrict__ col_s)
 {
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -199,7 +199,10 @@ __global__ void row_fill_kernel(int n, const double *__restrict__ x, const doubl
             }
             unsigned m = __ballot_sync(0xffffffffu, hit);
             const int at = pos + __popc(m & ((1u << lane) - 1u));
-            if (hit && at < rowend) col[at] = j;
+            if (hit && at < rowend) {
+                col[at] = j;
+                col_s[at] = k; // position of j in the cell-sorted order
+            }
             pos += __popc(m);
         }
     });
@@ -286,6 +289,10 @@ int alloc_csr_values(Engine &e, long cap)
     e.d_val = nullptr;
     e.d_valf = nullptr;
     if (cudaMalloc(&e.d_col, sizeof(int) * cap) != cudaSuccess) return SDDDST_ERR_NOMEM;
+    if (e.d_col_s) cudaFree(e.d_col_s);
+    e.d_col_s = nullptr;
+    e.col_s_valid = false;
+    if (cudaMalloc(&e.d_col_s, sizeof(int) * cap) != cudaSuccess) return SDDDST_ERR_NOMEM;
     if (e.valf) {
         if (cudaMalloc(&e.d_valf, sizeof(float) * cap) != cudaSuccess) return SDDDST_ERR_NOMEM;
     } else {
@@ -340,12 +347,12 @@ int jacobian_assemble(Engine &e, const double *x)
         row_fill_kernel<float><<<rb, 32 * wpb, 0, st>>>(n, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr,
                                                        e.one_per_cutoff_sqr, e.d_rowptr, e.d_col, e.d_valf,
                                                        e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag,
-                                                       e.d_tab_dx);
+                                                       e.d_tab_dx, e.d_col_s);
     else
         row_fill_kernel<double><<<rb, 32 * wpb, 0, st>>>(n, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr,
                                                         e.one_per_cutoff_sqr, e.d_rowptr, e.d_col, e.d_val,
                                                         e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag,
-                                                        e.d_tab_dx);
+                                                        e.d_tab_dx, e.d_col_s);
     e.launches += 1;
     int flag = 0;
     cudaMemcpyAsync(&flag, e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -354,6 +361,7 @@ int jacobian_assemble(Engine &e, const double *x)
         e.err = "jacobian: neighbour count and fill passes disagree";
         return SDDDST_ERR_CAPACITY;
     }
+    e.col_s_valid = true;
     return 0;
 }
 

@@ -35,6 +35,31 @@ __global__ void spmv_j_kernel(int n, double h, const double *__restrict__ hrow, 
     if (lane == 0) y[row] = v[row] + (1.0 + dvec[row]) * 0.5 * hh * acc;
 }
 
+// The same product with the off-diagonal gathers taken from a copy of v in
+// the cell-sorted order (vs[k] = v[sorted[k]]): a row's neighbours then lie in
+// nine contiguous runs of vs instead of random sectors of v.
+template <typename VT>
+__global__ void spmv_js_kernel(int n, double h, const int *__restrict__ rowptr, const int *__restrict__ col_s,
+                               const VT *__restrict__ val, const double *__restrict__ dvec,
+                               const double *__restrict__ v, const double *__restrict__ vs, double *__restrict__ y)
+{
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const int s = rowptr[row], e = rowptr[row + 1];
+    double acc = lane == 0 ? (double)val[s] * v[row] : 0.0; // diagonal slot
+    for (int q = s + 1 + lane; q < e; q += 32) acc += (double)val[q] * vs[col_s[q]];
+    acc = warp_sum(acc);
+    if (lane == 0) y[row] = v[row] + (1.0 + dvec[row]) * 0.5 * h * acc;
+}
+
+__global__ void gather_sorted_kernel(int n, const int *__restrict__ sorted, const double *__restrict__ v,
+                                     double *__restrict__ vs)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) vs[k] = v[sorted[k]];
+}
+
 // diag(J)_i = 1 + (1 + d_i)/2 h G_ii
 __global__ void jdiag_inv_kernel(int n, double h, const double *__restrict__ hrow, const double *__restrict__ gdiag,
                                  const double *__restrict__ dvec, double *__restrict__ dinv)
@@ -255,9 +280,21 @@ int Engine::max_ratio(double *out)
     return 0;
 }
 
-void launch_spmv_J(const Engine &e, double h, const double *dvec, const double *v, double *y, cudaStream_t st)
+void launch_spmv_J(Engine &e, double h, const double *dvec, const double *v, double *y, cudaStream_t st)
 {
     const int wpb = 8;
+    e.launches++;
+    if (e.col_s_valid && !e.d_hrow) {
+        e.launches++;
+        gather_sorted_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, e.d_sorted, v, e.d_vsort);
+        if (e.valf)
+            spmv_js_kernel<float><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_rowptr, e.d_col_s,
+                                                                              e.d_valf, dvec, v, e.d_vsort, y);
+        else
+            spmv_js_kernel<double><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_rowptr, e.d_col_s,
+                                                                               e.d_val, dvec, v, e.d_vsort, y);
+        return;
+    }
     if (e.valf)
         spmv_j_kernel<float><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_hrow, e.d_rowptr, e.d_col,
                                                                          e.d_valf, dvec, v, y);
@@ -444,7 +481,7 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
                 gs_fused_kernel<2><<<e.gs_blocks, 256, 0, st>>>(n, kk, V, ldv, w, rec + (m + 1), rec + 2 * (m + 1),
                                                                  e.d_partials, e.d_counter);
                 normalize_kernel<<<nb, 256, 0, st>>>(n, w, rec + 2 * (m + 1), V + (size_t)(jj + 1) * ldv);
-                e.launches += 5;
+                e.launches += 4;
             }
             cudaMemcpyAsync(hrec + (size_t)j * stride, e.d_hrec + (size_t)j * stride,
                             sizeof(double) * stride * (jend - j), cudaMemcpyDeviceToHost, st);
@@ -509,7 +546,7 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
         sub_kernel<<<nb, 256, 0, st>>>(n, rhs, w, r);
         gs_fused_kernel<3><<<e.gs_blocks, 256, 0, st>>>(n, 1, nullptr, ldv, r, nullptr, e.d_scal, e.d_partials,
                                                          e.d_counter);
-        e.launches += 3;
+        e.launches += 2;
         cudaMemcpyAsync(e.h_scal, e.d_scal, sizeof(double), cudaMemcpyDeviceToHost, st);
         if (int rc = e.sync_check("gmres restart")) return rc;
         beta = std::sqrt(e.h_scal[0]);
