@@ -37,7 +37,7 @@ Engine::~Engine()
                     d_g, d_sol, d_dvec, d_tol, d_tol_last, d_minr2, d_part, d_pdx, d_pdy, d_cell,
                     d_cell_count, d_cell_start, d_cell_fill, d_sorted, d_rowcnt, d_rowptr, d_col, d_val,
                     d_V, d_w, d_z, d_r, d_hcol, d_partials, d_scal, d_y_small, d_ys, d_bs, d_flag, d_xw,
-                    d_gdiag, d_valf, d_col_s, d_vsort};
+                    d_gdiag, d_valf, d_col_s, d_vsort, d_xsrt, d_ysrt, d_bsrt};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (h_scal) cudaFreeHost(h_scal);
@@ -123,7 +123,7 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     int rc = 0;
     double **vecs[] = {&d_x0, &d_y, &d_b, &d_xb, &d_x1, &d_x2, &d_xs, &d_v0, &d_v0b, &d_vs, &d_vs2,
                        &d_S0, &d_S1, &d_Stmp, &d_g, &d_sol, &d_dvec, &d_tol, &d_tol_last, &d_w, &d_z,
-                       &d_r, &d_ys, &d_bs, &d_xw, &d_gdiag, &d_vsort};
+                       &d_r, &d_ys, &d_bs, &d_xw, &d_gdiag, &d_vsort, &d_xsrt, &d_ysrt, &d_bsrt};
     for (double **v : vecs) rc |= dalloc(v, n);
     rc |= dalloc(&d_minr2, n);
     rc |= dalloc(&d_part, batch_backend ? 1 : pair_part_doubles(n));

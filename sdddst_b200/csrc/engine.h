@@ -52,6 +52,7 @@ struct Engine {
     double *d_gdiag = nullptr; // G_ii in FP64 (both paths)
     int *d_col_s = nullptr;    // column positions in the cell-sorted order (SpMV gathers; diagonal slot unused)
     double *d_vsort = nullptr; // SpMV input gathered into the cell-sorted order
+    double *d_xsrt = nullptr, *d_ysrt = nullptr, *d_bsrt = nullptr; // x, y, b in the cell-sorted order
     bool col_s_valid = false;  // d_col_s matches the assembled CSR
     double *d_hrow = nullptr;  // per-row step size of a batch of systems (null: one system, scalar h)
     long nnz_cap = 0, nnz = 0;

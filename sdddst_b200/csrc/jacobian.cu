@@ -105,6 +105,8 @@ struct CellScan {
     int G;
     const int *start;
     const int *sorted;
+    const double *xs, *ys; // positions in the cell-sorted order (contiguous per cell)
+    double keep_below, keep_above; // r^2 bounds of the cheap decision (see pair_kept_search)
 };
 
 // Visits the cells around (cx, cy) once each: 3x3 for G >= 3, all cells
@@ -138,6 +140,29 @@ __device__ __forceinline__ bool pair_kept(double r2, double c, double c2, double
     return keep;
 }
 
+// pair_kept without its weight, for the neighbour search: r^2 more than 1e-6
+// (relative) inside or outside the pattern radius (1 + sqrt(36.8)) c is
+// decided without the square root; only the thin shell between takes the
+// reference's rounded test, so every decision equals pair_kept's.
+__device__ __forceinline__ bool pair_kept_search(double r2, double c, double c2, double ic2, const CellScan &cs)
+{
+    if (r2 < cs.keep_below) return true;
+    if (r2 > cs.keep_above) return false;
+    return pair_kept(r2, c, c2, ic2, nullptr);
+}
+
+__global__ void gather_cells_kernel(int n, const int *__restrict__ sorted, const double *__restrict__ x,
+                                    const double *__restrict__ y, const double *__restrict__ b,
+                                    double *__restrict__ xs, double *__restrict__ ys, double *__restrict__ bs)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int j = sorted[k];
+    xs[k] = x[j];
+    ys[k] = y[j];
+    bs[k] = b[j];
+}
+
 __global__ void row_count_kernel(int n, const double *__restrict__ x, const double *__restrict__ y, CellScan cs,
                                  double c, double c2, double ic2, int *__restrict__ rowcnt)
 {
@@ -153,10 +178,10 @@ __global__ void row_count_kernel(int n, const double *__restrict__ x, const doub
         for (int k = s + lane; k < e; k += 32) {
             const int j = cs.sorted[k];
             if (j == i) continue;
-            const int lo = i < j ? i : j, hi = i < j ? j : i;
-            double dx = wrap_half(x[hi] - x[lo]);
-            double dy = wrap_half(y[hi] - y[lo]);
-            cnt += pair_kept(r2_exact(dx, dy), c, c2, ic2, nullptr);
+            const double xj = cs.xs[k], yj = cs.ys[k];
+            double dx = wrap_half(i < j ? xj - xi : xi - xj); // x[hi] - x[lo], as the reference orders it
+            double dy = wrap_half(i < j ? yj - yi : yi - yj);
+            cnt += pair_kept_search(r2_exact(dx, dy), c, c2, ic2, cs);
         }
     });
 #pragma unroll
@@ -170,7 +195,8 @@ __global__ void row_fill_kernel(int n, const double *__restrict__ x, const doubl
                                 const int *__restrict__ rowptr, int *__restrict__ col, VT *__restrict__ val,
                                 double *__restrict__ gdiag, int p, const double *__restrict__ pdx,
                                 const double *__restrict__ pdy, double A, double K, int *__restrict__ flag,
-                                const double *__restrict__ tab_dx, int *__restrict__ col_s)
+                                const double *__restrict__ tab_dx, int *__restrict__ col_s,
+                                const double *__restrict__ bs)
 {
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -191,10 +217,10 @@ __global__ void row_fill_kernel(int n, const double *__restrict__ x, const doubl
             if (k < e) {
                 j = cs.sorted[k];
                 if (j != i) {
-                    const int lo = i < j ? i : j, hi = i < j ? j : i;
-                    double dx = wrap_half(x[hi] - x[lo]);
-                    double dy = wrap_half(y[hi] - y[lo]);
-                    hit = pair_kept(r2_exact(dx, dy), c, c2, ic2, nullptr);
+                    const double xj = cs.xs[k], yj = cs.ys[k];
+                    double dx = wrap_half(i < j ? xj - xi : xi - xj); // x[hi] - x[lo]
+                    double dy = wrap_half(i < j ? yj - yi : yi - yj);
+                    hit = pair_kept_search(r2_exact(dx, dy), c, c2, ic2, cs);
                 }
             }
             unsigned m = __ballot_sync(0xffffffffu, hit);
@@ -215,17 +241,17 @@ __global__ void row_fill_kernel(int n, const double *__restrict__ x, const doubl
     const int end = rowend;
     double rs = 0.0;
     for (int q = base + 1 + lane; q < end; q += 32) {
-        const int j = col[q];
-        const int lo = i < j ? i : j, hi = i < j ? j : i;
-        double dx = wrap_half(x[hi] - x[lo]);
-        double dy = wrap_half(y[hi] - y[lo]);
+        const int j = col[q], ks = col_s[q];
+        const double xj = cs.xs[ks], yj = cs.ys[ks];
+        double dx = wrap_half(i < j ? xj - xi : xi - xj); // x[hi] - x[lo]
+        double dy = wrap_half(i < j ? yj - yi : yi - yj);
         double w;
         pair_kept(r2_exact(dx, dy), c, c2, ic2, &w);
         double tdx;
         if (tab_dx) tdx = tau0_xy_dx(dx, dy) + tab_interp(tab_dx, dx, dy); // tabulated field
         else if (sizeof(VT) == sizeof(double)) tdx = tau_xy_dx_f64(dx, dy);
         else tdx = (double)tau_xy_dx_f32(__double2float_rn(dx), __double2float_rn(dy));
-        const VT v = (VT)(bi * b[j] * tdx * w);
+        const VT v = (VT)(bi * bs[ks] * tdx * w);
         val[q] = v;
         rs += (double)v;
     }
@@ -322,13 +348,15 @@ int jacobian_assemble(Engine &e, const double *x)
     scan_kernel<<<1, 1024, 0, st>>>(e.d_cell_count, ncell, e.d_cell_start);
     cell_scatter_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, e.d_cell, e.d_cell_start, e.d_cell_fill, e.d_rowcnt);
     cell_sort_kernel<<<ncell, 256, 0, st>>>(e.d_cell_start, e.d_rowcnt, e.d_sorted);
-    CellScan cs{G, e.d_cell_start, e.d_sorted};
+    gather_cells_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, e.d_sorted, x, e.d_y, e.d_b, e.d_xsrt, e.d_ysrt, e.d_bsrt);
+    const double rp = e.cutoff * (1.0 + std::sqrt(36.8));
+    CellScan cs{G, e.d_cell_start, e.d_sorted, e.d_xsrt, e.d_ysrt, rp * rp * (1.0 - 1e-6), rp * rp * (1.0 + 1e-6)};
     const int wpb = 8; // warps per block
     const unsigned rb = (unsigned)((n + wpb - 1) / wpb);
     row_count_kernel<<<rb, 32 * wpb, 0, st>>>(n, x, e.d_y, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr,
                                               e.d_rowcnt);
     scan_kernel<<<1, 1024, 0, st>>>(e.d_rowcnt, n, e.d_rowptr);
-    e.launches += 7;
+    e.launches += 8;
     int total = 0;
     if (cudaMemcpyAsync(&total, e.d_rowptr + n, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return SDDDST_ERR_CUDA;
@@ -347,12 +375,12 @@ int jacobian_assemble(Engine &e, const double *x)
         row_fill_kernel<float><<<rb, 32 * wpb, 0, st>>>(n, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr,
                                                        e.one_per_cutoff_sqr, e.d_rowptr, e.d_col, e.d_valf,
                                                        e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag,
-                                                       e.d_tab_dx, e.d_col_s);
+                                                       e.d_tab_dx, e.d_col_s, e.d_bsrt);
     else
         row_fill_kernel<double><<<rb, 32 * wpb, 0, st>>>(n, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr,
                                                         e.one_per_cutoff_sqr, e.d_rowptr, e.d_col, e.d_val,
                                                         e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag,
-                                                        e.d_tab_dx, e.d_col_s);
+                                                        e.d_tab_dx, e.d_col_s, e.d_bsrt);
     e.launches += 1;
     int flag = 0;
     cudaMemcpyAsync(&flag, e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
