@@ -36,7 +36,7 @@ Engine::~Engine()
     void *bufs[] = {d_x0, d_y, d_b, d_xb, d_x1, d_x2, d_xs, d_v0, d_v0b, d_vs, d_vs2, d_S0, d_S1, d_Stmp,
                     d_g, d_sol, d_dvec, d_tol, d_tol_last, d_minr2, d_part, d_pdx, d_pdy, d_cell,
                     d_cell_count, d_cell_start, d_cell_fill, d_sorted, d_rowcnt, d_rowptr, d_col, d_val,
-                    d_V, d_w, d_z, d_r, d_hcol, d_partials, d_scal, d_y_small, d_ys, d_bs, d_flag, d_xw,
+                    d_V, d_w, d_z, d_r, d_hcol, d_partials, d_gs_partials, d_scal, d_y_small, d_ys, d_bs, d_flag, d_xw,
                     d_gdiag, d_valf, d_col_s, d_vsort, d_xsrt, d_ysrt, d_bsrt};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -142,6 +142,8 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     rc |= dalloc(&d_V, (size_t)(restart + 1) * n);
     rc |= dalloc(&d_hcol, 2 * (restart + 1) + 4);
     rc |= dalloc(&d_partials, (size_t)red_blocks * 32 + 64);
+    rc |= dalloc(&d_gs_partials, (size_t)3 * gs_blocks * 32);
+    coop_gs = gs_coop_supported(device, gs_blocks);
     rc |= dalloc(&d_hrec, (size_t)(restart + 1) * (2 * (restart + 1) + 1));
     rc |= dalloc(&d_counter, 4);
     if (cudaMallocHost((void **)&h_hrec, sizeof(double) * (restart + 1) * (2 * (restart + 1) + 1)) != cudaSuccess)

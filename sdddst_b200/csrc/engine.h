@@ -73,6 +73,8 @@ struct Engine {
     double *d_hrec = nullptr;             // per-iteration Gram-Schmidt records
     double *h_hrec = nullptr;             // pinned copy
     unsigned int *d_counter = nullptr;    // last-block ticket of the fused reductions
+    bool coop_gs = false;                 // one cooperative launch per Gram-Schmidt step
+    double *d_gs_partials = nullptr;      // its per-CTA partial sums (3 x gs_blocks x 32)
 
     // ---- cluster block-Jacobi preconditioner (precond.cu)
     int *pc_ptr = nullptr, *pc_parent = nullptr, *pc_tmp = nullptr, *pc_tmp2 = nullptr, *pc_members = nullptr;
@@ -148,6 +150,7 @@ void launch_export_jacobian(const Engine &e, double h, const double *dvec, doubl
 
 void launch_spmv_J(Engine &e, double h, const double *dvec, const double *v, double *y, cudaStream_t st);
 int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, double *x, int precond);
+bool gs_coop_supported(int device, int blocks);
 
 void launch_residual_g(const Engine &e, double h, const double *xn, const double *xo, const double *csp,
                        const double *isp, const double *dvec, double *g, cudaStream_t st);

@@ -12,6 +12,8 @@
 #include "engine.h"
 #include "common.cuh"
 
+#include <cooperative_groups.h>
+
 #include <cmath>
 #include <vector>
 
@@ -383,6 +385,99 @@ __global__ void __launch_bounds__(256) gs_fused_kernel(int n, int kk, const doub
     if (tid == 0) *counter = 0u;
 }
 
+// One whole Gram-Schmidt step of GMRES in a single cooperative launch (one
+// CTA per SM, grid-wide barriers between the passes): c1 = V^T w, w -= V c1,
+// c2 = V^T w, w -= V c2, nrm2 = |w|^2, V_{k+1} = w / sqrt(nrm2).  Each CTA owns
+// a contiguous range of the vectors; the per-CTA partial sums are reduced by
+// every CTA in the same fixed order (identical results, no further barrier).
+// rec receives c1 at [0, m1), c2 at [m1, 2 m1) and nrm2 at [2 m1], the layout
+// of the three separate passes.
+__device__ __forceinline__ void gs_block_dots(int kk, const double *__restrict__ V, size_t ldv, const double *w,
+                                              int s0, int e0, double (*red)[33], double *__restrict__ part,
+                                              bool norm_only)
+{
+    constexpr int KM = 32;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    double acc[KM];
+#pragma unroll
+    for (int k = 0; k < KM; ++k) acc[k] = 0.0;
+    for (int i = s0 + tid; i < e0; i += blockDim.x) {
+        const double wi = w[i];
+        if (norm_only) {
+            acc[0] += wi * wi;
+        } else {
+#pragma unroll
+            for (int k = 0; k < KM; ++k)
+                if (k < kk) acc[k] += V[(size_t)k * ldv + i] * wi;
+        }
+    }
+    const int nout = norm_only ? 1 : kk;
+#pragma unroll
+    for (int k = 0; k < KM; ++k) {
+        if (k < nout) {
+            const double v = warp_sum(acc[k]);
+            if (lane == 0) red[wid][k] = v;
+        }
+    }
+    __syncthreads();
+    if (tid < nout) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[q][tid];
+        part[tid] = t;
+    }
+    __threadfence();
+}
+
+__global__ void __launch_bounds__(256) gs_iter_kernel(int n, int kk, const double *__restrict__ V, size_t ldv,
+                                                      double *__restrict__ w, double *__restrict__ rec, int m1,
+                                                      double *__restrict__ partials, double *__restrict__ vnext)
+{
+    namespace cg = cooperative_groups;
+    cg::grid_group grid = cg::this_grid();
+    constexpr int KM = 32;
+    __shared__ double cs[KM];
+    __shared__ double red[8][KM + 1];
+    const int tid = threadIdx.x, nb = gridDim.x;
+    const int chunk = (n + nb - 1) / nb;
+    const int s0 = blockIdx.x * chunk, e0 = min(n, s0 + chunk);
+    for (int pass = 0; pass < 2; ++pass) {
+        double *part = partials + ((size_t)pass * nb) * KM;
+        gs_block_dots(kk, V, ldv, w, s0, e0, red, part + (size_t)blockIdx.x * KM, false);
+        grid.sync();
+        if (tid < kk) {
+            double t = 0.0;
+            for (int b = 0; b < nb; ++b) t += part[(size_t)b * KM + tid];
+            cs[tid] = t;
+            if (blockIdx.x == 0) rec[pass * m1 + tid] = t;
+        }
+        __syncthreads();
+        for (int i = s0 + tid; i < e0; i += blockDim.x) {
+            double u = 0.0;
+            for (int k = 0; k < kk; ++k) u += V[(size_t)k * ldv + i] * cs[k];
+            w[i] -= u;
+        }
+        __syncthreads();
+    }
+    double *part = partials + ((size_t)2 * nb) * KM;
+    gs_block_dots(kk, V, ldv, w, s0, e0, red, part + (size_t)blockIdx.x * KM, true);
+    grid.sync();
+    double nrm2 = 0.0;
+    for (int b = 0; b < nb; ++b) nrm2 += part[(size_t)b * KM];
+    if (blockIdx.x == 0 && tid == 0) rec[2 * m1] = nrm2;
+    for (int i = s0 + tid; i < e0; i += blockDim.x) vnext[i] = nrm2 > 0.0 ? w[i] * rsqrt(nrm2) : 0.0;
+}
+
+// The cooperative Gram-Schmidt step runs when the device supports cooperative
+// launches and `blocks` CTAs of it fit on the device at once.
+bool gs_coop_supported(int device, int blocks)
+{
+    int coop = 0, sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess || !coop) return false;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return false;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gs_iter_kernel, 256, 0) != cudaSuccess) return false;
+    return blocks <= per_sm * sms;
+}
+
 // V_{j+1} = w / sqrt(nrm2) (zero vector on breakdown)
 __global__ void normalize_kernel(int n, const double *__restrict__ w, const double *__restrict__ nrm2,
                                  double *__restrict__ v)
@@ -474,6 +569,20 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
                 launch_spmv_J(e, h, dvec, src, w, st);
                 double *rec = e.d_hrec + (size_t)jj * stride;
                 const int kk = jj + 1;
+                if (e.coop_gs) {
+                    int a_n = n, a_kk = kk, a_m1 = m + 1;
+                    size_t a_ldv = ldv;
+                    double *a_V = V, *a_w = w, *a_rec = rec, *a_part = e.d_gs_partials;
+                    double *a_next = V + (size_t)(jj + 1) * ldv;
+                    void *args[] = {&a_n, &a_kk, &a_V, &a_ldv, &a_w, &a_rec, &a_m1, &a_part, &a_next};
+                    if (cudaLaunchCooperativeKernel((const void *)gs_iter_kernel, dim3(e.gs_blocks), dim3(256), args,
+                                                    0, st) == cudaSuccess) {
+                        e.launches++;
+                        continue;
+                    }
+                    (void)cudaGetLastError(); // not launchable here: the separate passes from now on
+                    e.coop_gs = false;
+                }
                 gs_fused_kernel<0><<<e.gs_blocks, 256, 0, st>>>(n, kk, V, ldv, w, nullptr, rec, e.d_partials,
                                                                  e.d_counter);
                 gs_fused_kernel<1><<<e.gs_blocks, 256, 0, st>>>(n, kk, V, ldv, w, rec, rec + (m + 1), e.d_partials,
