@@ -361,6 +361,28 @@ __global__ void apply_kernel(int n, const int *__restrict__ rowptr, const int *_
     if (lane == 0) z[i] += acc;
 }
 
+// z += C v with the off-diagonal gathers from vs, v in the cell-sorted order
+__global__ void apply_sorted_kernel(int n, const int *__restrict__ rowptr, const int *__restrict__ col_s,
+                                    const float *__restrict__ cval, const double *__restrict__ v,
+                                    const double *__restrict__ vs, double *__restrict__ z)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const int s = rowptr[i], e = rowptr[i + 1];
+    double acc = lane == 0 ? (double)cval[s] * v[i] : 0.0; // diagonal slot
+    for (int q = s + 1 + lane; q < e; q += 32) acc += (double)cval[q] * vs[col_s[q]];
+    acc = warp_sum(acc);
+    if (lane == 0) z[i] += acc;
+}
+
+__global__ void gather_sorted_v_kernel(int n, const int *__restrict__ sorted, const double *__restrict__ v,
+                                       double *__restrict__ vs)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) vs[k] = v[sorted[k]];
+}
+
 } // namespace
 
 static int learned_ensure(Engine &e)
@@ -475,6 +497,13 @@ int learned_build(Engine &e, double h, const double *dvec, const double *x, bool
 void learned_apply_add(Engine &e, const double *v, double *z)
 {
     Learned &L = *LN(e);
+    if (e.col_s_valid && !e.d_hrow) { // contiguous gathers (the SpMV's staging buffer, free here)
+        gather_sorted_v_kernel<<<(unsigned)((e.n + 255) / 256), 256, 0, e.st>>>(e.n, e.d_sorted, v, e.d_vsort);
+        apply_sorted_kernel<<<(unsigned)((e.n + 7) / 8), 256, 0, e.st>>>(e.n, e.d_rowptr, e.d_col_s, L.d_cval, v,
+                                                                         e.d_vsort, z);
+        e.launches += 2;
+        return;
+    }
     apply_kernel<<<(unsigned)((e.n + 7) / 8), 256, 0, e.st>>>(e.n, e.d_rowptr, e.d_col, L.d_cval, v, z);
     e.launches++;
 }

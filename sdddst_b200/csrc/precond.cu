@@ -29,7 +29,8 @@ template <typename VT>
 __global__ void strongest_kernel(int n, double h0, const double *__restrict__ hrow, double theta,
                                  const int *__restrict__ rowptr, const int *__restrict__ col,
                                  const VT *__restrict__ val, const double *__restrict__ gdiag,
-                                 const double *__restrict__ dvec, int *__restrict__ ptr)
+                                 const double *__restrict__ dvec, int *__restrict__ ptr,
+                                 const int *__restrict__ col_s, const double *__restrict__ msrt)
 {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -41,7 +42,8 @@ __global__ void strongest_kernel(int n, double h0, const double *__restrict__ hr
     int bj = i;
     for (int q = s + 1 + lane; q < e; q += 32) {
         const int j = col[q];
-        const double mjj = 2.0 / (1.0 + dvec[j]) + h * gdiag[j];
+        // M_jj from the cell-sorted copy when present (contiguous reads), else gathered
+        const double mjj = msrt ? msrt[col_s[q]] : 2.0 / (1.0 + dvec[j]) + h * gdiag[j];
         const double den = sqrt(fabs(mii) * fabs(mjj));
         const double sij = den > 0 ? h * fabs((double)val[q]) / den : 0.0;
         if (sij >= theta && (sij > best || (sij == best && j < bj))) {
@@ -59,6 +61,16 @@ __global__ void strongest_kernel(int n, double h0, const double *__restrict__ hr
         }
     }
     if (lane == 0) ptr[i] = best >= theta ? bj : i;
+}
+
+// M_jj = 2 / (1 + d_j) + h G_jj in the cell-sorted order (single system)
+__global__ void msorted_kernel(int n, double h, const int *__restrict__ sorted, const double *__restrict__ gdiag,
+                               const double *__restrict__ dvec, double *__restrict__ msrt)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int j = sorted[k];
+    msrt[k] = 2.0 / (1.0 + dvec[j]) + h * gdiag[j];
 }
 
 __global__ void root_init_kernel(int n, const int *__restrict__ ptr, int *__restrict__ parent)
@@ -180,18 +192,18 @@ __global__ void block_invert_kernel(int nb, double h0, const double *__restrict_
     for (int r = 0; r < k; ++r)
         for (int c = lane; c < 2 * k; c += 32) M[r][c] = (c - k == r) ? 1.0 : 0.0;
     __syncwarp();
-    // gather the block: each lane owns rows lane, lane + 32 (k <= 32: one)
-    if (lane < k) {
-        const int i = members[s + lane];
+    // gather the block, one member row at a time, the warp scanning the row
+    // (the columns of one row are distinct: no two lanes write one entry)
+    for (int r = 0; r < k; ++r) {
+        const int i = members[s + r];
         const double ci = (1.0 + dvec[i]) * 0.5 * h;
-        M[lane][lane] += ci * gdiag[i];
-        for (int q = rowptr[i] + 1; q < rowptr[i + 1]; ++q) {
+        for (int q = rowptr[i] + 1 + lane; q < rowptr[i + 1]; q += 32) {
             const int j = col[q];
-            if (blk_of[j] == b) M[lane][loc[j]] += ci * (double)val[q];
+            if (blk_of[j] == b) M[r][loc[j]] += ci * (double)val[q];
         }
-        M[lane][lane] += 1.0;
+        if (lane == 0) M[r][r] += 1.0 + ci * gdiag[i];
+        __syncwarp();
     }
-    __syncwarp();
     bool singular = false;
     for (int p = 0; p < k; ++p) {
         // pivot search in column p (rows p..k-1)
@@ -271,12 +283,20 @@ int precond_build(Engine &e, double h, const double *dvec)
     const unsigned nb256 = (unsigned)((n + 255) / 256);
     const double theta = e.prm.precond_theta > 0 ? e.prm.precond_theta : 0.05;
     int *ptr = e.pc_ptr, *par = e.pc_parent, *par2 = e.pc_tmp;
+    // single system: M_jj in the cell-sorted order (the SpMV's staging buffer,
+    // free until the solve), read through the CSR's sorted column positions
+    const double *msrt = nullptr;
+    if (e.col_s_valid && !e.d_hrow) {
+        msorted_kernel<<<nb256, 256, 0, st>>>(n, h, e.d_sorted, e.d_gdiag, dvec, e.d_vsort);
+        msrt = e.d_vsort;
+        e.launches++;
+    }
     if (e.valf)
         strongest_kernel<float><<<(n + 7) / 8, 256, 0, st>>>(n, h, e.d_hrow, theta, e.d_rowptr, e.d_col, e.d_valf,
-                                                             e.d_gdiag, dvec, ptr);
+                                                             e.d_gdiag, dvec, ptr, e.d_col_s, msrt);
     else
         strongest_kernel<double><<<(n + 7) / 8, 256, 0, st>>>(n, h, e.d_hrow, theta, e.d_rowptr, e.d_col, e.d_val,
-                                                              e.d_gdiag, dvec, ptr);
+                                                              e.d_gdiag, dvec, ptr, e.d_col_s, msrt);
     root_init_kernel<<<nb256, 256, 0, st>>>(n, ptr, par);
     for (int it = 0; it < 12; ++it) {
         jump_kernel<<<nb256, 256, 0, st>>>(n, par, par2);
