@@ -392,11 +392,9 @@ int Engine::step(int *accepted)
     sum_avg_speed = 0;
     cudaMemcpyAsync(d_x2, d_x1, bytes, cudaMemcpyDeviceToDevice, st);
     if (int rc = integrate(0.5 * step_size, d_x2, d_x1, true, true, kEndFirst, kEndSecond, false)) return rc;
-    if (int rc = sum_sq(d_v0, &vsquare1)) return rc;
-    if (int rc = sum_sq(d_v0b, &vsquare2)) return rc;
-    energy_accum = (vsquare1 + vsquare2) * 0.5 * step_size * 0.5;
     double ratio = 0.0;
-    if (int rc = max_ratio(&ratio)) return rc;
+    if (int rc = stage_scalars(&vsquare1, &vsquare2, &ratio)) return rc;
+    energy_accum = (vsquare1 + vsquare2) * 0.5 * step_size * 0.5;
     if (!std::isfinite(ratio)) {
         err = "step: non-finite error ratio";
         return SDDDST_ERR_NONFINITE;

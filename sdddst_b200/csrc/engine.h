@@ -74,6 +74,7 @@ struct Engine {
     double *h_hrec = nullptr;             // pinned copy
     unsigned int *d_counter = nullptr;    // last-block ticket of the fused reductions
     bool coop_gs = false;                 // one cooperative launch per Gram-Schmidt step
+    int gmres_hint = 4;                   // iterations of the last solve (first convergence check)
     double *d_gs_partials = nullptr;      // its per-CTA partial sums (3 x gs_blocks x 32)
 
     // ---- cluster block-Jacobi preconditioner (precond.cu)
@@ -129,6 +130,7 @@ struct Engine {
     int sum_abs(const double *v, double *out);
     int strain_inc(const double *xo, const double *xn, double *out);
     int max_ratio(double *out);
+    int stage_scalars(double *vs1, double *vs2, double *ratio);
     int sync_check(const char *what);
 };
 

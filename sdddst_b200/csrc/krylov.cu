@@ -273,6 +273,20 @@ int Engine::strain_inc(const double *xo, const double *xn, double *out)
     return 0;
 }
 
+// |v0|^2, |v0b|^2 and the error ratio of the step, one copy to the host
+int Engine::stage_scalars(double *vs1, double *vs2, double *ratio)
+{
+    launch_reduce<0>(*this, n, d_v0, nullptr, nullptr, d_scal);
+    launch_reduce<0>(*this, n, d_v0b, nullptr, nullptr, d_scal + 1);
+    launch_reduce<3>(*this, n, d_xb, d_tol, d_x2, d_scal + 2);
+    cudaMemcpyAsync(h_scal, d_scal, 3 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (int rc = sync_check("step scalars")) return rc;
+    *vs1 = h_scal[0];
+    *vs2 = h_scal[1];
+    *ratio = h_scal[2];
+    return 0;
+}
+
 int Engine::max_ratio(double *out)
 {
     launch_reduce<3>(*this, n, d_xb, d_tol, d_x2, d_scal);
@@ -503,7 +517,11 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
     const unsigned nb = (unsigned)((n + 255) / 256);
     const double tol = e.prm.solver_tol > 0 ? e.prm.solver_tol : 1e-13;
     const int max_it = e.prm.max_iters > 0 ? e.prm.max_iters : 1000;
-    const int chk = 4;
+    // convergence is checked on the host after a chunk of iterations: the
+    // first chunk is as long as the previous solve of this engine took
+    // (consecutive solves of a step need similar counts), later ones 2
+    const int first_chk = std::max(2, std::min(m, e.gmres_hint));
+    const int chk = 2;
     const int stride = 2 * (m + 1) + 1; // per-iteration record: c1[m+1], c2[m+1], nrm2
     double *V = e.d_V, *w = e.d_w, *z = e.d_z, *r = e.d_r;
     double *dinv = nullptr;
@@ -562,8 +580,10 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
         int k = 0;
         int j = 0;
         bool stop = false;
+        bool first_chunk = true;
         while (j < m && !stop) {
-            const int jend = std::min(m, j + chk);
+            const int jend = std::min(m, j + (first_chunk ? first_chk : chk));
+            first_chunk = false;
             for (int jj = j; jj < jend; ++jj) {
                 const double *src = apply_precond(V + (size_t)jj * ldv, z);
                 launch_spmv_J(e, h, dvec, src, w, st);
@@ -665,6 +685,7 @@ int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, doub
         }
     }
     e.last_iters = total;
+    if (converged && total > 0) e.gmres_hint = total;
     e.solves++;
     e.iterations += total;
     if (!converged) {
