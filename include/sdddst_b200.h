@@ -99,6 +99,8 @@ typedef struct {
     int max_iters;            /* iteration cap per solve */
     double precond_theta;     /* coupling strength that joins two dislocations in a cluster */
     int device;               /* CUDA device ordinal */
+    double neumann_theta;     /* SDDDST_SOLVER_GMRES_NEUMANN: cross-block couplings of normalised strength
+                                 |A_ij| / sqrt(|J_ii J_jj|) below this are left out of the correction */
 } sdddst_params;
 
 /* Defaults of SimulationData() (simulation_data.cpp:43-109, constants.h):

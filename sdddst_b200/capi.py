@@ -53,7 +53,7 @@ class Params(C.Structure):
         ("stress_value", C.c_double), ("calculate_strain", C.c_int), ("max_step_limited", C.c_int),
         ("max_step", C.c_double), ("field", C.c_int), ("pairsum", C.c_int), ("solver", C.c_int),
         ("solver_tol", C.c_double), ("gmres_restart", C.c_int), ("max_iters", C.c_int),
-        ("precond_theta", C.c_double), ("device", C.c_int),
+        ("precond_theta", C.c_double), ("device", C.c_int), ("neumann_theta", C.c_double),
     ]
 
 

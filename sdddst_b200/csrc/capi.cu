@@ -86,6 +86,7 @@ void sdddst_default_params(sdddst_params *p)
     p->gmres_restart = 30;
     p->max_iters = 300;
     p->device = 0;
+    p->neumann_theta = 0.0;
 }
 
 const char *sdddst_last_error(void) { return g_last_error.c_str(); }
@@ -271,6 +272,7 @@ int sdddst_update_params(void *ctx, const sdddst_params *prm)
     e->prm.solver_tol = prm->solver_tol;
     e->prm.max_iters = prm->max_iters;
     e->prm.precond_theta = prm->precond_theta;
+    e->prm.neumann_theta = prm->neumann_theta;
     e->prm.gmres_restart = prm->gmres_restart < 2 ? restart_alloc : std::min(prm->gmres_restart, restart_alloc);
     e->restart = e->prm.gmres_restart;
     e->prec = prm->prec;

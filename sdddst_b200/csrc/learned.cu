@@ -30,6 +30,8 @@
 
 namespace sd {
 
+__global__ void scan_kernel(const int *__restrict__ in, int m, int *__restrict__ out);
+
 namespace {
 
 constexpr int kH = 64, kNF = 4, kEF = 5, kLayers = 3;
@@ -74,12 +76,15 @@ WeightOffsets offsets()
 
 struct Learned {
     bool has_weights = false;
+    bool compact = false;                   // the analytic correction is held in its compact CSR
+    int *d_crow = nullptr, *d_ccnt = nullptr, *d_ccol = nullptr;
+    float *d_cv = nullptr;
     __nv_bfloat16 *d_w = nullptr;
     WeightOffsets off{};
     float *d_nf = nullptr, *d_h = nullptr, *d_ph = nullptr, *d_qh = nullptr, *d_agg = nullptr;
     double *d_jii = nullptr;
     float *d_cval = nullptr;
-    long cval_cap = 0;
+    long cval_cap = 0, ccap = 0;
     long builds = 0;
 };
 
@@ -318,7 +323,7 @@ __global__ void __launch_bounds__(256) node_update_kernel(int n, float *__restri
 template <typename VT>
 __global__ void first_order_kernel(int n, double h, const int *__restrict__ rowptr, const int *__restrict__ col,
                                    const VT *__restrict__ val, const double *__restrict__ dvec,
-                                   const double *__restrict__ jii, const int *__restrict__ blk,
+                                   const double *__restrict__ jii, const int *__restrict__ blk, double theta2,
                                    float *__restrict__ cval)
 {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -329,9 +334,61 @@ __global__ void first_order_kernel(int n, double h, const int *__restrict__ rowp
     for (int q = rowptr[i] + lane; q < rowptr[i + 1]; q += 32) {
         const int j = col[q];
         float v = 0.0f;
-        if (j != i && blk[j] != bi) v = (float)(-(di * (double)val[q]) / (ji * jii[j]));
+        if (j != i && blk[j] != bi) {
+            const double aij = di * (double)val[q], jj = jii[j];
+            if (fabs(aij) >= theta2 * sqrt(fabs(ji * jj))) v = (float)(-aij / (ji * jj));
+        }
         cval[q] = v;
     }
+}
+
+// compaction of the analytic correction's nonzero off-diagonals into its own
+// CSR (column positions in the cell-sorted order), one warp per row
+__global__ void c_count_kernel(int n, const int *__restrict__ rowptr, const float *__restrict__ cval,
+                               int *__restrict__ cnt)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    int c = 0;
+    for (int q = rowptr[i] + 1 + lane; q < rowptr[i + 1]; q += 32) c += cval[q] != 0.0f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) cnt[i] = c;
+}
+
+__global__ void c_fill_kernel(int n, const int *__restrict__ rowptr, const int *__restrict__ col_s,
+                              const float *__restrict__ cval, const int *__restrict__ crow, int *__restrict__ ccol,
+                              float *__restrict__ cv)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    int at = crow[i];
+    for (int q0 = rowptr[i] + 1; q0 < rowptr[i + 1]; q0 += 32) {
+        const int q = q0 + lane;
+        const bool keep = q < rowptr[i + 1] && cval[q] != 0.0f;
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+            const int o = at + __popc(m & ((1u << lane) - 1u));
+            ccol[o] = col_s[q];
+            cv[o] = cval[q];
+        }
+        at += __popc(m);
+    }
+}
+
+// z += C v over the compact correction (v gathered in the cell-sorted order)
+__global__ void c_apply_kernel(int n, const int *__restrict__ crow, const int *__restrict__ ccol,
+                               const float *__restrict__ cv, const double *__restrict__ vs, double *__restrict__ z)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    double acc = 0.0;
+    for (int q = crow[i] + lane; q < crow[i + 1]; q += 32) acc += (double)cv[q] * vs[ccol[q]];
+    acc = warp_sum(acc);
+    if (lane == 0 && crow[i + 1] > crow[i]) z[i] += acc;
 }
 
 // C_ii = (w_d . h_i + b_d) / J_ii into each row's diagonal slot (slot 0)
@@ -454,13 +511,41 @@ int learned_build(Engine &e, double h, const double *dvec, const double *x, bool
         feat_kernel<double><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, e.d_gdiag, dvec, L.d_nf,
                                                    L.d_jii);
     if (analytic) {
+        const double th2 = e.prm.neumann_theta > 0 ? e.prm.neumann_theta : 0.0;
         if (e.valf)
             first_order_kernel<float><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_valf, dvec, L.d_jii,
-                                                             e.pc_blk_of, L.d_cval);
+                                                             e.pc_blk_of, th2, L.d_cval);
         else
             first_order_kernel<double><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, L.d_jii,
-                                                              e.pc_blk_of, L.d_cval);
+                                                              e.pc_blk_of, th2, L.d_cval);
         e.launches += 2;
+        L.compact = false;
+        if (th2 > 0.0 && e.col_s_valid && !e.d_hrow) {
+            // thresholded: keep the surviving entries in their own CSR
+            if (!L.d_crow && (cudaMalloc(&L.d_crow, sizeof(int) * (n + 1)) != cudaSuccess ||
+                              cudaMalloc(&L.d_ccnt, sizeof(int) * (n + 1)) != cudaSuccess)) {
+                e.err = "learned preconditioner: out of device memory";
+                return SDDDST_ERR_NOMEM;
+            }
+            if (L.cval_cap > L.ccap) {
+                if (L.d_ccol) cudaFree(L.d_ccol);
+                if (L.d_cv) cudaFree(L.d_cv);
+                L.d_ccol = nullptr;
+                L.d_cv = nullptr;
+                L.ccap = 0;
+                if (cudaMalloc(&L.d_ccol, sizeof(int) * L.cval_cap) != cudaSuccess ||
+                    cudaMalloc(&L.d_cv, sizeof(float) * L.cval_cap) != cudaSuccess) {
+                    e.err = "learned preconditioner: out of device memory";
+                    return SDDDST_ERR_NOMEM;
+                }
+                L.ccap = L.cval_cap;
+            }
+            c_count_kernel<<<wrows, 256, 0, st>>>(n, e.d_rowptr, L.d_cval, L.d_ccnt);
+            scan_kernel<<<1, 1024, 0, st>>>(L.d_ccnt, n, L.d_crow);
+            c_fill_kernel<<<wrows, 256, 0, st>>>(n, e.d_rowptr, e.d_col_s, L.d_cval, L.d_crow, L.d_ccol, L.d_cv);
+            e.launches += 3;
+            L.compact = true;
+        }
         L.builds++;
         return 0;
     }
@@ -497,6 +582,12 @@ int learned_build(Engine &e, double h, const double *dvec, const double *x, bool
 void learned_apply_add(Engine &e, const double *v, double *z)
 {
     Learned &L = *LN(e);
+    if (L.compact) {
+        gather_sorted_v_kernel<<<(unsigned)((e.n + 255) / 256), 256, 0, e.st>>>(e.n, e.d_sorted, v, e.d_vsort);
+        c_apply_kernel<<<(unsigned)((e.n + 7) / 8), 256, 0, e.st>>>(e.n, L.d_crow, L.d_ccol, L.d_cv, e.d_vsort, z);
+        e.launches += 2;
+        return;
+    }
     if (e.col_s_valid && !e.d_hrow) { // contiguous gathers (the SpMV's staging buffer, free here)
         gather_sorted_v_kernel<<<(unsigned)((e.n + 255) / 256), 256, 0, e.st>>>(e.n, e.d_sorted, v, e.d_vsort);
         apply_sorted_kernel<<<(unsigned)((e.n + 7) / 8), 256, 0, e.st>>>(e.n, e.d_rowptr, e.d_col_s, L.d_cval, v,
@@ -521,7 +612,8 @@ void learned_free(Engine &e)
 {
     Learned *L = LN(e);
     if (!L) return;
-    void *bufs[] = {L->d_w, L->d_nf, L->d_h, L->d_ph, L->d_qh, L->d_agg, L->d_jii, L->d_cval};
+    void *bufs[] = {L->d_w, L->d_nf, L->d_h, L->d_ph, L->d_qh, L->d_agg, L->d_jii, L->d_cval, L->d_crow, L->d_ccnt,
+                    L->d_ccol, L->d_cv};
     for (void *b : bufs)
         if (b) cudaFree(b);
     delete L;
