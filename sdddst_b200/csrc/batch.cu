@@ -199,7 +199,7 @@ __global__ void batch_row_fill_kernel(long ntot, const int *__restrict__ inst, c
                                       const double *__restrict__ cut, const int *__restrict__ start,
                                       const int *__restrict__ sorted, const int *__restrict__ rowptr,
                                       int *__restrict__ col, VT *__restrict__ val, double *__restrict__ gdiag,
-                                      int *__restrict__ flag)
+                                      int *__restrict__ flag, int *__restrict__ col_s)
 {
     const long gw = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -225,7 +225,10 @@ __global__ void batch_row_fill_kernel(long ntot, const int *__restrict__ inst, c
             }
             const unsigned m = __ballot_sync(0xffffffffu, hit);
             const int at = pos + __popc(m & ((1u << lane) - 1u));
-            if (hit && at < rowend) col[at] = j;
+            if (hit && at < rowend) {
+                col[at] = j;
+                col_s[at] = q; // position of j in the sorted list (cell-ordered SpMV gathers)
+            }
             pos += __popc(m);
         }
     });
@@ -397,11 +400,11 @@ static int batch_assemble(Batch &bt, const double *x)
     if (e.valf)
         batch_row_fill_kernel<float><<<nblocks(n * 32, 256), 256, 0, st>>>(
             n, bt.d_inst, x, e.d_y, e.d_b, bt.d_G, bt.d_celloff, bt.d_cut, bt.b_start, bt.b_sorted, e.d_rowptr,
-            e.d_col, e.d_valf, e.d_gdiag, e.d_flag);
+            e.d_col, e.d_valf, e.d_gdiag, e.d_flag, e.d_col_s);
     else
         batch_row_fill_kernel<double><<<nblocks(n * 32, 256), 256, 0, st>>>(
             n, bt.d_inst, x, e.d_y, e.d_b, bt.d_G, bt.d_celloff, bt.d_cut, bt.b_start, bt.b_sorted, e.d_rowptr,
-            e.d_col, e.d_val, e.d_gdiag, e.d_flag);
+            e.d_col, e.d_val, e.d_gdiag, e.d_flag, e.d_col_s);
     e.launches++;
     int flag = 0;
     cudaMemcpyAsync(&flag, e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -410,6 +413,8 @@ static int batch_assemble(Batch &bt, const double *x)
         e.err = "batch jacobian: count and fill passes disagree";
         return SDDDST_ERR_CAPACITY;
     }
+    e.col_s_valid = true;
+    e.spmv_sorted = bt.b_sorted;
     return 0;
 }
 

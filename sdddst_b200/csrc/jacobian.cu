@@ -390,6 +390,7 @@ int jacobian_assemble(Engine &e, const double *x)
         return SDDDST_ERR_CAPACITY;
     }
     e.col_s_valid = true;
+    e.spmv_sorted = e.d_sorted;
     return 0;
 }
 

@@ -41,9 +41,10 @@ __global__ void spmv_j_kernel(int n, double h, const double *__restrict__ hrow, 
 // the cell-sorted order (vs[k] = v[sorted[k]]): a row's neighbours then lie in
 // nine contiguous runs of vs instead of random sectors of v.
 template <typename VT>
-__global__ void spmv_js_kernel(int n, double h, const int *__restrict__ rowptr, const int *__restrict__ col_s,
-                               const VT *__restrict__ val, const double *__restrict__ dvec,
-                               const double *__restrict__ v, const double *__restrict__ vs, double *__restrict__ y)
+__global__ void spmv_js_kernel(int n, double h, const double *__restrict__ hrow, const int *__restrict__ rowptr,
+                               const int *__restrict__ col_s, const VT *__restrict__ val,
+                               const double *__restrict__ dvec, const double *__restrict__ v,
+                               const double *__restrict__ vs, double *__restrict__ y)
 {
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -52,7 +53,8 @@ __global__ void spmv_js_kernel(int n, double h, const int *__restrict__ rowptr, 
     double acc = lane == 0 ? (double)val[s] * v[row] : 0.0; // diagonal slot
     for (int q = s + 1 + lane; q < e; q += 32) acc += (double)val[q] * vs[col_s[q]];
     acc = warp_sum(acc);
-    if (lane == 0) y[row] = v[row] + (1.0 + dvec[row]) * 0.5 * h * acc;
+    const double hh = hrow ? hrow[row] : h;
+    if (lane == 0) y[row] = v[row] + (1.0 + dvec[row]) * 0.5 * hh * acc;
 }
 
 __global__ void gather_sorted_kernel(int n, const int *__restrict__ sorted, const double *__restrict__ v,
@@ -300,15 +302,16 @@ void launch_spmv_J(Engine &e, double h, const double *dvec, const double *v, dou
 {
     const int wpb = 8;
     e.launches++;
-    if (e.col_s_valid && !e.d_hrow) {
+    if (e.col_s_valid) {
         e.launches++;
-        gather_sorted_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, e.d_sorted, v, e.d_vsort);
+        gather_sorted_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, e.spmv_sorted, v, e.d_vsort);
         if (e.valf)
-            spmv_js_kernel<float><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_rowptr, e.d_col_s,
+            spmv_js_kernel<float><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_hrow, e.d_rowptr, e.d_col_s,
                                                                               e.d_valf, dvec, v, e.d_vsort, y);
         else
-            spmv_js_kernel<double><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_rowptr, e.d_col_s,
-                                                                               e.d_val, dvec, v, e.d_vsort, y);
+            spmv_js_kernel<double><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_hrow, e.d_rowptr,
+                                                                               e.d_col_s, e.d_val, dvec, v, e.d_vsort,
+                                                                               y);
         return;
     }
     if (e.valf)

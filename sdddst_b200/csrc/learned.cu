@@ -583,13 +583,13 @@ void learned_apply_add(Engine &e, const double *v, double *z)
 {
     Learned &L = *LN(e);
     if (L.compact) {
-        gather_sorted_v_kernel<<<(unsigned)((e.n + 255) / 256), 256, 0, e.st>>>(e.n, e.d_sorted, v, e.d_vsort);
+        gather_sorted_v_kernel<<<(unsigned)((e.n + 255) / 256), 256, 0, e.st>>>(e.n, e.spmv_sorted, v, e.d_vsort);
         c_apply_kernel<<<(unsigned)((e.n + 7) / 8), 256, 0, e.st>>>(e.n, L.d_crow, L.d_ccol, L.d_cv, e.d_vsort, z);
         e.launches += 2;
         return;
     }
     if (e.col_s_valid && !e.d_hrow) { // contiguous gathers (the SpMV's staging buffer, free here)
-        gather_sorted_v_kernel<<<(unsigned)((e.n + 255) / 256), 256, 0, e.st>>>(e.n, e.d_sorted, v, e.d_vsort);
+        gather_sorted_v_kernel<<<(unsigned)((e.n + 255) / 256), 256, 0, e.st>>>(e.n, e.spmv_sorted, v, e.d_vsort);
         apply_sorted_kernel<<<(unsigned)((e.n + 7) / 8), 256, 0, e.st>>>(e.n, e.d_rowptr, e.d_col_s, L.d_cval, v,
                                                                          e.d_vsort, z);
         e.launches += 2;

@@ -287,7 +287,7 @@ int precond_build(Engine &e, double h, const double *dvec)
     // free until the solve), read through the CSR's sorted column positions
     const double *msrt = nullptr;
     if (e.col_s_valid && !e.d_hrow) {
-        msorted_kernel<<<nb256, 256, 0, st>>>(n, h, e.d_sorted, e.d_gdiag, dvec, e.d_vsort);
+        msorted_kernel<<<nb256, 256, 0, st>>>(n, h, e.spmv_sorted, e.d_gdiag, dvec, e.d_vsort);
         msrt = e.d_vsort;
         e.launches++;
     }
