@@ -100,6 +100,97 @@ __device__ __forceinline__ float tau_xy_f32(float dx, float dy)
     return (acc + far) * kTwoPiSqF;
 }
 
+// ---------------------------------------------------------------------------
+// Two pairs at once in packed FP32 (sm_100 FFMA2 / FMUL2 / FADD2: one issue
+// slot per two lanes' arithmetic; the SFU work stays scalar).  Same series and
+// image truncation as tau_xy_f32, rearranged so that one pair needs two ex2
+// and one rcp:
+//  * sh = sinh(pi dx) from its odd series below |pi dx| = 0.5, else from
+//    e^{+-pi dx}; with E = e^{2 pi dx}:  E + 1/E = sigma = 2 + 4 sh^2 and
+//    (E - 1/E) / 2 = dl = sinh(2 pi dx) = sh (e^{pi dx} + e^{-pi dx}),
+//    E^2 + E^-2 = sigma^2 - 2, E^2 - E^-2 = 2 sigma dl;
+//  * C_{+-1} = cosh(2 pi (dx +- 1)) from E and 1/E as in tau_xy_f32 (a sum
+//    of two positive terms; the sigma/dl form cancels near |dx| = 1/2);
+//  * the k = 0 and |k| = 1 terms over one common denominator
+//    s^2 D+^2 D-^2 (s = sh^2 + sin^2(pi dy), D+- = C+- - cos(2 pi dy)),
+//    whose factors lie in [1e-26, 1e17] for separations above 1e-7.
+// Returns 2 tau_xy / (2 pi^2), so the caller's factor is pi^2; s is handed
+// back for the close-pair prefilter (s <= pi^2 r^2 (1 + pi^2 r^2 / 2)).
+__device__ __forceinline__ float2 f2c(float c) { return make_float2(c, c); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+__device__ __forceinline__ float ex2_fast(float x)
+{
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+constexpr float kPiLog2eF = 4.532360141827193f;   // pi log2(e)
+constexpr float kSinhSplitF = 0.15915494309189535f; // |pi dx| = 0.5
+constexpr float kPiSqF = 9.869604401089358f;
+
+__device__ __forceinline__ float2 tau_xy_f32x2(float2 dx, float2 dy, float2 &s_out)
+{
+    // sin(pi dy): odd Taylor series to degree 13
+    const float2 y2 = mul2(dy, dy);
+    float2 p = fma2(y2, f2c(0.00046630280576761f), f2c(-0.00737043094571435f));
+    p = fma2(p, y2, f2c(0.08214588661112823f));
+    p = fma2(p, y2, f2c(-0.59926452932079207f));
+    p = fma2(p, y2, f2c(2.55016403987734549f));
+    p = fma2(p, y2, f2c(-5.16771278004997003f));
+    p = fma2(p, y2, f2c(3.14159265358979324f));
+    const float2 sn = mul2(dy, p);
+    const float2 sn2 = mul2(sn, sn);
+    const float2 cy = fma2(sn2, f2c(-2.0f), f2c(1.0f));
+    // sinh(pi dx): series in dx (coefficients pi^{2k+1} / (2k+1)!) or exponentials
+    const float2 x2 = mul2(dx, dx);
+    float2 q = fma2(x2, f2c(0.5992645293207919f), f2c(2.550164039877345f));
+    q = fma2(q, x2, f2c(5.167712780049969f));
+    q = fma2(q, x2, f2c(3.141592653589793f));
+    q = mul2(dx, q);
+    const float2 xk = mul2(dx, f2c(kPiLog2eF));
+    float2 ep, epi;
+    ep.x = ex2_fast(xk.x);
+    ep.y = ex2_fast(xk.y);
+    epi.x = ex2_fast(-xk.x);
+    epi.y = ex2_fast(-xk.y);
+    const float2 shx = fma2(ep, f2c(0.5f), mul2(epi, f2c(-0.5f)));
+    float2 sh;
+    sh.x = fabsf(dx.x) < kSinhSplitF ? q.x : shx.x;
+    sh.y = fabsf(dx.y) < kSinhSplitF ? q.y : shx.y;
+    const float2 sh2 = mul2(sh, sh);
+    const float2 s = add2(sh2, sn2);
+    s_out = s;
+    const float2 n0 = fma2(sn2, f2c(-1.0f), mul2(sh2, cy)); // sh^2 cy - sn^2
+    const float2 dl = mul2(sh, add2(ep, epi));               // sinh(2 pi dx)
+    const float2 sg = fma2(sh2, f2c(4.0f), f2c(2.0f));       // E + 1/E
+    const float2 E = mul2(ep, ep), Ei = mul2(epi, epi);
+    const float2 cp = fma2(E, f2c(0.5f * kQP1), mul2(Ei, f2c(0.5f * kQN1)));
+    const float2 cm = fma2(E, f2c(0.5f * kQN1), mul2(Ei, f2c(0.5f * kQP1)));
+    const float2 dp = fma2(cy, f2c(-1.0f), cp), dm = fma2(cy, f2c(-1.0f), cm);
+    const float2 np = fma2(cp, cy, f2c(-1.0f)), nm = fma2(cm, cy, f2c(-1.0f));
+    const float2 dp2 = mul2(dp, dp), dm2 = mul2(dm, dm);
+    const float2 s2 = mul2(s, s), pq = mul2(dp2, dm2);
+    const float2 den = mul2(s2, pq);
+    float2 r;
+    r.x = rcp_fast(den.x);
+    r.y = rcp_fast(den.y);
+    // 2 [dx n0 / (2 s^2) + (dx + 1) N+ / D+^2 + (dx - 1) N- / D-^2]
+    const float2 u = mul2(fma2(dx, f2c(2.0f), f2c(2.0f)), np);
+    const float2 w = mul2(fma2(dx, f2c(2.0f), f2c(-2.0f)), nm);
+    const float2 bs = fma2(u, dm2, mul2(w, dp2));
+    const float2 near2 = mul2(fma2(mul2(dx, n0), pq, mul2(s2, bs)), r);
+    // 2 x the |k| >= 2 first-order sums and the k = 2 second order
+    const float2 g1 = fma2(dx, mul2(sg, f2c(4.0f * kA1)), mul2(dl, f2c(-8.0f * kB1)));
+    const float2 g2 = fma2(dx, fma2(sg, sg, f2c(-2.0f)), mul2(mul2(sg, dl), f2c(-4.0f)));
+    const float2 c2 = fma2(mul2(cy, cy), f2c(16.0f * kQN2SQ), f2c(-8.0f * kQN2SQ));
+    const float2 far2 = fma2(c2, g2, mul2(cy, g1));
+    return add2(near2, far2);
+}
+
 } // namespace sd
 
 namespace sd {

@@ -96,59 +96,83 @@ __device__ __forceinline__ void pair_tile_f64(const double *__restrict__ x, cons
 }
 
 
-// Mixed-precision tiles: separations in FP64 from positions pre-wrapped into
-// [-0.5, 0.5) (so x_i - x_j lies in (-1, 1) and one rint() gives the minimum
-// image), rounded once to FP32; field terms in FP32; row and column sums in
-// FP64.  Interior tiles (I < J, full blocks) skip every validity test.
+// Minimum-image separation of two FP64 coordinates: d - rint(d), with rint
+// as the add/subtract of 1.5 * 2^52 (exact round-to-nearest-even for
+// |d| < 2^51), two FP64 adds instead of a rounding instruction.
+__device__ __forceinline__ double min_image(double d)
+{
+    const double m = 6755399441055744.0;
+    return d - __dadd_rn(__dadd_rn(d, m), -m);
+}
+
+// Mixed-precision tiles: separations in FP64, rounded once to FP32; field
+// terms in packed FP32 for two columns at a time (tau_xy_f32x2); row and
+// column partials summed in FP32 over 16 terms, then carried in FP64.
+// t = pi^2 b_i tau2 (tau2 = tau_xy / pi^2 from the packed field); the row sum
+// takes b_j t, the column sum t (times b_j at the end).  Interior tiles
+// (I < J, full blocks) skip every validity test.
 template <int T, bool kChecked>
 __device__ __forceinline__ void f32_tile_body(const double *sx, const double *sy, const float *sb, double xi,
-                                              double yi, float bi, int n, int j0, int tid, bool row_ok, bool diag,
-                                              int i, float (*tb)[33], double *colsum_w, double &acc,
-                                              unsigned long long *minr2, float r2_track)
+                                              double yi, float bpi, int n, int j0, int tid, bool row_ok, bool diag,
+                                              int i, float *tb, double *colsum_w, double &acc,
+                                              unsigned long long *minr2, float r2_track, float s_track)
 {
     const int lane = tid & 31;
+    const float2 bpi2 = f2c(bpi);
     for (int c0 = 0; c0 < T; c0 += 32) {
-#pragma unroll 4
-        for (int k = 0; k < 32; ++k) {
-            const int jj = c0 + k;
-            double dd = xi - sx[jj];
-            dd -= rint(dd);
-            double ee = yi - sy[jj];
-            ee -= rint(ee);
-            float dx = __double2float_rn(dd), dy = __double2float_rn(ee);
-            bool valid = true;
+        float2 racc = f2c(0.0f);
+#pragma unroll 2
+        for (int m = 0; m < 16; ++m) {
+            const int jj = c0 + 2 * m;
+            const double2 X = *reinterpret_cast<const double2 *>(sx + jj);
+            const double2 Y = *reinterpret_cast<const double2 *>(sy + jj);
+            float2 dx = make_float2(__double2float_rn(min_image(xi - X.x)), __double2float_rn(min_image(xi - X.y)));
+            float2 dy = make_float2(__double2float_rn(min_image(yi - Y.x)), __double2float_rn(min_image(yi - Y.y)));
+            bool va = true, vb = true;
             if (kChecked) {
-                valid = row_ok && (j0 + jj < n) && (!diag || jj > tid);
-                if (!valid) {
-                    dx = 0.25f;
-                    dy = 0.25f;
+                va = row_ok && (j0 + jj < n) && (!diag || jj > tid);
+                vb = row_ok && (j0 + jj + 1 < n) && (!diag || jj + 1 > tid);
+                if (!va) dx.x = dy.x = 0.25f;
+                if (!vb) dx.y = dy.y = 0.25f;
+            }
+            float2 s;
+            float2 t = mul2(tau_xy_f32x2(dx, dy, s), bpi2);
+            if (kChecked) {
+                t.x = va ? t.x : 0.0f;
+                t.y = vb ? t.y : 0.0f;
+            }
+            racc = fma2(t, *reinterpret_cast<const float2 *>(sb + jj), racc);
+            if (fminf(s.x, s.y) < s_track) { // rare: pairs that can set a tolerance
+                const float ra = fmaf(dx.x, dx.x, dy.x * dy.x), rb = fmaf(dx.y, dx.y, dy.y * dy.y);
+                if (va && ra < r2_track) {
+                    atomic_min_nonneg(&minr2[i], (double)ra);
+                    atomic_min_nonneg(&minr2[j0 + jj], (double)ra);
+                }
+                if (vb && rb < r2_track) {
+                    atomic_min_nonneg(&minr2[i], (double)rb);
+                    atomic_min_nonneg(&minr2[j0 + jj + 1], (double)rb);
                 }
             }
-            float t = bi * sb[jj] * tau_xy_f32(dx, dy);
-            if (kChecked) t = valid ? t : 0.0f;
-            acc += (double)t;
-            const float r2 = fmaf(dx, dx, dy * dy);
-            if (r2 < r2_track && valid) { // rare: pairs that can set a tolerance
-                atomic_min_nonneg(&minr2[i], (double)r2);
-                atomic_min_nonneg(&minr2[j0 + jj], (double)r2);
-            }
-            tb[k][lane] = t;
+            *reinterpret_cast<float2 *>(tb + m * 66 + 2 * lane) = t;
         }
+        acc += (double)racc.x + (double)racc.y;
         __syncwarp();
-        // column partial of this 32-row chunk summed in FP32 (two halves),
-        // then carried in FP64
-        float c0s = 0.0f, c1s = 0.0f;
-#pragma unroll 8
-        for (int m = 0; m < 16; ++m) {
-            c0s += tb[lane][m];
-            c1s += tb[lane][m + 16];
-        }
-        colsum_w[c0 + lane] = (double)c0s + (double)c1s;
+        // columns c0 + 2 q, c0 + 2 q + 1 (q = lane & 15) over rows 16 h .. 16 h + 15
+        // (h = lane >> 4); the two row halves meet through a shuffle
+        const int q = lane & 15, h = lane >> 4;
+        float2 cs = f2c(0.0f);
+#pragma unroll
+        for (int r = 0; r < 16; ++r) cs = add2(cs, *reinterpret_cast<const float2 *>(tb + q * 66 + 2 * (16 * h + r)));
+        const float ox = __shfl_down_sync(0xffffffffu, cs.x, 16);
+        const float oy = __shfl_down_sync(0xffffffffu, cs.y, 16);
+        if (h == 0)
+            *reinterpret_cast<double2 *>(colsum_w + c0 + 2 * q) =
+                make_double2((double)cs.x + (double)ox, (double)cs.y + (double)oy);
         __syncwarp();
     }
 }
 
-// One T x T tile of the mixed-precision pair sum (positions pre-wrapped).
+// One T x T tile of the mixed-precision pair sum.
 template <int T>
 __device__ __forceinline__ void pair_tile_f32(const double *__restrict__ xw, const double *__restrict__ y,
                                               const double *__restrict__ b, int n, int I, int J,
@@ -156,10 +180,11 @@ __device__ __forceinline__ void pair_tile_f32(const double *__restrict__ xw, con
                                               float r2_track)
 {
     constexpr int W = T / 32;
-    __shared__ double sx[T], sy[T];
-    __shared__ float sb[T];
-    __shared__ float tbuf[W][32][33];
-    __shared__ double colsum[W][T];
+    __shared__ __align__(16) double sx[T];
+    __shared__ __align__(16) double sy[T];
+    __shared__ __align__(8) float sb[T];
+    __shared__ __align__(8) float tbuf[W][16 * 66];
+    __shared__ __align__(16) double colsum[W][T];
 
     const int tid = threadIdx.x, warp = tid >> 5;
     const int j0 = J * T;
@@ -174,21 +199,26 @@ __device__ __forceinline__ void pair_tile_f32(const double *__restrict__ xw, con
     const bool row_ok = i < n;
     const double xi = row_ok ? xw[i] : 0.0;
     const double yi = row_ok ? y[i] : 0.0;
-    const float bi = row_ok ? (float)b[i] : 0.0f;
+    const float bpi = row_ok ? kPiSqF * (float)b[i] : 0.0f;
     const bool diag = (I == J);
     const bool checked = diag || (j0 + T > n) || (I * T + T > n);
+    // s = sinh^2(pi dx) + sin^2(pi dy) <= pi^2 r^2 (1 + pi^2 r^2 / 2) for r^2 < 1e-3
+    const float s_track = r2_track <= 0.0f ? -1.0f
+                          : r2_track < 1e-3f ? kPiSqF * r2_track * (1.0f + kPiSqF * r2_track) * 1.0001f
+                                             : 3.0e38f;
     __syncthreads();
     double acc = 0.0;
     if (checked)
-        f32_tile_body<T, true>(sx, sy, sb, xi, yi, bi, n, j0, tid, row_ok, diag, i, tbuf[warp], colsum[warp], acc,
-                               minr2, r2_track);
+        f32_tile_body<T, true>(sx, sy, sb, xi, yi, bpi, n, j0, tid, row_ok, diag, i, tbuf[warp], colsum[warp], acc,
+                               minr2, r2_track, s_track);
     else
-        f32_tile_body<T, false>(sx, sy, sb, xi, yi, bi, n, j0, tid, row_ok, diag, i, tbuf[warp], colsum[warp], acc,
-                                minr2, r2_track);
+        f32_tile_body<T, false>(sx, sy, sb, xi, yi, bpi, n, j0, tid, row_ok, diag, i, tbuf[warp], colsum[warp], acc,
+                                minr2, r2_track, s_track);
     __syncthreads();
     double ctot = 0.0;
 #pragma unroll
     for (int w = 0; w < W; ++w) ctot += colsum[w][tid];
+    ctot *= (double)sb[tid];
     if (diag) {
         if (row_ok) part[(size_t)I * n + i] = acc - ctot;
     } else {
@@ -196,6 +226,5 @@ __device__ __forceinline__ void pair_tile_f32(const double *__restrict__ xw, con
         if (j0 + tid < n) part[(size_t)I * n + j0 + tid] = -ctot;
     }
 }
-
 
 } // namespace sd

@@ -199,6 +199,47 @@ def test_fp32_pairsum_accuracy(engine_lib, port_lib):
     assert rel < 1e-5, rel
 
 
+def test_fp32_pairsum_close_and_boundary_pairs(engine_lib, port_lib):
+    """Mixed precision on the pairs that are hardest for FP32 terms:
+    separations from 1e-6 to 1e-2 and pairs straddling the periodic boundary
+    in x and in y.  Every velocity is within 2e-6 of the sum of the magnitudes
+    of its terms (FP32 terms carry about 1e-7 relative error; 16-term FP32
+    partial sums add at most 15 roundings)."""
+    from sdddst_b200 import capi
+    rng = np.random.default_rng(21)
+    m = 192
+    base = rng.uniform(-0.5, 0.5, (m, 2))
+    r = 10.0 ** rng.uniform(-6, -2, m)
+    ang = rng.uniform(0, 2 * np.pi, m)
+    close = base + np.stack([r * np.cos(ang), r * np.sin(ang)], 1)
+    edge = rng.uniform(-0.5, 0.5, (128, 2))
+    edge[:64, 0] = 0.5 - 10.0 ** rng.uniform(-6, -3, 64) * rng.choice([1.0, 2.0], 64)
+    edge[64:, 1] = -0.5 + 10.0 ** rng.uniform(-6, -3, 64)
+    edge2 = edge.copy()
+    edge2[:64, 0] -= 1.0 - 10.0 ** rng.uniform(-6, -4, 64)
+    edge2[64:, 1] += 1.0 - 10.0 ** rng.uniform(-6, -4, 64)
+    pos = np.concatenate([base, close, edge, edge2])
+    pos -= np.rint(pos)
+    pos[pos >= 0.5] -= 1.0
+    n = len(pos)
+    b = rng.permutation(np.r_[np.ones(n // 2), -np.ones(n - n // 2)])
+    xyb = np.column_stack([pos, b])
+    o = ref.Sim(xyb, None, ref.params(cutoff_multiplier=1.0, prec=1e-5), "port")
+    v_ref, _ = o.speeds(xyb)
+    e = capi.Engine(capi.cli_params(n, 1.0, 1e-5, pairsum=capi.PAIRSUM_FP32), xyb)
+    v, _ = e.speeds(xyb)
+    dx = pos[:, None, 0] - pos[None, :, 0]
+    dy = pos[:, None, 1] - pos[None, :, 1]
+    dx -= np.rint(dx)
+    dy -= np.rint(dy)
+    off = ~np.eye(n, dtype=bool)
+    mag = np.zeros((n, n))
+    mag[off] = np.abs(ref.field(0, dx[off], dy[off], "port"))
+    scale = mag.sum(1)
+    err = (np.abs(v - v_ref) / scale).max()
+    assert err <= 2e-6, err
+
+
 def test_mixed_jacobian_close_to_oracle(engine_lib, port_lib):
     """Mixed path: FP32 dtau/dx and FP32 storage of G; J within FP32
     accuracy of the oracle's (the pattern is the same test in FP64)."""
