@@ -1,11 +1,14 @@
-// FP32 field kernel for the mixed-precision pair sum.
+// FP32 field kernels of the mixed-precision path: tau_xy for the pair sum
+// (two pairs at a time, packed) and d tau_xy / dx for the Jacobian.
 //
 // Same image structure as field_f64.cuh (AnalyticField.cpp:145-160).  The
-// separation is formed and wrapped in FP64 by the caller (so close pairs keep
-// full relative accuracy) and rounded to FP32 once; the image terms run in
-// FP32 with the SFU (ex2, rcp); the caller accumulates in FP64.
-//  * sin(pi dy), |dy| <= 0.5, is an odd degree-13 polynomial (Taylor; the
-//    remainder is below 7e-10);
+// caller forms the separation in FP64 (so close pairs keep full relative
+// accuracy) and rounds it to FP32 once; the image terms run in FP32 with the
+// SFU (ex2, rcp).
+//  * sin(pi dy), |dy| <= 0.5: an odd degree-13 polynomial (Taylor; the
+//    remainder is below 7e-10) in the Jacobian; the pair sum takes it from
+//    its caller, formed in FP64 as sin(pi y_i) cos(pi y_j) - cos(pi y_i)
+//    sin(pi y_j) (only its square enters, so the image in y is immaterial);
 //  * k = 0 uses cosh 2a - cos 2b = 2(sinh^2 a + sin^2 b) and
 //    cosh 2a cos 2b - 1 = 2(sinh^2 a - sin^2 b) - 4 sinh^2 a sin^2 b, with
 //    sinh a from its odd Taylor series below |a| = 0.5 (remainder < 4e-9
@@ -60,62 +63,22 @@ __device__ __forceinline__ float sinpi_poly(float y)
     return y * p;
 }
 
-// tau_xy(dx, dy) in FP32; dx, dy already minimum-image in [-0.5, 0.5].
-__device__ __forceinline__ float tau_xy_f32(float dx, float dy)
-{
-    const float sn = sinpi_poly(dy);
-    const float sn2 = sn * sn;
-    const float cy = fmaf(-2.0f, sn2, 1.0f);
-    const float a = kPiF * dx;
-    const float ep = __expf(a);
-    const float epi = __expf(-a);
-    const float a2 = a * a;
-    const float poly = a * fmaf(a2, fmaf(a2, fmaf(a2, 1.0f / 5040.0f, 1.0f / 120.0f), 1.0f / 6.0f), 1.0f);
-    const float sh = fabsf(a) < 0.5f ? poly : 0.5f * (ep - epi);
-    const float sh2 = sh * sh;
-    const float E = ep * ep, Ei = epi * epi;
-
-    // k = 0
-    const float D0 = 2.0f * (sh2 + sn2);
-    const float N0 = fmaf(-4.0f * sh2, sn2, 2.0f * (sh2 - sn2));
-    const float r0 = rcp_fast(D0);
-    float acc = dx * N0 * r0 * r0;
-
-    // |k| = 1, exact
-    {
-        const float Cp = 0.5f * fmaf(E, kQP1, Ei * kQN1);
-        const float Dp = Cp - cy;
-        const float rp = rcp_fast(Dp * Dp);
-        const float Cm = 0.5f * fmaf(E, kQN1, Ei * kQP1);
-        const float Dm = Cm - cy;
-        const float rm = rcp_fast(Dm * Dm);
-        acc = fmaf((dx + 1.0f) * fmaf(Cp, cy, -1.0f), rp, acc);
-        acc = fmaf((dx - 1.0f) * fmaf(Cm, cy, -1.0f), rm, acc);
-    }
-    // |u| >= 1.5: first-order sums over k = 2..4 (+k side uses E^-1, -k side E)
-    const float c2 = fmaf(2.0f * cy, cy, -1.0f);
-    const float base = dx * kA1;
-    float far = 2.0f * cy * fmaf(Ei, base + kB1, E * (base - kB1));
-    far = fmaf(4.0f * c2 * kQN2SQ, fmaf(Ei * Ei, dx + 2.0f, E * E * (dx - 2.0f)), far);
-    return (acc + far) * kTwoPiSqF;
-}
-
 // ---------------------------------------------------------------------------
-// Two pairs at once in packed FP32 (sm_100 FFMA2 / FMUL2 / FADD2: one issue
-// slot per two lanes' arithmetic; the SFU work stays scalar).  Same series and
-// image truncation as tau_xy_f32, rearranged so that one pair needs two ex2
-// and one rcp:
+// tau_xy of two pairs at once in packed FP32 (sm_100 FFMA2 / FMUL2 / FADD2:
+// one issue slot per two lanes' arithmetic; the SFU work stays scalar),
+// arranged so that one pair needs two ex2 and one rcp:
 //  * sh = sinh(pi dx) from its odd series below |pi dx| = 0.5, else from
 //    e^{+-pi dx}; with E = e^{2 pi dx}:  E + 1/E = sigma = 2 + 4 sh^2 and
 //    (E - 1/E) / 2 = dl = sinh(2 pi dx) = sh (e^{pi dx} + e^{-pi dx}),
 //    E^2 + E^-2 = sigma^2 - 2, E^2 - E^-2 = 2 sigma dl;
-//  * C_{+-1} = cosh(2 pi (dx +- 1)) from E and 1/E as in tau_xy_f32 (a sum
-//    of two positive terms; the sigma/dl form cancels near |dx| = 1/2);
+//  * C_{+-1} = cosh(2 pi (dx +- 1)) = (E e^{+-2 pi} + E^-1 e^{-+2 pi}) / 2, a
+//    sum of two positive terms (the sigma/dl form cancels near |dx| = 1/2);
 //  * the k = 0 and |k| = 1 terms over one common denominator
 //    s^2 D+^2 D-^2 (s = sh^2 + sin^2(pi dy), D+- = C+- - cos(2 pi dy)),
 //    whose factors lie in [1e-26, 1e17] for separations above 1e-7.
-// Returns 2 tau_xy / (2 pi^2), so the caller's factor is pi^2; s is handed
-// back for the close-pair prefilter (s <= pi^2 r^2 (1 + pi^2 r^2 / 2)).
+// dx is the minimum-image separation, sn = sin(pi dy).  Returns
+// 2 tau_xy / (2 pi^2), so the caller's factor is pi^2; s is handed back for
+// the close-pair prefilter (s <= pi^2 r^2 (1 + pi^2 r^2 / 2)).
 __device__ __forceinline__ float2 f2c(float c) { return make_float2(c, c); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
@@ -132,17 +95,8 @@ constexpr float kPiLog2eF = 4.532360141827193f;   // pi log2(e)
 constexpr float kSinhSplitF = 0.15915494309189535f; // |pi dx| = 0.5
 constexpr float kPiSqF = 9.869604401089358f;
 
-__device__ __forceinline__ float2 tau_xy_f32x2(float2 dx, float2 dy, float2 &s_out)
+__device__ __forceinline__ float2 tau_xy_f32x2(float2 dx, float2 sn, float2 &s_out)
 {
-    // sin(pi dy): odd Taylor series to degree 13
-    const float2 y2 = mul2(dy, dy);
-    float2 p = fma2(y2, f2c(0.00046630280576761f), f2c(-0.00737043094571435f));
-    p = fma2(p, y2, f2c(0.08214588661112823f));
-    p = fma2(p, y2, f2c(-0.59926452932079207f));
-    p = fma2(p, y2, f2c(2.55016403987734549f));
-    p = fma2(p, y2, f2c(-5.16771278004997003f));
-    p = fma2(p, y2, f2c(3.14159265358979324f));
-    const float2 sn = mul2(dy, p);
     const float2 sn2 = mul2(sn, sn);
     const float2 cy = fma2(sn2, f2c(-2.0f), f2c(1.0f));
     // sinh(pi dx): series in dx (coefficients pi^{2k+1} / (2k+1)!) or exponentials

@@ -105,45 +105,58 @@ __device__ __forceinline__ double min_image(double d)
     return d - __dadd_rn(__dadd_rn(d, m), -m);
 }
 
-// Mixed-precision tiles: separations in FP64, rounded once to FP32; field
-// terms in packed FP32 for two columns at a time (tau_xy_f32x2); row and
-// column partials summed in FP32 over 16 terms, then carried in FP64.
-// t = pi^2 b_i tau2 (tau2 = tau_xy / pi^2 from the packed field); the row sum
-// takes b_j t, the column sum t (times b_j at the end).  Interior tiles
-// (I < J, full blocks) skip every validity test.
+// Mixed-precision tiles.  Separations in FP64, rounded once to FP32: dx as
+// the minimum-image difference, sin(pi dy) as s_i c_j - c_i s_j from
+// per-dislocation s = sin(pi y), c = cos(pi y) (FP64, formed once per tile
+// and dislocation).  Field terms in packed FP32 for two columns at a time
+// (tau_xy_f32x2, which returns tau2 = tau_xy / pi^2); row and column partials
+// summed in FP32 over 16 terms, then carried in FP64:
+//   row i:    sum_j (pi^2 b_j) tau2_ij,  times b_i at the end;
+//   column j: sum_i (pi^2 b_i) tau2_ij,  times b_j at the end.
+// Interior tiles (I < J, full blocks) skip every validity test.
 template <int T, bool kChecked>
-__device__ __forceinline__ void f32_tile_body(const double *sx, const double *sy, const float *sb, double xi,
-                                              double yi, float bpi, int n, int j0, int tid, bool row_ok, bool diag,
-                                              int i, float *tb, double *colsum_w, double &acc,
+__device__ __forceinline__ void f32_tile_body(const double *sx, const double *sy, const double *ssn,
+                                              const double *scs, const float *sbp, const float *brow, double xi,
+                                              double yi, double si, double ci, int n, int j0, int tid, bool row_ok,
+                                              bool diag, int i, float *tb, double *colsum_w, double &acc,
                                               unsigned long long *minr2, float r2_track, float s_track)
 {
     const int lane = tid & 31;
-    const float2 bpi2 = f2c(bpi);
     for (int c0 = 0; c0 < T; c0 += 32) {
         float2 racc = f2c(0.0f);
-#pragma unroll 2
+#pragma unroll
         for (int m = 0; m < 16; ++m) {
             const int jj = c0 + 2 * m;
             const double2 X = *reinterpret_cast<const double2 *>(sx + jj);
-            const double2 Y = *reinterpret_cast<const double2 *>(sy + jj);
+            const double2 S = *reinterpret_cast<const double2 *>(ssn + jj);
+            const double2 C = *reinterpret_cast<const double2 *>(scs + jj);
             float2 dx = make_float2(__double2float_rn(min_image(xi - X.x)), __double2float_rn(min_image(xi - X.y)));
-            float2 dy = make_float2(__double2float_rn(min_image(yi - Y.x)), __double2float_rn(min_image(yi - Y.y)));
+            float2 sn = make_float2(__double2float_rn(fma(si, C.x, -ci * S.x)),
+                                    __double2float_rn(fma(si, C.y, -ci * S.y)));
             bool va = true, vb = true;
             if (kChecked) {
                 va = row_ok && (j0 + jj < n) && (!diag || jj > tid);
                 vb = row_ok && (j0 + jj + 1 < n) && (!diag || jj + 1 > tid);
-                if (!va) dx.x = dy.x = 0.25f;
-                if (!vb) dx.y = dy.y = 0.25f;
+                if (!va) {
+                    dx.x = 0.25f;
+                    sn.x = 0.70710678f;
+                }
+                if (!vb) {
+                    dx.y = 0.25f;
+                    sn.y = 0.70710678f;
+                }
             }
             float2 s;
-            float2 t = mul2(tau_xy_f32x2(dx, dy, s), bpi2);
+            float2 t = tau_xy_f32x2(dx, sn, s);
             if (kChecked) {
                 t.x = va ? t.x : 0.0f;
                 t.y = vb ? t.y : 0.0f;
             }
-            racc = fma2(t, *reinterpret_cast<const float2 *>(sb + jj), racc);
+            racc = fma2(t, *reinterpret_cast<const float2 *>(sbp + jj), racc);
             if (fminf(s.x, s.y) < s_track) { // rare: pairs that can set a tolerance
-                const float ra = fmaf(dx.x, dx.x, dy.x * dy.x), rb = fmaf(dx.y, dx.y, dy.y * dy.y);
+                const float dya = __double2float_rn(min_image(yi - sy[jj]));
+                const float dyb = __double2float_rn(min_image(yi - sy[jj + 1]));
+                const float ra = fmaf(dx.x, dx.x, dya * dya), rb = fmaf(dx.y, dx.y, dyb * dyb);
                 if (va && ra < r2_track) {
                     atomic_min_nonneg(&minr2[i], (double)ra);
                     atomic_min_nonneg(&minr2[j0 + jj], (double)ra);
@@ -158,11 +171,14 @@ __device__ __forceinline__ void f32_tile_body(const double *sx, const double *sy
         acc += (double)racc.x + (double)racc.y;
         __syncwarp();
         // columns c0 + 2 q, c0 + 2 q + 1 (q = lane & 15) over rows 16 h .. 16 h + 15
-        // (h = lane >> 4); the two row halves meet through a shuffle
+        // (h = lane >> 4), weighted by pi^2 b of each row; the two row halves meet
+        // through a shuffle
         const int q = lane & 15, h = lane >> 4;
         float2 cs = f2c(0.0f);
 #pragma unroll
-        for (int r = 0; r < 16; ++r) cs = add2(cs, *reinterpret_cast<const float2 *>(tb + q * 66 + 2 * (16 * h + r)));
+        for (int r = 0; r < 16; ++r)
+            cs = fma2(*reinterpret_cast<const float2 *>(tb + q * 66 + 2 * (16 * h + r)),
+                      *reinterpret_cast<const float2 *>(brow + 2 * (16 * h + r)), cs);
         const float ox = __shfl_down_sync(0xffffffffu, cs.x, 16);
         const float oy = __shfl_down_sync(0xffffffffu, cs.y, 16);
         if (h == 0)
@@ -182,24 +198,36 @@ __device__ __forceinline__ void pair_tile_f32(const double *__restrict__ xw, con
     constexpr int W = T / 32;
     __shared__ __align__(16) double sx[T];
     __shared__ __align__(16) double sy[T];
-    __shared__ __align__(8) float sb[T];
+    __shared__ __align__(16) double ssn[T];
+    __shared__ __align__(16) double scs[T];
+    __shared__ __align__(8) float sbp[T];
+    __shared__ __align__(8) float brow[W][64];
     __shared__ __align__(8) float tbuf[W][16 * 66];
     __shared__ __align__(16) double colsum[W][T];
 
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int j0 = J * T;
+    const double bj = j0 + tid < n ? b[j0 + tid] : 0.0;
     {
         const int j = j0 + tid;
         const bool ok = j < n;
+        const double yj = ok ? y[j] : 0.0;
+        double sj, cj;
+        sincospi(yj, &sj, &cj);
         sx[tid] = ok ? xw[j] : 0.0;
-        sy[tid] = ok ? y[j] : 0.0;
-        sb[tid] = ok ? (float)b[j] : 0.0f;
+        sy[tid] = yj;
+        ssn[tid] = sj;
+        scs[tid] = cj;
+        sbp[tid] = kPiSqF * (float)bj;
     }
     const int i = I * T + tid;
     const bool row_ok = i < n;
     const double xi = row_ok ? xw[i] : 0.0;
     const double yi = row_ok ? y[i] : 0.0;
-    const float bpi = row_ok ? kPiSqF * (float)b[i] : 0.0f;
+    const double bi = row_ok ? b[i] : 0.0;
+    double si, ci;
+    sincospi(yi, &si, &ci);
+    brow[warp][2 * lane] = brow[warp][2 * lane + 1] = kPiSqF * (float)bi;
     const bool diag = (I == J);
     const bool checked = diag || (j0 + T > n) || (I * T + T > n);
     // s = sinh^2(pi dx) + sin^2(pi dy) <= pi^2 r^2 (1 + pi^2 r^2 / 2) for r^2 < 1e-3
@@ -209,16 +237,17 @@ __device__ __forceinline__ void pair_tile_f32(const double *__restrict__ xw, con
     __syncthreads();
     double acc = 0.0;
     if (checked)
-        f32_tile_body<T, true>(sx, sy, sb, xi, yi, bpi, n, j0, tid, row_ok, diag, i, tbuf[warp], colsum[warp], acc,
-                               minr2, r2_track, s_track);
+        f32_tile_body<T, true>(sx, sy, ssn, scs, sbp, brow[warp], xi, yi, si, ci, n, j0, tid, row_ok, diag, i,
+                               tbuf[warp], colsum[warp], acc, minr2, r2_track, s_track);
     else
-        f32_tile_body<T, false>(sx, sy, sb, xi, yi, bpi, n, j0, tid, row_ok, diag, i, tbuf[warp], colsum[warp], acc,
-                                minr2, r2_track, s_track);
+        f32_tile_body<T, false>(sx, sy, ssn, scs, sbp, brow[warp], xi, yi, si, ci, n, j0, tid, row_ok, diag, i,
+                                tbuf[warp], colsum[warp], acc, minr2, r2_track, s_track);
     __syncthreads();
     double ctot = 0.0;
 #pragma unroll
     for (int w = 0; w < W; ++w) ctot += colsum[w][tid];
-    ctot *= (double)sb[tid];
+    ctot *= bj;
+    acc *= bi;
     if (diag) {
         if (row_ok) part[(size_t)I * n + i] = acc - ctot;
     } else {
