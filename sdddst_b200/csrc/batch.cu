@@ -414,6 +414,7 @@ static int batch_assemble(Batch &bt, const double *x)
         return SDDDST_ERR_CAPACITY;
     }
     e.col_s_valid = true;
+    e.col_s16_valid = false;
     e.spmv_sorted = bt.b_sorted;
     return 0;
 }

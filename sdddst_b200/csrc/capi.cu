@@ -332,6 +332,7 @@ int sdddst_solve_csc(void *ctx, const int *Ap, const int *Ai, const double *Ax, 
         }
         e->nnz = nnz;
         e->col_s_valid = false; // a caller's matrix: no cell-sorted column positions
+        e->col_s16_valid = false;
         cudaMemcpyAsync(e->d_rowptr, rp.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, e->st);
         cudaMemcpyAsync(e->d_col, cl.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, e->st);
         std::vector<float> vf;

@@ -54,6 +54,8 @@ struct Engine {
     double *d_vsort = nullptr; // SpMV input gathered into the cell-sorted order
     double *d_xsrt = nullptr, *d_ysrt = nullptr, *d_bsrt = nullptr; // x, y, b in the cell-sorted order
     bool col_s_valid = false;  // d_col_s matches the assembled CSR
+    unsigned short *d_col_s16 = nullptr; // d_col_s in 16 bits (systems of at most 65536), the SpMV's copy
+    bool col_s16_valid = false;
     const int *spmv_sorted = nullptr; // the sorted list d_col_s refers to
     double *d_hrow = nullptr;  // per-row step size of a batch of systems (null: one system, scalar h)
     long nnz_cap = 0, nnz = 0;

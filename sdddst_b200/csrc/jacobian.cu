@@ -39,40 +39,51 @@ __global__ void cell_assign_kernel(int n, const double *__restrict__ x, const do
 }
 
 // Exclusive scan of m ints by one block: out[0] = 0, out[k+1] = sum_{<=k}.
+// Tiles of blockDim.x x 16 consecutive elements: each thread sums its 16,
+// the block scans the thread totals (warp shuffles, then one warp over the
+// warp totals, two barriers per tile), and each thread writes its 16
+// prefixes.  Sums run in 64 bits.
 __global__ void scan_kernel(const int *__restrict__ in, int m, int *__restrict__ out)
 {
+    constexpr int IT = 16;
     __shared__ long long warp_tot[32];
-    __shared__ long long carry_s;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    if (tid == 0) carry_s = 0;
-    __syncthreads();
-    for (int base = 0; base < m; base += blockDim.x) {
-        int k = base + tid;
-        long long v = k < m ? in[k] : 0;
-        long long s = v;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    long long carry = 0;
+    for (int base = 0; base < m; base += blockDim.x * IT) {
+        const int k0 = base + tid * IT;
+        int v[IT];
+        long long tsum = 0;
+#pragma unroll
+        for (int q = 0; q < IT; ++q) {
+            v[q] = k0 + q < m ? in[k0 + q] : 0;
+            tsum += v[q];
+        }
+        long long s = tsum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            long long t = __shfl_up_sync(0xffffffffu, s, o);
+            const long long t = __shfl_up_sync(0xffffffffu, s, o);
             if (lane >= o) s += t;
         }
         if (lane == 31) warp_tot[wid] = s;
         __syncthreads();
         if (wid == 0) {
-            int nw = blockDim.x >> 5;
             long long t = lane < nw ? warp_tot[lane] : 0;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                long long u = __shfl_up_sync(0xffffffffu, t, o);
+                const long long u = __shfl_up_sync(0xffffffffu, t, o);
                 if (lane >= o) t += u;
             }
             if (lane < nw) warp_tot[lane] = t;
         }
         __syncthreads();
-        long long incl = s + (wid > 0 ? warp_tot[wid - 1] : 0) + carry_s;
-        if (k < m) out[k + 1] = (int)incl;
-        __syncthreads();
-        if (tid == blockDim.x - 1) carry_s = incl;
-        __syncthreads();
+        long long run = carry + (wid > 0 ? warp_tot[wid - 1] : 0) + s - tsum;
+#pragma unroll
+        for (int q = 0; q < IT; ++q) {
+            run += v[q];
+            if (k0 + q < m) out[k0 + q + 1] = (int)run;
+        }
+        carry += warp_tot[nw - 1];
+        __syncthreads(); // warp_tot is rewritten by the next tile
     }
     if (tid == 0) out[0] = 0;
 }
@@ -163,51 +174,40 @@ __global__ void gather_cells_kernel(int n, const int *__restrict__ sorted, const
     bs[k] = b[j];
 }
 
-__global__ void row_count_kernel(int n, const double *__restrict__ x, const double *__restrict__ y, CellScan cs,
-                                 double c, double c2, double ic2, int *__restrict__ rowcnt)
+// Candidate test of row i against candidate j at (xj, yj): the reference's
+// pattern rule with dx = x[hi] - x[lo].
+__device__ __forceinline__ bool cand_kept(int i, double xi, double yi, int j, double xj, double yj, double c,
+                                          double c2, double ic2, const CellScan &cs)
 {
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (gw >= n) return;
-    const int i = cs.sorted[gw];
-    const double xi = x[i], yi = y[i];
+    const double dx = wrap_half(i < j ? xj - xi : xi - xj);
+    const double dy = wrap_half(i < j ? yj - yi : yi - yj);
+    return pair_kept_search(r2_exact(dx, dy), c, c2, ic2, cs);
+}
+
+// Pattern entries of row i (diagonal excluded), candidates read from global
+// memory cell by cell (the fallback when a cell's 3x3 block does not fit in
+// shared memory).
+__device__ int row_count_global(int i, double xi, double yi, const CellScan &cs, double c, double c2, double ic2,
+                                int lane)
+{
     const int cx = cell_of(xi, cs.G), cy = cell_of(yi, cs.G);
     int cnt = 0;
     for_neighbour_cells(cx, cy, cs.G, [&](int cell) {
         const int s = cs.start[cell], e = cs.start[cell + 1];
         for (int k = s + lane; k < e; k += 32) {
             const int j = cs.sorted[k];
-            if (j == i) continue;
-            const double xj = cs.xs[k], yj = cs.ys[k];
-            double dx = wrap_half(i < j ? xj - xi : xi - xj); // x[hi] - x[lo], as the reference orders it
-            double dy = wrap_half(i < j ? yj - yi : yi - yj);
-            cnt += pair_kept_search(r2_exact(dx, dy), c, c2, ic2, cs);
+            if (j != i) cnt += cand_kept(i, xi, yi, j, cs.xs[k], cs.ys[k], c, c2, ic2, cs);
         }
     });
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-    if (lane == 0) rowcnt[i] = cnt + 1;
+    return cnt;
 }
 
-template <typename VT>
-__global__ void row_fill_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
-                                const double *__restrict__ b, CellScan cs, double c, double c2, double ic2,
-                                const int *__restrict__ rowptr, int *__restrict__ col, VT *__restrict__ val,
-                                double *__restrict__ gdiag, int p, const double *__restrict__ pdx,
-                                const double *__restrict__ pdy, double A, double K, int *__restrict__ flag,
-                                const double *__restrict__ tab_dx, int *__restrict__ col_s,
-                                const double *__restrict__ bs)
+// Columns of row i in cell order, ascending index inside a cell; returns the
+// next free slot (rowend when the count pass agreed).
+__device__ int row_cols_global(int i, double xi, double yi, const CellScan &cs, double c, double c2, double ic2,
+                               int pos, int rowend, int *col, int *col_s, unsigned short *col_s16, int lane)
 {
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (gw >= n) return;
-    const int i = cs.sorted[gw];
-    const double xi = x[i], yi = y[i], bi = b[i];
     const int cx = cell_of(xi, cs.G), cy = cell_of(yi, cs.G);
-    const int base = rowptr[i];
-    const int rowend = rowptr[i + 1];
-    int pos = base + 1;
-    // 1) columns, in cell order then ascending index inside a cell
     for_neighbour_cells(cx, cy, cs.G, [&](int cell) {
         const int s = cs.start[cell], e = cs.start[cell + 1];
         for (int k0 = s; k0 < e; k0 += 32) {
@@ -216,29 +216,30 @@ __global__ void row_fill_kernel(int n, const double *__restrict__ x, const doubl
             int j = -1;
             if (k < e) {
                 j = cs.sorted[k];
-                if (j != i) {
-                    const double xj = cs.xs[k], yj = cs.ys[k];
-                    double dx = wrap_half(i < j ? xj - xi : xi - xj); // x[hi] - x[lo]
-                    double dy = wrap_half(i < j ? yj - yi : yi - yj);
-                    hit = pair_kept_search(r2_exact(dx, dy), c, c2, ic2, cs);
-                }
+                if (j != i) hit = cand_kept(i, xi, yi, j, cs.xs[k], cs.ys[k], c, c2, ic2, cs);
             }
-            unsigned m = __ballot_sync(0xffffffffu, hit);
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
             const int at = pos + __popc(m & ((1u << lane) - 1u));
             if (hit && at < rowend) {
                 col[at] = j;
                 col_s[at] = k; // position of j in the cell-sorted order
+                if (col_s16) col_s16[at] = (unsigned short)k;
             }
             pos += __popc(m);
         }
     });
-    __syncwarp();
-    if (pos != rowend) { // count and fill passes disagree: report, never write past the row
-        if (lane == 0) atomicExch(flag, 1);
-        return;
-    }
-    // 2) values, all lanes busy
-    const int end = rowend;
+    return pos;
+}
+
+// Values of row i (all lanes busy) and its diagonal: G_ij for the columns
+// already in place, the point-defect seed (simulation.cpp:274-325), and
+// G_ii = -(row sum + defect sum) in the row's first slot.
+template <typename VT>
+__device__ void row_values(int i, double xi, double yi, double bi, const CellScan &cs, double c, double c2,
+                           double ic2, int base, int end, int *col, const int *col_s, VT *val, double *gdiag, int p,
+                           const double *pdx, const double *pdy, double A, double K, const double *tab_dx,
+                           const double *bs, int lane)
+{
     double rs = 0.0;
     for (int q = base + 1 + lane; q < end; q += 32) {
         const int j = col[q], ks = col_s[q];
@@ -255,7 +256,6 @@ __global__ void row_fill_kernel(int n, const double *__restrict__ x, const doubl
         val[q] = v;
         rs += (double)v;
     }
-    // 3) point-defect seed of the diagonal (simulation.cpp:274-325)
     double pd = 0.0;
     for (int q = lane; q < p; q += 32) {
         double dx = wrap_half(xi - pdx[q]);
@@ -269,6 +269,125 @@ __global__ void row_fill_kernel(int n, const double *__restrict__ x, const doubl
         col[base] = i;
         val[base] = (VT)(-(rs + pd));
         gdiag[i] = -(rs + pd);
+    }
+}
+
+// Count (kFill = false) or fill (kFill = true) pass over the rows of one
+// cell.  Block (cell, part) stages the cell's 3x3 neighbour block (positions
+// and indices of up to kCandCap candidates, in visiting order) in shared
+// memory once; its warps then test their rows against it without touching
+// global memory, one row per warp at a time, the cell's rows split into
+// `parts` contiguous ranges.  A block larger than kCandCap (or a grid below
+// 3x3 cells) walks global memory cell by cell instead.  Both routes visit
+// candidates in the same order, so the CSR layout is the same either way.
+constexpr int kCandCap = 2720;
+constexpr int kCellThreads = 256;
+constexpr size_t kCellSmem = (size_t)kCandCap * (2 * sizeof(double) + sizeof(int));
+
+template <bool kFill, typename VT>
+__global__ void __launch_bounds__(kCellThreads) cell_rows_kernel(
+    int parts, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ b, CellScan cs,
+    double c, double c2, double ic2, int *__restrict__ rowcnt, const int *__restrict__ rowptr, int *__restrict__ col,
+    VT *__restrict__ val, double *__restrict__ gdiag, int p, const double *__restrict__ pdx,
+    const double *__restrict__ pdy, double A, double K, int *__restrict__ flag, const double *__restrict__ tab_dx,
+    int *__restrict__ col_s, unsigned short *__restrict__ col_s16, const double *__restrict__ bs)
+{
+    extern __shared__ __align__(16) unsigned char cell_smem[];
+    double *sxc = reinterpret_cast<double *>(cell_smem);
+    double *syc = sxc + kCandCap;
+    int *sjc = reinterpret_cast<int *>(syc + kCandCap);
+    __shared__ int seg_start[9], seg_off[10];
+
+    const int G = cs.G;
+    const int cell = blockIdx.x / parts, part = blockIdx.x % parts;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int r0 = cs.start[cell], r1 = cs.start[cell + 1];
+    const int chunk = (r1 - r0 + parts - 1) / parts;
+    const int rbeg = r0 + part * chunk, rend = min(r0 + (part + 1) * chunk, r1);
+    if (rbeg >= rend) return; // whole block: no barrier below is reached
+
+    bool staged = false;
+    int ncand = 0;
+    if (G >= 3) {
+        if (threadIdx.x == 0) {
+            const int cx = cell % G, cy = cell / G;
+            int nseg = 0, off = 0;
+            for_neighbour_cells(cx, cy, G, [&](int nc) {
+                seg_start[nseg] = cs.start[nc];
+                seg_off[nseg] = off;
+                off += cs.start[nc + 1] - cs.start[nc];
+                ++nseg;
+            });
+            seg_off[9] = off;
+        }
+        __syncthreads();
+        ncand = seg_off[9];
+        staged = ncand <= kCandCap;
+        if (staged) {
+            for (int t = threadIdx.x; t < ncand; t += blockDim.x) {
+                int sgi = 0;
+                while (t >= seg_off[sgi + 1]) ++sgi;
+                const int k = seg_start[sgi] + (t - seg_off[sgi]);
+                sxc[t] = cs.xs[k];
+                syc[t] = cs.ys[k];
+                sjc[t] = cs.sorted[k];
+            }
+            __syncthreads();
+        }
+    }
+    for (int r = rbeg + warp; r < rend; r += nwarps) {
+        const int i = cs.sorted[r];
+        const double xi = x[i], yi = y[i];
+        if (!kFill) {
+            int cnt = 0;
+            if (staged) {
+                for (int t = lane; t < ncand; t += 32) {
+                    const int j = sjc[t];
+                    if (j != i) cnt += cand_kept(i, xi, yi, j, sxc[t], syc[t], c, c2, ic2, cs);
+                }
+            } else {
+                cnt = row_count_global(i, xi, yi, cs, c, c2, ic2, lane);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+            if (lane == 0) rowcnt[i] = cnt + 1;
+        } else {
+            const int base = rowptr[i], rowend = rowptr[i + 1];
+            int pos = base + 1;
+            if (staged) {
+                int sgi = 0; // segment of the chunk's first candidate (candidates ascend)
+                for (int t0 = 0; t0 < ncand; t0 += 32) {
+                    const int t = t0 + lane;
+                    bool hit = false;
+                    int j = -1;
+                    if (t < ncand) {
+                        j = sjc[t];
+                        if (j != i) hit = cand_kept(i, xi, yi, j, sxc[t], syc[t], c, c2, ic2, cs);
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, hit);
+                    const int at = pos + __popc(m & ((1u << lane) - 1u));
+                    if (hit && at < rowend) {
+                        int sg = sgi;
+                        while (t >= seg_off[sg + 1]) ++sg;
+                        const int k = seg_start[sg] + (t - seg_off[sg]);
+                        col[at] = j;
+                        col_s[at] = k;
+                        if (col_s16) col_s16[at] = (unsigned short)k;
+                    }
+                    pos += __popc(m);
+                    while (sgi < 8 && t0 + 32 >= seg_off[sgi + 1]) ++sgi;
+                }
+            } else {
+                pos = row_cols_global(i, xi, yi, cs, c, c2, ic2, pos, rowend, col, col_s, col_s16, lane);
+            }
+            __syncwarp();
+            if (pos != rowend) { // count and fill passes disagree: report, never write past the row
+                if (lane == 0) atomicExch(flag, 1);
+                continue;
+            }
+            row_values<VT>(i, xi, yi, b[i], cs, c, c2, ic2, base, rowend, col, col_s, val, gdiag, p, pdx, pdy, A, K,
+                           tab_dx, bs, lane);
+        }
     }
 }
 
@@ -319,6 +438,12 @@ int alloc_csr_values(Engine &e, long cap)
     e.d_col_s = nullptr;
     e.col_s_valid = false;
     if (cudaMalloc(&e.d_col_s, sizeof(int) * cap) != cudaSuccess) return SDDDST_ERR_NOMEM;
+    if (e.d_col_s16) cudaFree(e.d_col_s16);
+    e.d_col_s16 = nullptr;
+    e.col_s16_valid = false;
+    if (e.n <= 65536 && !e.batch_backend &&
+        cudaMalloc(&e.d_col_s16, sizeof(unsigned short) * cap) != cudaSuccess)
+        return SDDDST_ERR_NOMEM;
     if (e.valf) {
         if (cudaMalloc(&e.d_valf, sizeof(float) * cap) != cudaSuccess) return SDDDST_ERR_NOMEM;
     } else {
@@ -337,6 +462,26 @@ static int grow_csr(Engine &e, long need)
     return 0;
 }
 
+// Row ranges per cell for the cell kernels: about three blocks per SM in one
+// wave, at least one range per cell.  Sets the kernels' shared-memory limit
+// on first use on each device.
+static int cell_parts(const Engine &e, int ncell)
+{
+    static bool attr_set[256] = {};
+    const int dev = e.device & 255;
+    if (!attr_set[dev]) {
+        cudaFuncSetAttribute(cell_rows_kernel<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kCellSmem);
+        cudaFuncSetAttribute(cell_rows_kernel<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kCellSmem);
+        cudaFuncSetAttribute(cell_rows_kernel<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kCellSmem);
+        attr_set[dev] = true;
+    }
+    const int want = 3 * e.gs_blocks; // gs_blocks: one per SM
+    return ncell >= want ? 1 : (want + ncell - 1) / ncell;
+}
+
 int jacobian_assemble(Engine &e, const double *x)
 {
     const int n = e.n, G = e.G;
@@ -351,10 +496,11 @@ int jacobian_assemble(Engine &e, const double *x)
     gather_cells_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, e.d_sorted, x, e.d_y, e.d_b, e.d_xsrt, e.d_ysrt, e.d_bsrt);
     const double rp = e.cutoff * (1.0 + std::sqrt(36.8));
     CellScan cs{G, e.d_cell_start, e.d_sorted, e.d_xsrt, e.d_ysrt, rp * rp * (1.0 - 1e-6), rp * rp * (1.0 + 1e-6)};
-    const int wpb = 8; // warps per block
-    const unsigned rb = (unsigned)((n + wpb - 1) / wpb);
-    row_count_kernel<<<rb, 32 * wpb, 0, st>>>(n, x, e.d_y, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr,
-                                              e.d_rowcnt);
+    const int parts = cell_parts(e, ncell);
+    const unsigned nb = (unsigned)(ncell * parts);
+    cell_rows_kernel<false, float><<<nb, kCellThreads, kCellSmem, st>>>(
+        parts, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr, e.d_rowcnt, nullptr, nullptr,
+        nullptr, nullptr, 0, nullptr, nullptr, 0.0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr);
     scan_kernel<<<1, 1024, 0, st>>>(e.d_rowcnt, n, e.d_rowptr);
     e.launches += 8;
     int total = 0;
@@ -372,15 +518,15 @@ int jacobian_assemble(Engine &e, const double *x)
     e.nnz = total;
     cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
     if (e.valf)
-        row_fill_kernel<float><<<rb, 32 * wpb, 0, st>>>(n, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr,
-                                                       e.one_per_cutoff_sqr, e.d_rowptr, e.d_col, e.d_valf,
-                                                       e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag,
-                                                       e.d_tab_dx, e.d_col_s, e.d_bsrt);
+        cell_rows_kernel<true, float><<<nb, kCellThreads, kCellSmem, st>>>(
+            parts, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr, nullptr, e.d_rowptr, e.d_col,
+            e.d_valf, e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag, e.d_tab_dx, e.d_col_s, e.d_col_s16,
+            e.d_bsrt);
     else
-        row_fill_kernel<double><<<rb, 32 * wpb, 0, st>>>(n, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr,
-                                                        e.one_per_cutoff_sqr, e.d_rowptr, e.d_col, e.d_val,
-                                                        e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag,
-                                                        e.d_tab_dx, e.d_col_s, e.d_bsrt);
+        cell_rows_kernel<true, double><<<nb, kCellThreads, kCellSmem, st>>>(
+            parts, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr, nullptr, e.d_rowptr, e.d_col,
+            e.d_val, e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag, e.d_tab_dx, e.d_col_s, e.d_col_s16,
+            e.d_bsrt);
     e.launches += 1;
     int flag = 0;
     cudaMemcpyAsync(&flag, e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -390,6 +536,7 @@ int jacobian_assemble(Engine &e, const double *x)
         return SDDDST_ERR_CAPACITY;
     }
     e.col_s_valid = true;
+    e.col_s16_valid = e.d_col_s16 != nullptr;
     e.spmv_sorted = e.d_sorted;
     return 0;
 }

@@ -40,9 +40,9 @@ __global__ void spmv_j_kernel(int n, double h, const double *__restrict__ hrow, 
 // The same product with the off-diagonal gathers taken from a copy of v in
 // the cell-sorted order (vs[k] = v[sorted[k]]): a row's neighbours then lie in
 // nine contiguous runs of vs instead of random sectors of v.
-template <typename VT>
+template <typename VT, typename IT>
 __global__ void spmv_js_kernel(int n, double h, const double *__restrict__ hrow, const int *__restrict__ rowptr,
-                               const int *__restrict__ col_s, const VT *__restrict__ val,
+                               const IT *__restrict__ col_s, const VT *__restrict__ val,
                                const double *__restrict__ dvec, const double *__restrict__ v,
                                const double *__restrict__ vs, double *__restrict__ y)
 {
@@ -305,13 +305,23 @@ void launch_spmv_J(Engine &e, double h, const double *dvec, const double *v, dou
     if (e.col_s_valid) {
         e.launches++;
         gather_sorted_kernel<<<(e.n + 255) / 256, 256, 0, st>>>(e.n, e.spmv_sorted, v, e.d_vsort);
-        if (e.valf)
-            spmv_js_kernel<float><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_hrow, e.d_rowptr, e.d_col_s,
-                                                                              e.d_valf, dvec, v, e.d_vsort, y);
-        else
-            spmv_js_kernel<double><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, h, e.d_hrow, e.d_rowptr,
-                                                                               e.d_col_s, e.d_val, dvec, v, e.d_vsort,
-                                                                               y);
+        const unsigned nb = (unsigned)((e.n + wpb - 1) / wpb);
+        if (e.col_s16_valid) { // 16-bit positions: 2 bytes less per entry
+            if (e.valf)
+                spmv_js_kernel<float, unsigned short><<<nb, 32 * wpb, 0, st>>>(e.n, h, e.d_hrow, e.d_rowptr,
+                                                                                e.d_col_s16, e.d_valf, dvec, v,
+                                                                                e.d_vsort, y);
+            else
+                spmv_js_kernel<double, unsigned short><<<nb, 32 * wpb, 0, st>>>(e.n, h, e.d_hrow, e.d_rowptr,
+                                                                                 e.d_col_s16, e.d_val, dvec, v,
+                                                                                 e.d_vsort, y);
+        } else if (e.valf) {
+            spmv_js_kernel<float, int><<<nb, 32 * wpb, 0, st>>>(e.n, h, e.d_hrow, e.d_rowptr, e.d_col_s, e.d_valf,
+                                                                dvec, v, e.d_vsort, y);
+        } else {
+            spmv_js_kernel<double, int><<<nb, 32 * wpb, 0, st>>>(e.n, h, e.d_hrow, e.d_rowptr, e.d_col_s, e.d_val,
+                                                                 dvec, v, e.d_vsort, y);
+        }
         return;
     }
     if (e.valf)
@@ -445,6 +455,24 @@ __device__ __forceinline__ void gs_block_dots(int kk, const double *__restrict__
     __threadfence();
 }
 
+// sums_s[k] = sum over the nb per-CTA partials of entry k, k < cnt: one warp
+// per entry, lane-strided partial sums then a butterfly, lane 0's result
+// kept (a fixed order, so every CTA computes the same values).  A serial sum
+// over the partials would put nb dependent L2 round trips on the critical
+// path of every pass.
+__device__ __forceinline__ void gs_sum_partials(const double *__restrict__ part, int nb, int cnt, double *sums_s)
+{
+    constexpr int KM = 32;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = wid; k < cnt; k += nw) {
+        double t = 0.0;
+        for (int b = lane; b < nb; b += 32) t += part[(size_t)b * KM + k];
+        t = warp_sum(t);
+        if (lane == 0) sums_s[k] = t;
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(256) gs_iter_kernel(int n, int kk, const double *__restrict__ V, size_t ldv,
                                                       double *__restrict__ w, double *__restrict__ rec, int m1,
                                                       double *__restrict__ partials, double *__restrict__ vnext)
@@ -461,13 +489,8 @@ __global__ void __launch_bounds__(256) gs_iter_kernel(int n, int kk, const doubl
         double *part = partials + ((size_t)pass * nb) * KM;
         gs_block_dots(kk, V, ldv, w, s0, e0, red, part + (size_t)blockIdx.x * KM, false);
         grid.sync();
-        if (tid < kk) {
-            double t = 0.0;
-            for (int b = 0; b < nb; ++b) t += part[(size_t)b * KM + tid];
-            cs[tid] = t;
-            if (blockIdx.x == 0) rec[pass * m1 + tid] = t;
-        }
-        __syncthreads();
+        gs_sum_partials(part, nb, kk, cs);
+        if (blockIdx.x == 0 && tid < kk) rec[pass * m1 + tid] = cs[tid];
         for (int i = s0 + tid; i < e0; i += blockDim.x) {
             double u = 0.0;
             for (int k = 0; k < kk; ++k) u += V[(size_t)k * ldv + i] * cs[k];
@@ -478,8 +501,8 @@ __global__ void __launch_bounds__(256) gs_iter_kernel(int n, int kk, const doubl
     double *part = partials + ((size_t)2 * nb) * KM;
     gs_block_dots(kk, V, ldv, w, s0, e0, red, part + (size_t)blockIdx.x * KM, true);
     grid.sync();
-    double nrm2 = 0.0;
-    for (int b = 0; b < nb; ++b) nrm2 += part[(size_t)b * KM];
+    gs_sum_partials(part, nb, 1, cs);
+    const double nrm2 = cs[0];
     if (blockIdx.x == 0 && tid == 0) rec[2 * m1] = nrm2;
     for (int i = s0 + tid; i < e0; i += blockDim.x) vnext[i] = nrm2 > 0.0 ? w[i] * rsqrt(nrm2) : 0.0;
 }

@@ -25,12 +25,20 @@ namespace sd {
 
 constexpr int kMaxBlock = 32;
 
+// s_ij >= theta  <=>  v^2 / |M_jj| >= theta^2 |M_ii| / h^2  (v = G_ij), and
+// within row i the strongest j maximises v^2 / |M_jj|: the search compares
+// that key, so a row costs two multiplies per entry instead of a square root
+// and a division.  rm_j = 1 / |M_jj| (0 where M_jj = 0: no coupling) comes
+// from the cell-sorted copy when present (msrt, read through the CSR's sorted
+// column positions, ties broken by the sorted position), else it is formed
+// per entry (ties broken by the column index).
 template <typename VT>
 __global__ void strongest_kernel(int n, double h0, const double *__restrict__ hrow, double theta,
                                  const int *__restrict__ rowptr, const int *__restrict__ col,
                                  const VT *__restrict__ val, const double *__restrict__ gdiag,
                                  const double *__restrict__ dvec, int *__restrict__ ptr,
-                                 const int *__restrict__ col_s, const double *__restrict__ msrt)
+                                 const int *__restrict__ col_s, const VT *__restrict__ msrt,
+                                 const int *__restrict__ sorted)
 {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -38,39 +46,50 @@ __global__ void strongest_kernel(int n, double h0, const double *__restrict__ hr
     const double h = hrow ? hrow[i] : h0; // couplings never cross systems, so row i's h serves the pair
     const int s = rowptr[i], e = rowptr[i + 1];
     const double mii = 2.0 / (1.0 + dvec[i]) + h * gdiag[i];
-    double best = -1.0;
-    int bj = i;
+    const VT thr = (VT)(theta * theta * fabs(mii) / (h * h));
+    VT best = (VT)-1;
+    int bid = 0x7fffffff;
     for (int q = s + 1 + lane; q < e; q += 32) {
-        const int j = col[q];
-        // M_jj from the cell-sorted copy when present (contiguous reads), else gathered
-        const double mjj = msrt ? msrt[col_s[q]] : 2.0 / (1.0 + dvec[j]) + h * gdiag[j];
-        const double den = sqrt(fabs(mii) * fabs(mjj));
-        const double sij = den > 0 ? h * fabs((double)val[q]) / den : 0.0;
-        if (sij >= theta && (sij > best || (sij == best && j < bj))) {
-            best = sij;
-            bj = j;
+        const VT v = val[q];
+        VT rm;
+        int id;
+        if (msrt) {
+            id = col_s[q];
+            rm = msrt[id];
+        } else {
+            id = col[q];
+            const double mjj = 2.0 / (1.0 + dvec[id]) + h * gdiag[id];
+            rm = mjj != 0.0 ? (VT)(1.0 / fabs(mjj)) : (VT)0;
+        }
+        const VT key = v * v * rm;
+        if (key >= thr && (key > best || (key == best && id < bid))) {
+            best = key;
+            bid = id;
         }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        int oj = __shfl_xor_sync(0xffffffffu, bj, o);
-        if (ob > best || (ob == best && oj < bj)) {
+        const VT ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oid = __shfl_xor_sync(0xffffffffu, bid, o);
+        if (ob > best || (ob == best && oid < bid)) {
             best = ob;
-            bj = oj;
+            bid = oid;
         }
     }
-    if (lane == 0) ptr[i] = best >= theta ? bj : i;
+    if (lane == 0) ptr[i] = best >= thr && bid != 0x7fffffff ? (msrt ? sorted[bid] : bid) : i;
 }
 
-// M_jj = 2 / (1 + d_j) + h G_jj in the cell-sorted order (single system)
+// 1 / |M_jj| (M_jj = 2 / (1 + d_j) + h G_jj; 0 where M_jj = 0) in the
+// cell-sorted order (single system)
+template <typename VT>
 __global__ void msorted_kernel(int n, double h, const int *__restrict__ sorted, const double *__restrict__ gdiag,
-                               const double *__restrict__ dvec, double *__restrict__ msrt)
+                               const double *__restrict__ dvec, VT *__restrict__ msrt)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int j = sorted[k];
-    msrt[k] = 2.0 / (1.0 + dvec[j]) + h * gdiag[j];
+    const double m = 2.0 / (1.0 + dvec[j]) + h * gdiag[j];
+    msrt[k] = m != 0.0 ? (VT)(1.0 / fabs(m)) : (VT)0;
 }
 
 __global__ void root_init_kernel(int n, const int *__restrict__ ptr, int *__restrict__ parent)
@@ -249,27 +268,23 @@ __global__ void block_invert_kernel(int nb, double h0, const double *__restrict_
         for (int c = lane; c < k; c += 32) dst[r * k + c] = M[r][k + c];
 }
 
-__global__ void block_apply_kernel(int nb, const int *__restrict__ bstart, const int *__restrict__ blen,
+// z = M^-1 v, one thread per dislocation i: its row loc[i] of its block's
+// inverse against the block's members (most blocks hold one or two
+// dislocations, so a warp per block would leave most lanes idle).
+__global__ void block_apply_kernel(int n, const int *__restrict__ blk_of, const int *__restrict__ loc,
+                                   const int *__restrict__ bstart, const int *__restrict__ blen,
                                    const int *__restrict__ members, const int *__restrict__ off,
                                    const double *__restrict__ binv, const double *__restrict__ v,
                                    double *__restrict__ z)
 {
-    const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (b >= nb) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int b = blk_of[i];
     const int k = blen[b], s = bstart[b];
-    const double *B = binv + off[b];
-    if (k == 1) {
-        if (lane == 0) z[members[s]] = B[0] * v[members[s]];
-        return;
-    }
-    double vl = lane < k ? v[members[s + lane]] : 0.0;
+    const double *B = binv + off[b] + (size_t)loc[i] * k;
     double acc = 0.0;
-    for (int c = 0; c < k; ++c) {
-        double vc = __shfl_sync(0xffffffffu, vl, c);
-        if (lane < k) acc += B[lane * k + c] * vc;
-    }
-    if (lane < k) z[members[s + lane]] = acc;
+    for (int c = 0; c < k; ++c) acc += B[c] * v[members[s + c]];
+    z[i] = acc;
 }
 
 // scan helper from jacobian.cu
@@ -285,18 +300,19 @@ int precond_build(Engine &e, double h, const double *dvec)
     int *ptr = e.pc_ptr, *par = e.pc_parent, *par2 = e.pc_tmp;
     // single system: M_jj in the cell-sorted order (the SpMV's staging buffer,
     // free until the solve), read through the CSR's sorted column positions
-    const double *msrt = nullptr;
-    if (e.col_s_valid && !e.d_hrow) {
-        msorted_kernel<<<nb256, 256, 0, st>>>(n, h, e.spmv_sorted, e.d_gdiag, dvec, e.d_vsort);
-        msrt = e.d_vsort;
-        e.launches++;
-    }
-    if (e.valf)
+    const bool srt = e.col_s_valid && !e.d_hrow;
+    if (e.valf) {
+        float *msrt = srt ? reinterpret_cast<float *>(e.d_vsort) : nullptr;
+        if (srt) msorted_kernel<float><<<nb256, 256, 0, st>>>(n, h, e.spmv_sorted, e.d_gdiag, dvec, msrt);
         strongest_kernel<float><<<(n + 7) / 8, 256, 0, st>>>(n, h, e.d_hrow, theta, e.d_rowptr, e.d_col, e.d_valf,
-                                                             e.d_gdiag, dvec, ptr, e.d_col_s, msrt);
-    else
+                                                             e.d_gdiag, dvec, ptr, e.d_col_s, msrt, e.spmv_sorted);
+    } else {
+        double *msrt = srt ? e.d_vsort : nullptr;
+        if (srt) msorted_kernel<double><<<nb256, 256, 0, st>>>(n, h, e.spmv_sorted, e.d_gdiag, dvec, msrt);
         strongest_kernel<double><<<(n + 7) / 8, 256, 0, st>>>(n, h, e.d_hrow, theta, e.d_rowptr, e.d_col, e.d_val,
-                                                              e.d_gdiag, dvec, ptr, e.d_col_s, msrt);
+                                                              e.d_gdiag, dvec, ptr, e.d_col_s, msrt, e.spmv_sorted);
+    }
+    if (srt) e.launches++;
     root_init_kernel<<<nb256, 256, 0, st>>>(n, ptr, par);
     for (int it = 0; it < 12; ++it) {
         jump_kernel<<<nb256, 256, 0, st>>>(n, par, par2);
@@ -358,8 +374,8 @@ int precond_build(Engine &e, double h, const double *dvec)
 
 void precond_apply(Engine &e, const double *v, double *z)
 {
-    block_apply_kernel<<<(e.pc_nb + 7) / 8, 256, 0, e.st>>>(e.pc_nb, e.pc_bstart, e.pc_blen, e.pc_members, e.pc_off,
-                                                            e.pc_binv, v, z);
+    block_apply_kernel<<<(e.n + 255) / 256, 256, 0, e.st>>>(e.n, e.pc_blk_of, e.pc_loc, e.pc_bstart, e.pc_blen,
+                                                            e.pc_members, e.pc_off, e.pc_binv, v, z);
     e.launches++;
 }
 

@@ -103,6 +103,42 @@ def test_jacobian_matches_oracle(engine_lib, port_lib, n, seed, m, p, h):
     _compare_jacobian(e, h, xyb, Ap, Ai, Ax, d, n)
 
 
+def test_jacobian_clustered_cells(engine_lib, port_lib):
+    """A cluster of 2600 dislocations in one 0.04 x 0.04 square among 1400
+    spread ones (N=4000, cutoff multiplier 1, 8 x 8 cells): the neighbour
+    blocks around the cluster exceed the shared-memory stage of the
+    assembly and walk global memory, the others are staged; the CSR is the
+    oracle's either way (pattern exact, values 1e-10)."""
+    import scipy.sparse as sp
+    from sdddst_b200 import capi
+    rng = np.random.default_rng(8)
+    n, m, h = 4000, 1.0, 1e-6
+    pos = np.concatenate([rng.uniform(-0.5, 0.5, (1400, 2)), 0.1 + rng.uniform(-0.02, 0.02, (2600, 2))])
+    b = rng.permutation(np.r_[np.ones(n // 2), -np.ones(n // 2)])
+    xyb = np.column_stack([pos, b])
+    o = ref.Sim(xyb, None, ref.params(cutoff_multiplier=m, prec=1e-6), "port")
+    e = capi.Engine(capi.cli_params(n, m, 1e-6), xyb)
+    Ap, Ai, Ax, d_ref = o.jacobian(h, xyb)
+    rp, col, val, d = e.jacobian(h, xyb)
+    J = sp.csr_matrix((val, col, rp), shape=(n, n)).tocoo()
+    Jr = sp.csc_matrix((Ax, Ai, Ap), shape=(n, n)).tocsr()
+    pat = sp.csr_matrix((np.ones(J.nnz), (J.row, J.col)), shape=(n, n))
+    pr = Jr.copy()
+    pr.data[:] = 1.0
+    pr = ((pr + pr.T) > 0).astype(float)
+    assert (pat != pr).nnz == 0, "sparsity pattern differs"
+    diff = abs(J.tocsr() - Jr)
+    off = sp.triu(abs(Jr), 1)
+    assert diff.max() <= 1e-10 * max(off.max(), 1.0)
+    # d_i depends on the row sum G_ii, whose rounding grows with the row's
+    # cancellation kappa_i = sum_j |J_ij| / |J_ii - 1| (up to 1.5e4 inside the
+    # cluster, where terms of size 1e6 cancel): the bound scales with it
+    jd = Jr.diagonal()
+    rowabs = np.asarray(abs(Jr - sp.diags(jd)).sum(1)).ravel()
+    kappa = np.maximum(rowabs / np.maximum(np.abs(jd - 1.0), 1e-300), 1.0)
+    assert np.all(np.abs(d - d_ref) <= 1e-14 + 1e-9 * kappa * np.abs(d_ref))
+
+
 def test_solve_matches_dense(engine_lib, port_lib):
     n = 800
     xyb, pd, o, e = make_pair(n, 4, 1.0, 1e-6)
