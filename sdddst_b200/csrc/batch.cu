@@ -244,7 +244,17 @@ __global__ void batch_row_fill_kernel(long ntot, const int *__restrict__ inst, c
         const int lo = i < j ? i : j, hi = i < j ? j : i;
         double dx = wrap_half(x[hi] - x[lo]), dy = wrap_half(y[hi] - y[lo]);
         double w;
-        bpair_kept(r2_exact(dx, dy), c, c2, ic2, &w);
+        if (sizeof(VT) == sizeof(double)) {
+            bpair_kept(r2_exact(dx, dy), c, c2, ic2, &w);
+        } else { // FP32 value: FP32 weight
+            const double r2 = r2_exact(dx, dy);
+            float wf = 1.0f;
+            if (r2 > c2) {
+                const float t = sqrtf((float)r2) - (float)c;
+                wf = __expf(-(t * t) * (float)ic2);
+            }
+            w = (double)wf;
+        }
         double tdx;
         if (sizeof(VT) == sizeof(double)) tdx = tau_xy_dx_f64(dx, dy);
         else tdx = (double)tau_xy_dx_f32(__double2float_rn(dx), __double2float_rn(dy));

@@ -39,10 +39,12 @@ __global__ void cell_assign_kernel(int n, const double *__restrict__ x, const do
 }
 
 // Exclusive scan of m ints by one block: out[0] = 0, out[k+1] = sum_{<=k}.
-// Tiles of blockDim.x x 16 consecutive elements: each thread sums its 16,
-// the block scans the thread totals (warp shuffles, then one warp over the
-// warp totals, two barriers per tile), and each thread writes its 16
-// prefixes.  Sums run in 64 bits.
+// Tiles of blockDim.x x 16 consecutive elements: each thread loads its 16
+// (four 16-byte loads in flight at once where the input is aligned: one
+// block is bound by load round trips, not bandwidth) and sums them, the
+// block scans the thread totals (warp shuffles, then one warp over the warp
+// totals, two barriers per tile), and each thread writes its 16 prefixes.
+// Sums run in 64 bits.
 __global__ void scan_kernel(const int *__restrict__ in, int m, int *__restrict__ out)
 {
     constexpr int IT = 16;
@@ -52,12 +54,25 @@ __global__ void scan_kernel(const int *__restrict__ in, int m, int *__restrict__
     for (int base = 0; base < m; base += blockDim.x * IT) {
         const int k0 = base + tid * IT;
         int v[IT];
+        if (k0 + IT <= m && (reinterpret_cast<size_t>(in) & 15) == 0) {
+            const int4 *p4 = reinterpret_cast<const int4 *>(in + k0);
+            int4 a[IT / 4];
+#pragma unroll
+            for (int q = 0; q < IT / 4; ++q) a[q] = p4[q];
+#pragma unroll
+            for (int q = 0; q < IT / 4; ++q) {
+                v[4 * q] = a[q].x;
+                v[4 * q + 1] = a[q].y;
+                v[4 * q + 2] = a[q].z;
+                v[4 * q + 3] = a[q].w;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < IT; ++q) v[q] = k0 + q < m ? in[k0 + q] : 0;
+        }
         long long tsum = 0;
 #pragma unroll
-        for (int q = 0; q < IT; ++q) {
-            v[q] = k0 + q < m ? in[k0 + q] : 0;
-            tsum += v[q];
-        }
+        for (int q = 0; q < IT; ++q) tsum += v[q];
         long long s = tsum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -246,9 +261,18 @@ __device__ void row_values(int i, double xi, double yi, double bi, const CellSca
         const double xj = cs.xs[ks], yj = cs.ys[ks];
         double dx = wrap_half(i < j ? xj - xi : xi - xj); // x[hi] - x[lo]
         double dy = wrap_half(i < j ? yj - yi : yi - yj);
-        double w;
-        pair_kept(r2_exact(dx, dy), c, c2, ic2, &w);
-        double tdx;
+        double w, tdx;
+        if (sizeof(VT) == sizeof(double)) {
+            pair_kept(r2_exact(dx, dy), c, c2, ic2, &w);
+        } else { // the value is stored in FP32: its weight needs no FP64 square root and exponential
+            const double r2 = r2_exact(dx, dy);
+            float wf = 1.0f;
+            if (r2 > c2) {
+                const float t = sqrtf((float)r2) - (float)c;
+                wf = __expf(-(t * t) * (float)ic2);
+            }
+            w = (double)wf;
+        }
         if (tab_dx) tdx = tau0_xy_dx(dx, dy) + tab_interp(tab_dx, dx, dy); // tabulated field
         else if (sizeof(VT) == sizeof(double)) tdx = tau_xy_dx_f64(dx, dy);
         else tdx = (double)tau_xy_dx_f32(__double2float_rn(dx), __double2float_rn(dy));
@@ -341,6 +365,7 @@ __global__ void __launch_bounds__(kCellThreads) cell_rows_kernel(
         if (!kFill) {
             int cnt = 0;
             if (staged) {
+#pragma unroll 4
                 for (int t = lane; t < ncand; t += 32) {
                     const int j = sjc[t];
                     if (j != i) cnt += cand_kept(i, xi, yi, j, sxc[t], syc[t], c, c2, ic2, cs);

@@ -166,12 +166,13 @@ __global__ void block_list_kernel(int n, const int *__restrict__ count, const in
     }
 }
 
-__global__ void block_meta_kernel(int nb, const int *__restrict__ bstart, const int *__restrict__ blen,
-                                  const int *__restrict__ members, int *__restrict__ blk_of, int *__restrict__ loc,
-                                  int *__restrict__ sq)
+// nbp: the block count, on the device (no host round trip before the launch)
+__global__ void block_meta_kernel(const int *__restrict__ nbp, const int *__restrict__ bstart,
+                                  const int *__restrict__ blen, const int *__restrict__ members,
+                                  int *__restrict__ blk_of, int *__restrict__ loc, int *__restrict__ sq)
 {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
+    if (b >= *nbp) return;
     int s = bstart[b], k = blen[b];
     for (int t = 0; t < k; ++t) {
         int i = members[s + t];
@@ -184,7 +185,7 @@ __global__ void block_meta_kernel(int nb, const int *__restrict__ bstart, const 
 // One warp per block: dense J block, Gauss-Jordan inverse with partial
 // pivoting, written row-major at binv[off[b]].
 template <typename VT>
-__global__ void block_invert_kernel(int nb, double h0, const double *__restrict__ hrow, const int *__restrict__ bstart,
+__global__ void block_invert_kernel(const int *__restrict__ nbp, double h0, const double *__restrict__ hrow, const int *__restrict__ bstart,
                                     const int *__restrict__ blen,
                                     const int *__restrict__ members, const int *__restrict__ blk_of,
                                     const int *__restrict__ loc, const int *__restrict__ off,
@@ -196,7 +197,7 @@ __global__ void block_invert_kernel(int nb, double h0, const double *__restrict_
     __shared__ double A[2][kMaxBlock][2 * kMaxBlock + 1];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.x * 2 + wib;
-    if (b >= nb) return;
+    if (b >= *nbp) return;
     const int k = blen[b], s = bstart[b];
     double(*M)[2 * kMaxBlock + 1] = A[wib];
     const double h = hrow ? hrow[members[s]] : h0; // a block lies inside one system
@@ -326,44 +327,45 @@ int precond_build(Engine &e, double h, const double *dvec)
     cluster_sort_kernel<<<nb256, 256, 0, st>>>(n, e.pc_count, e.pc_start, e.pc_tmp2, e.pc_members, e.pc_nblk);
     scan_kernel<<<1, 1024, 0, st>>>(e.pc_nblk, n, e.pc_bbase);
     e.launches += 19;
-    int nb = 0;
-    cudaMemcpyAsync(&nb, e.pc_bbase + n, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (int rc = e.sync_check("precond clusters")) return rc;
-    if (nb <= 0 || nb > n) {
-        e.err = "precond: bad block count";
-        return SDDDST_ERR_SOLVER;
-    }
-    block_list_kernel<<<nb256, 256, 0, st>>>(n, e.pc_count, e.pc_start, e.pc_bbase, e.pc_bstart, e.pc_blen);
-    block_meta_kernel<<<(nb + 255) / 256, 256, 0, st>>>(nb, e.pc_bstart, e.pc_blen, e.pc_members, e.pc_blk_of,
-                                                        e.pc_loc, e.pc_sq);
-    scan_kernel<<<1, 1024, 0, st>>>(e.pc_sq, nb, e.pc_off);
-    e.launches += 3;
-    int total = 0;
-    cudaMemcpyAsync(&total, e.pc_off + nb, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (int rc = e.sync_check("precond blocks")) return rc;
-    if (total > e.pc_binv_cap) {
+    // the block count stays on the device (pc_bbase[n]); the block kernels
+    // run over n (an upper bound) and return beyond it, and the inverses'
+    // storage is sized for the bound sum k^2 <= kMaxBlock n once
+    const int *nbp = e.pc_bbase + n;
+    const long cap = (long)kMaxBlock * n + 1024;
+    if (cap > e.pc_binv_cap) {
         if (e.pc_binv) cudaFree(e.pc_binv);
         e.pc_binv = nullptr;
-        long cap = total + total / 4 + 1024;
+        e.pc_binv_cap = 0;
         if (cudaMalloc(&e.pc_binv, sizeof(double) * cap) != cudaSuccess) {
             e.err = "precond: allocation failed";
             return SDDDST_ERR_NOMEM;
         }
         e.pc_binv_cap = cap;
     }
+    block_list_kernel<<<nb256, 256, 0, st>>>(n, e.pc_count, e.pc_start, e.pc_bbase, e.pc_bstart, e.pc_blen);
+    cudaMemsetAsync(e.pc_sq, 0, sizeof(int) * (n + 1), st);
+    block_meta_kernel<<<nb256, 256, 0, st>>>(nbp, e.pc_bstart, e.pc_blen, e.pc_members, e.pc_blk_of, e.pc_loc,
+                                             e.pc_sq);
+    scan_kernel<<<1, 1024, 0, st>>>(e.pc_sq, n, e.pc_off);
     cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
+    const unsigned ib = (unsigned)((n + 1) / 2);
     if (e.valf)
-        block_invert_kernel<float><<<(nb + 1) / 2, 64, 0, st>>>(nb, h, e.d_hrow, e.pc_bstart, e.pc_blen, e.pc_members,
-                                                                e.pc_blk_of, e.pc_loc, e.pc_off, e.d_rowptr, e.d_col,
-                                                                e.d_valf, e.d_gdiag, dvec, e.pc_binv, e.d_flag);
+        block_invert_kernel<float><<<ib, 64, 0, st>>>(nbp, h, e.d_hrow, e.pc_bstart, e.pc_blen, e.pc_members,
+                                                      e.pc_blk_of, e.pc_loc, e.pc_off, e.d_rowptr, e.d_col, e.d_valf,
+                                                      e.d_gdiag, dvec, e.pc_binv, e.d_flag);
     else
-        block_invert_kernel<double><<<(nb + 1) / 2, 64, 0, st>>>(nb, h, e.d_hrow, e.pc_bstart, e.pc_blen, e.pc_members,
-                                                                 e.pc_blk_of, e.pc_loc, e.pc_off, e.d_rowptr, e.d_col,
-                                                                 e.d_val, e.d_gdiag, dvec, e.pc_binv, e.d_flag);
-    e.launches += 1;
-    int flag = 0;
+        block_invert_kernel<double><<<ib, 64, 0, st>>>(nbp, h, e.d_hrow, e.pc_bstart, e.pc_blen, e.pc_members,
+                                                       e.pc_blk_of, e.pc_loc, e.pc_off, e.d_rowptr, e.d_col, e.d_val,
+                                                       e.d_gdiag, dvec, e.pc_binv, e.d_flag);
+    e.launches += 4;
+    int flag = 0, nb = 0;
     cudaMemcpyAsync(&flag, e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (int rc = e.sync_check("precond invert")) return rc;
+    cudaMemcpyAsync(&nb, nbp, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (int rc = e.sync_check("precond build")) return rc;
+    if (nb <= 0 || nb > n) {
+        e.err = "precond: bad block count";
+        return SDDDST_ERR_SOLVER;
+    }
     if (flag) {
         e.err = "precond: singular cluster block";
         return SDDDST_ERR_SOLVER;
