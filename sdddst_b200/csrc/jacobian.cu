@@ -39,47 +39,39 @@ __global__ void cell_assign_kernel(int n, const double *__restrict__ x, const do
 }
 
 // Exclusive scan of m ints by one block: out[0] = 0, out[k+1] = sum_{<=k}.
-// Tiles of blockDim.x x 16 consecutive elements: each thread loads its 16
-// (four 16-byte loads in flight at once where the input is aligned: one
-// block is bound by load round trips, not bandwidth) and sums them, the
-// block scans the thread totals (warp shuffles, then one warp over the warp
-// totals, two barriers per tile), and each thread writes its 16 prefixes.
-// Sums run in 64 bits.
+// Tiles of 512 consecutive elements per warp (16 rounds of 32): each round
+// is loaded and stored lane-consecutive (coalesced; all sixteen loads are in
+// flight together) and scanned with shuffles, the round's total carried to
+// the next; one warp then scans the warp totals (two barriers per tile of
+// blockDim.x * 16 elements).  Sums run in 64 bits.
 __global__ void scan_kernel(const int *__restrict__ in, int m, int *__restrict__ out)
 {
-    constexpr int IT = 16;
+    constexpr int R = 16;
     __shared__ long long warp_tot[32];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
     long long carry = 0;
-    for (int base = 0; base < m; base += blockDim.x * IT) {
-        const int k0 = base + tid * IT;
-        int v[IT];
-        if (k0 + IT <= m && (reinterpret_cast<size_t>(in) & 15) == 0) {
-            const int4 *p4 = reinterpret_cast<const int4 *>(in + k0);
-            int4 a[IT / 4];
+    for (int base = 0; base < m; base += blockDim.x * R) {
+        const int w0 = base + wid * 32 * R;
+        int v[R];
 #pragma unroll
-            for (int q = 0; q < IT / 4; ++q) a[q] = p4[q];
+        for (int r = 0; r < R; ++r) {
+            const int k = w0 + r * 32 + lane;
+            v[r] = k < m ? in[k] : 0;
+        }
+        long long pre[R];
+        long long run = 0;
 #pragma unroll
-            for (int q = 0; q < IT / 4; ++q) {
-                v[4 * q] = a[q].x;
-                v[4 * q + 1] = a[q].y;
-                v[4 * q + 2] = a[q].z;
-                v[4 * q + 3] = a[q].w;
+        for (int r = 0; r < R; ++r) {
+            long long s = v[r];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long t = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += t;
             }
-        } else {
-#pragma unroll
-            for (int q = 0; q < IT; ++q) v[q] = k0 + q < m ? in[k0 + q] : 0;
+            pre[r] = run + s;
+            run += __shfl_sync(0xffffffffu, s, 31);
         }
-        long long tsum = 0;
-#pragma unroll
-        for (int q = 0; q < IT; ++q) tsum += v[q];
-        long long s = tsum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const long long t = __shfl_up_sync(0xffffffffu, s, o);
-            if (lane >= o) s += t;
-        }
-        if (lane == 31) warp_tot[wid] = s;
+        if (lane == 0) warp_tot[wid] = run;
         __syncthreads();
         if (wid == 0) {
             long long t = lane < nw ? warp_tot[lane] : 0;
@@ -91,11 +83,11 @@ __global__ void scan_kernel(const int *__restrict__ in, int m, int *__restrict__
             if (lane < nw) warp_tot[lane] = t;
         }
         __syncthreads();
-        long long run = carry + (wid > 0 ? warp_tot[wid - 1] : 0) + s - tsum;
+        const long long off = carry + (wid > 0 ? warp_tot[wid - 1] : 0);
 #pragma unroll
-        for (int q = 0; q < IT; ++q) {
-            run += v[q];
-            if (k0 + q < m) out[k0 + q + 1] = (int)run;
+        for (int r = 0; r < R; ++r) {
+            const int k = w0 + r * 32 + lane;
+            if (k < m) out[k + 1] = (int)(off + pre[r]);
         }
         carry += warp_tot[nw - 1];
         __syncthreads(); // warp_tot is rewritten by the next tile
@@ -133,7 +125,24 @@ struct CellScan {
     const int *sorted;
     const double *xs, *ys; // positions in the cell-sorted order (contiguous per cell)
     double keep_below, keep_above; // r^2 bounds of the cheap decision (see pair_kept_search)
+    float kb_f, ka_f;              // the same from FP32 copies of the positions, with a wider margin
 };
+
+// Minimum-image difference in FP32 for positions already wrapped into
+// [-0.5, 0.5): d - rint(d) with rint as the add/subtract of 1.5 * 2^23.
+__device__ __forceinline__ float wrap_diff_f32(float d)
+{
+    const float m = 12582912.0f;
+    return d - __fadd_rn(__fadd_rn(d, m), -m);
+}
+
+// Minimum-image difference in FP64 (branch-free; |d| < 2^51): the same value
+// as wrap_half except at exactly +1/2, which it keeps.
+__device__ __forceinline__ double wrap_diff_f64(double d)
+{
+    const double m = 6755399441055744.0;
+    return d - __dadd_rn(__dadd_rn(d, m), -m);
+}
 
 // Visits the cells around (cx, cy) once each: 3x3 for G >= 3, all cells
 // otherwise.
@@ -259,8 +268,10 @@ __device__ void row_values(int i, double xi, double yi, double bi, const CellSca
     for (int q = base + 1 + lane; q < end; q += 32) {
         const int j = col[q], ks = col_s[q];
         const double xj = cs.xs[ks], yj = cs.ys[ks];
-        double dx = wrap_half(i < j ? xj - xi : xi - xj); // x[hi] - x[lo]
-        double dy = wrap_half(i < j ? yj - yi : yi - yj);
+        const double ddx = i < j ? xj - xi : xi - xj, ddy = i < j ? yj - yi : yi - yj; // x[hi] - x[lo]
+        // FP64 values keep the reference's wrap; FP32 values take the branch-free one
+        const double dx = sizeof(VT) == sizeof(double) ? wrap_half(ddx) : wrap_diff_f64(ddx);
+        const double dy = sizeof(VT) == sizeof(double) ? wrap_half(ddy) : wrap_diff_f64(ddy);
         double w, tdx;
         if (sizeof(VT) == sizeof(double)) {
             pair_kept(r2_exact(dx, dy), c, c2, ic2, &w);
@@ -297,16 +308,45 @@ __device__ void row_values(int i, double xi, double yi, double bi, const CellSca
 }
 
 // Count (kFill = false) or fill (kFill = true) pass over the rows of one
-// cell.  Block (cell, part) stages the cell's 3x3 neighbour block (positions
-// and indices of up to kCandCap candidates, in visiting order) in shared
-// memory once; its warps then test their rows against it without touching
-// global memory, one row per warp at a time, the cell's rows split into
-// `parts` contiguous ranges.  A block larger than kCandCap (or a grid below
-// 3x3 cells) walks global memory cell by cell instead.  Both routes visit
-// candidates in the same order, so the CSR layout is the same either way.
-constexpr int kCandCap = 2720;
+// cell.  Block (cell, part) stages the cell's 3x3 neighbour block (FP32
+// copies of the wrapped positions and the indices of up to kCandCap
+// candidates, in visiting order) in shared memory once; its warps then test
+// their rows against it, one row per warp at a time, the cell's rows split
+// into `parts` contiguous ranges.  The FP32 r^2 decides every candidate
+// farther than the FP32 error (a relative margin of max(1e-4, 1e-5 / r_p) in
+// r^2, well above the 2e-7 (|dx| + |dy|) absolute error of the FP32 r^2)
+// from the pattern radius; candidates inside that shell take the reference's
+// rounded FP64 test on the FP64 positions.  The row's own entry is the
+// candidate at its own position in the centre cell.  A block larger than
+// kCandCap (or a grid below 3x3 cells) walks global memory cell by cell with
+// the FP64 test instead.  Both routes visit candidates in the same order and
+// make the same decisions, so the CSR is the same either way.
+constexpr int kCandCap = 4096;
 constexpr int kCellThreads = 256;
-constexpr size_t kCellSmem = (size_t)kCandCap * (2 * sizeof(double) + sizeof(int));
+constexpr size_t kCellSmem = (size_t)kCandCap * (2 * sizeof(float) + sizeof(int));
+
+// Sorted position of staged candidate t (segment search over the <= 9 cells).
+__device__ __forceinline__ int cand_pos(int t, const int *seg_start, const int *seg_off)
+{
+    int sg = 0;
+    while (t >= seg_off[sg + 1]) ++sg;
+    return seg_start[sg] + (t - seg_off[sg]);
+}
+
+// Staged decision for candidate t of row i: FP32 r^2 away from the pattern
+// radius, the FP64 test inside the shell.
+__device__ __forceinline__ bool staged_kept(int i, double xi, double yi, float xif, float yif, int t,
+                                            const float *sxc, const float *syc, const int *sjc,
+                                            const int *seg_start, const int *seg_off, double c, double c2,
+                                            double ic2, const CellScan &cs)
+{
+    const float dx = wrap_diff_f32(sxc[t] - xif), dy = wrap_diff_f32(syc[t] - yif);
+    const float r2f = fmaf(dx, dx, dy * dy);
+    if (r2f < cs.kb_f) return true;
+    if (r2f > cs.ka_f) return false;
+    const int k = cand_pos(t, seg_start, seg_off);
+    return cand_kept(i, xi, yi, sjc[t], cs.xs[k], cs.ys[k], c, c2, ic2, cs);
+}
 
 template <bool kFill, typename VT>
 __global__ void __launch_bounds__(kCellThreads) cell_rows_kernel(
@@ -317,8 +357,8 @@ __global__ void __launch_bounds__(kCellThreads) cell_rows_kernel(
     int *__restrict__ col_s, unsigned short *__restrict__ col_s16, const double *__restrict__ bs)
 {
     extern __shared__ __align__(16) unsigned char cell_smem[];
-    double *sxc = reinterpret_cast<double *>(cell_smem);
-    double *syc = sxc + kCandCap;
+    float *sxc = reinterpret_cast<float *>(cell_smem);
+    float *syc = sxc + kCandCap;
     int *sjc = reinterpret_cast<int *>(syc + kCandCap);
     __shared__ int seg_start[9], seg_off[10];
 
@@ -352,8 +392,8 @@ __global__ void __launch_bounds__(kCellThreads) cell_rows_kernel(
                 int sgi = 0;
                 while (t >= seg_off[sgi + 1]) ++sgi;
                 const int k = seg_start[sgi] + (t - seg_off[sgi]);
-                sxc[t] = cs.xs[k];
-                syc[t] = cs.ys[k];
+                sxc[t] = (float)wrap_half(cs.xs[k]);
+                syc[t] = (float)wrap_half(cs.ys[k]);
                 sjc[t] = cs.sorted[k];
             }
             __syncthreads();
@@ -362,14 +402,15 @@ __global__ void __launch_bounds__(kCellThreads) cell_rows_kernel(
     for (int r = rbeg + warp; r < rend; r += nwarps) {
         const int i = cs.sorted[r];
         const double xi = x[i], yi = y[i];
+        const float xif = (float)wrap_half(xi), yif = (float)wrap_half(yi);
+        const int own = staged ? seg_off[4] + (r - seg_start[4]) : -1; // the centre cell is visited fifth
         if (!kFill) {
             int cnt = 0;
             if (staged) {
 #pragma unroll 4
-                for (int t = lane; t < ncand; t += 32) {
-                    const int j = sjc[t];
-                    if (j != i) cnt += cand_kept(i, xi, yi, j, sxc[t], syc[t], c, c2, ic2, cs);
-                }
+                for (int t = lane; t < ncand; t += 32)
+                    cnt += t != own &&
+                           staged_kept(i, xi, yi, xif, yif, t, sxc, syc, sjc, seg_start, seg_off, c, c2, ic2, cs);
             } else {
                 cnt = row_count_global(i, xi, yi, cs, c, c2, ic2, lane);
             }
@@ -384,18 +425,16 @@ __global__ void __launch_bounds__(kCellThreads) cell_rows_kernel(
                 for (int t0 = 0; t0 < ncand; t0 += 32) {
                     const int t = t0 + lane;
                     bool hit = false;
-                    int j = -1;
-                    if (t < ncand) {
-                        j = sjc[t];
-                        if (j != i) hit = cand_kept(i, xi, yi, j, sxc[t], syc[t], c, c2, ic2, cs);
-                    }
+                    if (t < ncand && t != own)
+                        hit = staged_kept(i, xi, yi, xif, yif, t, sxc, syc, sjc, seg_start, seg_off, c, c2, ic2,
+                                          cs);
                     const unsigned m = __ballot_sync(0xffffffffu, hit);
                     const int at = pos + __popc(m & ((1u << lane) - 1u));
                     if (hit && at < rowend) {
                         int sg = sgi;
                         while (t >= seg_off[sg + 1]) ++sg;
                         const int k = seg_start[sg] + (t - seg_off[sg]);
-                        col[at] = j;
+                        col[at] = sjc[t];
                         col_s[at] = k;
                         if (col_s16) col_s16[at] = (unsigned short)k;
                     }
@@ -520,7 +559,9 @@ int jacobian_assemble(Engine &e, const double *x)
     cell_sort_kernel<<<ncell, 256, 0, st>>>(e.d_cell_start, e.d_rowcnt, e.d_sorted);
     gather_cells_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, e.d_sorted, x, e.d_y, e.d_b, e.d_xsrt, e.d_ysrt, e.d_bsrt);
     const double rp = e.cutoff * (1.0 + std::sqrt(36.8));
-    CellScan cs{G, e.d_cell_start, e.d_sorted, e.d_xsrt, e.d_ysrt, rp * rp * (1.0 - 1e-6), rp * rp * (1.0 + 1e-6)};
+    const double rel = std::max(1e-4, 1e-5 / rp);
+    CellScan cs{G, e.d_cell_start, e.d_sorted, e.d_xsrt, e.d_ysrt, rp * rp * (1.0 - 1e-6), rp * rp * (1.0 + 1e-6),
+                (float)(rp * rp * (1.0 - rel)), (float)(rp * rp * (1.0 + rel))};
     const int parts = cell_parts(e, ncell);
     const unsigned nb = (unsigned)(ncell * parts);
     cell_rows_kernel<false, float><<<nb, kCellThreads, kCellSmem, st>>>(

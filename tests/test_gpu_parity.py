@@ -104,16 +104,17 @@ def test_jacobian_matches_oracle(engine_lib, port_lib, n, seed, m, p, h):
 
 
 def test_jacobian_clustered_cells(engine_lib, port_lib):
-    """A cluster of 2600 dislocations in one 0.04 x 0.04 square among 1400
-    spread ones (N=4000, cutoff multiplier 1, 8 x 8 cells): the neighbour
-    blocks around the cluster exceed the shared-memory stage of the
-    assembly and walk global memory, the others are staged; the CSR is the
+    """A cluster of 4200 dislocations in one 0.04 x 0.04 square among 1800
+    spread ones (N=6000, cutoff multiplier 1, 10 x 10 cells): the four
+    neighbour blocks holding the whole cluster exceed the shared-memory stage
+    of the assembly (4096 candidates) and walk global memory with the FP64
+    test, the others are staged with the FP32 prefilter; the CSR is the
     oracle's either way (pattern exact, values 1e-10)."""
     import scipy.sparse as sp
     from sdddst_b200 import capi
     rng = np.random.default_rng(8)
-    n, m, h = 4000, 1.0, 1e-6
-    pos = np.concatenate([rng.uniform(-0.5, 0.5, (1400, 2)), 0.1 + rng.uniform(-0.02, 0.02, (2600, 2))])
+    n, m, h = 6000, 1.0, 1e-6
+    pos = np.concatenate([rng.uniform(-0.5, 0.5, (1800, 2)), 0.1 + rng.uniform(-0.02, 0.02, (4200, 2))])
     b = rng.permutation(np.r_[np.ones(n // 2), -np.ones(n // 2)])
     xyb = np.column_stack([pos, b])
     o = ref.Sim(xyb, None, ref.params(cutoff_multiplier=m, prec=1e-6), "port")
@@ -131,7 +132,7 @@ def test_jacobian_clustered_cells(engine_lib, port_lib):
     off = sp.triu(abs(Jr), 1)
     assert diff.max() <= 1e-10 * max(off.max(), 1.0)
     # d_i depends on the row sum G_ii, whose rounding grows with the row's
-    # cancellation kappa_i = sum_j |J_ij| / |J_ii - 1| (up to 1.5e4 inside the
+    # cancellation kappa_i = sum_j |J_ij| / |J_ii - 1| (above 1e4 inside the
     # cluster, where terms of size 1e6 cancel): the bound scales with it
     jd = Jr.diagonal()
     rowabs = np.asarray(abs(Jr - sp.diags(jd)).sum(1)).ravel()
