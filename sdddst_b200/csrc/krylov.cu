@@ -57,6 +57,38 @@ __global__ void spmv_js_kernel(int n, double h, const double *__restrict__ hrow,
     if (lane == 0) y[row] = v[row] + (1.0 + dvec[row]) * 0.5 * hh * acc;
 }
 
+// The FP32-value, 16-bit-position form with four entries per lane per step:
+// 16-byte value loads and 8-byte position loads from the first multiple of
+// four in the row on (fewer, wider requests in flight), the unaligned head
+// and the tail entry by entry.
+__global__ void spmv_js4_kernel(int n, double h, const double *__restrict__ hrow, const int *__restrict__ rowptr,
+                                const unsigned short *__restrict__ col_s, const float *__restrict__ val,
+                                const double *__restrict__ dvec, const double *__restrict__ v,
+                                const double *__restrict__ vs, double *__restrict__ y)
+{
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const int s = rowptr[row], e = rowptr[row + 1];
+    double acc = lane == 0 ? (double)val[s] * v[row] : 0.0; // diagonal slot
+    const int q0 = s + 1;
+    const int qa = min(e, (q0 + 3) & ~3);
+    if (q0 + lane < qa) acc += (double)val[q0 + lane] * vs[col_s[q0 + lane]];
+    for (int q = qa + 4 * lane; q + 3 < e; q += 128) {
+        const float4 w = *reinterpret_cast<const float4 *>(val + q);
+        const uint2 c = *reinterpret_cast<const uint2 *>(col_s + q);
+        acc += (double)w.x * vs[c.x & 0xffffu];
+        acc += (double)w.y * vs[c.x >> 16];
+        acc += (double)w.z * vs[c.y & 0xffffu];
+        acc += (double)w.w * vs[c.y >> 16];
+    }
+    const int qt = qa + ((e - qa) & ~3);
+    if (qt + lane < e) acc += (double)val[qt + lane] * vs[col_s[qt + lane]];
+    acc = warp_sum(acc);
+    const double hh = hrow ? hrow[row] : h;
+    if (lane == 0) y[row] = v[row] + (1.0 + dvec[row]) * 0.5 * hh * acc;
+}
+
 __global__ void gather_sorted_kernel(int n, const int *__restrict__ sorted, const double *__restrict__ v,
                                      double *__restrict__ vs)
 {
@@ -308,9 +340,8 @@ void launch_spmv_J(Engine &e, double h, const double *dvec, const double *v, dou
         const unsigned nb = (unsigned)((e.n + wpb - 1) / wpb);
         if (e.col_s16_valid) { // 16-bit positions: 2 bytes less per entry
             if (e.valf)
-                spmv_js_kernel<float, unsigned short><<<nb, 32 * wpb, 0, st>>>(e.n, h, e.d_hrow, e.d_rowptr,
-                                                                                e.d_col_s16, e.d_valf, dvec, v,
-                                                                                e.d_vsort, y);
+                spmv_js4_kernel<<<nb, 32 * wpb, 0, st>>>(e.n, h, e.d_hrow, e.d_rowptr, e.d_col_s16, e.d_valf, dvec, v,
+                                                         e.d_vsort, y);
             else
                 spmv_js_kernel<double, unsigned short><<<nb, 32 * wpb, 0, st>>>(e.n, h, e.d_hrow, e.d_rowptr,
                                                                                  e.d_col_s16, e.d_val, dvec, v,
@@ -414,35 +445,37 @@ __global__ void __launch_bounds__(256) gs_fused_kernel(int n, int kk, const doub
 
 // One whole Gram-Schmidt step of GMRES in a single cooperative launch (one
 // CTA per SM, grid-wide barriers between the passes): c1 = V^T w, w -= V c1,
-// c2 = V^T w, w -= V c2, nrm2 = |w|^2, V_{k+1} = w / sqrt(nrm2).  Each CTA owns
-// a contiguous range of the vectors; the per-CTA partial sums are reduced by
-// every CTA in the same fixed order (identical results, no further barrier).
-// rec receives c1 at [0, m1), c2 at [m1, 2 m1) and nrm2 at [2 m1], the layout
-// of the three separate passes.
+// c2 = V^T w with |w|^2, w -= V c2, nrm2 = |w|^2 before - |c2|^2,
+// V_{k+1} = w / sqrt(nrm2).  Each CTA owns a contiguous range of the
+// vectors; the per-CTA partial sums are reduced by every CTA in the same
+// fixed order (identical results, no further barrier).  rec receives c1 at
+// [0, m1), c2 at [m1, 2 m1) and nrm2 at [2 m1], the layout of the three
+// separate passes.
+//
+// Per-CTA partials of V^T w (entries 0 .. kk-1) and, with with_norm, of
+// |w|^2 as entry kk (kk <= 31).
 __device__ __forceinline__ void gs_block_dots(int kk, const double *__restrict__ V, size_t ldv, const double *w,
                                               int s0, int e0, double (*red)[33], double *__restrict__ part,
-                                              bool norm_only)
+                                              bool with_norm)
 {
     constexpr int KM = 32;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     double acc[KM];
+    double accn = 0.0;
 #pragma unroll
     for (int k = 0; k < KM; ++k) acc[k] = 0.0;
     for (int i = s0 + tid; i < e0; i += blockDim.x) {
         const double wi = w[i];
-        if (norm_only) {
-            acc[0] += wi * wi;
-        } else {
+        if (with_norm) accn += wi * wi;
 #pragma unroll
-            for (int k = 0; k < KM; ++k)
-                if (k < kk) acc[k] += V[(size_t)k * ldv + i] * wi;
-        }
+        for (int k = 0; k < KM; ++k)
+            if (k < kk) acc[k] += V[(size_t)k * ldv + i] * wi;
     }
-    const int nout = norm_only ? 1 : kk;
+    const int nout = with_norm ? kk + 1 : kk;
 #pragma unroll
     for (int k = 0; k < KM; ++k) {
         if (k < nout) {
-            const double v = warp_sum(acc[k]);
+            const double v = warp_sum(with_norm && k == kk ? accn : acc[k]);
             if (lane == 0) red[wid][k] = v;
         }
     }
@@ -485,26 +518,31 @@ __global__ void __launch_bounds__(256) gs_iter_kernel(int n, int kk, const doubl
     const int tid = threadIdx.x, nb = gridDim.x;
     const int chunk = (n + nb - 1) / nb;
     const int s0 = blockIdx.x * chunk, e0 = min(n, s0 + chunk);
+    // the second pass also sums |w1|^2; with V orthonormal the final norm is
+    // |w1 - V c2|^2 = |w1|^2 - |c2|^2, and c2 (the re-orthogonalisation) is
+    // tiny against w1, so the difference loses nothing: two grid barriers
+    double nrm2 = 0.0;
     for (int pass = 0; pass < 2; ++pass) {
         double *part = partials + ((size_t)pass * nb) * KM;
-        gs_block_dots(kk, V, ldv, w, s0, e0, red, part + (size_t)blockIdx.x * KM, false);
+        gs_block_dots(kk, V, ldv, w, s0, e0, red, part + (size_t)blockIdx.x * KM, pass == 1);
         grid.sync();
-        gs_sum_partials(part, nb, kk, cs);
+        gs_sum_partials(part, nb, pass == 1 ? kk + 1 : kk, cs);
         if (blockIdx.x == 0 && tid < kk) rec[pass * m1 + tid] = cs[tid];
+        if (pass == 1) {
+            double c2 = 0.0;
+            for (int k = 0; k < kk; ++k) c2 += cs[k] * cs[k];
+            nrm2 = fmax(cs[kk] - c2, 0.0);
+        }
         for (int i = s0 + tid; i < e0; i += blockDim.x) {
             double u = 0.0;
             for (int k = 0; k < kk; ++k) u += V[(size_t)k * ldv + i] * cs[k];
-            w[i] -= u;
+            const double wn = w[i] - u;
+            w[i] = wn;
+            if (pass == 1) vnext[i] = nrm2 > 0.0 ? wn * rsqrt(nrm2) : 0.0;
         }
         __syncthreads();
     }
-    double *part = partials + ((size_t)2 * nb) * KM;
-    gs_block_dots(kk, V, ldv, w, s0, e0, red, part + (size_t)blockIdx.x * KM, true);
-    grid.sync();
-    gs_sum_partials(part, nb, 1, cs);
-    const double nrm2 = cs[0];
     if (blockIdx.x == 0 && tid == 0) rec[2 * m1] = nrm2;
-    for (int i = s0 + tid; i < e0; i += blockDim.x) vnext[i] = nrm2 > 0.0 ? w[i] * rsqrt(nrm2) : 0.0;
 }
 
 // The cooperative Gram-Schmidt step runs when the device supports cooperative
