@@ -97,7 +97,9 @@ typedef struct {
     double solver_tol;        /* relative residual target of the iterative solve */
     int gmres_restart;        /* Krylov subspace size per cycle */
     int max_iters;            /* iteration cap per solve */
-    double precond_theta;     /* coupling strength that joins two dislocations in a cluster */
+    double precond_theta;     /* coupling strength that joins two dislocations in a cluster
+                                 (0: 0.01 for SDDDST_SOLVER_GMRES_CLUSTER, 0.05 under the learned
+                                 and analytic corrections) */
     int device;               /* CUDA device ordinal */
     double neumann_theta;     /* SDDDST_SOLVER_GMRES_NEUMANN: cross-block couplings of normalised strength
                                  |A_ij| / sqrt(|J_ii J_jj|) below this are left out of the correction */
@@ -106,7 +108,7 @@ typedef struct {
 /* Defaults of SimulationData() (simulation_data.cpp:43-109, constants.h):
  * cutoff multiplier 1, prec 1e-8, step 1, A = 1.6e-3, KASQR = 1.65^2*1e6/256,
  * ic = 2, zero stress, FP64 pair sum, cluster-preconditioned GMRES (coupling
- * threshold 0.05, at most 300 iterations, then retried with a rebuilt
+ * threshold 0.01, at most 300 iterations, then retried with a rebuilt
  * preconditioner) to 1e-13. */
 void sdddst_default_params(sdddst_params *prm);
 

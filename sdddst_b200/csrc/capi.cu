@@ -82,7 +82,7 @@ void sdddst_default_params(sdddst_params *p)
     p->pairsum = SDDDST_PAIRSUM_FP64;
     p->solver = SDDDST_SOLVER_GMRES_CLUSTER;
     p->solver_tol = 1e-13;
-    p->precond_theta = 0.05;
+    p->precond_theta = 0.0; // the solver's own default (cluster_theta)
     p->gmres_restart = 30;
     p->max_iters = 300;
     p->device = 0;

@@ -279,7 +279,7 @@ int Engine::solve(double h, const double *rhs, double *x_out)
     if (rc != SDDDST_ERR_SOLVER || precond != 2) return rc;
     const double theta0 = prm.precond_theta;
     for (int attempt = 0; attempt < 2 && rc == SDDDST_ERR_SOLVER; ++attempt) {
-        prm.precond_theta = (prm.precond_theta > 0 ? prm.precond_theta : 0.05) / 5.0;
+        prm.precond_theta = cluster_theta(*this) / 5.0;
         stalls++;
         if (int rc2 = precond_build(*this, h, d_dvec)) {
             prm.precond_theta = theta0;

@@ -150,6 +150,12 @@ void launch_speeds_raw(int n, const double *x, const double *y, const double *b,
 int jacobian_assemble(Engine &e, const double *x);
 int tabulated_build(Engine &e);
 int alloc_csr_values(Engine &e, long cap);
+// Coupling threshold of the cluster preconditioner: the caller's setting, else
+// 0.01 for the cluster-preconditioned GMRES (fewest step-time on the N=32768
+// workload: 0.01, 0.02, 0.05, 0.1, 0.2 give 11.20, 11.27, 11.59, 11.92,
+// 12.30 ms per attempt) and 0.05 under the learned and analytic corrections
+// (the network was trained on blocks built at 0.05).
+double cluster_theta(const Engine &e);
 void launch_make_dvec(const Engine &e, double h, double *dvec, cudaStream_t st);
 void launch_export_jacobian(const Engine &e, double h, const double *dvec, double *val_out, cudaStream_t st);
 

@@ -291,13 +291,21 @@ __global__ void block_apply_kernel(int n, const int *__restrict__ blk_of, const 
 // scan helper from jacobian.cu
 __global__ void scan_kernel(const int *__restrict__ in, int m, int *__restrict__ out);
 
+double cluster_theta(const Engine &e)
+{
+    if (e.prm.precond_theta > 0) return e.prm.precond_theta;
+    const bool corrected =
+        e.prm.solver == SDDDST_SOLVER_GMRES_LEARNED || e.prm.solver == SDDDST_SOLVER_GMRES_NEUMANN;
+    return corrected ? 0.05 : 0.01;
+}
+
 // Builds the cluster block-Jacobi inverse of J(h) for the assembled G.
 int precond_build(Engine &e, double h, const double *dvec)
 {
     const int n = e.n;
     cudaStream_t st = e.st;
     const unsigned nb256 = (unsigned)((n + 255) / 256);
-    const double theta = e.prm.precond_theta > 0 ? e.prm.precond_theta : 0.05;
+    const double theta = cluster_theta(e);
     int *ptr = e.pc_ptr, *par = e.pc_parent, *par2 = e.pc_tmp;
     // single system: M_jj in the cell-sorted order (the SpMV's staging buffer,
     // free until the solve), read through the CSR's sorted column positions
