@@ -45,6 +45,10 @@ def test_default_params_follow_reference_defaults(engine_lib):
     q = engine_lib.cli_params(4096, 1.0, 1e-7, p=256, pd_scaling=True)
     assert q.A == 1e-4 * 16.0 * (1.0 / np.sqrt(4096.0))
     assert q.KASQR == 1.65 * 1.65 * 1e6 / 256.0 * 4096.0
+    # solver defaults of this library (no reference counterpart): cluster-
+    # preconditioned GMRES(30), its coupling threshold left to the solver
+    assert p.solver == engine_lib.SOLVER_GMRES_CLUSTER and p.gmres_restart == 30
+    assert p.precond_theta == 0.0
 
 
 def test_workload_generator_is_frozen():
