@@ -210,4 +210,78 @@ __device__ __forceinline__ float tau_xy_dx_f32(float dx, float dy)
     return (acc + far) * kTwoPiSqF;
 }
 
+// tau_xy_dx_f32 for two pairs at once in packed FP32 (same terms and the same
+// order of operations as the scalar form; the SFU calls stay scalar).
+__device__ __forceinline__ float2 tau_xy_dx_f32x2(float2 dx, float2 dy)
+{
+    const float twopi = 6.28318530717959f;
+    const float2 y2 = mul2(dy, dy);
+    float2 p = fma2(f2c(0.00046630280576761f), y2, f2c(-0.00737043094571435f));
+    p = fma2(p, y2, f2c(0.08214588661112823f));
+    p = fma2(p, y2, f2c(-0.59926452932079207f));
+    p = fma2(p, y2, f2c(2.55016403987734549f));
+    p = fma2(p, y2, f2c(-5.16771278004997003f));
+    p = fma2(p, y2, f2c(3.14159265358979324f));
+    const float2 sn = mul2(dy, p);
+    const float2 sn2 = mul2(sn, sn);
+    const float2 cy = fma2(f2c(-2.0f), sn2, f2c(1.0f));
+    const float2 a = mul2(f2c(kPiF), dx);
+    float2 ep, epi;
+    ep.x = __expf(a.x);
+    ep.y = __expf(a.y);
+    epi.x = __expf(-a.x);
+    epi.y = __expf(-a.y);
+    const float2 a2 = mul2(a, a);
+    const float2 poly =
+        mul2(a, fma2(a2, fma2(a2, fma2(a2, f2c(1.0f / 5040.0f), f2c(1.0f / 120.0f)), f2c(1.0f / 6.0f)), f2c(1.0f)));
+    const float2 shx = mul2(f2c(0.5f), fma2(epi, f2c(-1.0f), ep));
+    float2 sh;
+    sh.x = fabsf(a.x) < 0.5f ? poly.x : shx.x;
+    sh.y = fabsf(a.y) < 0.5f ? poly.y : shx.y;
+    const float2 ch = mul2(f2c(0.5f), add2(ep, epi));
+    const float2 sh2 = mul2(sh, sh);
+    const float2 E = mul2(ep, ep), Ei = mul2(epi, epi);
+    // k = 0
+    const float2 D0 = mul2(f2c(2.0f), add2(sh2, sn2));
+    const float2 N0 = fma2(mul2(f2c(-4.0f), sh2), sn2, mul2(f2c(2.0f), fma2(sn2, f2c(-1.0f), sh2)));
+    const float2 S0 = mul2(mul2(f2c(2.0f), sh), ch);
+    float2 r0;
+    r0.x = rcp_fast(D0.x);
+    r0.y = rcp_fast(D0.y);
+    float2 acc = mul2(mul2(r0, r0), fma2(mul2(mul2(f2c(twopi), dx), S0), fma2(mul2(f2c(-2.0f), N0), r0, cy), N0));
+    // |k| = 1
+    {
+        const float2 ap = mul2(E, f2c(kQP1)), bp = mul2(Ei, f2c(kQN1));
+        const float2 Cp = mul2(f2c(0.5f), add2(ap, bp)), Sp = mul2(f2c(0.5f), fma2(bp, f2c(-1.0f), ap));
+        const float2 Dp = fma2(cy, f2c(-1.0f), Cp), Np = fma2(Cp, cy, f2c(-1.0f));
+        float2 rp;
+        rp.x = rcp_fast(Dp.x);
+        rp.y = rcp_fast(Dp.y);
+        acc = fma2(mul2(rp, rp),
+                   fma2(mul2(mul2(f2c(twopi), add2(dx, f2c(1.0f))), Sp), fma2(mul2(f2c(-2.0f), Np), rp, cy), Np),
+                   acc);
+        const float2 am = mul2(E, f2c(kQN1)), bm = mul2(Ei, f2c(kQP1));
+        const float2 Cm = mul2(f2c(0.5f), add2(am, bm)), Sm = mul2(f2c(0.5f), fma2(bm, f2c(-1.0f), am));
+        const float2 Dm = fma2(cy, f2c(-1.0f), Cm), Nm = fma2(Cm, cy, f2c(-1.0f));
+        float2 rm;
+        rm.x = rcp_fast(Dm.x);
+        rm.y = rcp_fast(Dm.y);
+        acc = fma2(mul2(rm, rm),
+                   fma2(mul2(mul2(f2c(twopi), add2(dx, f2c(-1.0f))), Sm), fma2(mul2(f2c(-2.0f), Nm), rm, cy), Nm),
+                   acc);
+    }
+    // |k| = 2..4, first order, + side (E^-1) and - side (E)
+    const float2 sp = fma2(fma2(f2c(-twopi), dx, f2c(1.0f)), f2c(kA1), f2c(-twopi * kB1));
+    const float2 sm = fma2(fma2(f2c(twopi), dx, f2c(1.0f)), f2c(kA1), f2c(-twopi * kB1));
+    float2 far = mul2(mul2(f2c(2.0f), cy), fma2(Ei, sp, mul2(E, sm)));
+    // second order, k = 2
+    {
+        const float2 c2 = fma2(mul2(f2c(2.0f), cy), cy, f2c(-1.0f)), c4 = fma2(mul2(f2c(-4.0f), cy), cy, f2c(2.0f));
+        const float2 tp = mul2(mul2(f2c(2.0f), Ei), f2c(kQN2)), tm = mul2(mul2(f2c(2.0f), E), f2c(kQN2));
+        far = fma2(mul2(tp, tp), fma2(mul2(f2c(twopi), add2(dx, f2c(2.0f))), c4, c2), far);
+        far = fma2(mul2(tm, tm), fma2(mul2(f2c(twopi), fma2(dx, f2c(-1.0f), f2c(2.0f))), c4, c2), far);
+    }
+    return mul2(add2(acc, far), f2c(kTwoPiSqF));
+}
+
 } // namespace sd

@@ -265,31 +265,71 @@ __device__ void row_values(int i, double xi, double yi, double bi, const CellSca
                            const double *bs, int lane)
 {
     double rs = 0.0;
-    for (int q = base + 1 + lane; q < end; q += 32) {
-        const int j = col[q], ks = col_s[q];
-        const double xj = cs.xs[ks], yj = cs.ys[ks];
-        const double ddx = i < j ? xj - xi : xi - xj, ddy = i < j ? yj - yi : yi - yj; // x[hi] - x[lo]
-        // FP64 values keep the reference's wrap; FP32 values take the branch-free one
-        const double dx = sizeof(VT) == sizeof(double) ? wrap_half(ddx) : wrap_diff_f64(ddx);
-        const double dy = sizeof(VT) == sizeof(double) ? wrap_half(ddy) : wrap_diff_f64(ddy);
-        double w, tdx;
-        if (sizeof(VT) == sizeof(double)) {
-            pair_kept(r2_exact(dx, dy), c, c2, ic2, &w);
-        } else { // the value is stored in FP32: its weight needs no FP64 square root and exponential
-            const double r2 = r2_exact(dx, dy);
-            float wf = 1.0f;
-            if (r2 > c2) {
-                const float t = sqrtf((float)r2) - (float)c;
-                wf = __expf(-(t * t) * (float)ic2);
+    if (sizeof(VT) == sizeof(float) && !tab_dx) {
+        // FP32 values: two entries per lane (q and q + 32) through the packed field
+        for (int qa = base + 1 + lane; qa < end; qa += 64) {
+            const int qb = qa + 32;
+            const bool hb = qb < end;
+            double dxs[2], dys[2], ws[2], bss[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int q = u ? qb : qa;
+                if (u && !hb) { // a stand-in pair, never stored
+                    dxs[u] = dys[u] = 0.25;
+                    ws[u] = bss[u] = 0.0;
+                    continue;
+                }
+                const int j = col[q], ks = col_s[q];
+                const double xj = cs.xs[ks], yj = cs.ys[ks];
+                dxs[u] = wrap_diff_f64(i < j ? xj - xi : xi - xj); // x[hi] - x[lo]
+                dys[u] = wrap_diff_f64(i < j ? yj - yi : yi - yj);
+                const double r2 = r2_exact(dxs[u], dys[u]);
+                float wf = 1.0f;
+                if (r2 > c2) {
+                    const float t = sqrtf((float)r2) - (float)c;
+                    wf = __expf(-(t * t) * (float)ic2);
+                }
+                ws[u] = (double)wf;
+                bss[u] = bs[ks];
             }
-            w = (double)wf;
+            const float2 t = tau_xy_dx_f32x2(make_float2(__double2float_rn(dxs[0]), __double2float_rn(dxs[1])),
+                                             make_float2(__double2float_rn(dys[0]), __double2float_rn(dys[1])));
+            const VT va = (VT)(bi * bss[0] * (double)t.x * ws[0]);
+            val[qa] = va;
+            rs += (double)va;
+            if (hb) {
+                const VT vb = (VT)(bi * bss[1] * (double)t.y * ws[1]);
+                val[qb] = vb;
+                rs += (double)vb;
+            }
         }
-        if (tab_dx) tdx = tau0_xy_dx(dx, dy) + tab_interp(tab_dx, dx, dy); // tabulated field
-        else if (sizeof(VT) == sizeof(double)) tdx = tau_xy_dx_f64(dx, dy);
-        else tdx = (double)tau_xy_dx_f32(__double2float_rn(dx), __double2float_rn(dy));
-        const VT v = (VT)(bi * bs[ks] * tdx * w);
-        val[q] = v;
-        rs += (double)v;
+    } else {
+        for (int q = base + 1 + lane; q < end; q += 32) {
+            const int j = col[q], ks = col_s[q];
+            const double xj = cs.xs[ks], yj = cs.ys[ks];
+            const double ddx = i < j ? xj - xi : xi - xj, ddy = i < j ? yj - yi : yi - yj; // x[hi] - x[lo]
+            // FP64 values keep the reference's wrap; FP32 values take the branch-free one
+            const double dx = sizeof(VT) == sizeof(double) ? wrap_half(ddx) : wrap_diff_f64(ddx);
+            const double dy = sizeof(VT) == sizeof(double) ? wrap_half(ddy) : wrap_diff_f64(ddy);
+            double w, tdx;
+            if (sizeof(VT) == sizeof(double)) {
+                pair_kept(r2_exact(dx, dy), c, c2, ic2, &w);
+            } else { // the value is stored in FP32: its weight needs no FP64 square root and exponential
+                const double r2 = r2_exact(dx, dy);
+                float wf = 1.0f;
+                if (r2 > c2) {
+                    const float t = sqrtf((float)r2) - (float)c;
+                    wf = __expf(-(t * t) * (float)ic2);
+                }
+                w = (double)wf;
+            }
+            if (tab_dx) tdx = tau0_xy_dx(dx, dy) + tab_interp(tab_dx, dx, dy); // tabulated field
+            else if (sizeof(VT) == sizeof(double)) tdx = tau_xy_dx_f64(dx, dy);
+            else tdx = (double)tau_xy_dx_f32(__double2float_rn(dx), __double2float_rn(dy));
+            const VT v = (VT)(bi * bs[ks] * tdx * w);
+            val[q] = v;
+            rs += (double)v;
+        }
     }
     double pd = 0.0;
     for (int q = lane; q < p; q += 32) {
