@@ -391,7 +391,7 @@ static int batch_assemble(Batch &bt, const double *x)
     cell_sort_kernel<<<bt.ncell_tot, 256, 0, st>>>(bt.b_start, e.d_rowcnt, bt.b_sorted);
     batch_row_count_kernel<<<nblocks(n * 32, 256), 256, 0, st>>>(n, bt.d_inst, x, e.d_y, bt.d_G, bt.d_celloff,
                                                                  bt.d_cut, bt.b_start, bt.b_sorted, e.d_rowcnt);
-    scan_kernel<<<1, 1024, 0, st>>>(e.d_rowcnt, (int)n, e.d_rowptr);
+    e.launches += launch_scan(e, e.d_rowcnt, (int)n, e.d_rowptr, st) - 1;
     e.launches += 6;
     int total = 0;
     cudaMemcpyAsync(&total, e.d_rowptr + n, sizeof(int), cudaMemcpyDeviceToHost, st);

@@ -56,6 +56,8 @@ struct Engine {
     bool col_s_valid = false;  // d_col_s matches the assembled CSR
     unsigned short *d_col_s16 = nullptr; // d_col_s in 16 bits (systems of at most 65536), the SpMV's copy
     bool col_s16_valid = false;
+    int *d_scan_tmp = nullptr; // chunk totals and offsets of launch_scan
+    int scan_tmp_cap = 0;
     const int *spmv_sorted = nullptr; // the sorted list d_col_s refers to
     double *d_hrow = nullptr;  // per-row step size of a batch of systems (null: one system, scalar h)
     long nnz_cap = 0, nnz = 0;
@@ -150,6 +152,9 @@ void launch_speeds_raw(int n, const double *x, const double *y, const double *b,
 int jacobian_assemble(Engine &e, const double *x);
 int tabulated_build(Engine &e);
 int alloc_csr_values(Engine &e, long cap);
+// Exclusive scan of m ints (out[0] = 0, out[k+1] = sum_{<=k}); returns the
+// number of kernels launched.
+int launch_scan(Engine &e, const int *in, int m, int *out, cudaStream_t st);
 // Coupling threshold of the cluster preconditioner: the caller's setting, else
 // 0.01 for the cluster-preconditioned GMRES (fewest step-time on the N=32768
 // workload: 0.01, 0.02, 0.05, 0.1, 0.2 give 11.20, 11.27, 11.59, 11.92,

@@ -95,6 +95,79 @@ __global__ void scan_kernel(const int *__restrict__ in, int m, int *__restrict__
     if (tid == 0) out[0] = 0;
 }
 
+// Chunk pass of the multi-block scan: block b scans elements [2048 b,
+// 2048 b + 2048) (8 warps x 8 rounds of 32, coalesced), writes the chunk's
+// inclusive prefixes to out[k + 1] and its total to tot[b].
+__global__ void __launch_bounds__(256) scan_chunks_kernel(const int *__restrict__ in, int m, int *__restrict__ out,
+                                                          int *__restrict__ tot)
+{
+    constexpr int R = 8;
+    __shared__ int warp_tot[8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int w0 = blockIdx.x * 2048 + wid * 32 * R;
+    int v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int k = w0 + r * 32 + lane;
+        v[r] = k < m ? in[k] : 0;
+    }
+    int pre[R];
+    int run = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        int s = v[r];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += t;
+        }
+        pre[r] = run + s;
+        run += __shfl_sync(0xffffffffu, s, 31);
+    }
+    if (lane == 0) warp_tot[wid] = run;
+    __syncthreads();
+    int off = 0;
+    for (int q = 0; q < wid; ++q) off += warp_tot[q];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int k = w0 + r * 32 + lane;
+        if (k < m) out[k + 1] = off + pre[r];
+    }
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int q = 0; q < 8; ++q) t += warp_tot[q];
+        tot[blockIdx.x] = t;
+    }
+}
+
+// Add pass: out[k + 1] += offs[b] over chunk b; out[0] = 0.
+__global__ void scan_add_kernel(int m, int *__restrict__ out, const int *__restrict__ offs)
+{
+    const int b = blockIdx.x;
+    const int add = offs[b];
+    for (int k = b * 2048 + threadIdx.x; k < min(m, (b + 1) * 2048); k += blockDim.x) out[k + 1] += add;
+    if (b == 0 && threadIdx.x == 0) out[0] = 0;
+}
+
+// Exclusive scan of m ints: one block up to 16384 entries; above, chunks of
+// 2048 scanned by one block each, their totals scanned by one block, and the
+// offsets added (the engine's scan scratch holds totals and offsets).  One
+// block alone is bound by its load and store round trips (about 22 us for
+// 32768 entries).
+int launch_scan(Engine &e, const int *in, int m, int *out, cudaStream_t st)
+{
+    const int nb = (m + 2047) / 2048;
+    if (m <= 16384 || !e.d_scan_tmp || 2 * nb + 2 > e.scan_tmp_cap) {
+        scan_kernel<<<1, 1024, 0, st>>>(in, m, out);
+        return 1;
+    }
+    int *tot = e.d_scan_tmp, *offs = e.d_scan_tmp + nb + 1;
+    scan_chunks_kernel<<<nb, 256, 0, st>>>(in, m, out, tot);
+    scan_kernel<<<1, 1024, 0, st>>>(tot, nb, offs);
+    scan_add_kernel<<<nb, 256, 0, st>>>(m, out, offs);
+    return 3;
+}
+
 __global__ void cell_scatter_kernel(int n, const int *__restrict__ cell, const int *__restrict__ start,
                                     int *__restrict__ fill, int *__restrict__ out)
 {
@@ -607,7 +680,7 @@ int jacobian_assemble(Engine &e, const double *x)
     cell_rows_kernel<false, float><<<nb, kCellThreads, kCellSmem, st>>>(
         parts, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr, e.d_rowcnt, nullptr, nullptr,
         nullptr, nullptr, 0, nullptr, nullptr, 0.0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr);
-    scan_kernel<<<1, 1024, 0, st>>>(e.d_rowcnt, n, e.d_rowptr);
+    e.launches += launch_scan(e, e.d_rowcnt, n, e.d_rowptr, st) - 1;
     e.launches += 8;
     int total = 0;
     if (cudaMemcpyAsync(&total, e.d_rowptr + n, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)

@@ -330,10 +330,10 @@ int precond_build(Engine &e, double h, const double *dvec)
     cudaMemsetAsync(e.pc_count, 0, sizeof(int) * (n + 1), st);
     cudaMemsetAsync(e.pc_fill, 0, sizeof(int) * (n + 1), st);
     root_fix_kernel<<<nb256, 256, 0, st>>>(n, par, e.pc_count);
-    scan_kernel<<<1, 1024, 0, st>>>(e.pc_count, n, e.pc_start);
+    e.launches += launch_scan(e, e.pc_count, n, e.pc_start, st) - 1;
     member_scatter_kernel<<<nb256, 256, 0, st>>>(n, par, e.pc_start, e.pc_fill, e.pc_tmp2);
     cluster_sort_kernel<<<nb256, 256, 0, st>>>(n, e.pc_count, e.pc_start, e.pc_tmp2, e.pc_members, e.pc_nblk);
-    scan_kernel<<<1, 1024, 0, st>>>(e.pc_nblk, n, e.pc_bbase);
+    e.launches += launch_scan(e, e.pc_nblk, n, e.pc_bbase, st) - 1;
     e.launches += 19;
     // the block count stays on the device (pc_bbase[n]); the block kernels
     // run over n (an upper bound) and return beyond it, and the inverses'
@@ -354,7 +354,7 @@ int precond_build(Engine &e, double h, const double *dvec)
     cudaMemsetAsync(e.pc_sq, 0, sizeof(int) * (n + 1), st);
     block_meta_kernel<<<nb256, 256, 0, st>>>(nbp, e.pc_bstart, e.pc_blen, e.pc_members, e.pc_blk_of, e.pc_loc,
                                              e.pc_sq);
-    scan_kernel<<<1, 1024, 0, st>>>(e.pc_sq, n, e.pc_off);
+    e.launches += launch_scan(e, e.pc_sq, n, e.pc_off, st) - 1;
     cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
     const unsigned ib = (unsigned)((n + 1) / 2);
     if (e.valf)
