@@ -30,8 +30,13 @@ replica (the path does not shard: replicas only); value = total accepted
 steps of all ranks / max over ranks of the device time.
 
 ``--impl reference`` times the reference's own CPU code (oracle/_ref, the
-hot path compiled in place) on a bounded sample of the same workload, see
-``reference_arm``.
+hot path compiled in place) for one step attempt of the full workload (five
+velocity evaluations and three Jacobian assemblies at N = 32768, one core,
+UMFPACK solve excluded), see ``reference_arm``; the repo arm's
+``cpu_baseline`` times one of each of those calls at full N in a separate
+process and composes the same attempt.  The timed window starts after
+``--settle`` accepted steps (default 10) and the warm-up; its step-size
+range is reported.
 """
 from __future__ import annotations
 
@@ -54,7 +59,10 @@ UNIT = "steps/s"
 N_FULL = 32768
 SEED = 4
 CUTOFF_M = 2.0
-PAIR_F32_DRAM_BYTES_N32768 = 812544 + 8764672  # measured, see the roofline note in main()
+# DRAM bytes (read + write) of one FP32 pair-sum launch at N = 32768, recorded
+# from one ncu capture (profiles/pair_tiles_f32_n32768.md); not measured by
+# this script, which has no access to the DRAM counters.
+PAIR_F32_DRAM_BYTES_N32768_RECORDED = 812544 + 8764672
 PREC = 1e-5
 H0 = 1e-6
 # Pair-sum FLOP convention: tau_xy = 130 FP operations per unique pair.
@@ -161,6 +169,7 @@ def time_steps(torch, eng, steps, warmup, flush, per_kernel=True):
     accepted = 0
     l0 = eng.launches()
     s0 = eng.solver_stats()
+    hs = [eng.scalars()["step_size"]]
     for _ in range(steps):
         flush.zero_()  # L2 flush between timed steps (outside the events)
         torch.cuda.synchronize()
@@ -171,7 +180,9 @@ def time_steps(torch, eng, steps, warmup, flush, per_kernel=True):
         b.record(stream)
         b.synchronize()
         total_ms += a.elapsed_time(b)
+        hs.append(eng.scalars()["step_size"])
     torch.cuda.synchronize()
+    time_steps.last_h = (min(hs), max(hs))
     s1 = eng.solver_stats()
     time_steps.last_solver = {"solves": s1[0] - s0[0], "iterations": s1[1] - s0[1]}
     return total_ms, accepted, eng.launches() - l0
@@ -253,67 +264,125 @@ def measure_precision(torch, steps, flush, device):
     return out
 
 
-def cpu_baseline_sample(n_full, sample_n=4096, reps=1):
-    """The reference hot path (compiled in place) on a bounded sample: the
-    first `sample_n` dislocations of the workload with the same cutoff radius
-    (multiplier scaled by sqrt(sample_n / N)); calculateSpeeds and
-    calculateJacobian are timed and scaled by the unique-pair ratio
-    N(N-1) / (n(n-1)) (both are O(N^2) scans; at fixed radius the Jacobian's
-    entries also grow as N^2).  One step attempt of the reference costs 5
-    velocity evaluations and 3 assemblies (zero stress,
-    simulation.cpp:62-84,435-650); the UMFPACK solve is not counted (it only
-    makes the reference slower)."""
-    sys.path.insert(0, ROOT)
+def _ref_sim(n_full):
+    """The reference hot path compiled in place (oracle/_ref) on the full
+    workload, or the oracle port where the reference could not be built."""
     from oracle import ref
     from sdddst_b200 import workloads
-    if not ref.available("ref"):
-        kind = "port"
-        if not ref.available("port"):
-            subprocess.run(["make", "-s", "port"], cwd=os.path.join(ROOT, "oracle"), check=True)
-    else:
-        kind = "reference"
+    kind = "reference" if ref.available("ref") else "port"
+    if kind == "port" and not ref.available("port"):
+        subprocess.run(["make", "-s", "port"], cwd=os.path.join(ROOT, "oracle"), check=True)
     xyb, _ = workloads.dislocations(n_full, SEED)
-    xs = np.ascontiguousarray(xyb[:sample_n])
-    m_s = CUTOFF_M * np.sqrt(sample_n / n_full)
-    sim = ref.Sim(xs, None, ref.params(cutoff_multiplier=m_s, prec=PREC, step_size=H0),
+    sim = ref.Sim(xyb, None, ref.params(cutoff_multiplier=CUTOFF_M, prec=PREC, step_size=H0),
                   "ref" if kind == "reference" else "port")
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        sim.speeds(xs)
-    t_sp = (time.perf_counter() - t0) / reps
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        sim.jacobian(H0, xs)
-    t_jac = (time.perf_counter() - t0) / reps
-    scale = (n_full * (n_full - 1.0)) / (sample_n * (sample_n - 1.0))
-    t_step = (5 * t_sp + 3 * t_jac) * scale
-    return {"value": 1.0 / t_step, "unit": UNIT, "cores": 1, "kind": kind,
-            "sample": (f"first {sample_n} dislocations of the workload, cutoff radius kept; calculateSpeeds "
-                       f"{t_sp:.3f} s + calculateJacobian {t_jac:.3f} s, scaled by N(N-1)/(n(n-1)) = {scale:.1f} "
-                       f"to 5 evaluations + 3 assemblies per attempt; solve not counted"),
+    return sim, xyb, kind
+
+
+def _jacobian_cap(n_full):
+    """Entry capacity of the reference Jacobian export at the workload's
+    cutoff (one call, no retry): N (1 + 1.3 pi r^2 N) with r the pattern
+    radius (1 + sqrt(36.8)) c."""
+    c = CUTOFF_M / np.sqrt(n_full)
+    r = c * (1.0 + np.sqrt(36.8))
+    return int(n_full * (1.0 + 1.3 * min(1.0, np.pi * r * r) * n_full)) + n_full + 1024
+
+
+def cpu_full_calls(n_full, speeds=1, jacobians=1):
+    """Times the reference's own calculateSpeeds (simulation.cpp:86-131) and
+    calculateJacobian (simulation.cpp:236-384) on the FULL workload
+    configuration, one core (the reference is single-threaded); returns the
+    per-call seconds of each kind."""
+    sim, xyb, kind = _ref_sim(n_full)
+    t_sp, t_jac = [], []
+    for _ in range(speeds):
+        t0 = time.perf_counter()
+        sim.speeds(xyb)
+        t_sp.append(time.perf_counter() - t0)
+    cap = _jacobian_cap(n_full)
+    for _ in range(jacobians):
+        t0 = time.perf_counter()
+        sim.jacobian(H0, xyb, cap=cap)
+        t_jac.append(time.perf_counter() - t0)
+    return {"kind": kind, "t_speeds": t_sp, "t_jacobian": t_jac}
+
+
+def cpu_baseline_worker(args):
+    """Subprocess body of the repo arm's CPU baseline: one full-N call of
+    the kind --cpu-baseline-worker names, on one core."""
+    which = args.cpu_baseline_worker
+    print(json.dumps(cpu_full_calls(args.n, int(which == "speeds"), int(which == "jacobian"))), flush=True)
+
+
+def start_cpu_baseline(n):
+    """Starts the CPU baseline: one full-N calculateSpeeds and one full-N
+    calculateJacobian, each in its own process on its own host core, beside
+    the GPU measurements (about 75 s each at N = 32768)."""
+    return [subprocess.Popen([sys.executable, os.path.abspath(__file__), "--cpu-baseline-worker", which,
+                              "--n", str(n)], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+            for which in ("speeds", "jacobian")]
+
+
+def finish_cpu_baseline(procs, timeout=900):
+    res = []
+    for proc in procs:
+        out, err = proc.communicate(timeout=timeout)
+        if proc.returncode != 0:
+            raise RuntimeError(err.strip().splitlines()[-1] if err.strip() else f"rc {proc.returncode}")
+        res.append(json.loads(out.strip().splitlines()[-1]))
+    r = {"kind": res[0]["kind"], "t_speeds": res[0]["t_speeds"], "t_jacobian": res[1]["t_jacobian"]}
+    t_sp, t_jac = r["t_speeds"][0], r["t_jacobian"][0]
+    t_step = 5 * t_sp + 3 * t_jac
+    return {"value": 1.0 / t_step, "unit": UNIT, "cores": 1, "kind": r["kind"],
+            "sample": (f"full N={N_FULL} workload configuration: one calculateSpeeds {t_sp:.2f} s and one "
+                       f"calculateJacobian {t_jac:.2f} s of the reference on one core, composed as an attempt's "
+                       f"5 velocity evaluations + 3 assemblies (zero stress, simulation.cpp:62-84,435-650); "
+                       f"UMFPACK solve excluded"),
             "seconds_per_step": t_step}
 
 
 def reference_arm(args):
+    """The reference's own CPU code for one step attempt at the full workload:
+    the five calculateSpeeds and three calculateJacobian calls of a
+    zero-stress attempt (simulation.cpp:62-84,435-650), executed one after
+    the other on one core (the reference is single-threaded) on the N = 32768
+    configuration and timed as one step.  The UMFPACK factorization and
+    solve are excluded (UMFPACK is not installed; the harness's stand-in LU
+    would only make the reference slower).  One such attempt takes about
+    ten minutes, so the arm times one attempt whatever --steps asks for,
+    after a warm-up of one small call."""
     ws, rank, _ = _dist()
     if rank != 0:
         return
     n = args.n
-    steps = max(1, args.steps)
-    vals = []
-    info = None
-    for k in range(args.warmup + steps):
-        info = cpu_baseline_sample(n, sample_n=min(n, 2048))
-        if k >= args.warmup:
-            vals.append(info["seconds_per_step"])
-    t = sum(vals) / len(vals)
+    sim, xyb, kind = _ref_sim(n)
+    from oracle import ref
+    small = ref.Sim(np.ascontiguousarray(xyb[:512]), None, ref.params(cutoff_multiplier=CUTOFF_M, prec=PREC,
+                                                                       step_size=H0),
+                    "ref" if kind == "reference" else "port")
+    small.speeds(np.ascontiguousarray(xyb[:512]))  # warm-up: library pages, allocator
+    calls = []
+    cap = _jacobian_cap(n)
+    t0 = time.perf_counter()
+    for what in ("speeds", "jacobian", "speeds", "speeds", "jacobian", "speeds", "jacobian", "speeds"):
+        c0 = time.perf_counter()
+        if what == "speeds":
+            sim.speeds(xyb)
+        else:
+            sim.jacobian(H0, xyb, cap=cap)
+        calls.append((what, time.perf_counter() - c0))
+    t = time.perf_counter() - t0
     v = 1.0 / t
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": steps,
-            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+    t_sp = [c for w, c in calls if w == "speeds"]
+    t_jac = [c for w, c in calls if w == "jacobian"]
+    sample = (f"one zero-stress step attempt of the reference at the full N={n} configuration on one core: "
+              f"5 calculateSpeeds ({min(t_sp):.1f}-{max(t_sp):.1f} s each) and 3 calculateJacobian "
+              f"({min(t_jac):.1f}-{max(t_jac):.1f} s each) run in sequence, {t:.1f} s; UMFPACK solve excluded")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": 1,
+            "requested_steps": args.steps, "warmup": 0, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"n{n}_m{CUTOFF_M}_seed{SEED}", "N": n, "cutoff_multiplier": CUTOFF_M,
-                       "prec": PREC, "parallelism": "replicas"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": info["kind"], "sample": info["sample"]},
+                       "prec": PREC, "parallelism": "none (single-threaded reference)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -415,7 +484,13 @@ def main():
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-realisations measurement")
     ap.add_argument("--no-variants", action="store_true", help="skip the preconditioner variants")
+    ap.add_argument("--settle", type=int, default=10,
+                    help="accepted steps run before the warm-up (the metric's window starts at step 10)")
+    ap.add_argument("--cpu-baseline-worker", default=None, choices=["speeds", "jacobian"], help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.cpu_baseline_worker:
+        cpu_baseline_worker(args)
+        return
     if args.impl == "reference":
         reference_arm(args)
         return
@@ -433,9 +508,19 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from sdddst_b200 import build
     build.build()
+    cpu_proc = None
+    if rank == 0 and not args.no_cpu and ws == 1:
+        cpu_proc = start_cpu_baseline(args.n)  # on its own host core, beside the GPU measurements
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     eng, xyb = make_engine(args.n, args.pairsum, local)
+    # the metric's window starts after the initial step-size transient:
+    # `settle` accepted steps (untimed, before the warm-up)
+    settled = 0
+    for _ in range(20 * max(1, args.settle)):
+        if settled >= args.settle:
+            break
+        settled += eng.step()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -443,6 +528,7 @@ def main():
     clocks.start()
     total_ms, accepted, launches = time_steps(torch, eng, args.steps, args.warmup, flush)
     clk = clocks.stop()
+    h_window = list(time_steps.last_h)
     solver_stats = dict(time_steps.last_solver)
     if dist:
         t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
@@ -474,11 +560,13 @@ def main():
     peak_src = "measured (FMA chain microbenchmark, sdddst_vector_peaks)" if peak else "nominal"
     if not peak:
         peak = 80.0 if args.pairsum == "fp32" else 40.0
-    # DRAM traffic of one full-size launch (dram__bytes_read.sum + dram__bytes_write.sum, one ncu
-    # capture at N=32768, profiles/pair_tiles_f32_n16384.md): positions read, partials mostly in L2
-    traffic = PAIR_F32_DRAM_BYTES_N32768 if (args.pairsum == "fp32" and args.n == N_FULL) else None
+    # DRAM traffic of one full-size launch (dram__bytes_read.sum + dram__bytes_write.sum of one ncu
+    # capture, recorded above): positions read, partials mostly in L2
+    traffic = PAIR_F32_DRAM_BYTES_N32768_RECORDED if (args.pairsum == "fp32" and args.n == N_FULL) else None
     roof = {"bound": args.pairsum, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak, "traffic": traffic, "traffic_unit": "bytes per launch", "peak_source": peak_src,
+            "frac": achieved / peak, "traffic": traffic, "traffic_unit": "bytes per launch",
+            "traffic_source": "recorded from one ncu capture of this kernel at this size (not measured in this run)",
+            "peak_source": peak_src,
             "kernel": "pair_tiles_kernel (one velocity evaluation)",
             "work": f"{FLOP_PER_PAIR:.0f} FLOP x N(N-1)/2 unique pairs", "ms": t_pair_ms}
 
@@ -547,9 +635,9 @@ def main():
             batch = {"error": str(ex)[:200]}
 
     cpu = None
-    if rank == 0 and not args.no_cpu and ws == 1:
+    if cpu_proc is not None:
         try:
-            cpu = cpu_baseline_sample(args.n)
+            cpu = finish_cpu_baseline(cpu_proc)
             cpu.pop("seconds_per_step", None)
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "unavailable", "sample": str(ex)[:200]}
@@ -564,6 +652,8 @@ def main():
                    "solver": "gmres(30) fp64, cluster block-Jacobi preconditioner",
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas" if ws > 1 else "none",
                    "accepted": accepted, "attempts": args.steps, "final_step_size": sc["step_size"],
+                   "window": f"attempts after {settled} accepted steps and {args.warmup} warm-up attempts",
+                   "step_size_range": h_window,
                    "solver_stats": solver_stats,
                    "gmres_iterations_per_solve": solver_stats["iterations"] / max(1, solver_stats["solves"])},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

@@ -11,7 +11,10 @@
  * Configuration arrays use the reference's layouts: dislocations as N rows of
  * {x, y, b} doubles (include/dislocation.h:27-31), point defects as P rows of
  * {x, y} (include/point_defect.h:27-30).  Host pointers unless a name says
- * "_device".
+ * "_device".  Host configuration arrays must be finite: every entry point
+ * that takes one checks it on the host before any device work and returns
+ * SDDDST_ERR_NONFINITE for a NaN or Inf (the reference carries such values
+ * into its velocities and accepts the step).
  */
 #ifndef SDDDST_B200_H
 #define SDDDST_B200_H
@@ -245,13 +248,24 @@ int sdddst_profile_pair_sum(void *ctx, int reps, double *ms_per_launch);
  * last call's contents: calls that overlap on the GPU (different streams, or
  * host threads using the same device) race and must be serialised by the
  * caller.  Every scratch slot is written before it is read, so nothing needs
- * clearing between calls. */
+ * clearing between calls.  The looked-up address is cached per device for
+ * the life of the process: after cudaDeviceReset (or any destruction of the
+ * device's primary context) in the calling process the cached address is
+ * stale and this entry point must not be called again. */
 int sdddst_speeds_noalloc(int n, const double *x_device, const double *y_device, const double *b_device,
                           double tau_ext, double *v_device, void *stream);
 
 /* Linear-solver statistics of this context: solves performed and their
  * total Krylov iterations. */
 int sdddst_solver_stats(void *ctx, long *solves, long *iterations);
+
+/* Recoveries from stalled solves (GMRES past max_iters) in this context:
+ * rebuilds counts cluster-preconditioner rebuilds with a five times lower
+ * coupling threshold (SDDDST_SOLVER_GMRES_CLUSTER, at most two per solve
+ * before SDDDST_ERR_SOLVER), fallbacks counts learned- or analytic-corrected
+ * solves redone by the sparse LU (the reference has neither: its UMFPACK
+ * status is ignored, simulation.cpp:388-395). */
+int sdddst_solver_recoveries(void *ctx, long *rebuilds, long *fallbacks);
 
 /* Sparse LU statistics of this context (SDDDST_SOLVER_DIRECT; zeros
  * otherwise): factorizations performed, pivots perturbed, FP64 flops of one

@@ -49,13 +49,47 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _objects_dir() -> str:
+    d = os.path.join(HERE, "_build")
+    os.makedirs(d, exist_ok=True)
+    return d
+
+
+def _compile_one(src: str, verbose: bool) -> str:
+    """Compiles one translation unit to an object under sdddst_b200/_build/
+    when the object is older than the source or any header."""
+    obj = os.path.join(_objects_dir(), os.path.basename(src) + ".o")
+    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
+    headers += glob.glob(os.path.join(HOST, "include", "*.h")) + glob.glob(os.path.join(HOST, "include", "*", "*.h"))
+    headers.append(os.path.join(ROOT, "include", "sdddst_b200.h"))
+    if os.path.exists(obj) and all(os.path.getmtime(d) <= os.path.getmtime(obj) for d in [src] + headers):
+        return obj
+    flags = [f for f in FLAGS if f != "-shared"]
+    cmd = [nvcc()] + ARCH + flags + ["-I", os.path.join(ROOT, "include"), "-I", os.path.join(HOST, "include"),
+                                     "-c", src, "-o", obj + ".tmp"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True, cwd=HERE)
+    os.replace(obj + ".tmp", obj)
+    return obj
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile the library if any source is newer than it; returns its path."""
+    """Compile the library if any source is newer than it; returns its path.
+    Translation units compile in parallel to objects, then one link."""
     if not force and not _stale():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
+    srcs = sources()
+    if force:
+        for s in srcs:
+            o = os.path.join(_objects_dir(), os.path.basename(s) + ".o")
+            if os.path.exists(o):
+                os.remove(o)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(lambda s: _compile_one(s, verbose), srcs))
     tmp = LIB + ".tmp"
-    cmd = [nvcc()] + ARCH + FLAGS + ["-I", os.path.join(ROOT, "include"), "-I", os.path.join(HOST, "include"),
-                                     "-o", tmp] + sources()
+    cmd = [nvcc()] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", tmp] + objs
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True, cwd=HERE)
@@ -84,6 +118,27 @@ def build_python_module(force: bool = False, verbose: bool = False) -> str:
     return out
 
 
+CLI_SRC = os.path.join(HERE, "cli", "sdddst_main.cpp")
+CLI = os.path.join(HERE, "sdddst")
+
+
+def build_cli(force: bool = False, verbose: bool = False) -> str:
+    """Compile the `sdddst` command-line drop-in against the engine library."""
+    lib = build(verbose=verbose)
+    if not force and os.path.exists(CLI) and os.path.getmtime(CLI) >= max(os.path.getmtime(lib),
+                                                                         os.path.getmtime(CLI_SRC)):
+        return CLI
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    cmd = [cxx, "-O2", "-std=c++17", "-I", os.path.join(HOST, "include"), "-I", os.path.join(ROOT, "include"),
+           CLI_SRC, "-o", CLI + ".tmp", "-L", HERE, "-lsdddst_b200", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True, cwd=HERE)
+    os.replace(CLI + ".tmp", CLI)
+    return CLI
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True)
     build_python_module(force="--force" in sys.argv, verbose=True)
+    build_cli(force="--force" in sys.argv, verbose=True)

@@ -40,7 +40,7 @@ EXPORTS = [
     "sdddst_update_params", "sdddst_solve_csc", "sdddst_batch_create", "sdddst_batch_destroy",
     "sdddst_batch_step", "sdddst_batch_get_scalars", "sdddst_batch_get_positions", "sdddst_batch_info",
     "sdddst_direct_stats", "sdddst_profile_direct", "sdddst_precond_apply", "sdddst_set_preconditioner_weights",
-    "sdddst_learned_correction",
+    "sdddst_learned_correction", "sdddst_solver_recoveries",
 ]
 
 
@@ -109,6 +109,7 @@ def load(path: str = LIB_PATH):
     lib.sdddst_batch_info.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_long), C.POINTER(C.c_long),
                                       C.POINTER(C.c_void_p)]
     lib.sdddst_solver_stats.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long)]
+    lib.sdddst_solver_recoveries.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long)]
     lib.sdddst_profile_pair_sum.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
     lib.sdddst_vector_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.sdddst_direct_stats.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long),
@@ -300,6 +301,20 @@ class Engine:
         a, b = C.c_long(0), C.c_long(0)
         _check(self.lib.sdddst_solver_stats(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def solver_recoveries(self):
+        """(preconditioner rebuilds, sparse-LU fallbacks) after stalled solves."""
+        a, b = C.c_long(0), C.c_long(0)
+        _check(self.lib.sdddst_solver_recoveries(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def update_params(self, **kw):
+        """Changes mutable parameters of the live context (sdddst_update_params)."""
+        for k, v in kw.items():
+            if not hasattr(self.prm, k):
+                raise AttributeError(k)
+            setattr(self.prm, k, v)
+        _check(self.lib.sdddst_update_params(self.h, C.byref(self.prm)))
 
     def direct_stats(self) -> dict:
         f, pp, fd = C.c_long(0), C.c_long(0), C.c_long(0)

@@ -703,6 +703,13 @@ int sdddst_batch_create(const sdddst_params *common, int count, const int *sizes
 {
     if (!common || !sizes || !xyb || !batch || count < 1) return SDDDST_ERR_INVALID;
     *batch = nullptr;
+    long total = 0;
+    for (int k = 0; k < count; ++k) total += sizes[k] > 0 ? sizes[k] : 0;
+    for (long q = 0; q < 3 * total; ++q)
+        if (!std::isfinite(xyb[q])) {
+            sd::set_last_error("batch configuration: non-finite value at index " + std::to_string(q));
+            return SDDDST_ERR_NONFINITE;
+        }
     sd::Batch *bt = new (std::nothrow) sd::Batch();
     if (!bt) return SDDDST_ERR_NOMEM;
     int rc = sd::batch_init(*bt, *common, count, sizes, xyb);

@@ -28,6 +28,18 @@ int from_engine(sd::Engine *e, int rc)
 
 sd::Engine *E(void *ctx) { return static_cast<sd::Engine *>(ctx); }
 
+// Rejects a caller array holding NaN or Inf before anything reaches the
+// device (the reference runs on with such values: a NaN velocity is accepted
+// as a step and spreads through the configuration).  Returns 0 or
+// SDDDST_ERR_NONFINITE with the first offending entry named.
+int check_finite(const double *a, long count, const char *what)
+{
+    for (long k = 0; k < count; ++k)
+        if (!std::isfinite(a[k]))
+            return fail(SDDDST_ERR_NONFINITE, std::string(what) + ": non-finite value at index " + std::to_string(k));
+    return 0;
+}
+
 // Uploads a caller configuration into the engine's scratch arrays and
 // temporarily routes y and b to them; restores on destruction.
 struct ScratchConfig {
@@ -106,6 +118,10 @@ int sdddst_ctx_create(const sdddst_params *prm, const double *xyb, const double 
         return fail(SDDDST_ERR_INVALID, "unsupported solver");
     if (!(prm->prec > 0) || !(prm->step_size > 0) || !(prm->cutoff_multiplier > 0))
         return fail(SDDDST_ERR_INVALID, "prec, step size and cutoff multiplier must be positive");
+    if (xyb && prm->n > 0)
+        if (int rc = check_finite(xyb, 3L * prm->n, "configuration")) return rc;
+    if (pd && prm->p > 0)
+        if (int rc = check_finite(pd, 2L * prm->p, "point defects")) return rc;
     sd::Engine *e = new (std::nothrow) sd::Engine();
     if (!e) return fail(SDDDST_ERR_NOMEM, "host allocation failed");
     int rc;
@@ -137,6 +153,7 @@ int sdddst_set_state(void *ctx, const double *xyb, double step_size, double sim_
     if (!ctx || !xyb) return fail(SDDDST_ERR_INVALID, "null argument");
     if (!(step_size > 0)) return fail(SDDDST_ERR_INVALID, "step size must be positive");
     sd::Engine *e = E(ctx);
+    if (int rc = check_finite(xyb, 3L * e->n, "configuration")) return rc;
     cudaSetDevice(e->device);
     try {
         return from_engine(e, e->set_state_host(xyb, step_size, sim_time, energy, strain, first_step));
@@ -199,6 +216,7 @@ int sdddst_speeds(void *ctx, const double *xyb, double sim_time, int stress_type
     if (!ctx || !xyb || !v || !tol || stress_type < 0 || stress_type > 3)
         return fail(SDDDST_ERR_INVALID, "bad argument");
     sd::Engine *e = E(ctx);
+    if (int rc = check_finite(xyb, 3L * e->n, "configuration")) return rc;
     cudaSetDevice(e->device);
     try {
         ScratchConfig sc(e, xyb);
@@ -221,6 +239,7 @@ int sdddst_speeds_ext(void *ctx, const double *xyb, double tau_ext, double *v, d
 {
     if (!ctx || !xyb || !v) return fail(SDDDST_ERR_INVALID, "bad argument");
     sd::Engine *e = E(ctx);
+    if (int rc = check_finite(xyb, 3L * e->n, "configuration")) return rc;
     cudaSetDevice(e->device);
     try {
         ScratchConfig sc(e, xyb);
@@ -363,6 +382,7 @@ int sdddst_jacobian(void *ctx, double h, const double *xyb, int *row_ptr, int *c
 {
     if (!ctx || !xyb || !row_ptr || !nnz) return fail(SDDDST_ERR_INVALID, "null argument");
     sd::Engine *e = E(ctx);
+    if (int rc = check_finite(xyb, 3L * e->n, "configuration")) return rc;
     cudaSetDevice(e->device);
     try {
         ScratchConfig sc(e, xyb);
@@ -389,6 +409,7 @@ int sdddst_solve(void *ctx, double h, const double *xyb, const double *rhs, doub
 {
     if (!ctx || !xyb || !rhs || !x) return fail(SDDDST_ERR_INVALID, "null argument");
     sd::Engine *e = E(ctx);
+    if (int rc = check_finite(xyb, 3L * e->n, "configuration")) return rc;
     cudaSetDevice(e->device);
     try {
         ScratchConfig sc(e, xyb);
@@ -452,6 +473,7 @@ int sdddst_upload_positions(void *ctx, const double *x, int recompute)
 {
     if (!ctx || !x) return fail(SDDDST_ERR_INVALID, "null argument");
     sd::Engine *e = E(ctx);
+    if (int rc = check_finite(x, e->n, "positions")) return rc;
     cudaSetDevice(e->device);
     cudaMemcpyAsync(e->d_x0, x, sizeof(double) * e->n, cudaMemcpyHostToDevice, e->st);
     if (recompute) {
@@ -550,7 +572,7 @@ int sdddst_precond_apply(void *ctx, double h, int k, const double *in_device, do
         if (int rc = sd::precond_build(*e, h, e->d_dvec)) return from_engine(e, rc);
         for (int q = 0; q < k; ++q) sd::precond_apply(*e, in_device + (size_t)q * e->n, out_device + (size_t)q * e->n);
         if (block_of_device)
-            cudaMemcpyAsync(block_of_device, e->pc_blk_of, sizeof(int) * e->n, cudaMemcpyDeviceToDevice, e->st);
+            cudaMemcpyAsync(block_of_device, e->pc.blk_of, sizeof(int) * e->n, cudaMemcpyDeviceToDevice, e->st);
         return from_engine(e, e->sync_check("precond apply"));
     } catch (const std::exception &ex) {
         return fail(SDDDST_ERR_NOMEM, ex.what());
@@ -591,6 +613,14 @@ int sdddst_solver_stats(void *ctx, long *solves, long *iterations)
     if (!ctx) return fail(SDDDST_ERR_INVALID, "null argument");
     if (solves) *solves = E(ctx)->solves;
     if (iterations) *iterations = E(ctx)->iterations;
+    return SDDDST_OK;
+}
+
+int sdddst_solver_recoveries(void *ctx, long *rebuilds, long *fallbacks)
+{
+    if (!ctx) return fail(SDDDST_ERR_INVALID, "null argument");
+    if (rebuilds) *rebuilds = E(ctx)->stalls;
+    if (fallbacks) *fallbacks = E(ctx)->fallbacks;
     return SDDDST_OK;
 }
 

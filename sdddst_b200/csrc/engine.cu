@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -44,7 +45,9 @@ Engine::~Engine()
     if (h_hrec) cudaFreeHost(h_hrec);
     if (d_hrec) cudaFree(d_hrec);
     if (d_counter) cudaFree(d_counter);
-    precond_free(*this);
+    precond_free(pc);
+    precond_free(pc2);
+    fused_free(*this);
     direct_free(*this);
     learned_free(*this);
     if (d_xasm) cudaFree(d_xasm);
@@ -154,7 +157,10 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     rc |= dalloc(&d_y_small, (size_t)n + restart + 8);
     if (cudaMallocHost((void **)&h_scal, sizeof(double) * (2 * (restart + 1) + 8)) != cudaSuccess)
         rc |= SDDDST_ERR_NOMEM;
-    rc |= precond_alloc(*this);
+    rc |= precond_alloc(*this, pc);
+    // the cluster solver runs device-resident on a single system (the CSR's
+    // cell-sorted column positions are then always present)
+    fused = !batch_backend && prm.solver == SDDDST_SOLVER_GMRES_CLUSTER && std::getenv("SDDDST_HOST_GMRES") == nullptr;
     if (rc) {
         err = "device allocation failed";
         return SDDDST_ERR_NOMEM;
@@ -271,11 +277,13 @@ int Engine::solve(double h, const double *rhs, double *x_out)
         // the same matrix (analysed at the assembly positions)
         int rc = gmres_solve(*this, h, d_dvec, rhs, x_out, 4);
         if (rc != SDDDST_ERR_SOLVER) return rc;
-        stalls++;
+        fallbacks++;
         if (int rc2 = direct_analyse(*this, d_xasm)) return rc2;
         if (int rc2 = direct_factor(*this, h, d_dvec)) return rc2;
         return direct_solve(*this, h, d_dvec, rhs, x_out);
     }
+    if (prm.solver == SDDDST_SOLVER_GMRES_CLUSTER && fused && fused_supported(*this))
+        return solve_fused(h, d_dvec, pc, rhs, x_out);
     int precond = prm.solver == SDDDST_SOLVER_GMRES_JACOBI ? 1 : prm.solver == SDDDST_SOLVER_GMRES_CLUSTER ? 2 : 0;
     int rc = gmres_solve(*this, h, d_dvec, rhs, x_out, precond);
     if (rc != SDDDST_ERR_SOLVER || precond != 2) return rc;
@@ -296,6 +304,38 @@ int Engine::solve(double h, const double *rhs, double *x_out)
     return rc;
 }
 
+// One device-resident solve with the cluster preconditioner c of J(h); on a
+// stall the preconditioner is rebuilt with a five times lower coupling
+// threshold and the solve repeated, at most twice (as Engine::solve), and c
+// is rebuilt at the setting afterwards.
+int Engine::solve_fused(double h, const double *dvec, Cluster &c, const double *rhs, double *x_out)
+{
+    const Cluster *pcs[1] = {&c};
+    int conv = 0;
+    if (int rc = fused_gmres(*this, 1, &h, &dvec, &rhs, &x_out, pcs, &conv)) return rc;
+    if (conv) return 0;
+    const double theta0 = prm.precond_theta;
+    for (int attempt = 0; attempt < 2 && !conv; ++attempt) {
+        prm.precond_theta = cluster_theta(*this) / 5.0;
+        stalls++;
+        if (int rc = precond_build(*this, c, h, dvec)) {
+            prm.precond_theta = theta0;
+            return rc;
+        }
+        if (int rc = fused_gmres(*this, 1, &h, &dvec, &rhs, &x_out, pcs, &conv)) {
+            prm.precond_theta = theta0;
+            return rc;
+        }
+    }
+    prm.precond_theta = theta0;
+    if (int rc = precond_build(*this, c, h, dvec)) return rc;
+    if (!conv) {
+        err = "solve: GMRES did not reach the residual target";
+        return SDDDST_ERR_SOLVER;
+    }
+    return 0;
+}
+
 int Engine::prepare_solver(double h)
 {
     if (prm.solver == SDDDST_SOLVER_GMRES_CLUSTER) return precond_build(*this, h, d_dvec);
@@ -305,6 +345,55 @@ int Engine::prepare_solver(double h)
         if (int rc = precond_build(*this, h, d_dvec)) return rc;
         return learned_build(*this, h, d_dvec, d_xasm, prm.solver == SDDDST_SOLVER_GMRES_NEUMANN);
     }
+    return 0;
+}
+
+// calculateG (simulation.cpp:133-193) of Newton iteration `it` of one stage.
+int Engine::stage_residual(double h, int it, double *xn, const double *xo, bool use2, bool init_speed, int origin,
+                           int end, double *csp0, const double *dvec, double *g)
+{
+    double *isp = use2 ? d_v0b : d_v0;
+    double *Sorig = use2 ? d_S1 : d_S0;
+    const bool calc_init = it == 0 ? init_speed : false;
+    const bool use_init_first = it == 0 ? zero_stress() : false;
+    double *csp = csp0;
+    if (calc_init) {
+        double t = sim_time, tasi = strain;
+        if (origin == kEndFirst) {
+            t += step_size * 0.5;
+            if (prm.stress_kind == SDDDST_STRESS_SPRING) {
+                double inc;
+                if (int rc = strain_inc(d_x0, d_x1, &inc)) return rc;
+                tasi += inc;
+            }
+        }
+        stress_calc(t, origin, tasi);
+        cur_stress = origin;
+        speeds(xo, isp, Sorig, origin, true);
+    }
+    if (use_init_first) {
+        csp = isp;
+    } else {
+        double t = sim_time + step_size, tasi = strain;
+        if (prm.stress_kind == SDDDST_STRESS_SPRING) {
+            double inc1 = 0, inc2 = 0;
+            if (end == kEndFirst) {
+                if (int rc = strain_inc(d_x0, d_x1, &inc1)) return rc;
+            } else if (end == kEndSecond) {
+                if (int rc = strain_inc(d_x0, d_x1, &inc1)) return rc;
+                if (int rc = strain_inc(d_x1, d_x2, &inc2)) return rc;
+            } else if (end == kEndBig) {
+                if (int rc = strain_inc(d_x0, d_xb, &inc1)) return rc;
+            }
+            tasi += inc1 + inc2;
+        }
+        if (end == kEndFirst) t -= step_size * 0.5;
+        stress_calc(t, end, tasi);
+        cur_stress = end;
+        speeds(xn, csp, d_Stmp, end, true);
+    }
+    launch_residual_g(*this, h, xn, xo, csp, isp, dvec, g, st);
+    launches++;
     return 0;
 }
 
@@ -318,53 +407,60 @@ int Engine::integrate(double h, double *xn, const double *xo, bool use2, bool in
     launch_make_dvec(*this, h, d_dvec, st);
     launches++;
     if (int rc = prepare_solver(h)) return rc;
-    double *isp = use2 ? d_v0b : d_v0;
     double *csp0 = use2 ? d_vs2 : d_vs;
-    double *Sorig = use2 ? d_S1 : d_S0;
     for (int it = 0; it < ic; ++it) {
-        const bool calc_init = it == 0 ? init_speed : false;
-        const bool use_init_first = it == 0 ? zero_stress() : false;
-        double *csp = csp0;
-        if (calc_init) {
-            double t = sim_time, tasi = strain;
-            if (origin == kEndFirst) {
-                t += step_size * 0.5;
-                if (prm.stress_kind == SDDDST_STRESS_SPRING) {
-                    double inc;
-                    if (int rc = strain_inc(d_x0, d_x1, &inc)) return rc;
-                    tasi += inc;
-                }
-            }
-            stress_calc(t, origin, tasi);
-            cur_stress = origin;
-            speeds(xo, isp, Sorig, origin, true);
-        }
-        if (use_init_first) {
-            csp = isp;
-        } else {
-            double t = sim_time + step_size, tasi = strain;
-            if (prm.stress_kind == SDDDST_STRESS_SPRING) {
-                double inc1 = 0, inc2 = 0;
-                if (end == kEndFirst) {
-                    if (int rc = strain_inc(d_x0, d_x1, &inc1)) return rc;
-                } else if (end == kEndSecond) {
-                    if (int rc = strain_inc(d_x0, d_x1, &inc1)) return rc;
-                    if (int rc = strain_inc(d_x1, d_x2, &inc2)) return rc;
-                } else if (end == kEndBig) {
-                    if (int rc = strain_inc(d_x0, d_xb, &inc1)) return rc;
-                }
-                tasi += inc1 + inc2;
-            }
-            if (end == kEndFirst) t -= step_size * 0.5;
-            stress_calc(t, end, tasi);
-            cur_stress = end;
-            speeds(xn, csp, d_Stmp, end, true);
-        }
-        launch_residual_g(*this, h, xn, xo, csp, isp, d_dvec, d_g, st);
-        launches++;
+        if (int rc = stage_residual(h, it, xn, xo, use2, init_speed, origin, end, csp0, d_dvec, d_g)) return rc;
         if (int rc = solve(h, d_g, d_sol)) return rc;
         launch_axpy_update(*this, xn, d_sol, st);
         launches++;
+    }
+    return 0;
+}
+
+// Stage I (integrate(h, bigStep, ...), simulation.cpp:443-492) and stage II
+// (integrate(h/2, firstSmall, ...), :494-499) side by side: both start from
+// the accepted configuration and share its assembly (H(h/2) = H(h)/2), and
+// each chord-Newton iteration computes both residuals and then solves both
+// systems in one device-resident launch that reads G once per SpMV pass.
+// The order of the host-side stress evaluations, the velocity evaluations
+// and the tolerance minimum is that of the two stages run one after the
+// other, so the results are the same.  Stage I's current speed goes to its
+// own buffer; stage II's to the speed vector the reference keeps.
+int Engine::stages_one_two()
+{
+    if (int rc = fused_alloc(*this, 2)) {
+        err = "fused solve: allocation failed";
+        return rc;
+    }
+    const double h1 = step_size, h2 = 0.5 * step_size;
+    if (int rc = assemble(d_xb)) return rc;
+    launch_make_dvec(*this, h1, d_dvecI, st);
+    launch_make_dvec(*this, h2, d_dvec, st);
+    launches += 2;
+    if (int rc = precond_build(*this, pc2, h1, d_dvecI, false)) return rc;
+    if (int rc = precond_build(*this, pc, h2, d_dvec, false)) return rc;
+    if (int rc = precond_check(*this, pc2)) return rc;
+    if (int rc = precond_check(*this, pc)) return rc;
+    for (int it = 0; it < ic; ++it) {
+        if (int rc = stage_residual(h1, it, d_xb, d_x0, false, init_speed_needed, kOrig, kEndBig, d_vsI, d_dvecI,
+                                    d_gI))
+            return rc;
+        if (int rc = stage_residual(h2, it, d_x1, d_x0, false, false, kOrig, kEndFirst, d_vs, d_dvec, d_g))
+            return rc;
+        const double hs[2] = {h1, h2};
+        const double *dv[2] = {d_dvecI, d_dvec};
+        const double *rhs[2] = {d_gI, d_g};
+        double *xs[2] = {d_solI, d_sol};
+        const Cluster *pcs[2] = {&pc2, &pc};
+        int conv[2] = {0, 0};
+        if (int rc = fused_gmres(*this, 2, hs, dv, rhs, xs, pcs, conv)) return rc;
+        if (!conv[0])
+            if (int rc = solve_fused(h1, d_dvecI, pc2, d_gI, d_solI)) return rc;
+        if (!conv[1])
+            if (int rc = solve_fused(h2, d_dvec, pc, d_g, d_sol)) return rc;
+        launch_axpy_update(*this, d_xb, d_solI, st);
+        launch_axpy_update(*this, d_x1, d_sol, st);
+        launches += 2;
     }
     return 0;
 }
@@ -385,11 +481,18 @@ int Engine::step(int *accepted)
         first_step = false;
     }
     cudaMemcpyAsync(d_xb, d_x0, bytes, cudaMemcpyDeviceToDevice, st);
-    if (int rc = integrate(step_size, d_xb, d_x0, false, init_speed_needed, kOrig, kEndBig, false)) return rc;
-    successful_step = false;
-    // ---- stage II (simulation.cpp:494-499): same configuration, same G
-    cudaMemcpyAsync(d_x1, d_x0, bytes, cudaMemcpyDeviceToDevice, st);
-    if (int rc = integrate(0.5 * step_size, d_x1, d_x0, false, false, kOrig, kEndFirst, true)) return rc;
+    if (fused && prm.solver == SDDDST_SOLVER_GMRES_CLUSTER) {
+        // ---- stages I and II together (one solve launch per Newton iteration)
+        cudaMemcpyAsync(d_x1, d_x0, bytes, cudaMemcpyDeviceToDevice, st);
+        if (int rc = stages_one_two()) return rc;
+        successful_step = false;
+    } else {
+        if (int rc = integrate(step_size, d_xb, d_x0, false, init_speed_needed, kOrig, kEndBig, false)) return rc;
+        successful_step = false;
+        // ---- stage II (simulation.cpp:494-499): same configuration, same G
+        cudaMemcpyAsync(d_x1, d_x0, bytes, cudaMemcpyDeviceToDevice, st);
+        if (int rc = integrate(0.5 * step_size, d_x1, d_x0, false, false, kOrig, kEndFirst, true)) return rc;
+    }
     // ---- stage III (simulation.cpp:501-650)
     sum_avg_speed = 0;
     cudaMemcpyAsync(d_x2, d_x1, bytes, cudaMemcpyDeviceToDevice, st);

@@ -14,6 +14,18 @@
 
 namespace sd {
 
+// One cluster block-Jacobi preconditioner: the block structure of J(h) and
+// the blocks' inverses (precond.cu).
+struct Cluster {
+    int *ptr = nullptr, *parent = nullptr, *tmp = nullptr, *tmp2 = nullptr, *members = nullptr;
+    int *blk_of = nullptr, *loc = nullptr, *count = nullptr, *fill = nullptr, *start = nullptr;
+    int *nblk = nullptr, *bbase = nullptr, *bstart = nullptr, *blen = nullptr, *sq = nullptr;
+    int *off = nullptr;
+    int *flag = nullptr; // set by the inversion when a block is singular
+    double *binv = nullptr;
+    long binv_cap = 0;
+};
+
 struct Engine {
     // ---- sizes and parameters
     int n = 0, p = 0, device = 0;
@@ -75,21 +87,24 @@ struct Engine {
     double last_resid = 0.0;
     long solves = 0, iterations = 0;      // solver statistics
     long stalls = 0;                      // solves repeated with a rebuilt preconditioner
+    long fallbacks = 0;                   // stalled learned-preconditioned solves redone by the sparse LU
     double *d_hrec = nullptr;             // per-iteration Gram-Schmidt records
     double *h_hrec = nullptr;             // pinned copy
     unsigned int *d_counter = nullptr;    // last-block ticket of the fused reductions
     bool coop_gs = false;                 // one cooperative launch per Gram-Schmidt step
     int gmres_hint = 4;                   // iterations of the last solve (first convergence check)
     double *d_gs_partials = nullptr;      // its per-CTA partial sums (3 x gs_blocks x 32)
+    // device-resident GMRES (fused_gmres.cu): partial sums, per-system status,
+    // and the second system's Krylov basis and vectors (joint stage I + II)
+    double *d_fpart = nullptr, *d_fstatus = nullptr, *h_fstatus = nullptr;
+    double *d_V2 = nullptr, *d_w2 = nullptr, *d_z2 = nullptr, *d_zs2 = nullptr;
+    double *d_gI = nullptr, *d_solI = nullptr, *d_dvecI = nullptr, *d_vsI = nullptr; // stage I's g, solution, d, speed
+    bool fused = false;                   // the cluster solver runs device-resident (set at init)
 
-    // ---- cluster block-Jacobi preconditioner (precond.cu)
-    int *pc_ptr = nullptr, *pc_parent = nullptr, *pc_tmp = nullptr, *pc_tmp2 = nullptr, *pc_members = nullptr;
-    int *pc_blk_of = nullptr, *pc_loc = nullptr, *pc_count = nullptr, *pc_fill = nullptr, *pc_start = nullptr;
-    int *pc_nblk = nullptr, *pc_bbase = nullptr, *pc_bstart = nullptr, *pc_blen = nullptr, *pc_sq = nullptr;
-    int *pc_off = nullptr;
-    double *pc_binv = nullptr;
-    long pc_binv_cap = 0;
-    int pc_nb = 0;
+    // ---- cluster block-Jacobi preconditioners (precond.cu): pc for the
+    // solves of the engine's generic path and of stage II/III, pc2 for stage
+    // I's J(h) while the joint stage I + II solve holds both
+    Cluster pc, pc2;
 
     // ---- sparse LU (direct.cu)
     void *direct = nullptr;
@@ -122,6 +137,14 @@ struct Engine {
     int prepare_solver(double h); // per matrix: preconditioner set-up
     int integrate(double h, double *xn, const double *xo, bool use2, bool init_speed, int origin, int end,
                   bool reuse_assembly);
+    // calculateG of one chord-Newton iteration of one stage: speeds at the
+    // iterate (csp) or the initial speeds, then g (simulation.cpp:133-193)
+    int stage_residual(double h, int it, double *xn, const double *xo, bool use2, bool init_speed, int origin,
+                       int end, double *csp0, const double *dvec, double *g);
+    // stage I (h) and stage II (h/2) from the accepted configuration with
+    // their solves in one device-resident launch per Newton iteration
+    int stages_one_two();
+    int solve_fused(double h, const double *dvec, Cluster &c, const double *rhs, double *x);
     int step(int *accepted);
     int set_state_host(const double *xyb, double step, double t, double e, double strain, int first);
 
@@ -175,10 +198,15 @@ void launch_axpy_update(const Engine &e, double *xn, const double *sol, cudaStre
 int reduce_sum(Engine &e, const double *a, const double *b, int n, int op, double *out);
 void set_last_error(const std::string &msg);
 
-int precond_alloc(Engine &e);
-void precond_free(Engine &e);
-int precond_build(Engine &e, double h, const double *dvec);
-void precond_apply(Engine &e, const double *v, double *z);
+int precond_alloc(Engine &e, Cluster &c);
+void precond_free(Cluster &c);
+// Builds c for J(h); with check, waits for the build and verifies the block
+// count and the inversions (else the caller checks later with precond_check).
+int precond_build(Engine &e, Cluster &c, double h, const double *dvec, bool check = true);
+int precond_check(Engine &e, const Cluster &c);
+inline int precond_build(Engine &e, double h, const double *dvec) { return precond_build(e, e.pc, h, dvec); }
+void precond_apply(Engine &e, const Cluster &c, const double *v, double *z);
+inline void precond_apply(Engine &e, const double *v, double *z) { precond_apply(e, e.pc, v, z); }
 
 int direct_analyse(Engine &e, const double *x);
 int direct_factor(Engine &e, double h, const double *dvec);
@@ -187,6 +215,12 @@ int direct_solve(Engine &e, double h, const double *dvec, const double *rhs, dou
 int direct_stats(const Engine &e, long *factorizations, long *perturbed, double *flops, long *front_doubles,
                  int *fronts, int *depth);
 void direct_free(Engine &e);
+
+bool fused_supported(const Engine &e);
+int fused_alloc(Engine &e, int ns);
+void fused_free(Engine &e);
+int fused_gmres(Engine &e, int ns, const double *h, const double *const *dvec, const double *const *rhs,
+                double *const *x, const Cluster *const *pcs, int *conv);
 
 int learned_set_weights(Engine &e, const unsigned short *bf16, long count);
 int learned_build(Engine &e, double h, const double *dvec, const double *x, bool analytic);

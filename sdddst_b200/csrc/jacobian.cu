@@ -153,7 +153,12 @@ __global__ void scan_add_kernel(int m, int *__restrict__ out, const int *__restr
 // 2048 scanned by one block each, their totals scanned by one block, and the
 // offsets added (the engine's scan scratch holds totals and offsets).  One
 // block alone is bound by its load and store round trips (about 22 us for
-// 32768 entries).
+// 32768 entries).  The output is int32 on both routes, so the total must fit
+// in an int: the one-block route sums in 64 bits and narrows on the store,
+// the chunked route sums in 32 bits; they agree whenever the total fits.  The
+// callers stay far below 2^31: a CSR total is at most N^2 (below 2^31 for
+// N <= 46340; N (1 + k) = 2.1e7 at N = 32768, k = 627) and the
+// preconditioner's pattern counts are below 32 N.
 int launch_scan(Engine &e, const int *in, int m, int *out, cudaStream_t st)
 {
     const int nb = (m + 2047) / 2048;

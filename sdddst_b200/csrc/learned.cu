@@ -514,10 +514,10 @@ int learned_build(Engine &e, double h, const double *dvec, const double *x, bool
         const double th2 = e.prm.neumann_theta > 0 ? e.prm.neumann_theta : 0.0;
         if (e.valf)
             first_order_kernel<float><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_valf, dvec, L.d_jii,
-                                                             e.pc_blk_of, th2, L.d_cval);
+                                                             e.pc.blk_of, th2, L.d_cval);
         else
             first_order_kernel<double><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, L.d_jii,
-                                                              e.pc_blk_of, th2, L.d_cval);
+                                                              e.pc.blk_of, th2, L.d_cval);
         e.launches += 2;
         L.compact = false;
         if (th2 > 0.0 && e.col_s_valid && !e.d_hrow) {
@@ -556,22 +556,22 @@ int learned_build(Engine &e, double h, const double *dvec, const double *x, bool
         proj_kernel<<<pgrid, 256, 0, st>>>(n, L.d_h, L.d_w, o.P[l], o.Pb[l], o.Q[l], L.d_ph, L.d_qh);
         if (e.valf)
             edge_kernel<float, false><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_valf, dvec, L.d_jii, x,
-                                                             e.d_y, e.pc_blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w,
+                                                             e.d_y, e.pc.blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w,
                                                              o.R[l], 0, 0, L.d_agg, nullptr);
         else
             edge_kernel<double, false><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, L.d_jii, x,
-                                                              e.d_y, e.pc_blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w,
+                                                              e.d_y, e.pc.blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w,
                                                               o.R[l], 0, 0, L.d_agg, nullptr);
         node_update_kernel<<<ugrid, 256, 0, st>>>(n, L.d_h, L.d_agg, L.d_w, o.U[l], o.Ub[l]);
     }
     proj_kernel<<<pgrid, 256, 0, st>>>(n, L.d_h, L.d_w, o.Po, o.Pob, o.Qo, L.d_ph, L.d_qh);
     if (e.valf)
         edge_kernel<float, true><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_valf, dvec, L.d_jii, x, e.d_y,
-                                                        e.pc_blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w, o.Ro, o.wo,
+                                                        e.pc.blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w, o.Ro, o.wo,
                                                         o.wob, nullptr, L.d_cval);
     else
         edge_kernel<double, true><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, L.d_jii, x,
-                                                         e.d_y, e.pc_blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w, o.Ro,
+                                                         e.d_y, e.pc.blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w, o.Ro,
                                                          o.wo, o.wob, nullptr, L.d_cval);
     diag_out_kernel<<<wrows, 256, 0, st>>>(n, L.d_h, L.d_w, o.wd, o.wdb, L.d_jii, e.d_rowptr, L.d_cval);
     e.launches += 4 + 3 * kLayers + 2;

@@ -300,13 +300,13 @@ double cluster_theta(const Engine &e)
 }
 
 // Builds the cluster block-Jacobi inverse of J(h) for the assembled G.
-int precond_build(Engine &e, double h, const double *dvec)
+int precond_build(Engine &e, Cluster &c, double h, const double *dvec, bool check)
 {
     const int n = e.n;
     cudaStream_t st = e.st;
     const unsigned nb256 = (unsigned)((n + 255) / 256);
     const double theta = cluster_theta(e);
-    int *ptr = e.pc_ptr, *par = e.pc_parent, *par2 = e.pc_tmp;
+    int *ptr = c.ptr, *par = c.parent, *par2 = c.tmp;
     // single system: M_jj in the cell-sorted order (the SpMV's staging buffer,
     // free until the solve), read through the CSR's sorted column positions
     const bool srt = e.col_s_valid && !e.d_hrow;
@@ -327,50 +327,57 @@ int precond_build(Engine &e, double h, const double *dvec)
         jump_kernel<<<nb256, 256, 0, st>>>(n, par, par2);
         std::swap(par, par2);
     }
-    cudaMemsetAsync(e.pc_count, 0, sizeof(int) * (n + 1), st);
-    cudaMemsetAsync(e.pc_fill, 0, sizeof(int) * (n + 1), st);
-    root_fix_kernel<<<nb256, 256, 0, st>>>(n, par, e.pc_count);
-    e.launches += launch_scan(e, e.pc_count, n, e.pc_start, st) - 1;
-    member_scatter_kernel<<<nb256, 256, 0, st>>>(n, par, e.pc_start, e.pc_fill, e.pc_tmp2);
-    cluster_sort_kernel<<<nb256, 256, 0, st>>>(n, e.pc_count, e.pc_start, e.pc_tmp2, e.pc_members, e.pc_nblk);
-    e.launches += launch_scan(e, e.pc_nblk, n, e.pc_bbase, st) - 1;
+    cudaMemsetAsync(c.count, 0, sizeof(int) * (n + 1), st);
+    cudaMemsetAsync(c.fill, 0, sizeof(int) * (n + 1), st);
+    root_fix_kernel<<<nb256, 256, 0, st>>>(n, par, c.count);
+    e.launches += launch_scan(e, c.count, n, c.start, st) - 1;
+    member_scatter_kernel<<<nb256, 256, 0, st>>>(n, par, c.start, c.fill, c.tmp2);
+    cluster_sort_kernel<<<nb256, 256, 0, st>>>(n, c.count, c.start, c.tmp2, c.members, c.nblk);
+    e.launches += launch_scan(e, c.nblk, n, c.bbase, st) - 1;
     e.launches += 19;
     // the block count stays on the device (pc_bbase[n]); the block kernels
     // run over n (an upper bound) and return beyond it, and the inverses'
     // storage is sized for the bound sum k^2 <= kMaxBlock n once
-    const int *nbp = e.pc_bbase + n;
+    const int *nbp = c.bbase + n;
     const long cap = (long)kMaxBlock * n + 1024;
-    if (cap > e.pc_binv_cap) {
-        if (e.pc_binv) cudaFree(e.pc_binv);
-        e.pc_binv = nullptr;
-        e.pc_binv_cap = 0;
-        if (cudaMalloc(&e.pc_binv, sizeof(double) * cap) != cudaSuccess) {
+    if (cap > c.binv_cap) {
+        if (c.binv) cudaFree(c.binv);
+        c.binv = nullptr;
+        c.binv_cap = 0;
+        if (cudaMalloc(&c.binv, sizeof(double) * cap) != cudaSuccess) {
             e.err = "precond: allocation failed";
             return SDDDST_ERR_NOMEM;
         }
-        e.pc_binv_cap = cap;
+        c.binv_cap = cap;
     }
-    block_list_kernel<<<nb256, 256, 0, st>>>(n, e.pc_count, e.pc_start, e.pc_bbase, e.pc_bstart, e.pc_blen);
-    cudaMemsetAsync(e.pc_sq, 0, sizeof(int) * (n + 1), st);
-    block_meta_kernel<<<nb256, 256, 0, st>>>(nbp, e.pc_bstart, e.pc_blen, e.pc_members, e.pc_blk_of, e.pc_loc,
-                                             e.pc_sq);
-    e.launches += launch_scan(e, e.pc_sq, n, e.pc_off, st) - 1;
-    cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
+    block_list_kernel<<<nb256, 256, 0, st>>>(n, c.count, c.start, c.bbase, c.bstart, c.blen);
+    cudaMemsetAsync(c.sq, 0, sizeof(int) * (n + 1), st);
+    block_meta_kernel<<<nb256, 256, 0, st>>>(nbp, c.bstart, c.blen, c.members, c.blk_of, c.loc,
+                                             c.sq);
+    e.launches += launch_scan(e, c.sq, n, c.off, st) - 1;
+    cudaMemsetAsync(c.flag, 0, sizeof(int), st);
     const unsigned ib = (unsigned)((n + 1) / 2);
     if (e.valf)
-        block_invert_kernel<float><<<ib, 64, 0, st>>>(nbp, h, e.d_hrow, e.pc_bstart, e.pc_blen, e.pc_members,
-                                                      e.pc_blk_of, e.pc_loc, e.pc_off, e.d_rowptr, e.d_col, e.d_valf,
-                                                      e.d_gdiag, dvec, e.pc_binv, e.d_flag);
+        block_invert_kernel<float><<<ib, 64, 0, st>>>(nbp, h, e.d_hrow, c.bstart, c.blen, c.members,
+                                                      c.blk_of, c.loc, c.off, e.d_rowptr, e.d_col, e.d_valf,
+                                                      e.d_gdiag, dvec, c.binv, c.flag);
     else
-        block_invert_kernel<double><<<ib, 64, 0, st>>>(nbp, h, e.d_hrow, e.pc_bstart, e.pc_blen, e.pc_members,
-                                                       e.pc_blk_of, e.pc_loc, e.pc_off, e.d_rowptr, e.d_col, e.d_val,
-                                                       e.d_gdiag, dvec, e.pc_binv, e.d_flag);
+        block_invert_kernel<double><<<ib, 64, 0, st>>>(nbp, h, e.d_hrow, c.bstart, c.blen, c.members,
+                                                       c.blk_of, c.loc, c.off, e.d_rowptr, e.d_col, e.d_val,
+                                                       e.d_gdiag, dvec, c.binv, c.flag);
     e.launches += 4;
+    return check ? precond_check(e, c) : 0;
+}
+
+// Waits for the build and checks it: a block count in 1..n and no singular
+// block.
+int precond_check(Engine &e, const Cluster &c)
+{
     int flag = 0, nb = 0;
-    cudaMemcpyAsync(&flag, e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(&nb, nbp, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&flag, c.flag, sizeof(int), cudaMemcpyDeviceToHost, e.st);
+    cudaMemcpyAsync(&nb, c.bbase + e.n, sizeof(int), cudaMemcpyDeviceToHost, e.st);
     if (int rc = e.sync_check("precond build")) return rc;
-    if (nb <= 0 || nb > n) {
+    if (nb <= 0 || nb > e.n) {
         e.err = "precond: bad block count";
         return SDDDST_ERR_SOLVER;
     }
@@ -378,38 +385,37 @@ int precond_build(Engine &e, double h, const double *dvec)
         e.err = "precond: singular cluster block";
         return SDDDST_ERR_SOLVER;
     }
-    e.pc_nb = nb;
     return 0;
 }
 
-void precond_apply(Engine &e, const double *v, double *z)
+void precond_apply(Engine &e, const Cluster &c, const double *v, double *z)
 {
-    block_apply_kernel<<<(e.n + 255) / 256, 256, 0, e.st>>>(e.n, e.pc_blk_of, e.pc_loc, e.pc_bstart, e.pc_blen,
-                                                            e.pc_members, e.pc_off, e.pc_binv, v, z);
+    block_apply_kernel<<<(e.n + 255) / 256, 256, 0, e.st>>>(e.n, c.blk_of, c.loc, c.bstart, c.blen, c.members,
+                                                            c.off, c.binv, v, z);
     e.launches++;
 }
 
-int precond_alloc(Engine &e)
+int precond_alloc(Engine &e, Cluster &c)
 {
     const int n = e.n;
-    int **arrs[] = {&e.pc_ptr, &e.pc_parent, &e.pc_tmp, &e.pc_tmp2, &e.pc_members, &e.pc_blk_of, &e.pc_loc};
+    int **arrs[] = {&c.ptr, &c.parent, &c.tmp, &c.tmp2, &c.members, &c.blk_of, &c.loc};
     for (int **a : arrs)
         if (cudaMalloc(a, sizeof(int) * n) != cudaSuccess) return SDDDST_ERR_NOMEM;
-    int **arrs1[] = {&e.pc_count, &e.pc_fill, &e.pc_start, &e.pc_nblk, &e.pc_bbase, &e.pc_bstart, &e.pc_blen,
-                     &e.pc_sq, &e.pc_off};
+    int **arrs1[] = {&c.count, &c.fill, &c.start, &c.nblk, &c.bbase, &c.bstart, &c.blen, &c.sq, &c.off};
     for (int **a : arrs1)
         if (cudaMalloc(a, sizeof(int) * (n + 1)) != cudaSuccess) return SDDDST_ERR_NOMEM;
+    if (cudaMalloc(&c.flag, sizeof(int)) != cudaSuccess) return SDDDST_ERR_NOMEM;
     return 0;
 }
 
-void precond_free(Engine &e)
+void precond_free(Cluster &c)
 {
-    int *arrs[] = {e.pc_ptr, e.pc_parent, e.pc_tmp, e.pc_tmp2, e.pc_members, e.pc_blk_of, e.pc_loc,
-                   e.pc_count, e.pc_fill, e.pc_start, e.pc_nblk, e.pc_bbase, e.pc_bstart, e.pc_blen,
-                   e.pc_sq, e.pc_off};
+    int *arrs[] = {c.ptr, c.parent, c.tmp, c.tmp2, c.members, c.blk_of, c.loc, c.count, c.fill, c.start,
+                   c.nblk, c.bbase, c.bstart, c.blen, c.sq, c.off, c.flag};
     for (int *a : arrs)
         if (a) cudaFree(a);
-    if (e.pc_binv) cudaFree(e.pc_binv);
+    if (c.binv) cudaFree(c.binv);
+    c = Cluster{};
 }
 
 } // namespace sd

@@ -46,3 +46,37 @@ def test_batch_mixed_precision_runs(engine_lib):
         same = acc_a == acc_b
         for k in np.nonzero(same)[0]:
             assert np.abs(a.positions(0)[k] - b.positions(0)[k]).max() < 1e-8
+
+
+def test_batch_workload_systems_match_oracle(engine_lib, port_lib):
+    """Eight systems of the batched workload itself (sizes drawn from
+    U[64, 2048] with seed 3, each system's own seed; cutoff multiplier 0.5,
+    precision 1e-6): per-system decisions, positions, step sizes, times,
+    counters and energies against independent oracle runs over 6 attempts,
+    with the systems accepting and rejecting unevenly."""
+    from concurrent.futures import ThreadPoolExecutor
+    from sdddst_b200 import capi
+    sizes = workloads.batch_sizes(workloads.BATCH_COUNT, workloads.BATCH_SEED)[:8]
+    systems = [workloads.dislocations(int(n), workloads.BATCH_SEED * 100003 + k)[0] for k, n in enumerate(sizes)]
+    prm = capi.default_params(cutoff_multiplier=workloads.BATCH_M, prec=1e-6, step_size=1e-6)
+    bt = capi.Batch(prm, systems)
+    oracles = [ref.Sim(s, None, ref.params(cutoff_multiplier=workloads.BATCH_M, prec=1e-6, step_size=1e-6), "port")
+               for s in systems]
+    uneven = False
+    with ThreadPoolExecutor(max_workers=8) as pool:  # the oracle releases the GIL inside its C calls
+        for step in range(6):
+            acc = bt.step()
+            acc_ref = np.array(list(pool.map(lambda o: o.step(), oracles)))
+            assert np.array_equal(acc, acc_ref), step
+            uneven |= bool(acc.any() and not acc.all())
+            xs = bt.positions(0)
+            sc = bt.scalars()
+            for k, o in enumerate(oracles):
+                assert np.abs(xs[k] - o.config(0)[:, 0]).max() <= 1e-9, (step, k)
+                s = o.scalars()
+                assert np.isclose(sc[k, 1], s["step_size"], rtol=1e-6), (step, k)
+                assert np.isclose(sc[k, 0], s["sim_time"], rtol=1e-6, atol=0)
+                assert sc[k, 2] == s["successful_steps"] and sc[k, 3] == s["failed_steps"]
+                assert np.isclose(sc[k, 4], s["energy"], rtol=1e-8)
+    assert uneven, "every attempt was accepted or rejected by all systems together"
+    bt.close()

@@ -5,9 +5,13 @@ bit-for-bit to the reference (tests/test_oracle.py); the committed golden
 fixtures of the reference are checked directly too.
 
 Tolerances (FP64 plain path):
-  * velocities: |dv_i| <= 1e-10 * max|v| + 1e-9 |v_i|  (the device sums pairs
-    in a different order and evaluates the field with a shared exp and exact
-    near-field identities instead of per-image cosh and a Taylor branch);
+  * velocities: 1e-10 relative in the max norm, |dv_i| <= 1e-10 * max_j |v_j|
+    for every i (the device sums pairs in a different order and evaluates the
+    field with a shared exp and exact near-field identities instead of
+    per-image cosh and a Taylor branch).  The bar is normwise, not
+    element-wise: a velocity is a sum of O(N) terms of both signs, and where
+    they cancel |v_i| is far below the terms it is made of, so no summation
+    order reproduces it to 1e-10 of itself;
   * tolerances: bit-exact without point defects (same r^2 arithmetic);
   * Jacobian: same sparsity pattern, |dJ_ij| <= 1e-10 * max|J offdiag|;
   * positions after a teacher-forced step: 1e-10 relative, error ratio 1e-6
@@ -26,22 +30,26 @@ pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
-def make_pair(n, seed, m, prec, p=0, sk=0, sv=0.0, step=1e-6, **kw):
+def make_pair(n, seed, m, prec, p=0, sk=0, sv=0.0, step=1e-6, rate=0.0, spring=1.0, strain=False, **kw):
+    """The oracle and a CUDA engine on the same seeded configuration and
+    parameters (stress protocol: sk kind, sv constant value, rate for the
+    fixed-rate and spring protocols, spring constant, strain bookkeeping)."""
     from sdddst_b200 import capi
     xyb, pd = workloads.dislocations(n, seed, p)
     rp = ref.params(cutoff_multiplier=m, prec=prec, step_size=step, stress_kind=sk, stress_value=sv,
-                    pd_scaling=p > 0)
+                    stress_rate=rate, spring_constant=spring, calculate_strain=strain, pd_scaling=p > 0)
     oracle = ref.Sim(xyb, pd if p else None, rp, "port")
-    prm = capi.cli_params(n, m, prec, step_size=step, p=p, pd_scaling=p > 0, stress_kind=sk, stress_value=sv, **kw)
+    prm = capi.cli_params(n, m, prec, step_size=step, p=p, pd_scaling=p > 0, stress_kind=sk, stress_value=sv,
+                          stress_rate=rate, spring_constant=spring, calculate_strain=int(strain), **kw)
     eng = capi.Engine(prm, xyb, pd if p else None)
     return xyb, pd, oracle, eng
 
 
 def assert_speeds_close(v, v_ref):
+    """1e-10 relative in the max norm (see the module docstring)."""
     scale = np.abs(v_ref).max()
     err = np.abs(v - v_ref)
-    bound = 1e-10 * scale + 1e-9 * np.abs(v_ref)
-    assert np.all(err <= bound), (err.max(), scale, (err / np.maximum(np.abs(v_ref), 1e-300)).max())
+    assert np.all(err <= 1e-10 * scale), (err.max() / scale, scale)
 
 
 @pytest.mark.parametrize("n,seed,m,p,sk,sv", [(256, 0, 0.5, 0, 0, 0.0), (1000, 5, 1.0, 64, 3, 0.01),
@@ -157,11 +165,22 @@ def test_solve_matches_dense(engine_lib, port_lib):
     assert np.abs(x - x_ref).max() <= 1e-13 * cond * np.abs(x_ref).max()
 
 
-def _teacher_forced(n, seed, m, prec, p=0, sk=0, sv=0.0, steps=12, **kw):
+def _teacher_forced(n, seed, m, prec, p=0, sk=0, sv=0.0, steps=12, warm=0, **kw):
+    """`steps` attempts, each started on both sides from the oracle's accepted
+    state.  warm > 0: the engine first runs `warm` attempts alone (the step
+    size leaves the initial transient), and the oracle starts from the
+    engine's state after them."""
     xyb, pd, o, e = make_pair(n, seed, m, prec, p, sk, sv, **kw)
     first = True
     worst = 0.0
     decisions = 0
+    if warm:
+        for _ in range(warm):
+            e.step()
+        sc = e.scalars()
+        o.set_state(e.config(0), sc["step_size"], sc["sim_time"], sc["energy"], sc["strain"], False)
+        first = False
+    accepted = 0
     for k in range(steps):
         x = o.config(0)
         sc = o.scalars()
@@ -175,6 +194,7 @@ def _teacher_forced(n, seed, m, prec, p=0, sk=0, sv=0.0, steps=12, **kw):
         so, se = o.scalars(), e.scalars()
         assert a == a_ref, (k, so, se)
         decisions += 1
+        accepted += a
         for which in (1, 2, 3):
             xr = o.config(which)[:, 0]
             xd = e.config(which)[:, 0]
@@ -184,6 +204,9 @@ def _teacher_forced(n, seed, m, prec, p=0, sk=0, sv=0.0, steps=12, **kw):
         assert np.isclose(se["step_size"], so["step_size"], rtol=1e-6), k
         assert np.isclose(se["energy"], so["energy"], rtol=1e-9, atol=1e-300), k
         assert np.allclose(e.vector(6), o.vector(6), rtol=1e-9, atol=0)
+        assert np.isclose(se["stress"], so["stress"], rtol=1e-12, atol=0), k
+        assert np.isclose(se["strain"], so["strain"], rtol=1e-9, atol=1e-18), k
+    _teacher_forced.accepted = accepted
     return worst, decisions
 
 
@@ -294,3 +317,96 @@ def test_mixed_jacobian_close_to_oracle(engine_lib, port_lib):
     off = ~np.eye(n, dtype=bool)
     assert np.abs(J - Jr)[off].max() <= 2e-5 * np.abs(Jr[off]).max()
     assert np.abs(np.diag(J) - np.diag(Jr)).max() <= 2e-5 * np.abs(np.diag(Jr)).max()
+
+
+def test_step_teacher_forced_config2_scale(engine_lib, port_lib):
+    """The plain-method workload at scale: N=4096 + 256 point defects
+    (seed 1), constant external stress 0.01, cutoff multiplier 1, precision
+    1e-7, device sparse LU.  Five attempts teacher-forced against the oracle
+    after the step size has left the initial transient (12 attempts of the
+    engine alone): stage positions within 1e-10, identical decisions, error
+    ratio, step size and energy as in the smaller cases."""
+    from sdddst_b200 import capi
+    worst, k = _teacher_forced(4096, 1, 1.0, 1e-7, p=256, sk=3, sv=0.01, steps=5, warm=12,
+                               solver=capi.SOLVER_DIRECT)
+    assert k == 5 and _teacher_forced.accepted >= 2, _teacher_forced.accepted
+
+
+def test_step_teacher_forced_config2_gmres(engine_lib, port_lib):
+    """The same workload with the cluster-preconditioned GMRES solver."""
+    worst, k = _teacher_forced(4096, 1, 1.0, 1e-7, p=256, sk=3, sv=0.01, steps=3, warm=12)
+    assert k == 3
+
+
+@pytest.mark.parametrize("sk,rate,spring", [(1, 2.0e4, 1.0), (2, 5.0e5, 20.0)])
+def test_step_teacher_forced_stress_protocols(engine_lib, port_lib, sk, rate, spring):
+    """FixedRateProtocol (fixed_rate_protocol.cpp:39-57: tau = t * rate per
+    stage) and SpringProtocol (spring_protocol.cpp:33-54: tau = k (t rate -
+    strain), clamped at 0, with the strain of the stage's configuration fed
+    back, simulation.cpp:154,180,544) teacher-forced against the oracle with
+    strain bookkeeping on: stage positions, decisions, stress and strain.
+    The rate makes the external stress comparable with the internal stresses
+    within the run."""
+    worst, k = _teacher_forced(600, 13, 1.0, 1e-6, sk=sk, rate=rate, spring=spring, strain=True, steps=10, warm=4)
+    assert k == 10 and _teacher_forced.accepted >= 3
+
+
+def test_free_running_stress_protocols_reach_stress(engine_lib, port_lib):
+    """Free-running fixed-rate and spring runs of 30 attempts against the
+    oracle: the stress of the accepted state grows with the simulated time
+    (spring: by k (t rate - strain)), and the two sides stay together."""
+    from sdddst_b200 import capi
+    for sk, rate, spring in ((1, 2.0e4, 1.0), (2, 5.0e5, 20.0)):
+        xyb, pd, o, e = make_pair(400, 14, 1.0, 1e-6, sk=sk, rate=rate, spring=spring, strain=True)
+        for k in range(30):
+            assert e.step() == o.step(), (sk, k)
+            so, se = o.scalars(), e.scalars()
+            assert np.abs(e.config(0)[:, 0] - o.config(0)[:, 0]).max() <= 1e-9, (sk, k)
+            assert np.isclose(se["stress"], so["stress"], rtol=1e-9, atol=1e-300), (sk, k)
+            assert np.isclose(se["strain"], so["strain"], rtol=1e-7, atol=1e-18), (sk, k)
+        assert se["stress"] > 0.0, (sk, se)
+
+
+def test_order_parameter_matches_oracle(engine_lib, port_lib):
+    """calculateOrderParameter (simulation.cpp:407-415): sum_i b_i v_i of the
+    accepted configuration over the step's speed vector, after teacher-forced
+    steps; the speed vectors themselves within the velocity bar."""
+    xyb, pd, o, e = make_pair(500, 15, 1.0, 1e-6)
+    for k in range(6):
+        x, sc = o.config(0), o.scalars()
+        e.set_state(x, sc["step_size"], sc["sim_time"], sc["energy"], sc["strain"], k == 0)
+        if k:
+            o.set_state(x, sc["step_size"], sc["sim_time"], sc["energy"], sc["strain"], False)
+        assert e.step() == o.step(), k
+        for which in (2, 3):  # speed, speed2
+            assert_speeds_close(e.vector(which), o.vector(which))
+        b = o.config(0)[:, 2]
+        op_ref = float(np.dot(b, o.vector(2)))
+        op = float(np.dot(e.config(0)[:, 2], e.vector(2)))
+        assert abs(op - op_ref) <= 1e-10 * np.abs(b * o.vector(2)).sum(), (k, op, op_ref)
+
+
+def test_jacobian_multiblock_scan_n20001(engine_lib, port_lib):
+    """N = 20001 (above the one-block scan's 16384 entries and not a multiple
+    of its 2048-entry chunks): the row pointers, columns and values of the
+    assembled CSR against the oracle (pattern exact, values 1e-10), and a
+    solve through the preconditioner whose pattern counts use the same
+    multi-block scan."""
+    import scipy.sparse as sp
+    n, h = 20001, 2e-6
+    xyb, pd, o, e = make_pair(n, 17, 1.0, 1e-6)
+    Ap, Ai, Ax, d_ref = o.jacobian(h, xyb)
+    rp, col, val, d = e.jacobian(h, xyb)
+    J = sp.csr_matrix((val, col, rp), shape=(n, n))
+    Jr = sp.csc_matrix((Ax, Ai, Ap), shape=(n, n)).tocsr()
+    pr = Jr.copy()
+    pr.data[:] = 1.0
+    pr = ((pr + pr.T) > 0).astype(np.int8).tocsr()
+    pat = sp.csr_matrix((np.ones(len(col), dtype=np.int8), col, rp), shape=(n, n))
+    assert np.array_equal(np.diff(rp), np.diff(pr.indptr)), "row counts differ"
+    assert (pat != pr).nnz == 0, "sparsity pattern differs"
+    off = sp.triu(abs(Jr), 1)
+    assert abs(J - Jr).max() <= 1e-10 * max(off.max(), 1.0)
+    rhs = np.random.default_rng(3).standard_normal(n) * 1e-4
+    x, iters = e.solve(h, xyb, rhs)
+    assert np.linalg.norm(J @ x - rhs) <= 1e-12 * np.linalg.norm(rhs)

@@ -1,0 +1,64 @@
+"""Parity of the chosen forms at the headline configuration.
+
+N = 32768 dislocations (seed 4), cutoff multiplier 2.0, precision 1e-5,
+initial step 1e-6, zero stress.  The FP64 oracle at this size is the plain GPU
+path (FP64 pair sum, FP64 Jacobian, device sparse LU refined to 1e-13), itself
+checked against the reference's CPU code at smaller sizes (test_gpu_parity,
+test_direct).  The chosen forms are
+
+* mixed: FP32 pair terms with compensated FP64 accumulation, FP32 Jacobian
+  values, FP64 GMRES(30) with the cluster block-Jacobi preconditioner;
+* learned: the same with the learned correction added to the preconditioner.
+
+Teacher forcing (src/simulation.cpp:435-650 per attempt): every attempt
+starts all three engines from the plain path's accepted state and step size;
+the three stage configurations (big step, first and second small step) must
+agree within 1e-8 (the bar of the precision forms) and the accept/reject
+decisions must be identical, for at least three accepted attempts.  The
+decision is exempt only when the plain path's error ratio is within 1e-4 of
+the threshold 1 (the ratio divides a ~1e-6 position difference by a ~1e-12
+tolerance, so a 1e-12 position difference moves it by ~1e-6 relative).
+"""
+import numpy as np
+import pytest
+
+from sdddst_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+N, SEED, M, PREC, H0 = 32768, 4, 2.0, 1e-5, 1e-6
+
+
+def _engines():
+    from sdddst_b200 import capi
+    xyb, _ = workloads.dislocations(N, SEED)
+    mk = lambda ps, sv: capi.Engine(capi.cli_params(N, M, PREC, step_size=H0, pairsum=ps, solver=sv), xyb)
+    plain = mk(capi.PAIRSUM_FP64, capi.SOLVER_DIRECT)
+    mixed = mk(capi.PAIRSUM_FP32, capi.SOLVER_GMRES_CLUSTER)
+    learned = mk(capi.PAIRSUM_FP32, capi.SOLVER_GMRES_LEARNED)
+    learned.set_preconditioner_weights()
+    return plain, {"mixed": mixed, "learned": learned}
+
+
+def test_headline_forms_against_plain_fp64_teacher_forced(engine_lib):
+    plain, forms = _engines()
+    accepted = attempts = 0
+    worst = {k: 0.0 for k in forms}
+    while accepted < 3 and attempts < 16:
+        x, sc = plain.config(0), plain.scalars()
+        for e in (plain, *forms.values()):
+            e.set_state(x, sc["step_size"], sc["sim_time"], sc["energy"], sc["strain"], False)
+        a_plain = plain.step()
+        ratio = plain.scalars()["max_error_ratio_sqr"]
+        for name, e in forms.items():
+            a = e.step()
+            if abs(ratio - 1.0) > 1e-4:
+                assert a == a_plain, (name, attempts, ratio, e.scalars()["max_error_ratio_sqr"])
+            for which in (1, 2, 3):
+                d = float(np.abs(e.config(which)[:, 0] - plain.config(which)[:, 0]).max())
+                worst[name] = max(worst[name], d)
+                assert d <= 1e-8, (name, attempts, which, d)
+        attempts += 1
+        accepted += a_plain
+    assert accepted >= 3, (accepted, attempts)
+    print("max |dx| against the plain FP64 path:", worst)
