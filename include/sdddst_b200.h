@@ -259,13 +259,17 @@ int sdddst_speeds_noalloc(int n, const double *x_device, const double *y_device,
  * total Krylov iterations. */
 int sdddst_solver_stats(void *ctx, long *solves, long *iterations);
 
-/* Recoveries from stalled solves (GMRES past max_iters) in this context:
- * rebuilds counts cluster-preconditioner rebuilds with a five times lower
- * coupling threshold (SDDDST_SOLVER_GMRES_CLUSTER, at most two per solve
- * before SDDDST_ERR_SOLVER), fallbacks counts learned- or analytic-corrected
- * solves redone by the sparse LU (the reference has neither: its UMFPACK
- * status is ignored, simulation.cpp:388-395). */
-int sdddst_solver_recoveries(void *ctx, long *rebuilds, long *fallbacks);
+/* Recoveries in this context (each pointer optional): rebuilds counts
+ * cluster-preconditioner rebuilds with a five times lower coupling threshold
+ * after a stalled solve (GMRES past max_iters; SDDDST_SOLVER_GMRES_CLUSTER,
+ * at most two per solve before SDDDST_ERR_SOLVER), fallbacks counts
+ * learned- or analytic-corrected solves redone by the sparse LU, and redone
+ * counts step attempts of the cluster solver that ran without waiting for the
+ * device, failed a deferred check (a stalled solve, a pattern larger than the
+ * Jacobian storage) and were repeated with a wait at every check.  The
+ * reference has none of these: its UMFPACK status is ignored
+ * (simulation.cpp:388-395). */
+int sdddst_solver_recoveries(void *ctx, long *rebuilds, long *fallbacks, long *redone);
 
 /* Sparse LU statistics of this context (SDDDST_SOLVER_DIRECT; zeros
  * otherwise): factorizations performed, pivots perturbed, FP64 flops of one
@@ -326,6 +330,14 @@ int sdddst_batch_get_positions(void *batch, int which, double *x);
 /* Pair-sum tile chosen by the autotuner, total dislocations, kernels launched
  * so far and the batch's cudaStream_t (each pointer optional). */
 int sdddst_batch_info(void *batch, int *tile, long *total, long *launches, void **stream);
+
+/* How the batch steps (each pointer optional): *graph = 1 when its steps
+ * after the first replay one captured CUDA graph (no host round trip until
+ * the step's end), 0 when they are enqueued directly or host-driven;
+ * *redone counts steps whose deferred checks failed (a stalled solve, a
+ * pattern larger than the Jacobian storage, a non-finite error ratio) and
+ * were repeated host-driven from the step's snapshot. */
+int sdddst_batch_stats(void *batch, int *graph, long *redone);
 
 /* Launch statistics: number of kernels this context has launched so far. */
 long sdddst_kernel_launches(void *ctx);

@@ -40,7 +40,7 @@ EXPORTS = [
     "sdddst_update_params", "sdddst_solve_csc", "sdddst_batch_create", "sdddst_batch_destroy",
     "sdddst_batch_step", "sdddst_batch_get_scalars", "sdddst_batch_get_positions", "sdddst_batch_info",
     "sdddst_direct_stats", "sdddst_profile_direct", "sdddst_precond_apply", "sdddst_set_preconditioner_weights",
-    "sdddst_learned_correction", "sdddst_solver_recoveries",
+    "sdddst_learned_correction", "sdddst_solver_recoveries", "sdddst_batch_stats",
 ]
 
 
@@ -109,7 +109,9 @@ def load(path: str = LIB_PATH):
     lib.sdddst_batch_info.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_long), C.POINTER(C.c_long),
                                       C.POINTER(C.c_void_p)]
     lib.sdddst_solver_stats.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long)]
-    lib.sdddst_solver_recoveries.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long)]
+    lib.sdddst_batch_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_long)]
+    lib.sdddst_solver_recoveries.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long),
+                                             C.POINTER(C.c_long)]
     lib.sdddst_profile_pair_sum.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
     lib.sdddst_vector_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.sdddst_direct_stats.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long),
@@ -303,10 +305,10 @@ class Engine:
         return a.value, b.value
 
     def solver_recoveries(self):
-        """(preconditioner rebuilds, sparse-LU fallbacks) after stalled solves."""
-        a, b = C.c_long(0), C.c_long(0)
-        _check(self.lib.sdddst_solver_recoveries(self.h, C.byref(a), C.byref(b)))
-        return a.value, b.value
+        """(preconditioner rebuilds, sparse-LU fallbacks, redone attempts)."""
+        a, b, c = C.c_long(0), C.c_long(0), C.c_long(0)
+        _check(self.lib.sdddst_solver_recoveries(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
 
     def update_params(self, **kw):
         """Changes mutable parameters of the live context (sdddst_update_params)."""
@@ -402,6 +404,13 @@ class Batch:
         x = np.zeros(int(self.offsets[-1]))
         _check(self.lib.sdddst_batch_get_positions(self.h, which, x))
         return [x[self.offsets[k]:self.offsets[k + 1]] for k in range(self.count)]
+
+    def stats(self):
+        """{"graph": 1 when steps replay a captured CUDA graph, "redone": steps
+        repeated host-driven after a failed deferred check}."""
+        g, r = C.c_int(0), C.c_long(0)
+        _check(self.lib.sdddst_batch_stats(self.h, C.byref(g), C.byref(r)))
+        return {"graph": g.value, "redone": r.value}
 
     def info(self):
         t, n, l, s = C.c_int(0), C.c_long(0), C.c_long(0), C.c_void_p()

@@ -17,6 +17,17 @@
 //     own step size (src/simulation.cpp:501-650 per system).
 // The tile size is chosen at creation by timing the pair sum with 32, 64
 // and 128 (the autotuner).
+//
+// After the first step, a step runs with no host round trip and is captured
+// once in a CUDA graph, then replayed: the per-system state (step size,
+// time, energy, counters, error ratio, speed sums) lives on the device, the
+// accept/reject decisions and step-size updates are kernels, the solves are
+// the device-resident GMRES, and the assemblies, preconditioner builds and
+// solves leave their checks on the device.  One copy after the replay
+// brings back the accept flags and the checks; when a check failed (a
+// stalled solve, a pattern larger than the CSR storage, a non-finite ratio)
+// the step's snapshot is restored and the step is redone by the host-driven
+// path, which waits at every check.
 #include "engine.h"
 #include "pair_tile.cuh"
 
@@ -47,30 +58,55 @@ struct Batch {
     std::vector<int> accepted;
     bool first = true;
     double *h_seg = nullptr; // pinned, B doubles
+    // device-resident stepping: per-system state rows (kState x B doubles),
+    // its snapshot and those of x0, v0 and the tolerances, the checks of a
+    // step, the captured graph
+    double *d_state = nullptr, *d_state_snap = nullptr, *d_x0_snap = nullptr, *d_v0_snap = nullptr;
+    double *d_tol_snap = nullptr;
+    int *d_check = nullptr;   // [0..2*3) assembly guards, [6..12) preconditioner flags and block counts,
+                              // [12] non-finite ratio
+    int *h_check = nullptr;   // pinned: checks then accept flags
+    bool dev_master = false;  // the device state rows hold the current per-system state
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    bool graph_failed = false; // capture or instantiation refused: the step is enqueued directly
+    long graph_launches = 0;   // kernels one replay launches
+    long redone = 0;           // steps redone by the host-driven path
     ~Batch();
 };
+
+// rows of Batch::d_state
+enum { kSH = 0, kST, kSEnergy, kSRatio, kSVsq1, kSVsq2, kSVsq, kSAvg, kSSucc, kSFailed, kState };
 
 Batch::~Batch()
 {
     cudaSetDevice(e.device);
-    void *bufs[] = {d_inst, d_off, d_tiles, d_partoff, d_bpart, d_hinst, d_cut, d_seg, d_scale, d_G,
-                    d_celloff, d_acc, b_cell, b_count, b_start, b_fill, b_sorted, e.d_hrow};
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    void *bufs[] = {d_inst, d_off, d_tiles, d_partoff, d_bpart, d_cut, d_seg, d_scale, d_G,
+                    d_celloff, d_acc, b_cell, b_count, b_start, b_fill, b_sorted, e.d_hrow, d_state,
+                    d_state_snap, d_x0_snap, d_v0_snap, d_tol_snap, d_check};
     for (void *p : bufs)
         if (p) cudaFree(p);
     e.d_hrow = nullptr;
     if (h_seg) cudaFreeHost(h_seg);
+    if (h_check) cudaFreeHost(h_check);
 }
 
 // ---------------------------------------------------------------- kernels
 
+// only: when not null, systems with only[k] == 0 are skipped (their slabs
+// keep their contents)
 template <int T, int kMode>
 __global__ void __launch_bounds__(T) batch_pair_kernel(const int *__restrict__ tiles, const int *__restrict__ off,
                                                        const long long *__restrict__ partoff,
                                                        const double *__restrict__ x, const double *__restrict__ y,
                                                        const double *__restrict__ b, double *__restrict__ part,
-                                                       unsigned long long *__restrict__ minr2, double r2_track)
+                                                       unsigned long long *__restrict__ minr2, double r2_track,
+                                                       const int *__restrict__ only)
 {
     const int k = tiles[3 * blockIdx.x], I = tiles[3 * blockIdx.x + 1], J = tiles[3 * blockIdx.x + 2];
+    if (only && !only[k]) return;
     const int base = off[k], n = off[k + 1] - base;
     if (kMode == 0)
         pair_tile_f64<T>(x + base, y + base, b + base, n, I, J, part + partoff[k], minr2 + base, r2_track);
@@ -82,11 +118,13 @@ __global__ void batch_finish_kernel(long ntot, int T, const int *__restrict__ in
                                     const long long *__restrict__ partoff, const double *__restrict__ part,
                                     const double *__restrict__ b, double tau_ext, double *__restrict__ S,
                                     double *__restrict__ v, const unsigned long long *__restrict__ minr2,
-                                    double *__restrict__ tol, double prec_sqr, int update_tol)
+                                    double *__restrict__ tol, double prec_sqr, int update_tol,
+                                    const int *__restrict__ only)
 {
     const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (i >= ntot) return;
     const int k = inst[i];
+    if (only && !only[k]) return;
     const int base = off[k], n = off[k + 1] - base, il = (int)(i - base);
     const int nblk = (n + T - 1) / T;
     const double *pk = part + partoff[k];
@@ -199,7 +237,7 @@ __global__ void batch_row_fill_kernel(long ntot, const int *__restrict__ inst, c
                                       const double *__restrict__ cut, const int *__restrict__ start,
                                       const int *__restrict__ sorted, const int *__restrict__ rowptr,
                                       int *__restrict__ col, VT *__restrict__ val, double *__restrict__ gdiag,
-                                      int *__restrict__ flag, int *__restrict__ col_s)
+                                      int *__restrict__ flag, int *__restrict__ col_s, long cap)
 {
     const long gw = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -208,6 +246,10 @@ __global__ void batch_row_fill_kernel(long ntot, const int *__restrict__ inst, c
     const int k = inst[i];
     const double c = cut[3 * k], c2 = cut[3 * k + 1], ic2 = cut[3 * k + 2];
     const int base = rowptr[i], rowend = rowptr[i + 1];
+    if ((long)rowend > cap) { // the pattern outgrew the CSR storage: report, write nothing
+        if (lane == 0) atomicExch(flag, 2);
+        return;
+    }
     int pos = base + 1;
     batch_cells_around(k, x[i], y[i], G, celloff, [&](int cell) {
         const int s = start[cell], e = start[cell + 1];
@@ -315,6 +357,49 @@ __global__ void batch_accept_copy_kernel(long ntot, const int *__restrict__ inst
     if (i < ntot && acc[inst[i]]) dst[i] = src[i];
 }
 
+// Accept/reject of every system (simulation.cpp:516): acc = ratio < 1; a
+// non-finite ratio is reported in check[0].
+__global__ void batch_decide_kernel(int B, const double *__restrict__ state, int *__restrict__ acc,
+                                    int *__restrict__ check)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= B) return;
+    const double r = state[kSRatio * B + k];
+    if (!isfinite(r)) atomicExch(check, 1);
+    acc[k] = r < 1.0 ? 1 : 0;
+}
+
+// Bookkeeping of every system after its decision (simulation.cpp:501-650)
+// and PrecisionHandler::getNewStepSize (precision_handler.cpp:103-119): time,
+// counters, energy, <|v|>, new step size.  avg_sum: sum |v0| at the (new)
+// accepted configuration.
+__global__ void batch_update_kernel(int B, const int *__restrict__ off, const int *__restrict__ acc,
+                                    const double *__restrict__ avg_sum, double *__restrict__ state,
+                                    int max_step_limited, double max_step)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= B) return;
+    double *h = state + kSH * B, *t = state + kST * B, *en = state + kSEnergy * B;
+    const double hk = h[k];
+    const double vsq1 = state[kSVsq1 * B + k], vsq2 = state[kSVsq2 * B + k], vsq = state[kSVsq * B + k];
+    double eacc = (vsq1 + vsq2) * 0.5 * hk * 0.5;
+    if (acc[k]) {
+        t[k] += hk;
+        state[kSSucc * B + k] += 1.0;
+        eacc += (vsq2 + vsq) * 0.5 * hk * 0.5;
+        en[k] += eacc;
+        state[kSAvg * B + k] = avg_sum[k] / double(off[k + 1] - off[k]);
+    } else {
+        state[kSFailed * B + k] += 1.0;
+    }
+    const double r = state[kSRatio * B + k];
+    double hn;
+    if (r == 0.0) hn = 2.0 * hk;
+    else hn = 0.9 * hk * fmin(2.0, pow(1. / sqrt(r), 1. / 3.));
+    if (max_step_limited && max_step < hn) hn = max_step;
+    h[k] = hn;
+}
+
 // ------------------------------------------------------------ host side
 
 static unsigned nblocks(long n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -335,7 +420,7 @@ static void batch_tiles(Batch &bt, int T, std::vector<int> &tiles, std::vector<l
     }
 }
 
-static void launch_batch_pair(Batch &bt, const double *x, double r2_track)
+static void launch_batch_pair(Batch &bt, const double *x, double r2_track, const int *only = nullptr)
 {
     Engine &e = bt.e;
     cudaStream_t st = e.st;
@@ -351,10 +436,10 @@ static void launch_batch_pair(Batch &bt, const double *x, double r2_track)
 #define SD_BATCH_LAUNCH(TT)                                                                                       \
     if (mode == 0)                                                                                                \
         batch_pair_kernel<TT, 0><<<g, TT, 0, st>>>(bt.d_tiles, bt.d_off, bt.d_partoff, xin, e.d_y, e.d_b,         \
-                                                   bt.d_bpart, e.d_minr2, r2_track);                              \
+                                                   bt.d_bpart, e.d_minr2, r2_track, only);                        \
     else                                                                                                          \
         batch_pair_kernel<TT, 1><<<g, TT, 0, st>>>(bt.d_tiles, bt.d_off, bt.d_partoff, xin, e.d_y, e.d_b,         \
-                                                   bt.d_bpart, e.d_minr2, r2_track);
+                                                   bt.d_bpart, e.d_minr2, r2_track, only);
     if (bt.T == 32) {
         SD_BATCH_LAUNCH(32)
     } else if (bt.T == 128) {
@@ -366,14 +451,15 @@ static void launch_batch_pair(Batch &bt, const double *x, double r2_track)
     e.launches++;
 }
 
-static void batch_speeds(Batch &bt, const double *x, double *v, double *S, bool update_tol)
+static void batch_speeds(Batch &bt, const double *x, double *v, double *S, bool update_tol,
+                         const int *only = nullptr)
 {
     Engine &e = bt.e;
     const double r2_track = update_tol ? 400.0 * e.prec * e.prec * (1.0 + 1e-9) : 0.0;
-    launch_batch_pair(bt, x, r2_track);
+    launch_batch_pair(bt, x, r2_track, only);
     batch_finish_kernel<<<nblocks(bt.ntot, 256), 256, 0, e.st>>>(bt.ntot, bt.T, bt.d_inst, bt.d_off, bt.d_partoff,
                                                                  bt.d_bpart, e.d_b, 0.0, S, v, e.d_minr2, e.d_tol,
-                                                                 e.prec * e.prec, update_tol ? 1 : 0);
+                                                                 e.prec * e.prec, update_tol ? 1 : 0, only);
     e.launches++;
 }
 
@@ -410,11 +496,11 @@ static int batch_assemble(Batch &bt, const double *x)
     if (e.valf)
         batch_row_fill_kernel<float><<<nblocks(n * 32, 256), 256, 0, st>>>(
             n, bt.d_inst, x, e.d_y, e.d_b, bt.d_G, bt.d_celloff, bt.d_cut, bt.b_start, bt.b_sorted, e.d_rowptr,
-            e.d_col, e.d_valf, e.d_gdiag, e.d_flag, e.d_col_s);
+            e.d_col, e.d_valf, e.d_gdiag, e.d_flag, e.d_col_s, e.nnz_cap);
     else
         batch_row_fill_kernel<double><<<nblocks(n * 32, 256), 256, 0, st>>>(
             n, bt.d_inst, x, e.d_y, e.d_b, bt.d_G, bt.d_celloff, bt.d_cut, bt.b_start, bt.b_sorted, e.d_rowptr,
-            e.d_col, e.d_val, e.d_gdiag, e.d_flag, e.d_col_s);
+            e.d_col, e.d_val, e.d_gdiag, e.d_flag, e.d_col_s, e.nnz_cap);
     e.launches++;
     int flag = 0;
     cudaMemcpyAsync(&flag, e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -485,7 +571,7 @@ static int batch_integrate(Batch &bt, double factor, double *xn, const double *x
     return 0;
 }
 
-static int batch_step(Batch &bt, int *accepted_out)
+static int batch_step_host(Batch &bt, int *accepted_out)
 {
     Engine &e = bt.e;
     cudaStream_t st = e.st;
@@ -516,12 +602,13 @@ static int batch_step(Batch &bt, int *accepted_out)
     cudaMemcpyAsync(bt.d_acc, bt.accepted.data(), sizeof(int) * bt.B, cudaMemcpyHostToDevice, st);
     batch_accept_copy_kernel<<<nblocks(bt.ntot, 256), 256, 0, st>>>(bt.ntot, bt.d_inst, bt.d_acc, e.d_x2, e.d_x0);
     e.launches++;
+    std::vector<double> abs_sum(bt.B, 0.0);
     if (nacc > 0) {
-        // velocities at the new configurations; rejected systems keep x0, so
-        // their v0 is recomputed unchanged
-        batch_speeds(bt, e.d_x0, e.d_v0, nullptr, false);
+        // velocities at the accepted systems' new configurations (the
+        // rejected keep x0 and v0)
+        batch_speeds(bt, e.d_x0, e.d_v0, nullptr, false, bt.d_acc);
         if (int rc = batch_seg(bt, 0, e.d_v0, nullptr, nullptr, bt.vsq)) return rc;
-        if (int rc = batch_seg(bt, 1, e.d_v0, nullptr, nullptr, bt.avg)) return rc;
+        if (int rc = batch_seg(bt, 1, e.d_v0, nullptr, nullptr, abs_sum)) return rc;
     }
     for (int k = 0; k < bt.B; ++k) {
         const double hk = bt.h[k];
@@ -531,7 +618,7 @@ static int batch_step(Batch &bt, int *accepted_out)
             bt.succ[k]++;
             eacc += (bt.vsq2[k] + bt.vsq[k]) * 0.5 * hk * 0.5;
             bt.energy[k] += eacc;
-            bt.avg[k] = bt.avg[k] / double(bt.nk[k]);
+            bt.avg[k] = abs_sum[k] / double(bt.nk[k]);
         } else {
             bt.failed[k]++;
         }
@@ -548,6 +635,270 @@ static int batch_step(Batch &bt, int *accepted_out)
     cudaMemcpyAsync(e.d_tol, t0.data(), bytes, cudaMemcpyHostToDevice, st);
     if (accepted_out) std::copy(bt.accepted.begin(), bt.accepted.end(), accepted_out);
     return e.sync_check("batch step");
+}
+
+// ---- device-resident stepping
+
+// per-system state rows <-> the host vectors of the host-driven path
+static void state_to_device(Batch &bt)
+{
+    const int B = bt.B;
+    std::vector<double> st((size_t)kState * B);
+    for (int k = 0; k < B; ++k) {
+        st[kSH * B + k] = bt.h[k];
+        st[kST * B + k] = bt.t[k];
+        st[kSEnergy * B + k] = bt.energy[k];
+        st[kSRatio * B + k] = bt.ratio[k];
+        st[kSVsq1 * B + k] = bt.vsq1[k];
+        st[kSVsq2 * B + k] = bt.vsq2[k];
+        st[kSVsq * B + k] = bt.vsq[k];
+        st[kSAvg * B + k] = bt.avg[k];
+        st[kSSucc * B + k] = (double)bt.succ[k];
+        st[kSFailed * B + k] = (double)bt.failed[k];
+    }
+    cudaMemcpyAsync(bt.d_state, st.data(), sizeof(double) * st.size(), cudaMemcpyHostToDevice, bt.e.st);
+    cudaStreamSynchronize(bt.e.st);
+}
+
+static int state_to_host(Batch &bt)
+{
+    const int B = bt.B;
+    std::vector<double> st((size_t)kState * B);
+    cudaMemcpyAsync(st.data(), bt.d_state, sizeof(double) * st.size(), cudaMemcpyDeviceToHost, bt.e.st);
+    if (int rc = bt.e.sync_check("batch state")) return rc;
+    for (int k = 0; k < B; ++k) {
+        bt.h[k] = st[kSH * B + k];
+        bt.t[k] = st[kST * B + k];
+        bt.energy[k] = st[kSEnergy * B + k];
+        bt.ratio[k] = st[kSRatio * B + k];
+        bt.vsq1[k] = st[kSVsq1 * B + k];
+        bt.vsq2[k] = st[kSVsq2 * B + k];
+        bt.vsq[k] = st[kSVsq * B + k];
+        bt.avg[k] = st[kSAvg * B + k];
+        bt.succ[k] = (long)st[kSSucc * B + k];
+        bt.failed[k] = (long)st[kSFailed * B + k];
+    }
+    return 0;
+}
+
+// The assembly without waits: counts, scan, fill bounded by the storage,
+// the guard recording the entry total and the fill flag at check[2 slot].
+static void batch_assemble_dev(Batch &bt, const double *x, int slot)
+{
+    Engine &e = bt.e;
+    cudaStream_t st = e.st;
+    const long n = bt.ntot;
+    cudaMemsetAsync(bt.b_count, 0, sizeof(int) * (bt.ncell_tot + 1), st);
+    cudaMemsetAsync(bt.b_fill, 0, sizeof(int) * (bt.ncell_tot + 1), st);
+    batch_cell_assign_kernel<<<nblocks(n, 256), 256, 0, st>>>(n, bt.d_inst, x, e.d_y, bt.d_G, bt.d_celloff, bt.b_cell,
+                                                              bt.b_count);
+    scan_kernel<<<1, 1024, 0, st>>>(bt.b_count, bt.ncell_tot, bt.b_start);
+    cell_scatter_kernel<<<nblocks(n, 256), 256, 0, st>>>((int)n, bt.b_cell, bt.b_start, bt.b_fill, e.d_rowcnt);
+    cell_sort_kernel<<<bt.ncell_tot, 256, 0, st>>>(bt.b_start, e.d_rowcnt, bt.b_sorted);
+    batch_row_count_kernel<<<nblocks(n * 32, 256), 256, 0, st>>>(n, bt.d_inst, x, e.d_y, bt.d_G, bt.d_celloff,
+                                                                 bt.d_cut, bt.b_start, bt.b_sorted, e.d_rowcnt);
+    e.launches += launch_scan(e, e.d_rowcnt, (int)n, e.d_rowptr, st) - 1;
+    e.launches += 6;
+    cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
+    if (e.valf)
+        batch_row_fill_kernel<float><<<nblocks(n * 32, 256), 256, 0, st>>>(
+            n, bt.d_inst, x, e.d_y, e.d_b, bt.d_G, bt.d_celloff, bt.d_cut, bt.b_start, bt.b_sorted, e.d_rowptr,
+            e.d_col, e.d_valf, e.d_gdiag, e.d_flag, e.d_col_s, e.nnz_cap);
+    else
+        batch_row_fill_kernel<double><<<nblocks(n * 32, 256), 256, 0, st>>>(
+            n, bt.d_inst, x, e.d_y, e.d_b, bt.d_G, bt.d_celloff, bt.d_cut, bt.b_start, bt.b_sorted, e.d_rowptr,
+            e.d_col, e.d_val, e.d_gdiag, e.d_flag, e.d_col_s, e.nnz_cap);
+    e.launches++;
+    launch_csr_guard(e, bt.d_check + 2 * slot);
+    e.col_s_valid = true;
+    e.col_s16_valid = false;
+    e.spmv_sorted = bt.b_sorted;
+}
+
+// batch_integrate without waits: the solves are the device-resident GMRES
+// with deferred statuses (slots slot * ic + it), the preconditioner's flag
+// and block count go to check[6 + 2 slot].
+static int batch_integrate_dev(Batch &bt, double factor, double *xn, const double *xo, bool use2, bool init_speed,
+                               bool reuse, int slot)
+{
+    Engine &e = bt.e;
+    cudaStream_t st = e.st;
+    set_hrow(bt, factor);
+    if (!reuse) batch_assemble_dev(bt, xn, slot);
+    launch_make_dvec(e, 0.0, e.d_dvec, st);
+    e.launches++;
+    if (int rc = precond_build(e, e.pc, 0.0, e.d_dvec, false)) return rc;
+    cudaMemcpyAsync(bt.d_check + 6 + 2 * slot, e.pc.flag, sizeof(int), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(bt.d_check + 7 + 2 * slot, e.pc.bbase + bt.ntot, sizeof(int), cudaMemcpyDeviceToDevice, st);
+    double *isp = use2 ? e.d_v0b : e.d_v0, *csp0 = use2 ? e.d_vs2 : e.d_vs;
+    for (int it = 0; it < e.ic; ++it) {
+        if (it == 0 && init_speed) batch_speeds(bt, xo, isp, nullptr, true);
+        double *csp = csp0;
+        if (it == 0) csp = isp;
+        else batch_speeds(bt, xn, csp, nullptr, true);
+        launch_residual_g(e, 0.0, xn, xo, csp, isp, e.d_dvec, e.d_g, st);
+        batch_seg_kernel<3><<<bt.B, 256, 0, st>>>(bt.d_off, e.d_g, nullptr, nullptr, bt.d_scale);
+        batch_scale_kernel<<<nblocks(bt.ntot, 256), 256, 0, st>>>(bt.ntot, bt.d_inst, bt.d_scale, e.d_g, 0);
+        e.launches += 3;
+        const double h0 = 0.0;
+        const double *dv = e.d_dvec, *rhs = e.d_g;
+        double *xs = e.d_sol;
+        const Cluster *pcs[1] = {&e.pc};
+        if (int rc = fused_gmres(e, 1, &h0, &dv, &rhs, &xs, pcs, nullptr, true, slot * e.ic + it)) return rc;
+        batch_scale_kernel<<<nblocks(bt.ntot, 256), 256, 0, st>>>(bt.ntot, bt.d_inst, bt.d_scale, e.d_sol, 1);
+        launch_axpy_update(e, xn, e.d_sol, st);
+        e.launches += 2;
+    }
+    return 0;
+}
+
+// One whole step of every system, enqueued with no host round trip (the body
+// of the captured graph): snapshot, the three stages, reductions, decisions,
+// accepted configurations, their speeds, bookkeeping, tolerance reset.
+static int batch_enqueue_step(Batch &bt)
+{
+    Engine &e = bt.e;
+    cudaStream_t st = e.st;
+    const size_t bytes = sizeof(double) * bt.ntot;
+    const int B = bt.B;
+    cudaMemcpyAsync(bt.d_state_snap, bt.d_state, sizeof(double) * kState * B, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(bt.d_x0_snap, e.d_x0, bytes, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(bt.d_v0_snap, e.d_v0, bytes, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(bt.d_tol_snap, e.d_tol, bytes, cudaMemcpyDeviceToDevice, st);
+    cudaMemsetAsync(bt.d_check, 0, sizeof(int) * 16, st);
+    cudaMemcpyAsync(e.d_xb, e.d_x0, bytes, cudaMemcpyDeviceToDevice, st);
+    if (int rc = batch_integrate_dev(bt, 1.0, e.d_xb, e.d_x0, false, false, false, 0)) return rc;
+    cudaMemcpyAsync(e.d_x1, e.d_x0, bytes, cudaMemcpyDeviceToDevice, st);
+    if (int rc = batch_integrate_dev(bt, 0.5, e.d_x1, e.d_x0, false, false, true, 1)) return rc;
+    cudaMemcpyAsync(e.d_x2, e.d_x1, bytes, cudaMemcpyDeviceToDevice, st);
+    if (int rc = batch_integrate_dev(bt, 0.5, e.d_x2, e.d_x1, true, true, false, 2)) return rc;
+    batch_seg_kernel<0><<<B, 256, 0, st>>>(bt.d_off, e.d_v0, nullptr, nullptr, bt.d_state + kSVsq1 * B);
+    batch_seg_kernel<0><<<B, 256, 0, st>>>(bt.d_off, e.d_v0b, nullptr, nullptr, bt.d_state + kSVsq2 * B);
+    batch_seg_kernel<2><<<B, 256, 0, st>>>(bt.d_off, e.d_xb, e.d_tol, e.d_x2, bt.d_state + kSRatio * B);
+    batch_decide_kernel<<<nblocks(B, 128), 128, 0, st>>>(B, bt.d_state, bt.d_acc, bt.d_check + 12);
+    batch_accept_copy_kernel<<<nblocks(bt.ntot, 256), 256, 0, st>>>(bt.ntot, bt.d_inst, bt.d_acc, e.d_x2, e.d_x0);
+    // speeds at the accepted systems' new configurations (the rejected keep x0 and v0)
+    batch_speeds(bt, e.d_x0, e.d_v0, nullptr, false, bt.d_acc);
+    batch_seg_kernel<0><<<B, 256, 0, st>>>(bt.d_off, e.d_v0, nullptr, nullptr, bt.d_state + kSVsq * B);
+    batch_seg_kernel<1><<<B, 256, 0, st>>>(bt.d_off, e.d_v0, nullptr, nullptr, bt.d_seg);
+    batch_update_kernel<<<nblocks(B, 128), 128, 0, st>>>(B, bt.d_off, bt.d_acc, bt.d_seg, bt.d_state,
+                                                         e.prm.max_step_limited, e.prm.max_step);
+    cudaMemcpyAsync(e.d_tol_last, e.d_tol, bytes, cudaMemcpyDeviceToDevice, st);
+    launch_fill(e, e.d_tol, e.prec * e.prec);
+    e.launches += 9;
+    return 0;
+}
+
+// Restores the step's snapshot (per-system state, x0, v0, tolerances).
+static void batch_restore(Batch &bt)
+{
+    Engine &e = bt.e;
+    const size_t bytes = sizeof(double) * bt.ntot;
+    cudaMemcpyAsync(bt.d_state, bt.d_state_snap, sizeof(double) * kState * bt.B, cudaMemcpyDeviceToDevice, e.st);
+    cudaMemcpyAsync(e.d_x0, bt.d_x0_snap, bytes, cudaMemcpyDeviceToDevice, e.st);
+    cudaMemcpyAsync(e.d_v0, bt.d_v0_snap, bytes, cudaMemcpyDeviceToDevice, e.st);
+    cudaMemcpyAsync(e.d_tol, bt.d_tol_snap, bytes, cudaMemcpyDeviceToDevice, e.st);
+}
+
+// One step: the first (and any after a failed check) host-driven; the others
+// as a replay of the captured step (or enqueued directly where capture is
+// refused), one copy of the checks and accept flags, one wait.
+static int batch_step(Batch &bt, int *accepted_out)
+{
+    Engine &e = bt.e;
+    cudaStream_t st = e.st;
+    const bool device_path = !bt.first && e.fused && fused_supported(e) && e.ic <= 2;
+    if (!device_path) {
+        if (bt.dev_master) {
+            if (int rc = state_to_host(bt)) return rc;
+            bt.dev_master = false;
+        }
+        return batch_step_host(bt, accepted_out);
+    }
+    if (!bt.dev_master) {
+        state_to_device(bt);
+        bt.dev_master = true;
+    }
+    if (int rc = fused_alloc(e, 1)) {
+        e.err = "fused solve: allocation failed";
+        return rc;
+    }
+    if (!bt.gexec && !bt.graph_failed) {
+        const long l0 = e.launches;
+        bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        int rc = ok ? batch_enqueue_step(bt) : 0;
+        cudaGraph_t g = nullptr;
+        const bool ended = ok && cudaStreamEndCapture(st, &g) == cudaSuccess && g;
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ended && cudaGraphInstantiate(&bt.gexec, g, 0) == cudaSuccess) {
+            bt.graph = g;
+            bt.graph_launches = e.launches - l0;
+            e.launches = l0;
+        } else {
+            if (g) cudaGraphDestroy(g);
+            bt.gexec = nullptr;
+            bt.graph_failed = true;
+            e.launches = l0;
+        }
+        (void)cudaGetLastError();
+    }
+    if (bt.gexec) {
+        if (cudaGraphLaunch(bt.gexec, st) != cudaSuccess) {
+            e.err = "batch: graph launch failed";
+            return SDDDST_ERR_CUDA;
+        }
+        e.launches += bt.graph_launches;
+    } else {
+        if (int rc = batch_enqueue_step(bt)) return rc;
+    }
+    const int B = bt.B;
+    cudaMemcpyAsync(bt.h_check, bt.d_check, sizeof(int) * 16, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(bt.h_check + 16, bt.d_acc, sizeof(int) * B, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(e.h_fstatus, e.d_fstatus, sizeof(double) * 4 * 3 * e.ic, cudaMemcpyDeviceToHost, st);
+    if (int rc = e.sync_check("batch step")) return rc;
+    const int *ck = bt.h_check;
+    bool ok = ck[12] == 0;
+    int grow = 0;
+    for (int a = 0; a < 3; ++a) {
+        if (a == 1) continue; // stage II reuses stage I's assembly
+        if (ck[2 * a + 1] == 1) {
+            e.err = "batch jacobian: count and fill passes disagree";
+            return SDDDST_ERR_CAPACITY;
+        }
+        if (ck[2 * a + 1] == 2) {
+            ok = false;
+            grow = std::max(grow, ck[2 * a]);
+        }
+    }
+    for (int b = 0; b < 3 && ok; ++b)
+        if (ck[6 + 2 * b] != 0 || ck[7 + 2 * b] <= 0 || ck[7 + 2 * b] > bt.ntot) ok = false;
+    long its = 0;
+    for (int q = 0; q < 3 * e.ic && ok; ++q) {
+        const double *sq = e.h_fstatus + 4 * q;
+        if (sq[1] == 0.0 || sq[3] != 0.0) ok = false;
+        its += (long)sq[0];
+    }
+    if (!ok) {
+        // a deferred check failed: the snapshot back, the step host-driven
+        bt.redone++;
+        batch_restore(bt);
+        if (int rc = state_to_host(bt)) return rc;
+        bt.dev_master = false;
+        if (grow > 0) { // the storage grows: the captured graph holds the old buffers
+            if (bt.gexec) cudaGraphExecDestroy(bt.gexec);
+            if (bt.graph) cudaGraphDestroy(bt.graph);
+            bt.gexec = nullptr;
+            bt.graph = nullptr;
+        }
+        return batch_step_host(bt, accepted_out);
+    }
+    e.solves += 3 * e.ic;
+    e.iterations += its;
+    if (accepted_out) std::copy(bt.h_check + 16, bt.h_check + 16 + B, accepted_out);
+    return 0;
 }
 
 static double time_pair(Batch &bt, int T)
@@ -644,7 +995,13 @@ static int batch_init(Batch &bt, const sdddst_params &common, int count, const i
     int rc = 0;
     rc |= cudaMalloc(&bt.d_inst, sizeof(int) * bt.ntot) != cudaSuccess;
     rc |= cudaMalloc(&bt.d_off, sizeof(int) * (B + 1)) != cudaSuccess;
-    rc |= cudaMalloc(&bt.d_hinst, sizeof(double) * B) != cudaSuccess;
+    rc |= cudaMalloc(&bt.d_state, sizeof(double) * kState * B) != cudaSuccess;
+    rc |= cudaMalloc(&bt.d_state_snap, sizeof(double) * kState * B) != cudaSuccess;
+    rc |= cudaMalloc(&bt.d_x0_snap, sizeof(double) * bt.ntot) != cudaSuccess;
+    rc |= cudaMalloc(&bt.d_v0_snap, sizeof(double) * bt.ntot) != cudaSuccess;
+    rc |= cudaMalloc(&bt.d_tol_snap, sizeof(double) * bt.ntot) != cudaSuccess;
+    rc |= cudaMalloc(&bt.d_check, sizeof(int) * 16) != cudaSuccess;
+    rc |= cudaMallocHost(&bt.h_check, sizeof(int) * (16 + B)) != cudaSuccess;
     rc |= cudaMalloc(&bt.d_cut, sizeof(double) * 3 * B) != cudaSuccess;
     rc |= cudaMalloc(&bt.d_seg, sizeof(double) * B) != cudaSuccess;
     rc |= cudaMalloc(&bt.d_scale, sizeof(double) * B) != cudaSuccess;
@@ -662,6 +1019,7 @@ static int batch_init(Batch &bt, const sdddst_params &common, int count, const i
         e.err = "batch: allocation failed";
         return SDDDST_ERR_NOMEM;
     }
+    bt.d_hinst = bt.d_state + kSH * B;
     cudaMemcpy(bt.d_inst, inst.data(), sizeof(int) * bt.ntot, cudaMemcpyHostToDevice);
     cudaMemcpy(bt.d_off, bt.off.data(), sizeof(int) * (B + 1), cudaMemcpyHostToDevice);
     cudaMemcpy(bt.d_cut, cut.data(), sizeof(double) * 3 * B, cudaMemcpyHostToDevice);
@@ -742,6 +1100,14 @@ int sdddst_batch_get_scalars(void *batch, double *out)
 {
     if (!batch || !out) return SDDDST_ERR_INVALID;
     sd::Batch *bt = static_cast<sd::Batch *>(batch);
+    cudaSetDevice(bt->e.device);
+    if (bt->dev_master) {
+        int rc = sd::state_to_host(*bt);
+        if (rc) {
+            sd::set_last_error(bt->e.err);
+            return rc;
+        }
+    }
     for (int k = 0; k < bt->B; ++k) {
         double *o = out + 12 * k;
         o[0] = bt->t[k];
@@ -769,6 +1135,15 @@ int sdddst_batch_get_positions(void *batch, int which, double *x)
     const double *src = which == 0 ? e.d_x0 : which == 1 ? e.d_xb : which == 2 ? e.d_x1 : e.d_x2;
     cudaMemcpyAsync(x, src, sizeof(double) * bt->ntot, cudaMemcpyDeviceToHost, e.st);
     return e.sync_check("batch positions");
+}
+
+int sdddst_batch_stats(void *batch, int *graph, long *redone)
+{
+    if (!batch) return SDDDST_ERR_INVALID;
+    sd::Batch *bt = static_cast<sd::Batch *>(batch);
+    if (graph) *graph = bt->gexec != nullptr ? 1 : 0;
+    if (redone) *redone = bt->redone;
+    return SDDDST_OK;
 }
 
 int sdddst_batch_info(void *batch, int *tile, long *total, long *launches, void **stream)

@@ -616,11 +616,12 @@ int sdddst_solver_stats(void *ctx, long *solves, long *iterations)
     return SDDDST_OK;
 }
 
-int sdddst_solver_recoveries(void *ctx, long *rebuilds, long *fallbacks)
+int sdddst_solver_recoveries(void *ctx, long *rebuilds, long *fallbacks, long *redone)
 {
     if (!ctx) return fail(SDDDST_ERR_INVALID, "null argument");
     if (rebuilds) *rebuilds = E(ctx)->stalls;
     if (fallbacks) *fallbacks = E(ctx)->fallbacks;
+    if (redone) *redone = E(ctx)->redone;
     return SDDDST_OK;
 }
 

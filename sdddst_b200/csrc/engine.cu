@@ -51,6 +51,9 @@ Engine::~Engine()
     direct_free(*this);
     learned_free(*this);
     if (d_xasm) cudaFree(d_xasm);
+    if (d_tol_snap) cudaFree(d_tol_snap);
+    if (d_astat) cudaFree(d_astat);
+    if (h_status) cudaFreeHost(h_status);
     if (d_tab_xy) cudaFree(d_tab_xy);
     if (d_tab_dx) cudaFree(d_tab_dx);
     if (st) cudaStreamDestroy(st);
@@ -160,7 +163,7 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     rc |= precond_alloc(*this, pc);
     // the cluster solver runs device-resident on a single system (the CSR's
     // cell-sorted column positions are then always present)
-    fused = !batch_backend && prm.solver == SDDDST_SOLVER_GMRES_CLUSTER && std::getenv("SDDDST_HOST_GMRES") == nullptr;
+    fused = prm.solver == SDDDST_SOLVER_GMRES_CLUSTER && std::getenv("SDDDST_HOST_GMRES") == nullptr;
     if (rc) {
         err = "device allocation failed";
         return SDDDST_ERR_NOMEM;
@@ -465,21 +468,12 @@ int Engine::stages_one_two()
     return 0;
 }
 
-// Simulation::step = stepStageI + II + III (simulation.cpp:435-650).
-int Engine::step(int *accepted)
+// The three stages of an attempt with a wait at every check (assembly row
+// counts, preconditioner builds, each solve): the path of every solver, and
+// the fallback of an optimistic attempt that failed a check.
+int Engine::stages_sync(double *ratio)
 {
     const size_t bytes = sizeof(double) * n;
-    // ---- stage I (simulation.cpp:443-492)
-    energy_accum = 0;
-    vsquare = 0;
-    cur_stress = kOrig;
-    if (first_step) {
-        stress_calc(sim_time, kOrig, strain);
-        speeds(d_x0, d_v0, d_S0, kOrig, true);
-        init_speed_needed = false;
-        if (int rc = sum_sq(d_v0, &vsquare)) return rc;
-        first_step = false;
-    }
     cudaMemcpyAsync(d_xb, d_x0, bytes, cudaMemcpyDeviceToDevice, st);
     if (fused && prm.solver == SDDDST_SOLVER_GMRES_CLUSTER) {
         // ---- stages I and II together (one solve launch per Newton iteration)
@@ -497,8 +491,181 @@ int Engine::step(int *accepted)
     sum_avg_speed = 0;
     cudaMemcpyAsync(d_x2, d_x1, bytes, cudaMemcpyDeviceToDevice, st);
     if (int rc = integrate(0.5 * step_size, d_x2, d_x1, true, true, kEndFirst, kEndSecond, false)) return rc;
+    return stage_scalars(&vsquare1, &vsquare2, ratio);
+}
+
+// The three stages of an attempt of the device-resident cluster solver with
+// no wait until they end: the assemblies do not read their row counts back
+// (bounded by the CSR storage, guarded), the preconditioner builds and the
+// solves leave their statuses on the device, and one copy after stage III
+// brings back every status with |v0|^2, |v0b|^2 and the error ratio.  The
+// work and its order are those of stages_sync.  *ok is false when a check
+// failed (a stalled solve, a pattern larger than the storage, a
+// non-finite Krylov quantity): the caller then redoes the attempt with waits,
+// which repeats and reports the failure exactly as the waiting path does.
+int Engine::stages_async(double *ratio, bool *ok)
+{
+    *ok = false;
+    const size_t bytes = sizeof(double) * n;
+    if (int rc = fused_alloc(*this, 2)) {
+        err = "fused solve: allocation failed";
+        return rc;
+    }
+    const double h1 = step_size, h2 = 0.5 * step_size;
+    cudaMemcpyAsync(d_xb, d_x0, bytes, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(d_x1, d_x0, bytes, cudaMemcpyDeviceToDevice, st);
+    // ---- stages I and II: shared assembly at the accepted configuration
+    if (int rc = jacobian_assemble(*this, d_xb, true)) return rc;
+    launch_csr_guard(*this, d_astat);
+    launch_make_dvec(*this, h1, d_dvecI, st);
+    launch_make_dvec(*this, h2, d_dvec, st);
+    launches += 2;
+    if (int rc = precond_build(*this, pc2, h1, d_dvecI, false)) return rc;
+    cudaMemcpyAsync(d_astat + 4, pc2.flag, sizeof(int), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(d_astat + 5, pc2.bbase + n, sizeof(int), cudaMemcpyDeviceToDevice, st);
+    if (int rc = precond_build(*this, pc, h2, d_dvec, false)) return rc;
+    cudaMemcpyAsync(d_astat + 6, pc.flag, sizeof(int), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(d_astat + 7, pc.bbase + n, sizeof(int), cudaMemcpyDeviceToDevice, st);
+    for (int it = 0; it < ic; ++it) {
+        if (int rc = stage_residual(h1, it, d_xb, d_x0, false, init_speed_needed, kOrig, kEndBig, d_vsI, d_dvecI,
+                                    d_gI))
+            return rc;
+        if (int rc = stage_residual(h2, it, d_x1, d_x0, false, false, kOrig, kEndFirst, d_vs, d_dvec, d_g))
+            return rc;
+        const double hs[2] = {h1, h2};
+        const double *dv[2] = {d_dvecI, d_dvec};
+        const double *rhs[2] = {d_gI, d_g};
+        double *xs[2] = {d_solI, d_sol};
+        const Cluster *pcs[2] = {&pc2, &pc};
+        if (int rc = fused_gmres(*this, 2, hs, dv, rhs, xs, pcs, nullptr, true, 2 * it)) return rc;
+        launch_axpy_update(*this, d_xb, d_solI, st);
+        launch_axpy_update(*this, d_x1, d_sol, st);
+        launches += 2;
+    }
+    successful_step = false;
+    // ---- stage III: assembly at the first small step's end
+    sum_avg_speed = 0;
+    cudaMemcpyAsync(d_x2, d_x1, bytes, cudaMemcpyDeviceToDevice, st);
+    if (int rc = jacobian_assemble(*this, d_x2, true)) return rc;
+    launch_csr_guard(*this, d_astat + 2);
+    launch_make_dvec(*this, h2, d_dvec, st);
+    launches++;
+    if (int rc = precond_build(*this, pc, h2, d_dvec, false)) return rc;
+    cudaMemcpyAsync(d_astat + 8, pc.flag, sizeof(int), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(d_astat + 9, pc.bbase + n, sizeof(int), cudaMemcpyDeviceToDevice, st);
+    const int slot3 = 2 * ic;
+    for (int it = 0; it < ic; ++it) {
+        if (int rc = stage_residual(h2, it, d_x2, d_x1, true, true, kEndFirst, kEndSecond, d_vs2, d_dvec, d_g))
+            return rc;
+        const Cluster *pcs[1] = {&pc};
+        const double *dv = d_dvec, *rhs = d_g;
+        double *xs = d_sol;
+        if (int rc = fused_gmres(*this, 1, &h2, &dv, &rhs, &xs, pcs, nullptr, true, slot3 + it)) return rc;
+        launch_axpy_update(*this, d_x2, d_sol, st);
+        launches++;
+    }
+    // ---- one copy of every status and the stage scalars, one wait
+    launch_stage_scalars(*this);
+    const int nslots = slot3 + ic;
+    double *hs = h_status;
+    cudaMemcpyAsync(hs, d_fstatus, sizeof(double) * 4 * nslots, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hs + 4 * kAttemptSlots, d_scal, sizeof(double) * 3, cudaMemcpyDeviceToHost, st);
+    int *ha = reinterpret_cast<int *>(hs + 4 * kAttemptSlots + 4);
+    cudaMemcpyAsync(ha, d_astat, sizeof(int) * 10, cudaMemcpyDeviceToHost, st);
+    if (int rc = sync_check("step")) return rc;
+    // assemblies: a pattern beyond the storage grows it (the attempt is redone)
+    for (int a = 0; a < 2; ++a) {
+        const int total = ha[2 * a], flag = ha[2 * a + 1];
+        if (flag == 1) {
+            err = "jacobian: neighbour count and fill passes disagree";
+            return SDDDST_ERR_CAPACITY;
+        }
+        if (flag == 2) {
+            if (total < n) {
+                err = "jacobian: row count overflow";
+                return SDDDST_ERR_CAPACITY;
+            }
+            if (alloc_csr_values(*this, (long)total + total / 4 + 1024)) {
+                err = "jacobian: CSR allocation failed";
+                return SDDDST_ERR_NOMEM;
+            }
+            nnz_cap = (long)total + total / 4 + 1024;
+            cudaMemsetAsync(d_col, 0, sizeof(int) * nnz_cap, st);
+            return 0;
+        }
+    }
+    nnz = ha[2];
+    for (int b = 0; b < 3; ++b) {
+        const int flag = ha[4 + 2 * b], nb = ha[5 + 2 * b];
+        if (nb <= 0 || nb > n) {
+            err = "precond: bad block count";
+            return SDDDST_ERR_SOLVER;
+        }
+        if (flag) {
+            err = "precond: singular cluster block";
+            return SDDDST_ERR_SOLVER;
+        }
+    }
+    long its = 0;
+    for (int q = 0; q < nslots; ++q) {
+        const double *sq = hs + 4 * q;
+        if (sq[1] == 0.0 || sq[3] != 0.0) return 0; // a stall or a non-finite value: redo with waits
+        its += (long)sq[0];
+    }
+    solves += nslots;
+    iterations += its;
+    last_iters = (int)hs[4 * (nslots - 1)];
+    vsquare1 = hs[4 * kAttemptSlots];
+    vsquare2 = hs[4 * kAttemptSlots + 1];
+    *ratio = hs[4 * kAttemptSlots + 2];
+    *ok = true;
+    return 0;
+}
+
+// Simulation::step = stepStageI + II + III (simulation.cpp:435-650).
+int Engine::step(int *accepted)
+{
+    const size_t bytes = sizeof(double) * n;
+    // ---- stage I (simulation.cpp:443-492)
+    energy_accum = 0;
+    vsquare = 0;
+    cur_stress = kOrig;
+    if (first_step) {
+        stress_calc(sim_time, kOrig, strain);
+        speeds(d_x0, d_v0, d_S0, kOrig, true);
+        init_speed_needed = false;
+        if (int rc = sum_sq(d_v0, &vsquare)) return rc;
+        first_step = false;
+    }
     double ratio = 0.0;
-    if (int rc = stage_scalars(&vsquare1, &vsquare2, &ratio)) return rc;
+    if (fused && prm.solver == SDDDST_SOLVER_GMRES_CLUSTER && ic <= 2) {
+        if (!d_tol_snap) {
+            if (cudaMalloc(&d_tol_snap, bytes) != cudaSuccess || cudaMalloc(&d_astat, sizeof(int) * 16) != cudaSuccess ||
+                cudaMallocHost(&h_status, sizeof(double) * (4 * kAttemptSlots + 16)) != cudaSuccess) {
+                err = "step: allocation failed";
+                return SDDDST_ERR_NOMEM;
+            }
+        }
+        cudaMemcpyAsync(d_tol_snap, d_tol, bytes, cudaMemcpyDeviceToDevice, st);
+        bool ok = false;
+        if (int rc = stages_async(&ratio, &ok)) return rc;
+        if (!ok) {
+            // a deferred check failed: the same attempt again, waiting at every check
+            redone++;
+            cudaMemcpyAsync(d_tol, d_tol_snap, bytes, cudaMemcpyDeviceToDevice, st);
+            if (int rc = stages_sync(&ratio)) return rc;
+        }
+    } else {
+        if (int rc = stages_sync(&ratio)) return rc;
+    }
+    return finish_step(ratio, accepted);
+}
+
+// Error control, accept/reject and the new step size of an attempt
+// (simulation.cpp:501-650, precision_handler.cpp:103-119).
+int Engine::finish_step(double ratio, int *accepted)
+{
+    const size_t bytes = sizeof(double) * n;
     energy_accum = (vsquare1 + vsquare2) * 0.5 * step_size * 0.5;
     if (!std::isfinite(ratio)) {
         err = "step: non-finite error ratio";
@@ -521,10 +688,10 @@ int Engine::step(int *accepted)
         stress_calc(sim_time, kOrig, strain);
         speeds(d_x0, d_v0, d_S0, kOrig, true);
         init_speed_needed = false;
-        double sa;
-        if (int rc = sum_abs(d_v0, &sa)) return rc;
+        double sa, sq;
+        if (int rc = abs_and_sq(d_v0, &sa, &sq)) return rc;
         sum_avg_speed = sa / double(n);
-        if (int rc = sum_sq(d_v0, &vsquare)) return rc;
+        vsquare = sq;
         energy_accum += (vsquare2 + vsquare) * 0.5 * step_size * 0.5;
         energy += energy_accum;
     } else {
@@ -542,8 +709,10 @@ int Engine::step(int *accepted)
     }
     step_size = hn;
     last_ratio = ratio;
+    // PrecisionHandler::reset (precision_handler.cpp:62-70), kept for the
+    // tolerance export
     cudaMemcpyAsync(d_tol_last, d_tol, bytes, cudaMemcpyDeviceToDevice, st);
-    reset_tol(*this);
+    launch_fill(*this, d_tol, prec * prec);
     if (prm.max_step_limited && prm.max_step < step_size) step_size = prm.max_step;
     if (accepted) *accepted = successful_step ? 1 : 0;
     return sync_check("step");

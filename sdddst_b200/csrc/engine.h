@@ -100,6 +100,13 @@ struct Engine {
     double *d_V2 = nullptr, *d_w2 = nullptr, *d_z2 = nullptr, *d_zs2 = nullptr;
     double *d_gI = nullptr, *d_solI = nullptr, *d_dvecI = nullptr, *d_vsI = nullptr; // stage I's g, solution, d, speed
     bool fused = false;                   // the cluster solver runs device-resident (set at init)
+    // optimistic attempts (no host round trip until the stages end): the
+    // statuses they leave on the device, read back in one copy, and the
+    // tolerance snapshot restored when an attempt has to be redone
+    int *d_astat = nullptr;               // per deferred assembly: entry total, fill flag
+    double *d_tol_snap = nullptr;
+    double *h_status = nullptr;           // pinned: fused statuses, assembly and preconditioner checks, scalars
+    long redone = 0;                      // attempts redone with waits after a deferred failure
 
     // ---- cluster block-Jacobi preconditioners (precond.cu): pc for the
     // solves of the engine's generic path and of stage II/III, pc2 for stage
@@ -144,6 +151,10 @@ struct Engine {
     // stage I (h) and stage II (h/2) from the accepted configuration with
     // their solves in one device-resident launch per Newton iteration
     int stages_one_two();
+    int stages_sync(double *ratio);
+    int stages_async(double *ratio, bool *ok);
+    int finish_step(double ratio, int *accepted);
+    int abs_and_sq(const double *v, double *sum_abs, double *sum_sq);
     int solve_fused(double h, const double *dvec, Cluster &c, const double *rhs, double *x);
     int step(int *accepted);
     int set_state_host(const double *xyb, double step, double t, double e, double strain, int first);
@@ -172,7 +183,8 @@ void launch_add_stress(const Engine &e, const double *S, double tau_ext, double 
 void launch_speeds_raw(int n, const double *x, const double *y, const double *b, double tau_ext, double *part,
                        double *v, cudaStream_t st);
 
-int jacobian_assemble(Engine &e, const double *x);
+int jacobian_assemble(Engine &e, const double *x, bool defer = false);
+void launch_csr_guard(Engine &e, int *stat);
 int tabulated_build(Engine &e);
 int alloc_csr_values(Engine &e, long cap);
 // Exclusive scan of m ints (out[0] = 0, out[k+1] = sum_{<=k}); returns the
@@ -191,6 +203,10 @@ void launch_spmv_J(Engine &e, double h, const double *dvec, const double *v, dou
 int gmres_solve(Engine &e, double h, const double *dvec, const double *rhs, double *x, int precond);
 bool gs_coop_supported(int device, int blocks);
 
+constexpr int kAttemptSlots = 8; // solve statuses of one optimistic attempt (2 ic joint + ic stage III)
+// |v0|^2, |v0b|^2 and the error ratio of the attempt into d_scal[0..2] (no wait)
+void launch_stage_scalars(Engine &e);
+void launch_fill(Engine &e, double *p, double v);
 void launch_residual_g(const Engine &e, double h, const double *xn, const double *xo, const double *csp,
                        const double *isp, const double *dvec, double *g, cudaStream_t st);
 void launch_axpy_update(const Engine &e, double *xn, const double *sol, cudaStream_t st);
@@ -219,8 +235,11 @@ void direct_free(Engine &e);
 bool fused_supported(const Engine &e);
 int fused_alloc(Engine &e, int ns);
 void fused_free(Engine &e);
+// With defer, the launch is not waited for: the statuses stay in
+// d_fstatus[4 (slot + s) ...] ([0] iterations [1] converged [2] residual
+// [3] non-finite) for the caller to read; conv is not written.
 int fused_gmres(Engine &e, int ns, const double *h, const double *const *dvec, const double *const *rhs,
-                double *const *x, const Cluster *const *pcs, int *conv);
+                double *const *x, const Cluster *const *pcs, int *conv, bool defer = false, int slot = 0);
 
 int learned_set_weights(Engine &e, const unsigned short *bf16, long count);
 int learned_build(Engine &e, double h, const double *dvec, const double *x, bool analytic);

@@ -35,9 +35,11 @@ namespace {
 
 constexpr int kThreads = 512;
 constexpr int kKM = 32; // restart length bound (m <= 31) and partial-sum stride
+constexpr int kStatusSlots = 8; // solves whose statuses one attempt can leave on the device
 
 struct FusedSys {
     double h;
+    const double *hrow; // per-row step size (a batch of systems), or null: h
     const double *dvec;
     const double *rhs;
     double *x;
@@ -160,12 +162,14 @@ __device__ __forceinline__ void spmv_rows(const FusedArgs &a, int r0, int r1, co
         if (lane == 0) {
             if (act0) {
                 const FusedSys &S = a.sys[0];
-                const double y = v0[row] + (1.0 + S.dvec[row]) * 0.5 * S.h * acc0;
+                const double hh = S.hrow ? S.hrow[row] : S.h;
+                const double y = v0[row] + (1.0 + S.dvec[row]) * 0.5 * hh * acc0;
                 o0[row] = residual ? S.rhs[row] - y : y;
             }
             if (NS == 2 && act1) {
                 const FusedSys &S = a.sys[1];
-                const double y = v1[row] + (1.0 + S.dvec[row]) * 0.5 * S.h * acc1;
+                const double hh = S.hrow ? S.hrow[row] : S.h;
+                const double y = v1[row] + (1.0 + S.dvec[row]) * 0.5 * hh * acc1;
                 o1[row] = residual ? S.rhs[row] - y : y;
             }
         }
@@ -485,7 +489,7 @@ static int fused_grid(const Engine &e, const void *kern)
 
 bool fused_supported(const Engine &e)
 {
-    return e.col_s_valid && !e.d_hrow && e.restart <= kKM - 1 &&
+    return e.col_s_valid && e.restart <= kKM - 1 &&
            fused_grid(e, pick_kernel(e.valf, e.col_s16_valid, 1)) > 0;
 }
 
@@ -494,8 +498,8 @@ int fused_alloc(Engine &e, int ns)
     const size_t n = (size_t)e.n;
     if (!e.d_fpart) {
         if (cudaMalloc(&e.d_fpart, sizeof(double) * 2 * 2 * 1024 * kKM) != cudaSuccess) return SDDDST_ERR_NOMEM;
-        if (cudaMalloc(&e.d_fstatus, sizeof(double) * 8) != cudaSuccess) return SDDDST_ERR_NOMEM;
-        if (cudaMallocHost(&e.h_fstatus, sizeof(double) * 8) != cudaSuccess) return SDDDST_ERR_NOMEM;
+        if (cudaMalloc(&e.d_fstatus, sizeof(double) * 4 * kStatusSlots) != cudaSuccess) return SDDDST_ERR_NOMEM;
+        if (cudaMallocHost(&e.h_fstatus, sizeof(double) * 4 * kStatusSlots) != cudaSuccess) return SDDDST_ERR_NOMEM;
     }
     if (ns == 2 && !e.d_V2) {
         if (cudaMalloc(&e.d_V2, sizeof(double) * (e.restart + 1) * n) != cudaSuccess) return SDDDST_ERR_NOMEM;
@@ -520,7 +524,7 @@ void fused_free(Engine &e)
 // conv[s] receives 1 where system s reached the residual target.  Returns
 // SDDDST_ERR_NONFINITE when a Krylov quantity is not finite.
 int fused_gmres(Engine &e, int ns, const double *h, const double *const *dvec, const double *const *rhs,
-                double *const *x, const Cluster *const *pcs, int *conv)
+                double *const *x, const Cluster *const *pcs, int *conv, bool defer, int slot)
 {
     if (int rc = fused_alloc(e, ns)) {
         e.err = "fused solve: allocation failed";
@@ -544,6 +548,7 @@ int fused_gmres(Engine &e, int ns, const double *h, const double *const *dvec, c
         FusedSys &S = a.sys[s];
         const Cluster &c = *pcs[s];
         S.h = h[s];
+        S.hrow = e.d_hrow;
         S.dvec = dvec[s];
         S.rhs = rhs[s];
         S.x = x[s];
@@ -558,7 +563,7 @@ int fused_gmres(Engine &e, int ns, const double *h, const double *const *dvec, c
         S.members = c.members;
         S.off = c.off;
         S.binv = c.binv;
-        S.status = e.d_fstatus + 4 * s;
+        S.status = e.d_fstatus + 4 * (slot + s);
     }
     if (ns == 1) a.sys[1] = a.sys[0];
     const void *kern = pick_kernel(e.valf, e.col_s16_valid, ns);
@@ -574,7 +579,8 @@ int fused_gmres(Engine &e, int ns, const double *h, const double *const *dvec, c
         return SDDDST_ERR_CUDA;
     }
     e.launches++;
-    cudaMemcpyAsync(e.h_fstatus, e.d_fstatus, sizeof(double) * 4 * ns, cudaMemcpyDeviceToHost, e.st);
+    if (defer) return 0;
+    cudaMemcpyAsync(e.h_fstatus, e.d_fstatus + 4 * slot, sizeof(double) * 4 * ns, cudaMemcpyDeviceToHost, e.st);
     if (int rc = e.sync_check("fused solve")) return rc;
     int res = 0;
     for (int s = 0; s < ns; ++s) {

@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(kCellThreads) cell_rows_kernel(
     double c, double c2, double ic2, int *__restrict__ rowcnt, const int *__restrict__ rowptr, int *__restrict__ col,
     VT *__restrict__ val, double *__restrict__ gdiag, int p, const double *__restrict__ pdx,
     const double *__restrict__ pdy, double A, double K, int *__restrict__ flag, const double *__restrict__ tab_dx,
-    int *__restrict__ col_s, unsigned short *__restrict__ col_s16, const double *__restrict__ bs)
+    int *__restrict__ col_s, unsigned short *__restrict__ col_s16, const double *__restrict__ bs, long cap)
 {
     extern __shared__ __align__(16) unsigned char cell_smem[];
     float *sxc = reinterpret_cast<float *>(cell_smem);
@@ -537,6 +537,10 @@ __global__ void __launch_bounds__(kCellThreads) cell_rows_kernel(
             if (lane == 0) rowcnt[i] = cnt + 1;
         } else {
             const int base = rowptr[i], rowend = rowptr[i + 1];
+            if ((long)rowend > cap) { // the pattern outgrew the CSR storage: report, write nothing
+                if (lane == 0) atomicExch(flag, 2);
+                continue;
+            }
             int pos = base + 1;
             if (staged) {
                 int sgi = 0; // segment of the chunk's first candidate (candidates ascend)
@@ -664,7 +668,11 @@ static int cell_parts(const Engine &e, int ncell)
     return ncell >= want ? 1 : (want + ncell - 1) / ncell;
 }
 
-int jacobian_assemble(Engine &e, const double *x)
+// With defer, nothing waits for the device: the row counts are not read
+// back (the fill is bounded by the current storage and flags an overflow
+// with 2 in d_flag) and the fill's flag is left for the caller to read;
+// e.nnz is unknown (-1) until then.
+int jacobian_assemble(Engine &e, const double *x, bool defer)
 {
     const int n = e.n, G = e.G;
     cudaStream_t st = e.st;
@@ -684,9 +692,28 @@ int jacobian_assemble(Engine &e, const double *x)
     const unsigned nb = (unsigned)(ncell * parts);
     cell_rows_kernel<false, float><<<nb, kCellThreads, kCellSmem, st>>>(
         parts, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr, e.d_rowcnt, nullptr, nullptr,
-        nullptr, nullptr, 0, nullptr, nullptr, 0.0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr);
+        nullptr, nullptr, 0, nullptr, nullptr, 0.0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, 0L);
     e.launches += launch_scan(e, e.d_rowcnt, n, e.d_rowptr, st) - 1;
     e.launches += 8;
+    if (defer) {
+        cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
+        if (e.valf)
+            cell_rows_kernel<true, float><<<nb, kCellThreads, kCellSmem, st>>>(
+                parts, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr, nullptr, e.d_rowptr,
+                e.d_col, e.d_valf, e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag, e.d_tab_dx, e.d_col_s,
+                e.d_col_s16, e.d_bsrt, e.nnz_cap);
+        else
+            cell_rows_kernel<true, double><<<nb, kCellThreads, kCellSmem, st>>>(
+                parts, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr, nullptr, e.d_rowptr,
+                e.d_col, e.d_val, e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag, e.d_tab_dx, e.d_col_s,
+                e.d_col_s16, e.d_bsrt, e.nnz_cap);
+        e.launches += 1;
+        e.nnz = -1;
+        e.col_s_valid = true;
+        e.col_s16_valid = e.d_col_s16 != nullptr;
+        e.spmv_sorted = e.d_sorted;
+        return 0;
+    }
     int total = 0;
     if (cudaMemcpyAsync(&total, e.d_rowptr + n, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return SDDDST_ERR_CUDA;
@@ -705,12 +732,12 @@ int jacobian_assemble(Engine &e, const double *x)
         cell_rows_kernel<true, float><<<nb, kCellThreads, kCellSmem, st>>>(
             parts, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr, nullptr, e.d_rowptr, e.d_col,
             e.d_valf, e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag, e.d_tab_dx, e.d_col_s, e.d_col_s16,
-            e.d_bsrt);
+            e.d_bsrt, e.nnz_cap);
     else
         cell_rows_kernel<true, double><<<nb, kCellThreads, kCellSmem, st>>>(
             parts, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr, nullptr, e.d_rowptr, e.d_col,
             e.d_val, e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag, e.d_tab_dx, e.d_col_s, e.d_col_s16,
-            e.d_bsrt);
+            e.d_bsrt, e.nnz_cap);
     e.launches += 1;
     int flag = 0;
     cudaMemcpyAsync(&flag, e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -723,6 +750,31 @@ int jacobian_assemble(Engine &e, const double *x)
     e.col_s16_valid = e.d_col_s16 != nullptr;
     e.spmv_sorted = e.d_sorted;
     return 0;
+}
+
+// After a deferred fill: stat[0] = entry total of the count pass, stat[1] =
+// the fill's flag (1: count and fill disagree, 2: storage overflow); on a
+// flag every row pointer is zeroed, so the kernels that follow in the same
+// attempt see an empty pattern and read nothing past the storage (the attempt
+// is redone on the host's request).  One block.
+__global__ void csr_guard_kernel(int n, int *__restrict__ rowptr, const int *__restrict__ flag,
+                                 int *__restrict__ stat)
+{
+    __shared__ int f;
+    if (threadIdx.x == 0) {
+        f = *flag;
+        stat[0] = rowptr[n];
+        stat[1] = f;
+    }
+    __syncthreads();
+    if (f != 0)
+        for (int i = threadIdx.x; i <= n; i += blockDim.x) rowptr[i] = 0;
+}
+
+void launch_csr_guard(Engine &e, int *stat)
+{
+    csr_guard_kernel<<<1, 256, 0, e.st>>>(e.n, e.d_rowptr, e.d_flag, stat);
+    e.launches++;
 }
 
 void launch_make_dvec(const Engine &e, double h, double *dvec, cudaStream_t st)

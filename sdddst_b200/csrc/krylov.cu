@@ -307,6 +307,37 @@ int Engine::strain_inc(const double *xo, const double *xn, double *out)
     return 0;
 }
 
+void launch_stage_scalars(Engine &e)
+{
+    launch_reduce<0>(e, e.n, e.d_v0, nullptr, nullptr, e.d_scal);
+    launch_reduce<0>(e, e.n, e.d_v0b, nullptr, nullptr, e.d_scal + 1);
+    launch_reduce<3>(e, e.n, e.d_xb, e.d_tol, e.d_x2, e.d_scal + 2);
+}
+
+__global__ void fill_kernel(int n, double *__restrict__ p, double v)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+void launch_fill(Engine &e, double *p, double v)
+{
+    fill_kernel<<<(e.n + 255) / 256, 256, 0, e.st>>>(e.n, p, v);
+    e.launches++;
+}
+
+// sum |v| and sum v^2 in one copy to the host
+int Engine::abs_and_sq(const double *v, double *sa, double *sq)
+{
+    launch_reduce<1>(*this, n, v, nullptr, nullptr, d_scal + 3);
+    launch_reduce<0>(*this, n, v, nullptr, nullptr, d_scal + 4);
+    cudaMemcpyAsync(h_scal, d_scal + 3, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (int rc = sync_check("speed sums")) return rc;
+    *sa = h_scal[0];
+    *sq = h_scal[1];
+    return 0;
+}
+
 // |v0|^2, |v0b|^2 and the error ratio of the step, one copy to the host
 int Engine::stage_scalars(double *vs1, double *vs2, double *ratio)
 {

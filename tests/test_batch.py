@@ -79,4 +79,6 @@ def test_batch_workload_systems_match_oracle(engine_lib, port_lib):
                 assert sc[k, 2] == s["successful_steps"] and sc[k, 3] == s["failed_steps"]
                 assert np.isclose(sc[k, 4], s["energy"], rtol=1e-8)
     assert uneven, "every attempt was accepted or rejected by all systems together"
+    # after the host-driven first step, every step replays the captured graph
+    assert bt.stats() == {"graph": 1, "redone": 0}, bt.stats()
     bt.close()

@@ -163,3 +163,29 @@ def test_jacobian_capacity_reports_needed_size(engine_lib):
     assert rc == capi.ERR_CAPACITY and nnz.value > 16
     rp2, col2, val2, _ = e.jacobian(1e-6, xyb)
     assert len(col2) == nnz.value == rp2[-1]
+
+
+@pytest.mark.gpu
+def test_pattern_growth_redoes_the_attempt(engine_lib, port_lib):
+    """The cluster solver's attempts run without waiting for the device and
+    check everything once at the end.  An engine whose Jacobian storage was
+    sized for a uniform configuration is given a strongly clustered one (4200
+    of 6000 dislocations in a 0.04 x 0.04 square): the first assembly of the
+    attempt outgrows the storage, is guarded (no access past it), the storage
+    grows, and the attempt is redone with waits.  The step still matches the
+    oracle's (decision, stage positions within 1e-10)."""
+    from sdddst_b200 import capi
+    rng = np.random.default_rng(8)
+    n, m = 6000, 1.0
+    uniform, _ = workloads.dislocations(n, 9)
+    e = capi.Engine(capi.cli_params(n, m, 1e-6), uniform)
+    pos = np.concatenate([rng.uniform(-0.5, 0.5, (1800, 2)), 0.1 + rng.uniform(-0.02, 0.02, (4200, 2))])
+    b = rng.permutation(np.r_[np.ones(n // 2), -np.ones(n // 2)])
+    xyb = np.column_stack([pos, b])
+    o = ref.Sim(xyb, None, ref.params(cutoff_multiplier=m, prec=1e-6, step_size=1e-9), "port")
+    o.set_state(xyb, 1e-9, 0.0, 0.0, 0.0, False)
+    e.set_state(xyb, 1e-9, 0.0, 0.0, 0.0, False)
+    assert e.step() == o.step()
+    for which in (1, 2, 3):
+        assert np.abs(e.config(which)[:, 0] - o.config(which)[:, 0]).max() <= 1e-10, which
+    assert e.solver_recoveries()[2] >= 1
