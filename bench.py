@@ -427,7 +427,56 @@ def profile_target(args):
     eng.close()
 
 
-def measure_batch(torch, steps, warmup, pairsum, rank, world, dist=None):
+def _ref_attempt_seconds(args):
+    """One zero-stress step attempt of the reference (5 calculateSpeeds + 3
+    calculateJacobian, simulation.cpp:62-84,435-650) on one system, one core."""
+    n, seed, m = args
+    sys.path.insert(0, ROOT)
+    from oracle import ref
+    from sdddst_b200 import workloads
+    xyb, _ = workloads.dislocations(int(n), int(seed))
+    kind = "ref" if ref.available("ref") else "port"
+    sim = ref.Sim(xyb, None, ref.params(cutoff_multiplier=m, prec=1e-6, step_size=H0), kind)
+    t0 = time.perf_counter()
+    for what in ("s", "j", "s", "s", "j", "s", "j", "s"):
+        if what == "s":
+            sim.speeds(xyb)
+        else:
+            sim.jacobian(H0, xyb, cap=max(1024, int(n) * 256))
+    return time.perf_counter() - t0, kind
+
+
+def cpu_batch_baseline(sizes, seeds, accept_fraction, procs=8, sample=8):
+    """The reference on `procs` host cores for the batched workload: the
+    realisations are independent, so P single-threaded reference processes
+    step P systems at once.  Sample: `sample` systems of the workload at
+    evenly spaced size quantiles, one attempt each (one per process, all at
+    once); the attempt time t(N) = a N^2 is fitted to them, summed over all
+    systems and divided by P (perfect packing), and the attempts/s converted
+    to accepted system-steps/s with the GPU run's acceptance fraction."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    order = np.argsort(sizes)
+    pick = order[np.linspace(0, len(sizes) - 1, sample).round().astype(int)]
+    jobs = [(int(sizes[k]), int(seeds[k]), 0.5) for k in pick]
+    with ProcessPoolExecutor(max_workers=min(procs, sample), mp_context=mp.get_context("spawn")) as ex:
+        res = list(ex.map(_ref_attempt_seconds, jobs))
+    ts = np.array([r[0] for r in res])
+    ns = np.array([j[0] for j in jobs], dtype=np.float64)
+    a = float(np.sum(ts * ns ** 2) / np.sum(ns ** 4))
+    total = a * float(np.sum(np.asarray(sizes, dtype=np.float64) ** 2))
+    wall = total / procs
+    attempts_per_s = len(sizes) / wall
+    return {"value": attempts_per_s * accept_fraction, "unit": "accepted system-steps/s", "cores": procs,
+            "kind": "reference" if res[0][1] == "ref" else "port",
+            "sample": (f"{sample} systems of the workload at size quantiles (N = {int(ns.min())}..{int(ns.max())}), "
+                       f"one reference attempt each (5 calculateSpeeds + 3 calculateJacobian, one core per system, "
+                       f"{sample} at once, {ts.max():.1f} s), t(N) = {a:.3e} N^2 s summed over the "
+                       f"{len(sizes)} systems on {procs} cores, times the GPU run's acceptance "
+                       f"{accept_fraction:.3f}; solve excluded")}
+
+
+def measure_batch(torch, steps, warmup, pairsum, rank, world, dist=None, cpu=False):
     """The batched workload: 512 independent realisations, N_k uniform in
     [64, 2048] (seed 3), cutoff multiplier 0.5, zero stress, all stepped
     together; ranks step their LPT share.  Value: accepted system-steps/s of
@@ -455,6 +504,17 @@ def measure_batch(torch, steps, warmup, pairsum, rank, world, dist=None):
         b.synchronize()
         total_ms += a.elapsed_time(b)
     launches = bt.info()["launches"] - l0
+    stats = bt.stats()
+    attempts = len(mine) * steps
+    # roofline of its dominant kernel: the pair sum over all systems' tiles
+    pair_ms, pairs = bt.profile_pair_sum(3)
+    vp = _vector_peaks(torch.cuda.current_device())
+    peak = vp.get("fp32_tflops" if pairsum == "fp32" else "fp64_tflops")
+    ach = FLOP_PER_PAIR * pairs / (pair_ms * 1e-3) / 1e12 if pair_ms > 0 else 0.0
+    roof = {"bound": pairsum, "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+            "frac": ach / peak if peak else None, "kernel": "batch_pair_kernel (all systems, one launch)",
+            "work": f"{FLOP_PER_PAIR:.0f} FLOP x sum_k N_k(N_k-1)/2 = {pairs:.3e} pairs", "ms": pair_ms,
+            "peak_source": "measured (FMA chain microbenchmark, sdddst_vector_peaks)", "traffic": None}
     if dist is not None:
         t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -462,11 +522,19 @@ def measure_batch(torch, steps, warmup, pairsum, rank, world, dist=None):
         dist.all_reduce(n, op=dist.ReduceOp.SUM)
         total_ms, acc = float(t.item()), int(n.item())
     bt.close()
-    return {"value": acc / (total_ms * 1e-3) if total_ms > 0 else 0.0, "unit": "accepted system-steps/s",
-            "systems": len(sizes), "systems_per_rank": len(mine), "total_dislocations": int(sum(sizes)),
-            "steps": steps, "ms_per_step": total_ms / max(1, steps), "tile": info["tile"],
-            "pairsum": pairsum, "gpu_launches": launches,
-            "config": "N_k ~ U[64, 2048] seed 3, cutoff multiplier 0.5, prec 1e-6, zero stress"}
+    out = {"value": acc / (total_ms * 1e-3) if total_ms > 0 else 0.0, "unit": "accepted system-steps/s",
+           "systems": len(sizes), "systems_per_rank": len(mine), "total_dislocations": int(sum(sizes)),
+           "steps": steps, "ms_per_step": total_ms / max(1, steps), "tile": info["tile"],
+           "pairsum": pairsum, "gpu_launches": launches, "graph_replay": bool(stats["graph"]),
+           "redone_steps": stats["redone"], "roofline": roof,
+           "config": "N_k ~ U[64, 2048] seed 3, cutoff multiplier 0.5, prec 1e-6, zero stress"}
+    if cpu and rank == 0:
+        try:
+            seeds = [workloads.BATCH_SEED * 100003 + k for k in range(len(sizes))]
+            out["cpu_baseline"] = cpu_batch_baseline(sizes, seeds, acc / max(1, attempts))
+        except Exception as ex:
+            out["cpu_baseline"] = {"value": None, "kind": "unavailable", "sample": str(ex)[:200]}
+    return out
 
 
 def main():
@@ -630,7 +698,8 @@ def main():
     batch = None
     if not args.no_batch:
         try:
-            batch = measure_batch(torch, max(2, args.steps // 2), 2, args.pairsum, rank, ws, dist)
+            batch = measure_batch(torch, max(2, args.steps // 2), 2, args.pairsum, rank, ws, dist,
+                                  cpu=not args.no_cpu and ws == 1)
         except Exception as ex:  # reported, never required for the main line
             batch = {"error": str(ex)[:200]}
 

@@ -339,6 +339,12 @@ int sdddst_batch_info(void *batch, int *tile, long *total, long *launches, void 
  * were repeated host-driven from the step's snapshot. */
 int sdddst_batch_stats(void *batch, int *graph, long *redone);
 
+/* Times `reps` launches of the batch's pair-sum kernel (all systems' tiles,
+ * FP32 or FP64 as created) on the accepted configurations with CUDA events
+ * on the batch's stream; writes the mean device milliseconds of one launch
+ * and the number of unique pairs it evaluates. */
+int sdddst_batch_profile_pair_sum(void *batch, int reps, double *ms_per_launch, double *pairs);
+
 /* Launch statistics: number of kernels this context has launched so far. */
 long sdddst_kernel_launches(void *ctx);
 

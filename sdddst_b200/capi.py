@@ -41,6 +41,7 @@ EXPORTS = [
     "sdddst_batch_step", "sdddst_batch_get_scalars", "sdddst_batch_get_positions", "sdddst_batch_info",
     "sdddst_direct_stats", "sdddst_profile_direct", "sdddst_precond_apply", "sdddst_set_preconditioner_weights",
     "sdddst_learned_correction", "sdddst_solver_recoveries", "sdddst_batch_stats",
+    "sdddst_batch_profile_pair_sum",
 ]
 
 
@@ -110,6 +111,8 @@ def load(path: str = LIB_PATH):
                                       C.POINTER(C.c_void_p)]
     lib.sdddst_solver_stats.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long)]
     lib.sdddst_batch_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_long)]
+    lib.sdddst_batch_profile_pair_sum.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double),
+                                                  C.POINTER(C.c_double)]
     lib.sdddst_solver_recoveries.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long),
                                              C.POINTER(C.c_long)]
     lib.sdddst_profile_pair_sum.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
@@ -411,6 +414,12 @@ class Batch:
         g, r = C.c_int(0), C.c_long(0)
         _check(self.lib.sdddst_batch_stats(self.h, C.byref(g), C.byref(r)))
         return {"graph": g.value, "redone": r.value}
+
+    def profile_pair_sum(self, reps: int = 3):
+        """(mean device ms of one pair-sum launch over all systems, unique pairs)."""
+        ms, pairs = C.c_double(0), C.c_double(0)
+        _check(self.lib.sdddst_batch_profile_pair_sum(self.h, int(reps), C.byref(ms), C.byref(pairs)))
+        return ms.value, pairs.value
 
     def info(self):
         t, n, l, s = C.c_int(0), C.c_long(0), C.c_long(0), C.c_void_p()

@@ -1137,6 +1137,33 @@ int sdddst_batch_get_positions(void *batch, int which, double *x)
     return e.sync_check("batch positions");
 }
 
+int sdddst_batch_profile_pair_sum(void *batch, int reps, double *ms_per_launch, double *pairs)
+{
+    if (!batch || reps < 1) return SDDDST_ERR_INVALID;
+    sd::Batch *bt = static_cast<sd::Batch *>(batch);
+    sd::Engine &e = bt->e;
+    cudaSetDevice(e.device);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    sd::launch_batch_pair(*bt, e.d_x0, 0.0);
+    cudaEventRecord(a, e.st);
+    for (int r = 0; r < reps; ++r) sd::launch_batch_pair(*bt, e.d_x0, 0.0);
+    cudaEventRecord(b, e.st);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (ms_per_launch) *ms_per_launch = ms / reps;
+    if (pairs) {
+        double p = 0;
+        for (int k = 0; k < bt->B; ++k) p += 0.5 * (double)bt->nk[k] * (double)(bt->nk[k] - 1);
+        *pairs = p;
+    }
+    return e.sync_check("batch pair profile") ? SDDDST_ERR_CUDA : SDDDST_OK;
+}
+
 int sdddst_batch_stats(void *batch, int *graph, long *redone)
 {
     if (!batch) return SDDDST_ERR_INVALID;

@@ -5,6 +5,7 @@ import os
 import socket
 
 import numpy as np
+import pytest
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
@@ -63,3 +64,64 @@ def test_two_rank_gloo_share_and_gather():
         assert p.exitcode == 0
     expect = sorted((k, float(np.sum(workloads.dislocations(n, 1000 + k)[0][:, 0]))) for k, n in enumerate(sizes))
     assert res == expect
+
+
+def _batch_worker(rank, world, port, sizes, steps, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    from sdddst_b200 import capi
+    mine = sharding.rank_share(sizes, rank, world)
+    systems = [workloads.dislocations(int(sizes[k]), 700 + k)[0] for k in mine]
+    prm = capi.default_params(cutoff_multiplier=0.5, prec=1e-6, step_size=1e-6)
+    bt = capi.Batch(prm, systems)
+    acc = np.zeros(len(mine), dtype=np.int64)
+    for _ in range(steps):
+        acc += bt.step()
+    local = {k: (bt.positions(0)[q].tolist(), int(acc[q]), bt.scalars()[q, :5].tolist()) for q, k in enumerate(mine)}
+    bt.close()
+    gathered = [None] * world
+    dist.all_gather_object(gathered, local)
+    if rank == 0:
+        merged = {}
+        for g in gathered:
+            merged.update(g)
+        out.put(merged)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_two_rank_sharded_batch_equals_unsharded(engine_lib):
+    """The batched workload's host side at world size 2: each gloo rank steps
+    its LPT share of 24 systems (N in [64, 2048]) with capi.Batch on the GPU,
+    the per-system results are gathered once, and they equal an unsharded
+    batch of all 24 systems (same decisions and counters, positions within
+    1e-9: the union GMRES of a shard and of the whole batch stop after
+    different iteration counts, both below the residual target)."""
+    from sdddst_b200 import capi
+    sizes = [int(s) for s in workloads.batch_sizes(24, 3)]
+    steps = 4
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_batch_worker, args=(r, 2, port, sizes, steps, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = q.get(timeout=600)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert sorted(res) == list(range(len(sizes)))
+    systems = [workloads.dislocations(n, 700 + k)[0] for k, n in enumerate(sizes)]
+    bt = capi.Batch(capi.default_params(cutoff_multiplier=0.5, prec=1e-6, step_size=1e-6), systems)
+    acc = np.zeros(len(sizes), dtype=np.int64)
+    for _ in range(steps):
+        acc += bt.step()
+    xs, sc = bt.positions(0), bt.scalars()
+    for k in range(len(sizes)):
+        x_k, a_k, s_k = res[k]
+        assert a_k == acc[k], k
+        assert np.abs(np.array(x_k) - xs[k]).max() <= 1e-9, k
+        assert s_k[2] == sc[k, 2] and s_k[3] == sc[k, 3], k
+        assert np.isclose(s_k[1], sc[k, 1], rtol=1e-6), k
