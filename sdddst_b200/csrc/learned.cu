@@ -2,7 +2,11 @@
 // GMRES preconditioner of SDDDST_SOLVER_GMRES_LEARNED is M = B + C, C on the
 // sparsity pattern of J, its values from a message-passing network over the
 // cutoff-neighbour graph (hidden width 64, three rounds, ReLU).  Weights are
-// held in BF16 and converted on load; all arithmetic is FP32.
+// held in BF16.  The node products (P h, Q h, U [h; a], P_o h, Q_o h) run on
+// the tensor cores (node_gemm_tc.cu: BF16 node states and weights, FP32
+// accumulation in tensor memory; Q h kept in BF16 for the edge pass's
+// gather); the per-edge sums and the small input and output layers are FP32
+// on the CUDA cores.
 //
 //   h_i  = relu(W_in f_i + b_in)
 //   3 x: m_ij = relu(P h_i + b_P + Q h_j + R e_ij), a_i = mean_j m_ij,
@@ -17,9 +21,9 @@
 // t(sum_j |A_ji|), deg / 627]; edge [t(A_ij), t(A_ji), dx / 7c, dy / 7c,
 // same cluster block].  The message function is linear in [h_i; h_j; e_ij]
 // before its activation, so it splits into per-node projections (P h, Q h:
-// N x 64 x 64 products, shared-memory tiled) and a per-edge sum over the
-// CSR rows (one warp per row, one or two channels per lane); no edge-sized
-// matrix product exists.  The flat weight order and the features follow
+// N x 64 x 64 products, on the tensor cores) and a per-edge sum over the CSR
+// rows (one warp per row, two channels per lane); no edge-sized matrix
+// product exists.  The flat weight order and the features follow
 // sdddst_b200/learned.py, the PyTorch definition the network was trained in.
 #include <cuda_bf16.h>
 
@@ -31,6 +35,12 @@
 namespace sd {
 
 __global__ void scan_kernel(const int *__restrict__ in, int m, int *__restrict__ out);
+
+// node_gemm_tc.cu: the node products on the tensor cores
+void launch_node_proj_tc(int n, const float *h, const __nv_bfloat16 *w, long oP, long oPb, long oQ, float *ph,
+                         __nv_bfloat16 *qh, int *err, cudaStream_t st);
+void launch_node_update_tc(int n, float *h, const float *a, const __nv_bfloat16 *w, long oU, long oUb, int *err,
+                           cudaStream_t st);
 
 namespace {
 
@@ -81,7 +91,9 @@ struct Learned {
     float *d_cv = nullptr;
     __nv_bfloat16 *d_w = nullptr;
     WeightOffsets off{};
-    float *d_nf = nullptr, *d_h = nullptr, *d_ph = nullptr, *d_qh = nullptr, *d_agg = nullptr;
+    float *d_nf = nullptr, *d_h = nullptr, *d_ph = nullptr, *d_agg = nullptr;
+    __nv_bfloat16 *d_qh = nullptr;          // Q h in BF16 (the per-edge gather)
+    int *d_err = nullptr, *h_err = nullptr; // a tensor-core wait that ran out (device flag, pinned copy)
     double *d_jii = nullptr;
     float *d_cval = nullptr;
     long cval_cap = 0, ccap = 0;
@@ -139,43 +151,6 @@ __global__ void node_in_kernel(int n, const float *__restrict__ nf, const __nv_b
     hout[idx] = fmaxf(acc, 0.0f);
 }
 
-// ph = P h + b_P and qh = Q h for 32 nodes per CTA (weights transposed in
-// shared memory so that a warp reads consecutive output channels)
-constexpr int kProjNodes = 32;
-
-__global__ void __launch_bounds__(256) proj_kernel(int n, const float *__restrict__ hin,
-                                                   const __nv_bfloat16 *__restrict__ w, long oP, long oPb, long oQ,
-                                                   float *__restrict__ ph, float *__restrict__ qh)
-{
-    __shared__ float PT[kH][kH], QT[kH][kH], hs[kProjNodes][kH + 1];
-    const int tid = threadIdx.x;
-    for (int idx = tid; idx < kH * kH; idx += 256) {
-        const int c = idx >> 6, k = idx & 63;
-        PT[k][c] = bf(w, oP + idx);
-        QT[k][c] = bf(w, oQ + idx);
-    }
-    const int i0 = blockIdx.x * kProjNodes;
-    for (int idx = tid; idx < kProjNodes * kH; idx += 256) {
-        const int r = idx >> 6, k = idx & 63;
-        hs[r][k] = i0 + r < n ? hin[(long)(i0 + r) * kH + k] : 0.0f;
-    }
-    __syncthreads();
-    const int c = tid & 63, g = tid >> 6;
-    const float bp = bf(w, oPb + c);
-    for (int r = g; r < kProjNodes; r += 4) {
-        if (i0 + r >= n) break;
-        float a = bp, b = 0.0f;
-#pragma unroll 16
-        for (int k = 0; k < kH; ++k) {
-            const float hv = hs[r][k];
-            a = fmaf(PT[k][c], hv, a);
-            b = fmaf(QT[k][c], hv, b);
-        }
-        ph[(long)(i0 + r) * kH + c] = a;
-        qh[(long)(i0 + r) * kH + c] = b;
-    }
-}
-
 // per-edge pass, one warp per row: lane l holds channels l and l + 32.
 // kOut = false: agg_i = mean_j relu(ph_i + qh_j + R e_ij);
 // kOut = true:  C_ij = (w_o . relu(ph_i + qh_j + R e_ij) + b_o) A_ij / (J_ii J_jj)
@@ -184,7 +159,7 @@ __global__ void edge_kernel(int n, double h, const int *__restrict__ rowptr, con
                             const VT *__restrict__ val, const double *__restrict__ dvec,
                             const double *__restrict__ jii, const double *__restrict__ x,
                             const double *__restrict__ y, const int *__restrict__ blk, double cutoff,
-                            const float *__restrict__ ph, const float *__restrict__ qh,
+                            const float *__restrict__ ph, const __nv_bfloat16 *__restrict__ qh,
                             const __nv_bfloat16 *__restrict__ w, long oR, long owo, long owob,
                             float *__restrict__ agg, float *__restrict__ cval)
 {
@@ -247,8 +222,8 @@ __global__ void edge_kernel(int n, double h, const int *__restrict__ rowptr, con
             const float f4 = __shfl_sync(0xffffffffu, e4, t);
             float a = 0.0f, b = 0.0f;
             if (jt >= 0) {
-                a = p0 + qh[(long)jt * kH + c0];
-                b = p1 + qh[(long)jt * kH + c1];
+                a = p0 + __bfloat162float(qh[(long)jt * kH + c0]);
+                b = p1 + __bfloat162float(qh[(long)jt * kH + c1]);
                 a = fmaf(r0[0], f0, a); a = fmaf(r0[1], f1, a); a = fmaf(r0[2], f2, a);
                 a = fmaf(r0[3], f3, a); a = fmaf(r0[4], f4, a);
                 b = fmaf(r1[0], f0, b); b = fmaf(r1[1], f1, b); b = fmaf(r1[2], f2, b);
@@ -283,38 +258,6 @@ __global__ void edge_kernel(int n, double h, const int *__restrict__ rowptr, con
         const float inv = 1.0f / (float)max(cnt, 1);
         agg[(long)i * kH + c0] = s0 * inv;
         agg[(long)i * kH + c1] = s1 * inv;
-    }
-}
-
-// h_i += relu(U [h_i; a_i] + b_U), 16 nodes per CTA
-constexpr int kUpdNodes = 16;
-
-__global__ void __launch_bounds__(256) node_update_kernel(int n, float *__restrict__ hio, const float *__restrict__ agg,
-                                                     const __nv_bfloat16 *__restrict__ w, long oU, long oUb)
-{
-    __shared__ float UT[2 * kH][kH];
-    __shared__ float xs[kUpdNodes][2 * kH + 1];
-    const int tid = threadIdx.x;
-    for (int idx = tid; idx < kH * 2 * kH; idx += 256) {
-        const int c = idx / (2 * kH), k = idx % (2 * kH);
-        UT[k][c] = bf(w, oU + idx);
-    }
-    const int i0 = blockIdx.x * kUpdNodes;
-    for (int idx = tid; idx < kUpdNodes * 2 * kH; idx += 256) {
-        const int r = idx / (2 * kH), k = idx % (2 * kH);
-        float v = 0.0f;
-        if (i0 + r < n) v = k < kH ? hio[(long)(i0 + r) * kH + k] : agg[(long)(i0 + r) * kH + k - kH];
-        xs[r][k] = v;
-    }
-    __syncthreads();
-    const int c = tid & 63, g = tid >> 6;
-    const float bu = bf(w, oUb + c);
-    for (int r = g; r < kUpdNodes; r += 4) {
-        if (i0 + r >= n) break;
-        float a = bu;
-#pragma unroll 16
-        for (int k = 0; k < 2 * kH; ++k) a = fmaf(UT[k][c], xs[r][k], a);
-        hio[(long)(i0 + r) * kH + c] = xs[r][c] + fmaxf(a, 0.0f);
     }
 }
 
@@ -452,7 +395,10 @@ static int learned_ensure(Engine &e)
                     cudaMalloc(&L->d_nf, sizeof(float) * 4 * e.n) == cudaSuccess &&
                     cudaMalloc(&L->d_h, sizeof(float) * nh) == cudaSuccess &&
                     cudaMalloc(&L->d_ph, sizeof(float) * nh) == cudaSuccess &&
-                    cudaMalloc(&L->d_qh, sizeof(float) * nh) == cudaSuccess &&
+                    cudaMalloc(&L->d_qh, sizeof(__nv_bfloat16) * nh) == cudaSuccess &&
+                    cudaMalloc(&L->d_err, sizeof(int)) == cudaSuccess &&
+                    cudaMallocHost(&L->h_err, sizeof(int)) == cudaSuccess &&
+                    cudaMemset(L->d_err, 0, sizeof(int)) == cudaSuccess &&
                     cudaMalloc(&L->d_agg, sizeof(float) * nh) == cudaSuccess &&
                     cudaMalloc(&L->d_jii, sizeof(double) * e.n) == cudaSuccess;
     if (!ok) {
@@ -549,11 +495,13 @@ int learned_build(Engine &e, double h, const double *dvec, const double *x, bool
         L.builds++;
         return 0;
     }
+    if (*L.h_err) { // the previous build's tensor-core wait ran out
+        e.err = "learned preconditioner: a tensor-core product did not complete";
+        return SDDDST_ERR_CUDA;
+    }
     node_in_kernel<<<(unsigned)(((long)n * kH + 255) / 256), 256, 0, st>>>(n, L.d_nf, L.d_w, o.in_w, o.in_b, L.d_h);
-    const unsigned pgrid = (unsigned)((n + kProjNodes - 1) / kProjNodes);
-    const unsigned ugrid = (unsigned)((n + kUpdNodes - 1) / kUpdNodes);
     for (int l = 0; l < kLayers; ++l) {
-        proj_kernel<<<pgrid, 256, 0, st>>>(n, L.d_h, L.d_w, o.P[l], o.Pb[l], o.Q[l], L.d_ph, L.d_qh);
+        launch_node_proj_tc(n, L.d_h, L.d_w, o.P[l], o.Pb[l], o.Q[l], L.d_ph, L.d_qh, L.d_err, st);
         if (e.valf)
             edge_kernel<float, false><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_valf, dvec, L.d_jii, x,
                                                              e.d_y, e.pc.blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w,
@@ -562,9 +510,9 @@ int learned_build(Engine &e, double h, const double *dvec, const double *x, bool
             edge_kernel<double, false><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, L.d_jii, x,
                                                               e.d_y, e.pc.blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w,
                                                               o.R[l], 0, 0, L.d_agg, nullptr);
-        node_update_kernel<<<ugrid, 256, 0, st>>>(n, L.d_h, L.d_agg, L.d_w, o.U[l], o.Ub[l]);
+        launch_node_update_tc(n, L.d_h, L.d_agg, L.d_w, o.U[l], o.Ub[l], L.d_err, st);
     }
-    proj_kernel<<<pgrid, 256, 0, st>>>(n, L.d_h, L.d_w, o.Po, o.Pob, o.Qo, L.d_ph, L.d_qh);
+    launch_node_proj_tc(n, L.d_h, L.d_w, o.Po, o.Pob, o.Qo, L.d_ph, L.d_qh, L.d_err, st);
     if (e.valf)
         edge_kernel<float, true><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_valf, dvec, L.d_jii, x, e.d_y,
                                                         e.pc.blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w, o.Ro, o.wo,
@@ -574,6 +522,7 @@ int learned_build(Engine &e, double h, const double *dvec, const double *x, bool
                                                          e.d_y, e.pc.blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w, o.Ro,
                                                          o.wo, o.wob, nullptr, L.d_cval);
     diag_out_kernel<<<wrows, 256, 0, st>>>(n, L.d_h, L.d_w, o.wd, o.wdb, L.d_jii, e.d_rowptr, L.d_cval);
+    cudaMemcpyAsync(L.h_err, L.d_err, sizeof(int), cudaMemcpyDeviceToHost, st); // read at the next build
     e.launches += 4 + 3 * kLayers + 2;
     L.builds++;
     return 0;
@@ -605,7 +554,12 @@ int learned_export(Engine &e, float *host, long cap)
     if (!Lp || !Lp->d_cval) return SDDDST_ERR_INVALID;
     if (cap < e.nnz) return SDDDST_ERR_CAPACITY;
     cudaMemcpyAsync(host, Lp->d_cval, sizeof(float) * e.nnz, cudaMemcpyDeviceToHost, e.st);
-    return e.sync_check("learned export");
+    if (int rc = e.sync_check("learned export")) return rc;
+    if (*Lp->h_err) {
+        e.err = "learned preconditioner: a tensor-core product did not complete";
+        return SDDDST_ERR_CUDA;
+    }
+    return 0;
 }
 
 void learned_free(Engine &e)
@@ -613,9 +567,10 @@ void learned_free(Engine &e)
     Learned *L = LN(e);
     if (!L) return;
     void *bufs[] = {L->d_w, L->d_nf, L->d_h, L->d_ph, L->d_qh, L->d_agg, L->d_jii, L->d_cval, L->d_crow, L->d_ccnt,
-                    L->d_ccol, L->d_cv};
+                    L->d_ccol, L->d_cv, L->d_err};
     for (void *b : bufs)
         if (b) cudaFree(b);
+    if (L->h_err) cudaFreeHost(L->h_err);
     delete L;
     e.learned = nullptr;
 }

@@ -7,8 +7,10 @@ The GMRES preconditioner of the learned solver mode is M = B + C:
 * C has the sparsity pattern of J (the cutoff-neighbour graph) and its values
   come from a small message-passing network over that graph.
 
-Network (hidden width H = 64, ReLU, weights stored in BF16, arithmetic in
-FP32):
+Network (hidden width H = 64, ReLU, weights stored in BF16; the node
+products P h, Q h, U [h; a], P_o h, Q_o h take BF16 operands and accumulate
+in FP32 (the tensor-core form of csrc/node_gemm_tc.cu), Q h and Q_o h are
+kept in BF16, everything else is FP32):
 
     h_i  = relu(W_in f_i + b_in)                                  node input
     3 x: m_ij = relu(P h_i + b_P + Q h_j + R e_ij)               messages
@@ -134,14 +136,18 @@ def make_net():
 
         def forward(self, g):
             relu = torch.relu
+            # the node products take BF16 operands (node states rounded to
+            # BF16, BF16 weights) and accumulate in FP32, as on the tensor
+            # cores; Q h is kept in BF16 for the per-edge gather
+            bf = lambda t: t.to(torch.bfloat16).float()
             h = relu(self.inp(g.node_f))
             deg = g.deg.float().clamp(min=1.0)[:, None]
             for l in range(LAYERS):
-                ph, qh = self.P[l](h), self.Q[l](h)
+                ph, qh = self.P[l](bf(h)), bf(self.Q[l](bf(h)))
                 m = relu(ph[g.r] + qh[g.c] + self.R[l](g.edge_f))
                 a = torch.zeros_like(h).index_add_(0, g.r, m) / deg
-                h = h + relu(self.U[l](torch.cat([h, a], 1)))
-            po, qo = self.Po(h), self.Qo(h)
+                h = h + relu(self.U[l](torch.cat([bf(h), bf(a)], 1)))
+            po, qo = self.Po(bf(h)), bf(self.Qo(bf(h)))
             c_edge = self.wo(relu(po[g.r] + qo[g.c] + self.Ro(g.edge_f))).squeeze(1) - (1.0 - g.edge_f[:, 4])
             c_diag = self.wd(h).squeeze(1)
             return c_edge, c_diag

@@ -4,8 +4,12 @@
   through the BF16 packing.
 * GPU: the CUDA inference (csrc/learned.cu) against the PyTorch FP32
   definition of the same network (sdddst_b200/learned.py) with the same BF16
-  weights, on the same Jacobian and cluster blocks (FP32 arithmetic in both,
-  different summation orders: 2e-5 of the largest |C| plus 1e-4 relative);
+  weights, on the same Jacobian and cluster blocks (BF16 operands and FP32
+  accumulation in the node products of both, different summation orders:
+  a node state or Q h near a BF16 rounding tie can round to neighbouring
+  BF16 values, 2^-8 apart, so entries agree within 2e-3 of the largest |C|
+  plus 1e-2 relative, the median within 1e-5 of it; C only preconditions
+  GMRES, which solves to 1e-13 either way, as the trajectory test checks);
   the learned solver's trajectory against the cluster-preconditioned one
   (both solve to a 1e-13 residual: same decisions, positions within 1e-9).
 """
@@ -66,7 +70,8 @@ def test_learned_inference_matches_torch(engine_lib):
     scale = np.abs(ref).max()
     assert scale > 0
     err = np.abs(cval.astype(np.float64) - ref)
-    assert np.all(err <= 2e-5 * scale + 1e-4 * np.abs(ref)), (err.max(), scale)
+    assert np.all(err <= 2e-3 * scale + 1e-2 * np.abs(ref)), (err.max(), scale)
+    assert np.median(err) <= 1e-5 * scale, (np.median(err), scale)
 
 
 @pytest.mark.gpu
