@@ -317,6 +317,7 @@ int sdddst_solve_csc(void *ctx, const int *Ap, const int *Ai, const double *Ax, 
     sd::Engine *e = E(ctx);
     cudaSetDevice(e->device);
     const int n = e->n;
+    sd::learned_invalidate(*e); // the CSR is replaced below
     try {
         // CSC of A -> CSR rows of G = A - I with the diagonal in each row's first slot
         std::vector<int> cnt(n + 1, 1);

@@ -253,6 +253,7 @@ int Engine::speeds(const double *x, double *v_out, double *S_out, int stress_typ
 
 int Engine::assemble(const double *x)
 {
+    learned_invalidate(*this);
     int rc = jacobian_assemble(*this, x);
     if (rc == 0 && (prm.solver == SDDDST_SOLVER_DIRECT || prm.solver == SDDDST_SOLVER_DIRECT_MIXED))
         rc = direct_analyse(*this, x);
@@ -339,13 +340,17 @@ int Engine::solve_fused(double h, const double *dvec, Cluster &c, const double *
     return 0;
 }
 
-int Engine::prepare_solver(double h)
+int Engine::prepare_solver(double h, bool same_assembly)
 {
     if (prm.solver == SDDDST_SOLVER_GMRES_CLUSTER) return precond_build(*this, h, d_dvec);
     if (prm.solver == SDDDST_SOLVER_DIRECT || prm.solver == SDDDST_SOLVER_DIRECT_MIXED)
         return direct_factor(*this, h, d_dvec);
     if (prm.solver == SDDDST_SOLVER_GMRES_LEARNED || prm.solver == SDDDST_SOLVER_GMRES_NEUMANN) {
         if (int rc = precond_build(*this, h, d_dvec)) return rc;
+        // the network runs once per assembly: a second step size on the same
+        // assembly (stage II's h/2 after stage I's h) rescales its outputs
+        if (same_assembly && prm.solver == SDDDST_SOLVER_GMRES_LEARNED && learned_rescale(*this, h, d_dvec))
+            return 0;
         return learned_build(*this, h, d_dvec, d_xasm, prm.solver == SDDDST_SOLVER_GMRES_NEUMANN);
     }
     return 0;
@@ -409,7 +414,7 @@ int Engine::integrate(double h, double *xn, const double *xo, bool use2, bool in
         if (int rc = assemble(xn)) return rc;
     launch_make_dvec(*this, h, d_dvec, st);
     launches++;
-    if (int rc = prepare_solver(h)) return rc;
+    if (int rc = prepare_solver(h, reuse_assembly)) return rc;
     double *csp0 = use2 ? d_vs2 : d_vs;
     for (int it = 0; it < ic; ++it) {
         if (int rc = stage_residual(h, it, xn, xo, use2, init_speed, origin, end, csp0, d_dvec, d_g)) return rc;

@@ -141,7 +141,9 @@ struct Engine {
     int speeds(const double *x, double *v_out, double *S_out, int stress_type, bool update_tol);
     int assemble(const double *x);
     int solve(double h, const double *rhs, double *x_out);
-    int prepare_solver(double h); // per matrix: preconditioner set-up
+    // per matrix: preconditioner set-up; same_assembly: the matrix shares the
+    // previous set-up's assembly (only h differs)
+    int prepare_solver(double h, bool same_assembly = false);
     int integrate(double h, double *xn, const double *xo, bool use2, bool init_speed, int origin, int end,
                   bool reuse_assembly);
     // calculateG of one chord-Newton iteration of one stage: speeds at the
@@ -244,6 +246,8 @@ int fused_gmres(Engine &e, int ns, const double *h, const double *const *dvec, c
 int learned_set_weights(Engine &e, const unsigned short *bf16, long count);
 int learned_build(Engine &e, double h, const double *dvec, const double *x, bool analytic);
 void learned_apply_add(Engine &e, const double *v, double *z);
+bool learned_rescale(Engine &e, double h, const double *dvec);
+void learned_invalidate(Engine &e);
 int learned_export(Engine &e, float *host, long cap);
 void learned_free(Engine &e);
 long learned_weight_count();

@@ -96,8 +96,10 @@ struct Learned {
     int *d_err = nullptr, *h_err = nullptr; // a tensor-core wait that ran out (device flag, pinned copy)
     double *d_jii = nullptr;
     float *d_cval = nullptr;
+    float *d_craw = nullptr, *d_crawd = nullptr; // the network's raw outputs of the last inference
     long cval_cap = 0, ccap = 0;
-    long builds = 0;
+    long builds = 0, rescales = 0;
+    bool raw_valid = false; // d_craw / d_crawd hold the outputs of an inference on the current assembly
 };
 
 Learned *LN(Engine &e) { return static_cast<Learned *>(e.learned); }
@@ -161,7 +163,7 @@ __global__ void edge_kernel(int n, double h, const int *__restrict__ rowptr, con
                             const double *__restrict__ y, const int *__restrict__ blk, double cutoff,
                             const float *__restrict__ ph, const __nv_bfloat16 *__restrict__ qh,
                             const __nv_bfloat16 *__restrict__ w, long oR, long owo, long owob,
-                            float *__restrict__ agg, float *__restrict__ cval)
+                            float *__restrict__ agg, float *__restrict__ cval, float *__restrict__ craw)
 {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -251,7 +253,11 @@ __global__ void edge_kernel(int n, double h, const int *__restrict__ rowptr, con
                     v[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
                 }
             }
-            if (j >= 0) cval[q] = (v[0] + bo - (1.0f - e4)) * sc;
+            if (j >= 0) {
+                const float c = v[0] + bo; // the network's part of c_ij
+                cval[q] = (c - (1.0f - e4)) * sc;
+                craw[q] = c;
+            }
         }
     }
     if (!kOut) {
@@ -337,7 +343,7 @@ __global__ void c_apply_kernel(int n, const int *__restrict__ crow, const int *_
 // C_ii = (w_d . h_i + b_d) / J_ii into each row's diagonal slot (slot 0)
 __global__ void diag_out_kernel(int n, const float *__restrict__ hin, const __nv_bfloat16 *__restrict__ w, long owd,
                                 long owdb, const double *__restrict__ jii, const int *__restrict__ rowptr,
-                                float *__restrict__ cval)
+                                float *__restrict__ cval, float *__restrict__ crawd)
 {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -345,7 +351,43 @@ __global__ void diag_out_kernel(int n, const float *__restrict__ hin, const __nv
     float v = bf(w, owd + lane) * hin[(long)i * kH + lane] + bf(w, owd + lane + 32) * hin[(long)i * kH + lane + 32];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) cval[rowptr[i]] = (float)((v + bf(w, owdb)) / jii[i]);
+    if (lane == 0) {
+        const float c = v + bf(w, owdb);
+        cval[rowptr[i]] = (float)(c / jii[i]);
+        crawd[i] = c;
+    }
+}
+
+// C for J(h') from the network outputs of another step size on the same
+// assembly: C_ij = (c_ij - (1 - s_ij)) A_ij / (J_ii J_jj), C_ii = c_ii / J_ii
+// with A, J and the cluster blocks s of h' (one warp per row).  The network
+// runs once per assembly; stage II's J(h/2) reuses stage I's outputs.
+template <typename VT>
+__global__ void rescale_kernel(int n, double h, const int *__restrict__ rowptr, const int *__restrict__ col,
+                               const VT *__restrict__ val, const double *__restrict__ gdiag,
+                               const double *__restrict__ dvec, const int *__restrict__ blk,
+                               const float *__restrict__ craw, const float *__restrict__ crawd,
+                               float *__restrict__ cval)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const double di = (1.0 + dvec[i]) * 0.5 * h;
+    const double ji = 1.0 + di * gdiag[i];
+    const int bi = blk[i];
+    const int s = rowptr[i], e = rowptr[i + 1];
+    for (int q = s + lane; q < e; q += 32) {
+        const int j = col[q];
+        if (j == i) {
+            cval[q] = (float)(crawd[i] / ji);
+            continue;
+        }
+        const double aij = di * (double)val[q];
+        const double jj = 1.0 + (1.0 + dvec[j]) * 0.5 * h * gdiag[j];
+        const float sc = (float)(aij / (ji * jj));
+        const float e4 = blk[j] == bi ? 1.0f : 0.0f;
+        cval[q] = (craw[q] - (1.0f - e4)) * sc;
+    }
 }
 
 // z += C v, one warp per row
@@ -400,6 +442,7 @@ static int learned_ensure(Engine &e)
                     cudaMallocHost(&L->h_err, sizeof(int)) == cudaSuccess &&
                     cudaMemset(L->d_err, 0, sizeof(int)) == cudaSuccess &&
                     cudaMalloc(&L->d_agg, sizeof(float) * nh) == cudaSuccess &&
+                    cudaMalloc(&L->d_crawd, sizeof(float) * e.n) == cudaSuccess &&
                     cudaMalloc(&L->d_jii, sizeof(double) * e.n) == cudaSuccess;
     if (!ok) {
         e.err = "learned preconditioner: out of device memory";
@@ -437,10 +480,13 @@ int learned_build(Engine &e, double h, const double *dvec, const double *x, bool
     Learned &L = *LN(e);
     if (e.nnz > L.cval_cap) {
         if (L.d_cval) cudaFree(L.d_cval);
+        if (L.d_craw) cudaFree(L.d_craw);
         L.d_cval = nullptr;
+        L.d_craw = nullptr;
         L.cval_cap = 0;
         const long cap = e.nnz + e.nnz / 8;
-        if (cudaMalloc(&L.d_cval, sizeof(float) * cap) != cudaSuccess) {
+        if (cudaMalloc(&L.d_cval, sizeof(float) * cap) != cudaSuccess ||
+            cudaMalloc(&L.d_craw, sizeof(float) * cap) != cudaSuccess) {
             e.err = "learned preconditioner: out of device memory";
             return SDDDST_ERR_NOMEM;
         }
@@ -505,27 +551,52 @@ int learned_build(Engine &e, double h, const double *dvec, const double *x, bool
         if (e.valf)
             edge_kernel<float, false><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_valf, dvec, L.d_jii, x,
                                                              e.d_y, e.pc.blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w,
-                                                             o.R[l], 0, 0, L.d_agg, nullptr);
+                                                             o.R[l], 0, 0, L.d_agg, nullptr, nullptr);
         else
             edge_kernel<double, false><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, L.d_jii, x,
                                                               e.d_y, e.pc.blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w,
-                                                              o.R[l], 0, 0, L.d_agg, nullptr);
+                                                              o.R[l], 0, 0, L.d_agg, nullptr, nullptr);
         launch_node_update_tc(n, L.d_h, L.d_agg, L.d_w, o.U[l], o.Ub[l], L.d_err, st);
     }
     launch_node_proj_tc(n, L.d_h, L.d_w, o.Po, o.Pob, o.Qo, L.d_ph, L.d_qh, L.d_err, st);
     if (e.valf)
         edge_kernel<float, true><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_valf, dvec, L.d_jii, x, e.d_y,
                                                         e.pc.blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w, o.Ro, o.wo,
-                                                        o.wob, nullptr, L.d_cval);
+                                                        o.wob, nullptr, L.d_cval, L.d_craw);
     else
         edge_kernel<double, true><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, e.d_val, dvec, L.d_jii, x,
                                                          e.d_y, e.pc.blk_of, e.cutoff, L.d_ph, L.d_qh, L.d_w, o.Ro,
-                                                         o.wo, o.wob, nullptr, L.d_cval);
-    diag_out_kernel<<<wrows, 256, 0, st>>>(n, L.d_h, L.d_w, o.wd, o.wdb, L.d_jii, e.d_rowptr, L.d_cval);
+                                                         o.wo, o.wob, nullptr, L.d_cval, L.d_craw);
+    diag_out_kernel<<<wrows, 256, 0, st>>>(n, L.d_h, L.d_w, o.wd, o.wdb, L.d_jii, e.d_rowptr, L.d_cval, L.d_crawd);
     cudaMemcpyAsync(L.h_err, L.d_err, sizeof(int), cudaMemcpyDeviceToHost, st); // read at the next build
     e.launches += 4 + 3 * kLayers + 2;
     L.builds++;
+    L.raw_valid = true;
     return 0;
+}
+
+// C of the network for J(h) from the outputs of the last inference on the
+// same assembly (false when there is none: run learned_build)
+bool learned_rescale(Engine &e, double h, const double *dvec)
+{
+    Learned *Lp = LN(e);
+    if (!Lp || !Lp->raw_valid || !Lp->has_weights) return false;
+    const unsigned wrows = (unsigned)((e.n + 7) / 8);
+    if (e.valf)
+        rescale_kernel<float><<<wrows, 256, 0, e.st>>>(e.n, h, e.d_rowptr, e.d_col, e.d_valf, e.d_gdiag, dvec,
+                                                       e.pc.blk_of, Lp->d_craw, Lp->d_crawd, Lp->d_cval);
+    else
+        rescale_kernel<double><<<wrows, 256, 0, e.st>>>(e.n, h, e.d_rowptr, e.d_col, e.d_val, e.d_gdiag, dvec,
+                                                        e.pc.blk_of, Lp->d_craw, Lp->d_crawd, Lp->d_cval);
+    e.launches++;
+    Lp->rescales++;
+    return true;
+}
+
+// a new assembly: the network's outputs no longer match the pattern
+void learned_invalidate(Engine &e)
+{
+    if (Learned *Lp = LN(e)) Lp->raw_valid = false;
 }
 
 void learned_apply_add(Engine &e, const double *v, double *z)
@@ -567,7 +638,7 @@ void learned_free(Engine &e)
     Learned *L = LN(e);
     if (!L) return;
     void *bufs[] = {L->d_w, L->d_nf, L->d_h, L->d_ph, L->d_qh, L->d_agg, L->d_jii, L->d_cval, L->d_crow, L->d_ccnt,
-                    L->d_ccol, L->d_cv, L->d_err};
+                    L->d_ccol, L->d_cv, L->d_err, L->d_craw, L->d_crawd};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (L->h_err) cudaFreeHost(L->h_err);
