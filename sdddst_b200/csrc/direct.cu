@@ -40,6 +40,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
 #include <vector>
 
 #include "common.cuh"
@@ -749,6 +750,179 @@ __global__ void __launch_bounds__(256, sizeof(FT) == 4 ? 2 : 1)
     }
 }
 
+// The same trailing update for FP32 fronts on the 5th-gen tensor cores
+// (tcgen05, kind::tf32): one CTA of 128 threads per 128 x 128 tile of C,
+// D = A B accumulated in FP32 in tensor memory, C -= D in the epilogue.  A
+// TF32 operand keeps 10 mantissa bits, so the product is compensated: with
+// A_lo = A - tf32(A) and B_lo = B - tf32(B) (exact in FP32),
+//   A B ~ A B + A B_lo + A_lo B   (tf32 parts; the dropped A_lo B_lo is
+// below 2^-20 of A B), which keeps the factors near FP32 accuracy and the
+// FP64 refinement at its usual step count.  K runs in chunks of 32: the
+// threads stage A, A_lo (128 x 32, K-major) and B, B_lo (transposed to
+// 128 x 32, K-major) in shared memory in the no-swizzle core-matrix layout
+// (8 rows x 16 bytes per core matrix, K-adjacent ones 128 bytes apart, 8-row
+// groups 1024 bytes apart), one thread issues 3 x 4 MMAs (M = N = 128,
+// K = 8) and commits them to an mbarrier whose phase the CTA waits for
+// (bounded; past the limit *err is set and the tile is left unchanged)
+// before restaging.  Same modes and tile order as update_kernel.
+constexpr int kTcK = 32;                                  // K chunk
+constexpr unsigned kTcOp = 128 * kTcK * 4;                // one staged operand: 16 KB
+constexpr size_t kTcSmem = 4 * (size_t)kTcOp + 1024;      // A, A_lo, B, B_lo (+ alignment slack)
+
+__device__ __forceinline__ unsigned tc_off(int r, int k) // element (r, k) of a 128 x kTcK FP32 tile
+{
+    return (unsigned)((r >> 3) * 1024 + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4);
+}
+
+__device__ __forceinline__ unsigned long long tc_desc(unsigned addr)
+{
+    // start address, leading byte offset 128 (K-adjacent core matrices),
+    // stride byte offset 1024 (8-row groups), version 1, no swizzle
+    return (unsigned long long)((addr >> 4) & 0x3FFFu) | ((unsigned long long)(128u >> 4) << 16) |
+           ((unsigned long long)(1024u >> 4) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ float tf32_lo(float v) // v - (v with its low 13 mantissa bits cleared)
+{
+    return v - __uint_as_float(__float_as_uint(v) & 0xFFFFE000u);
+}
+
+__global__ void __launch_bounds__(128)
+    update_tc_kernel(const FrontInfo *__restrict__ fr, const int *__restrict__ list, int J, int mode,
+                     float *__restrict__ F, int *__restrict__ err)
+{
+    // instruction descriptor: FP32 accumulator, TF32 A and B, both K-major, N = 128, M = 128
+    constexpr unsigned kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+    const FrontInfo f = fr[list[blockIdx.y]];
+    const int s = J * 2 * kNB;
+    if (s >= f.p) return;
+    const int e0 = s + min(kNB, f.p - s), e1 = min(f.p, s + 2 * kNB);
+    int rlo, rhi, clo, chi, kend;
+    if (mode == 0) {
+        rlo = e0; rhi = f.n; clo = e0; chi = e1; kend = e0;
+    } else if (mode == 1) {
+        rlo = e0; rhi = e1; clo = e1; chi = f.n; kend = e0;
+    } else if (mode == 2) {
+        rlo = e1; rhi = f.n; clo = e1; chi = min(f.n, s + 4 * kNB); kend = e1;
+    } else {
+        rlo = e1; rhi = f.n; clo = s + 4 * kNB; chi = f.n; kend = e1;
+    }
+    if (rlo >= rhi || clo >= chi) return;
+    const int b = kend - s;
+    const int tm = (rhi - rlo + kBM - 1) / kBM, tn = (chi - clo + kBM - 1) / kBM;
+    if ((int)blockIdx.x >= tm * tn) return; // whole CTA: before any barrier or allocation
+    const int row0 = rlo + (blockIdx.x / tn) * kBM, col0 = clo + (blockIdx.x % tn) * kBM;
+    extern __shared__ __align__(16) unsigned char tcs_raw[];
+    // 1024-byte aligned operand area
+    unsigned char *tcs = tcs_raw + ((1024u - ((unsigned)__cvta_generic_to_shared(tcs_raw) & 1023u)) & 1023u);
+    unsigned char *sA = tcs, *sAl = tcs + kTcOp, *sB = tcs + 2 * kTcOp, *sBl = tcs + 3 * kTcOp;
+    __shared__ __align__(8) unsigned long long mbar;
+    __shared__ unsigned tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float *Ff = F + f.foff;
+    const long ld = f.ld;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (unsigned)__cvta_generic_to_shared(&tmem_slot)),
+                     "r"(128u));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(&mbar)),
+                     "r"(1u));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = tmem_slot;
+    const unsigned mb = (unsigned)__cvta_generic_to_shared(&mbar);
+    const int nk = (b + kTcK - 1) / kTcK;
+    bool ok = true;
+    for (int kc = 0; kc < nk && ok; ++kc) {
+        const int k0 = kc * kTcK;
+        // stage (zeros outside the ranges): a warp reads 32 consecutive K of
+        // one row of A, and 32 consecutive columns of one row of B
+#pragma unroll 4
+        for (int q = 0; q < kTcK; ++q) {
+            const int idx = tid + 128 * q;
+            const int ra = idx >> 5, ka = idx & 31;      // A: row ra, K ka
+            const int kb = idx >> 7, cb = idx & 127;     // B: K kb, column cb
+            const float a = (k0 + ka < b && row0 + ra < rhi) ? Ff[(long)(row0 + ra) * ld + s + k0 + ka] : 0.0f;
+            const float bb = (k0 + kb < b && col0 + cb < chi) ? Ff[(long)(s + k0 + kb) * ld + col0 + cb] : 0.0f;
+            const unsigned oa = tc_off(ra, ka), ob = tc_off(cb, kb);
+            *reinterpret_cast<float *>(sA + oa) = a;
+            *reinterpret_cast<float *>(sAl + oa) = tf32_lo(a);
+            *reinterpret_cast<float *>(sB + ob) = bb;
+            *reinterpret_cast<float *>(sBl + ob) = tf32_lo(bb);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) {
+            const unsigned a0 = (unsigned)__cvta_generic_to_shared(sA), al0 = (unsigned)__cvta_generic_to_shared(sAl);
+            const unsigned b0 = (unsigned)__cvta_generic_to_shared(sB), bl0 = (unsigned)__cvta_generic_to_shared(sBl);
+#pragma unroll
+            for (int t = 0; t < kTcK / 8; ++t) {
+                const unsigned off = 256u * t;
+                const unsigned long long pa[3] = {tc_desc(a0 + off), tc_desc(a0 + off), tc_desc(al0 + off)};
+                const unsigned long long pb[3] = {tc_desc(b0 + off), tc_desc(bl0 + off), tc_desc(b0 + off)};
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    const unsigned acc = (kc > 0 || t > 0 || q > 0) ? 1u : 0u;
+                    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                 "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                                 "l"(pa[q]), "l"(pb[q]), "r"(kIdesc), "r"(acc));
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mb)
+                         : "memory");
+        }
+        // the chunk's MMAs done (phase kc & 1) before the operands are restaged or D is read
+        unsigned done = 0;
+        for (int it = 0; it < (1 << 22) && !done; ++it) {
+            asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                         "selp.u32 %0, 1, 0, p;\n\t}"
+                         : "=r"(done)
+                         : "r"(mb), "r"((unsigned)(kc & 1))
+                         : "memory");
+            if (!done && it > 32) __nanosleep(64);
+        }
+        ok = __syncthreads_and(done) != 0;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(err, 1);
+    } else {
+        // epilogue: warp w holds rows 32 w .. 32 w + 31 (one TMEM lane each)
+        const int r = row0 + warp * 32 + lane;
+        const unsigned lane_base = (unsigned)(warp * 32) << 16;
+        float *row = Ff + (long)min(r, rhi - 1) * ld;
+#pragma unroll 1
+        for (int c0 = 0; c0 < kBM; c0 += 16) {
+            unsigned v[16];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                         "%12, %13, %14, %15}, [%16];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                           "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                           "=r"(v[14]), "=r"(v[15])
+                         : "r"(tmem + lane_base + (unsigned)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (r < rhi) {
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const int cc = col0 + c0 + q;
+                    if (cc < chi) row[cc] -= __uint_as_float(v[q]);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128u));
+}
+
 // ------------------------------------------------------------ solve kernels
 
 // forward, per front: own part from the right-hand side, update part zero,
@@ -1049,7 +1223,7 @@ int direct_analyse(Engine &e, const double *x)
                   cudaMalloc(&d->d_xw, sizeof(double) * n) == cudaSuccess &&
                   cudaMalloc(&d->d_yw, sizeof(double) * n) == cudaSuccess &&
                   cudaMalloc(&d->d_Y, sizeof(double) * n) == cudaSuccess &&
-                  cudaMalloc(&d->d_npert, sizeof(int)) == cudaSuccess;
+                  cudaMalloc(&d->d_npert, 2 * sizeof(int)) == cudaSuccess; // perturbed pivots, tensor-core failures
         if (!ok) {
             e.err = "direct solver: out of device memory";
             return SDDDST_ERR_NOMEM;
@@ -1073,7 +1247,7 @@ int direct_analyse(Engine &e, const double *x)
     }
     d.analysed = d.factored = false;
     const int T = d.T;
-    if (int rc = ensure_host_buf(d, 2 * T)) {
+    if (int rc = ensure_host_buf(d, 2 * T + 4)) {
         e.err = "direct solver: pinned buffer";
         return rc;
     }
@@ -1190,7 +1364,19 @@ template <typename FT> static int factor_impl(Engine &e, Direct &d, double h, co
     }
     cudaMemsetAsync(F, 0, sizeof(FT) * (size_t)d.F_used, st);
     cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
-    cudaMemsetAsync(d.d_npert, 0, sizeof(int), st);
+    cudaMemsetAsync(d.d_npert, 0, 2 * sizeof(int), st);
+    // FP32 fronts: the trailing updates on the tensor cores (compensated TF32)
+    // unless SDDDST_LU_CUDA_CORES is set
+    const int *list_cur = nullptr;
+    const bool tc = sizeof(FT) == 4 && std::getenv("SDDDST_LU_CUDA_CORES") == nullptr;
+    if (tc) cudaFuncSetAttribute(update_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+    auto update = [&](unsigned gx, int nf_, cudaStream_t s_, int J_, int mode) {
+        if (tc)
+            update_tc_kernel<<<dim3(gx, nf_), 128, kTcSmem, s_>>>(d.d_fr, list_cur, J_, mode,
+                                                                 reinterpret_cast<float *>(F), d.d_npert + 1);
+        else
+            update_kernel<FT><<<dim3(gx, nf_), 256, upd_smem<FT>(), s_>>>(d.d_fr, list_cur, J_, mode, F);
+    };
     const int wpb = 8;
     if (e.valf)
         assemble_kernel<float, FT><<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(
@@ -1204,6 +1390,7 @@ template <typename FT> static int factor_impl(Engine &e, Direct &d, double h, co
     for (int l = d.maxdepth; l >= 0; --l) {
         const int nf = (int)d.levels[l].size();
         const int *list = d.d_levels + d.level_off[l];
+        list_cur = list;
         if (d.level_umax[l] > 0) {
             const int tiles = (d.level_umax[l] + 31) / 32;
             for (int slot = 0; slot < 2; ++slot)
@@ -1228,28 +1415,33 @@ template <typename FT> static int factor_impl(Engine &e, Direct &d, double h, co
                                                                                 d.d_perm, d.d_npert);
             panel_kernel<FT><<<dim3(1 + half, nf), 256, kPanelSmem, d.side>>>(d.d_fr, list, j0, F, d.d_inv,
                                                                          d.d_perm, 1, 1, 1);
-            update_kernel<FT><<<dim3(tiles, nf), 256, upd_smem<FT>(), d.side>>>(d.d_fr, list, J, 0, F);
+            update(tiles, nf, d.side, J, 0);
             diag_block_kernel<FT><<<dim3(1, nf), kDiagThreads, kDiagSmem, d.side>>>(d.d_fr, list, j1, F, d.d_inv,
                                                                                 d.d_perm, d.d_npert);
             cudaEventRecord(d.ev_side, d.side);
             cudaStreamWaitEvent(st, d.ev_side, 0);
             panel_kernel<FT><<<dim3(half, nf), 256, kPanelSmem, st>>>(d.d_fr, list, j0, F, d.d_inv, d.d_perm, 2,
                                                                  half, 0);
-            update_kernel<FT><<<dim3(tiles, nf), 256, upd_smem<FT>(), st>>>(d.d_fr, list, J, 1, F);
+            update(tiles, nf, st, J, 1);
             panel_kernel<FT><<<dim3(2 * half, nf), 256, kPanelSmem, st>>>(d.d_fr, list, j1, F, d.d_inv, d.d_perm,
                                                                      3, half, 1);
-            update_kernel<FT><<<dim3(2 * tiles, nf), 256, upd_smem<FT>(), st>>>(d.d_fr, list, J, 2, F);
+            update(2 * tiles, nf, st, J, 2);
             cudaEventRecord(d.ev_next, st);
-            update_kernel<FT><<<dim3(tiles * tiles, nf), 256, upd_smem<FT>(), st>>>(d.d_fr, list, J, 3, F);
+            update(tiles * tiles, nf, st, J, 3);
             e.launches += 9;
         }
     }
-    int hv[2];
+    int hv[3];
     cudaMemcpyAsync(&d.h_buf[0], e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(&d.h_buf[1], d.d_npert, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&d.h_buf[1], d.d_npert, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
     if (int rc = e.sync_check("direct factor")) return rc;
     hv[0] = d.h_buf[0];
     hv[1] = d.h_buf[1];
+    hv[2] = d.h_buf[2];
+    if (hv[2]) {
+        e.err = "direct solver: a tensor-core update did not complete";
+        return SDDDST_ERR_CUDA;
+    }
     if (hv[0]) {
         e.err = "direct solver: a Jacobian entry falls outside its front";
         return SDDDST_ERR_CAPACITY;
