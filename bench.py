@@ -393,11 +393,13 @@ def profile_target(args):
     sparse-LU solve (plain FP64 engine, h = 1e-6), or one inference of the
     learned preconditioner correction (h = 1e-7)."""
     from sdddst_b200 import capi
-    if args.only == "direct":
-        eng, xyb = make_engine(args.n, "fp64", 0, solver=capi.SOLVER_DIRECT)
+    if args.only in ("direct", "direct_mixed"):
+        mixed = args.only == "direct_mixed"
+        eng, xyb = make_engine(args.n, "fp32" if mixed else "fp64", 0,
+                               solver=capi.SOLVER_DIRECT_MIXED if mixed else capi.SOLVER_DIRECT)
         rhs = np.random.default_rng(0).standard_normal(args.n)
         x, refinements = eng.solve(1e-6, xyb, rhs)
-        print(json.dumps({"target": "direct", "n": args.n, "refinements": refinements, **eng.direct_stats()}))
+        print(json.dumps({"target": args.only, "n": args.n, "refinements": refinements, **eng.direct_stats()}))
         eng.close()
         return
     if args.only == "learned":
@@ -547,7 +549,7 @@ def main():
     ap.add_argument("--n", type=int, default=N_FULL)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--only", default=None, choices=["pairsum", "step", "direct", "learned"],
+    ap.add_argument("--only", default=None, choices=["pairsum", "step", "direct", "direct_mixed", "learned"],
                     help="profiling target: launch only the pair-sum kernels (or only steps) and exit")
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-realisations measurement")

@@ -100,7 +100,9 @@ def test_cli_run_matches_oracle(exe, port_lib, tmp_path):
         assert rw[6] == "-"
         assert float(rw[7]) == s["stress"], k
         assert np.isclose(float(rw[9]), s["strain"], rtol=1e-7, atol=1e-18), k
-        assert np.isclose(float(rw[10]), s["vsquare"], rtol=1e-9), k
+        # sum v^2 weights the largest velocities, which agree to 1e-10 of the
+        # largest: 1e-8 relative
+        assert np.isclose(float(rw[10]), s["vsquare"], rtol=1e-8), k
         assert np.isclose(float(rw[11]), s["energy"], rtol=1e-8), k
         k += 1
     assert k == w.steps + 1

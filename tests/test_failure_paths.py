@@ -97,17 +97,17 @@ def test_coincident_dislocations(engine_lib, port_lib):
 
 @pytest.mark.gpu
 def test_cluster_gmres_stall_rebuilds_then_reports(engine_lib):
-    """A one-iteration cap on a stiff system (h = 3e-3, h |G| >> 1 for close
-    pairs): the cluster-preconditioned GMRES stalls, the preconditioner is
-    rebuilt twice with a lower coupling threshold, and the solve reports
-    SDDDST_ERR_SOLVER.  With the cap lifted the same context solves to the
-    residual target."""
+    """A one-iteration cap (no preconditioned solve of this system reaches a
+    1e-13 residual in one iteration): the cluster-preconditioned GMRES stalls,
+    the preconditioner is rebuilt twice with a lower coupling threshold, and
+    the solve reports SDDDST_ERR_SOLVER.  With the cap lifted the same context
+    solves to the residual target."""
     import scipy.sparse as sp
     from sdddst_b200 import capi
-    n, h = 700, 3e-3
-    xyb, _ = workloads.dislocations(n, 6)
+    n, h = 800, 2e-5
+    xyb, _ = workloads.dislocations(n, 4)
     e = capi.Engine(capi.cli_params(n, 1.0, 1e-6, max_iters=1), xyb)
-    rhs = np.random.default_rng(6).standard_normal(n)
+    rhs = np.random.default_rng(6).standard_normal(n) * 1e-4
     with pytest.raises(capi.EngineError) as ex:
         e.solve(h, xyb, rhs)
     assert ex.value.rc == capi.ERR_SOLVER
@@ -139,8 +139,10 @@ def test_learned_stall_falls_back_to_sparse_lu(engine_lib, port_lib):
         assert e.step() == o.step(), k
         for which in (1, 2, 3):
             assert np.abs(e.config(which)[:, 0] - o.config(which)[:, 0]).max() <= 1e-10, (k, which)
+    # every GMRES solve stalled and was redone by the LU; both count as solves
     solves, _ = e.solver_stats()
-    assert e.solver_recoveries()[1] == solves and solves >= 5
+    fallbacks = e.solver_recoveries()[1]
+    assert fallbacks >= 5 and solves == 2 * fallbacks, (fallbacks, solves)
 
 
 @pytest.mark.gpu

@@ -410,3 +410,20 @@ def test_jacobian_multiblock_scan_n20001(engine_lib, port_lib):
     rhs = np.random.default_rng(3).standard_normal(n) * 1e-4
     x, iters = e.solve(h, xyb, rhs)
     assert np.linalg.norm(J @ x - rhs) <= 1e-12 * np.linalg.norm(rhs)
+
+
+def test_solve_with_restarts_matches_dense(engine_lib, port_lib):
+    """The device-resident GMRES with a restart length of 4 (several restart
+    cycles: the true residual recomputed, the basis rebuilt) against a dense
+    solve with the oracle's Jacobian, as test_solve_matches_dense."""
+    n = 800
+    xyb, pd, o, e = make_pair(n, 4, 1.0, 1e-6, gmres_restart=4)
+    h = 2e-5
+    Ap, Ai, Ax, d = o.jacobian(h, xyb)
+    J = ref.csc_to_dense(Ap, Ai, Ax, n)
+    b = np.random.default_rng(0).standard_normal(n) * 1e-4
+    x, iters = e.solve(h, xyb, b)
+    assert iters > 4
+    assert np.linalg.norm(J @ x - b) <= 1e-11 * np.linalg.norm(b)
+    x_ref = np.linalg.solve(J, b)
+    assert np.abs(x - x_ref).max() <= 1e-13 * np.linalg.cond(J) * np.abs(x_ref).max()

@@ -10,8 +10,11 @@ test_direct).  The chosen forms are
   values, FP64 GMRES(30) with the cluster block-Jacobi preconditioner;
 * learned: the same with the learned correction added to the preconditioner.
 
-Teacher forcing (src/simulation.cpp:435-650 per attempt): every attempt
-starts all three engines from the plain path's accepted state and step size;
+Teacher forcing (src/simulation.cpp:435-650 per attempt), after the plain
+path has taken its first 10 accepted steps alone (the initial step 1e-6 is
+far too large: its two chord-Newton iterations leave iterates that differ
+between any two arithmetics before the error control rejects them): every
+attempt starts all three engines from the plain path's accepted state and step size;
 the three stage configurations (big step, first and second small step) must
 agree within 1e-8 (the bar of the precision forms) and the accept/reject
 decisions must be identical, for at least three accepted attempts.  The
@@ -42,6 +45,16 @@ def _engines():
 
 def test_headline_forms_against_plain_fp64_teacher_forced(engine_lib):
     plain, forms = _engines()
+    # the plain path alone through the initial step-size transient (at the
+    # initial step 1e-6 the two chord-Newton iterations of a stage are far
+    # from converged and its iterate is rejected; the metric's window starts
+    # at step 10): teacher forcing starts after 10 accepted steps
+    settled = 0
+    for _ in range(60):
+        settled += plain.step()
+        if settled >= 10:
+            break
+    assert settled >= 10
     accepted = attempts = 0
     worst = {k: 0.0 for k in forms}
     while accepted < 3 and attempts < 16:
