@@ -273,6 +273,7 @@ int sdddst_update_params(void *ctx, const sdddst_params *prm)
 {
     if (!ctx || !prm) return fail(SDDDST_ERR_INVALID, "null argument");
     sd::Engine *e = E(ctx);
+    e->pre_assembled = false; // the stored pattern no longer matches the next attempt
     if (prm->n != e->n || prm->p != e->p || prm->field != e->prm.field || prm->pairsum != e->prm.pairsum)
         return fail(SDDDST_ERR_INVALID, "sizes, field and pair-sum mode cannot change on a live context");
     if (!(prm->prec > 0) || !(prm->cutoff_multiplier > 0)) return fail(SDDDST_ERR_INVALID, "bad parameter");
@@ -315,6 +316,7 @@ int sdddst_solve_csc(void *ctx, const int *Ap, const int *Ai, const double *Ax, 
 {
     if (!ctx || !Ap || !Ai || !Ax || !b || !x) return fail(SDDDST_ERR_INVALID, "null argument");
     sd::Engine *e = E(ctx);
+    e->pre_assembled = false; // the stored pattern no longer matches the next attempt
     cudaSetDevice(e->device);
     const int n = e->n;
     sd::learned_invalidate(*e); // the CSR is replaced below
@@ -474,6 +476,7 @@ int sdddst_upload_positions(void *ctx, const double *x, int recompute)
 {
     if (!ctx || !x) return fail(SDDDST_ERR_INVALID, "null argument");
     sd::Engine *e = E(ctx);
+    e->pre_assembled = false; // the stored pattern no longer matches the next attempt
     if (int rc = check_finite(x, e->n, "positions")) return rc;
     cudaSetDevice(e->device);
     cudaMemcpyAsync(e->d_x0, x, sizeof(double) * e->n, cudaMemcpyHostToDevice, e->st);

@@ -757,22 +757,20 @@ __global__ void __launch_bounds__(256, sizeof(FT) == 4 ? 2 : 1)
 // A_lo = A - tf32(A) and B_lo = B - tf32(B) (exact in FP32),
 //   A B ~ A B + A B_lo + A_lo B   (tf32 parts; the dropped A_lo B_lo is
 // below 2^-20 of A B), which keeps the factors near FP32 accuracy and the
-// FP64 refinement at its usual step count.  K runs in chunks of 32: the
-// threads stage A, A_lo (128 x 32, K-major) and B, B_lo (transposed to
-// 128 x 32, K-major) in shared memory in the no-swizzle core-matrix layout
-// (8 rows x 16 bytes per core matrix, K-adjacent ones 128 bytes apart, 8-row
-// groups 1024 bytes apart), one thread issues 3 x 4 MMAs (M = N = 128,
-// K = 8) and commits them to an mbarrier whose phase the CTA waits for
-// (bounded; past the limit *err is set and the tile is left unchanged)
-// before restaging.  Same modes and tile order as update_kernel.
+// FP64 refinement at its usual step count.  K runs in chunks of 32: A, A_lo
+// (128 x 32) and B, B_lo (transposed to 128 x 32) are staged in shared memory
+// in the no-swizzle K-major core-matrix layout (8 rows x 16 bytes per core
+// matrix, K-adjacent ones 128 bytes apart, 8-row groups 1024 bytes apart);
+// a warp covers 8 rows x 4 K per store, so its 32 lanes write 128
+// contiguous bytes.  The next chunk's global loads are issued into registers
+// before the CTA waits for the current chunk's MMAs (one thread issues 3 x 4
+// MMAs, M = N = 128, K = 8, and commits them to an mbarrier; bounded wait,
+// past the limit *err is set and the tile is left unchanged).  The epilogue
+// moves D through shared memory (rows padded to 129 words) so that C is read
+// and written row-contiguously.  Same modes and tile order as update_kernel.
 constexpr int kTcK = 32;                                  // K chunk
 constexpr unsigned kTcOp = 128 * kTcK * 4;                // one staged operand: 16 KB
-constexpr size_t kTcSmem = 4 * (size_t)kTcOp + 1024;      // A, A_lo, B, B_lo (+ alignment slack)
-
-__device__ __forceinline__ unsigned tc_off(int r, int k) // element (r, k) of a 128 x kTcK FP32 tile
-{
-    return (unsigned)((r >> 3) * 1024 + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4);
-}
+constexpr size_t kTcSmem = 68 * 1024;                     // A, A_lo, B, B_lo or D (128 x 129 words), aligned
 
 __device__ __forceinline__ unsigned long long tc_desc(unsigned addr)
 {
@@ -813,7 +811,6 @@ __global__ void __launch_bounds__(128)
     if ((int)blockIdx.x >= tm * tn) return; // whole CTA: before any barrier or allocation
     const int row0 = rlo + (blockIdx.x / tn) * kBM, col0 = clo + (blockIdx.x % tn) * kBM;
     extern __shared__ __align__(16) unsigned char tcs_raw[];
-    // 1024-byte aligned operand area
     unsigned char *tcs = tcs_raw + ((1024u - ((unsigned)__cvta_generic_to_shared(tcs_raw) & 1023u)) & 1023u);
     unsigned char *sA = tcs, *sAl = tcs + kTcOp, *sB = tcs + 2 * kTcOp, *sBl = tcs + 3 * kTcOp;
     __shared__ __align__(8) unsigned long long mbar;
@@ -838,23 +835,30 @@ __global__ void __launch_bounds__(128)
     const unsigned tmem = tmem_slot;
     const unsigned mb = (unsigned)__cvta_generic_to_shared(&mbar);
     const int nk = (b + kTcK - 1) / kTcK;
+    // step `it` of a warp covers 8 rows (lane >> 2) x 4 K (lane & 3) of core
+    // matrix group g = 4 it + warp: row group g >> 3, K quad g & 7
+    const int lr = lane >> 2, lk = lane & 3;
+    float ra[32], rb[32];
+    auto load_chunk = [&](int k0) {
+#pragma unroll
+        for (int it = 0; it < 32; ++it) {
+            const int g = 4 * it + warp, r8 = g >> 3, kq = g & 7;
+            const int r = r8 * 8 + lr, k = k0 + kq * 4 + lk;
+            ra[it] = (k < b && row0 + r < rhi) ? Ff[(long)(row0 + r) * ld + s + k] : 0.0f;
+            rb[it] = (k < b && col0 + r < chi) ? Ff[(long)(s + k) * ld + col0 + r] : 0.0f;
+        }
+    };
+    load_chunk(0);
     bool ok = true;
     for (int kc = 0; kc < nk && ok; ++kc) {
-        const int k0 = kc * kTcK;
-        // stage (zeros outside the ranges): a warp reads 32 consecutive K of
-        // one row of A, and 32 consecutive columns of one row of B
-#pragma unroll 4
-        for (int q = 0; q < kTcK; ++q) {
-            const int idx = tid + 128 * q;
-            const int ra = idx >> 5, ka = idx & 31;      // A: row ra, K ka
-            const int kb = idx >> 7, cb = idx & 127;     // B: K kb, column cb
-            const float a = (k0 + ka < b && row0 + ra < rhi) ? Ff[(long)(row0 + ra) * ld + s + k0 + ka] : 0.0f;
-            const float bb = (k0 + kb < b && col0 + cb < chi) ? Ff[(long)(s + k0 + kb) * ld + col0 + cb] : 0.0f;
-            const unsigned oa = tc_off(ra, ka), ob = tc_off(cb, kb);
-            *reinterpret_cast<float *>(sA + oa) = a;
-            *reinterpret_cast<float *>(sAl + oa) = tf32_lo(a);
-            *reinterpret_cast<float *>(sB + ob) = bb;
-            *reinterpret_cast<float *>(sBl + ob) = tf32_lo(bb);
+#pragma unroll
+        for (int it = 0; it < 32; ++it) {
+            const int g = 4 * it + warp;
+            const unsigned o = (unsigned)((g >> 3) * 1024 + (g & 7) * 128 + lane * 4);
+            *reinterpret_cast<float *>(sA + o) = ra[it];
+            *reinterpret_cast<float *>(sAl + o) = tf32_lo(ra[it]);
+            *reinterpret_cast<float *>(sB + o) = rb[it];
+            *reinterpret_cast<float *>(sBl + o) = tf32_lo(rb[it]);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -879,7 +883,8 @@ __global__ void __launch_bounds__(128)
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mb)
                          : "memory");
         }
-        // the chunk's MMAs done (phase kc & 1) before the operands are restaged or D is read
+        // the next chunk's loads in flight while the MMAs run
+        if (kc + 1 < nk) load_chunk((kc + 1) * kTcK);
         unsigned done = 0;
         for (int it = 0; it < (1 << 22) && !done; ++it) {
             asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -895,10 +900,11 @@ __global__ void __launch_bounds__(128)
     if (!ok) {
         if (tid == 0) atomicExch(err, 1);
     } else {
-        // epilogue: warp w holds rows 32 w .. 32 w + 31 (one TMEM lane each)
-        const int r = row0 + warp * 32 + lane;
+        // D through shared memory (the operands are no longer read): warp w
+        // holds rows 32 w .. 32 w + 31 of D, one TMEM lane each
+        float *Ds = reinterpret_cast<float *>(tcs);
+        const int r = warp * 32 + lane;
         const unsigned lane_base = (unsigned)(warp * 32) << 16;
-        float *row = Ff + (long)min(r, rhi - 1) * ld;
 #pragma unroll 1
         for (int c0 = 0; c0 < kBM; c0 += 16) {
             unsigned v[16];
@@ -909,12 +915,19 @@ __global__ void __launch_bounds__(128)
                            "=r"(v[14]), "=r"(v[15])
                          : "r"(tmem + lane_base + (unsigned)c0));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (r < rhi) {
 #pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    const int cc = col0 + c0 + q;
-                    if (cc < chi) row[cc] -= __uint_as_float(v[q]);
-                }
+            for (int q = 0; q < 16; ++q) Ds[r * 129 + c0 + q] = __uint_as_float(v[q]);
+        }
+        __syncthreads();
+        // C -= D, a warp per row at a time, columns contiguous
+        for (int rr = warp; rr < kBM; rr += 4) {
+            const int gr = row0 + rr;
+            if (gr >= rhi) break;
+            float *row = Ff + (long)gr * ld + col0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int c = lane + 32 * q;
+                if (col0 + c < chi) row[c] -= Ds[rr * 129 + c];
             }
         }
     }

@@ -56,8 +56,40 @@ Engine::~Engine()
     if (h_status) cudaFreeHost(h_status);
     if (d_tab_xy) cudaFree(d_tab_xy);
     if (d_tab_dx) cudaFree(d_tab_dx);
+    if (st2) cudaStreamDestroy(st2);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
     if (st) cudaStreamDestroy(st);
 }
+
+int Engine::side_streams()
+{
+    if (st2) return 0;
+    if (cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        err = "side stream creation failed";
+        return SDDDST_ERR_CUDA;
+    }
+    return 0;
+}
+
+// The engine's launch functions all use `st`; exchanging it with st2 routes
+// them to the side stream.
+void Engine::fork_side()
+{
+    cudaEventRecord(ev_fork, st);
+    cudaStreamWaitEvent(st2, ev_fork, 0);
+    std::swap(st, st2);
+}
+
+void Engine::end_side()
+{
+    std::swap(st, st2);
+    cudaEventRecord(ev_join, st2);
+}
+
+void Engine::join_side() { cudaStreamWaitEvent(st, ev_join, 0); }
 
 int Engine::sync_check(const char *what)
 {
@@ -254,6 +286,7 @@ int Engine::speeds(const double *x, double *v_out, double *S_out, int stress_typ
 int Engine::assemble(const double *x)
 {
     learned_invalidate(*this);
+    pre_assembled = false;
     int rc = jacobian_assemble(*this, x);
     if (rc == 0 && (prm.solver == SDDDST_SOLVER_DIRECT || prm.solver == SDDDST_SOLVER_DIRECT_MIXED))
         rc = direct_analyse(*this, x);
@@ -356,29 +389,33 @@ int Engine::prepare_solver(double h, bool same_assembly)
     return 0;
 }
 
+int Engine::init_speeds(int origin, const double *xo, bool use2)
+{
+    double t = sim_time, tasi = strain;
+    if (origin == kEndFirst) {
+        t += step_size * 0.5;
+        if (prm.stress_kind == SDDDST_STRESS_SPRING) {
+            double inc;
+            if (int rc = strain_inc(d_x0, d_x1, &inc)) return rc;
+            tasi += inc;
+        }
+    }
+    stress_calc(t, origin, tasi);
+    cur_stress = origin;
+    speeds(xo, use2 ? d_v0b : d_v0, use2 ? d_S1 : d_S0, origin, true);
+    return 0;
+}
+
 // calculateG (simulation.cpp:133-193) of Newton iteration `it` of one stage.
 int Engine::stage_residual(double h, int it, double *xn, const double *xo, bool use2, bool init_speed, int origin,
                            int end, double *csp0, const double *dvec, double *g)
 {
     double *isp = use2 ? d_v0b : d_v0;
-    double *Sorig = use2 ? d_S1 : d_S0;
     const bool calc_init = it == 0 ? init_speed : false;
     const bool use_init_first = it == 0 ? zero_stress() : false;
     double *csp = csp0;
-    if (calc_init) {
-        double t = sim_time, tasi = strain;
-        if (origin == kEndFirst) {
-            t += step_size * 0.5;
-            if (prm.stress_kind == SDDDST_STRESS_SPRING) {
-                double inc;
-                if (int rc = strain_inc(d_x0, d_x1, &inc)) return rc;
-                tasi += inc;
-            }
-        }
-        stress_calc(t, origin, tasi);
-        cur_stress = origin;
-        speeds(xo, isp, Sorig, origin, true);
-    }
+    if (calc_init)
+        if (int rc = init_speeds(origin, xo, use2)) return rc;
     if (use_init_first) {
         csp = isp;
     } else {
@@ -520,8 +557,14 @@ int Engine::stages_async(double *ratio, bool *ok)
     cudaMemcpyAsync(d_xb, d_x0, bytes, cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(d_x1, d_x0, bytes, cudaMemcpyDeviceToDevice, st);
     // ---- stages I and II: shared assembly at the accepted configuration
-    if (int rc = jacobian_assemble(*this, d_xb, true)) return rc;
-    launch_csr_guard(*this, d_astat);
+    // (already built beside the previous attempt's last velocity evaluation
+    // when that attempt was accepted)
+    if (pre_assembled) {
+        pre_assembled = false;
+    } else {
+        if (int rc = jacobian_assemble(*this, d_xb, true)) return rc;
+        launch_csr_guard(*this, d_astat);
+    }
     launch_make_dvec(*this, h1, d_dvecI, st);
     launch_make_dvec(*this, h2, d_dvec, st);
     launches += 2;
@@ -551,16 +594,29 @@ int Engine::stages_async(double *ratio, bool *ok)
     // ---- stage III: assembly at the first small step's end
     sum_avg_speed = 0;
     cudaMemcpyAsync(d_x2, d_x1, bytes, cudaMemcpyDeviceToDevice, st);
-    if (int rc = jacobian_assemble(*this, d_x2, true)) return rc;
+    // the assembly, d and the preconditioner at the first small step's end on
+    // the side stream, beside the velocity evaluation at the same
+    // configuration (stage III's initial speeds) on the main stream
+    fork_side();
+    if (int rc = jacobian_assemble(*this, d_x2, true)) {
+        end_side();
+        return rc;
+    }
     launch_csr_guard(*this, d_astat + 2);
     launch_make_dvec(*this, h2, d_dvec, st);
     launches++;
-    if (int rc = precond_build(*this, pc, h2, d_dvec, false)) return rc;
+    if (int rc = precond_build(*this, pc, h2, d_dvec, false)) {
+        end_side();
+        return rc;
+    }
     cudaMemcpyAsync(d_astat + 8, pc.flag, sizeof(int), cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(d_astat + 9, pc.bbase + n, sizeof(int), cudaMemcpyDeviceToDevice, st);
+    end_side();
+    if (int rc = init_speeds(kEndFirst, d_x1, true)) return rc;
+    join_side();
     const int slot3 = 2 * ic;
     for (int it = 0; it < ic; ++it) {
-        if (int rc = stage_residual(h2, it, d_x2, d_x1, true, true, kEndFirst, kEndSecond, d_vs2, d_dvec, d_g))
+        if (int rc = stage_residual(h2, it, d_x2, d_x1, true, false, kEndFirst, kEndSecond, d_vs2, d_dvec, d_g))
             return rc;
         const Cluster *pcs[1] = {&pc};
         const double *dv = d_dvec, *rhs = d_g;
@@ -651,12 +707,14 @@ int Engine::step(int *accepted)
                 return SDDDST_ERR_NOMEM;
             }
         }
+        if (int rc = side_streams()) return rc;
         cudaMemcpyAsync(d_tol_snap, d_tol, bytes, cudaMemcpyDeviceToDevice, st);
         bool ok = false;
         if (int rc = stages_async(&ratio, &ok)) return rc;
         if (!ok) {
             // a deferred check failed: the same attempt again, waiting at every check
             redone++;
+            pre_assembled = false;
             cudaMemcpyAsync(d_tol, d_tol_snap, bytes, cudaMemcpyDeviceToDevice, st);
             if (int rc = stages_sync(&ratio)) return rc;
         }
@@ -691,10 +749,25 @@ int Engine::finish_step(double ratio, int *accepted)
         succ++;
         cur_stress = kOrig;
         stress_calc(sim_time, kOrig, strain);
+        // the next attempt's stage I assembly at the new configuration on the
+        // side stream, beside its velocity evaluation
+        const bool pre = fused && prm.solver == SDDDST_SOLVER_GMRES_CLUSTER && ic <= 2 && st2;
+        if (pre) {
+            fork_side();
+            const int rc = jacobian_assemble(*this, d_x0, true);
+            if (rc == 0) launch_csr_guard(*this, d_astat);
+            end_side();
+            if (rc) return rc;
+        }
         speeds(d_x0, d_v0, d_S0, kOrig, true);
         init_speed_needed = false;
         double sa, sq;
         if (int rc = abs_and_sq(d_v0, &sa, &sq)) return rc;
+        if (pre) {
+            // nothing stays in flight past the step: later calls may use the CSR
+            if (cudaStreamSynchronize(st2) != cudaSuccess) return sync_check("side stream");
+            pre_assembled = true;
+        }
         sum_avg_speed = sa / double(n);
         vsquare = sq;
         energy_accum += (vsquare2 + vsquare) * 0.5 * step_size * 0.5;
@@ -725,6 +798,7 @@ int Engine::finish_step(double ratio, int *accepted)
 
 int Engine::set_state_host(const double *xyb, double h, double t, double e, double s, int first)
 {
+    pre_assembled = false;
     std::vector<double> hx(n), hy(n), hb(n);
     for (int i = 0; i < n; ++i) {
         hx[i] = xyb[3 * i];

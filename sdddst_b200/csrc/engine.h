@@ -107,6 +107,11 @@ struct Engine {
     double *d_tol_snap = nullptr;
     double *h_status = nullptr;           // pinned: fused statuses, assembly and preconditioner checks, scalars
     long redone = 0;                      // attempts redone with waits after a deferred failure
+    // side stream of the optimistic attempts: assemblies and preconditioner
+    // builds beside the pair sum at the same configuration
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool pre_assembled = false;           // the CSR holds the next attempt's stage I assembly (at x0)
 
     // ---- cluster block-Jacobi preconditioners (precond.cu): pc for the
     // solves of the engine's generic path and of stage II/III, pc2 for stage
@@ -157,6 +162,13 @@ struct Engine {
     int stages_async(double *ratio, bool *ok);
     int finish_step(double ratio, int *accepted);
     int abs_and_sq(const double *v, double *sum_abs, double *sum_sq);
+    // the calculateSpeeds of a stage's initial configuration (calculateG's
+    // first part, simulation.cpp:143-160)
+    int init_speeds(int origin, const double *xo, bool use2);
+    int side_streams();                   // creates st2 and its events once
+    void fork_side();                     // st2 waits for st; launches go to st2 until join_side
+    void end_side();                      // launches back on st; the side work is recorded
+    void join_side();                     // st waits for the recorded side work
     int solve_fused(double h, const double *dvec, Cluster &c, const double *rhs, double *x);
     int step(int *accepted);
     int set_state_host(const double *xyb, double step, double t, double e, double strain, int first);
