@@ -271,6 +271,42 @@ int sdddst_solver_stats(void *ctx, long *solves, long *iterations);
  * (simulation.cpp:388-395). */
 int sdddst_solver_recoveries(void *ctx, long *rebuilds, long *fallbacks, long *redone);
 
+/* ---- eigenvalue analysis: the reference's --ev-analyzation mode
+ * (src/main.cpp:36-41; TimeSeriesProcessor::run, src/time_series_processor.cpp:21-204;
+ * SpectralDecompositor::decompose, src/spectral_decompositor.cpp:63-201).
+ * The context supplies n, the point defects and the stress protocol; xyb is
+ * the configuration (n x 3, x y b).  The Hessian's defect term uses the
+ * decomposer's own scaling, A = 1.6e-3 / sqrt(defect count) and
+ * K = 1.65^2 1e6 / 256 * n (spectral_decompositor.cpp:76-84); the velocities
+ * use the context's A and KASQR (DataTimeSeries::next sets A = 1.6e-3 /
+ * sqrt(n), KASQR = 1.65^2 1e6 / 256 * n, data_time_series.cpp:34-35). */
+
+/* The dense Hessian decompose() hands to LAPACKE_dsyevd: H (n x n,
+ * symmetric) with H_ij = b_i b_j xy_diff_x(x_i - x_j, y_i - y_j) off the
+ * diagonal and H_ii = -sum_{j != i} H_ij - b_i sum_defects d/dx(defect force). */
+int sdddst_ev_hessian(void *ctx, const double *xyb, double *H);
+
+/* One configuration of TimeSeriesProcessor::run.  Every output may be NULL:
+ *   eigenvalues    n, ascending (getEigenValue)
+ *   participation  n, 1 / sum_j v_mj^4                         (:46-53)
+ *   burgers_sum    n, s_m = sum_j v_mj b_j                      (:77-84)
+ *   gan            n, s_m^2 / lambda_m                          (:55-62)
+ *   speeds         n, calculateSpeeds at sim_time, stress Original (:64-68)
+ *   eigenvectors   nvec x n (eigenvector m contiguous), nvec <= n (:86-91)
+ *   derivatives    n, eigenvalue derivatives (:93-121) under a fixed-rate
+ *                  protocol; zeros under any other, as in the reference
+ *   correlations   n x 3 x S x S: per mode the equal-sign, opposite-sign and
+ *                  all-pairs histograms of (:145-197), S = corr_bins
+ * Eigenvector signs are those of the device eigensolver (any sign is an
+ * eigenvector; the sign-free outputs do not depend on it). */
+int sdddst_ev_analyze(void *ctx, const double *xyb, double sim_time, double *eigenvalues, double *participation,
+                      double *burgers_sum, double *gan, double *speeds, double *eigenvectors, int nvec,
+                      double *derivatives, double *correlations, int corr_bins);
+
+/* Device times (ms, CUDA events) of the last sdddst_ev_analyze: Hessian,
+ * eigensolver, observables, derivatives, correlation matrices. */
+int sdddst_ev_timings(void *ctx, double *ms5);
+
 /* Sparse LU statistics of this context (SDDDST_SOLVER_DIRECT; zeros
  * otherwise): factorizations performed, pivots perturbed, FP64 flops of one
  * factorization of the last analysed pattern, doubles held by its fronts,

@@ -183,3 +183,78 @@ def csc_to_dense(Ap, Ai, Ax, n):
         for p in range(Ap[j], Ap[j + 1]):
             A[Ai[p], j] += Ax[p]
     return A
+
+
+# ------------------------------------------------------- eigenvalue analysis
+
+def _ev_lib(kind: str):
+    lib = _load(REF_LIB if kind == "ref" else PORT_LIB)
+    if kind == "ref":
+        if not hasattr(lib, "_ev_bound"):
+            lib.ref_ev_decompose.argtypes = [C.c_int, _D, C.c_int, C.c_void_p, _D, _D, _D]
+            lib._ev_bound = True
+    elif not hasattr(lib, "_ev_bound"):
+        lib.orc_ev_hessian.argtypes = [C.c_int, _D, C.c_int, C.c_void_p, _D]
+        lib.orc_ev_deriv_literal.argtypes = [C.c_int, _D, _D, _D, C.c_double, _D]
+        lib.orc_ev_correl_literal.argtypes = [C.c_int, _D, _D, C.c_int, _D]
+        lib._ev_bound = True
+    return lib
+
+
+def _pd_arg(pd):
+    pd = np.ascontiguousarray(pd if pd is not None else np.zeros((0, 2)), dtype=np.float64)
+    return pd, (pd.ctypes.data_as(C.c_void_p) if pd.shape[0] else None)
+
+
+def ev_decompose_ref(xyb, pd=None):
+    """SpectralDecompositor::decompose of the reference compiled in place
+    (src/spectral_decompositor.cpp:63-201) with the LAPACKE shim: (H, w, V),
+    H the Hessian handed to LAPACKE_dsyevd, V[m] eigenvector m."""
+    lib = _ev_lib("ref")
+    a = np.ascontiguousarray(xyb, dtype=np.float64)
+    n = a.shape[0]
+    pd, pp = _pd_arg(pd)
+    H, w, V = np.zeros(n * n), np.zeros(n), np.zeros(n * n)
+    lib.ref_ev_decompose(n, a.reshape(-1), pd.shape[0], pp, H, w, V)
+    return H.reshape(n, n), w, V.reshape(n, n)
+
+
+def ev_hessian(xyb, pd=None) -> np.ndarray:
+    """The restated Hessian (sdddst_oracle.c orc_ev_hessian), n x n."""
+    lib = _ev_lib("port")
+    a = np.ascontiguousarray(xyb, dtype=np.float64)
+    n = a.shape[0]
+    pd, pp = _pd_arg(pd)
+    H = np.zeros(n * n)
+    lib.orc_ev_hessian(n, a.reshape(-1), pd.shape[0], pp, H)
+    return H.reshape(n, n)
+
+
+def ev_analysis(xyb, pd, speeds, stress_derivative=1.0, nvec=10, deriv=False, corr_bins=0) -> dict:
+    """The observables TimeSeriesProcessor::run writes for one configuration
+    (src/time_series_processor.cpp:33-199): eigenvalues (ascending), the
+    participation numbers 1/sum_j v_mj^4, the Burgers sums s_m = sum_j v_mj b_j
+    and 1/Gael = s_m^2 / lambda_m, the first nvec eigenvectors, optionally the
+    eigenvalue derivatives (literal n^4 loop) and the correlation matrices.
+    The eigenpairs come from numpy.linalg.eigh (LAPACK's syevd driver, the
+    one the reference calls)."""
+    a = np.ascontiguousarray(xyb, dtype=np.float64)
+    n = a.shape[0]
+    H = ev_hessian(a, pd)
+    w, Vc = np.linalg.eigh(H)
+    V = np.ascontiguousarray(Vc.T)
+    b = a[:, 2]
+    s = V @ b
+    out = dict(eigenvalues=w, participation=1.0 / np.sum(V ** 4, axis=1), burgers_sum=s, gan=s ** 2 / w,
+               eigenvectors=V[:nvec].copy(), speeds=np.asarray(speeds, dtype=np.float64), hessian=H, V=V)
+    lib = _ev_lib("port")
+    if deriv:
+        d = np.zeros(n)
+        lib.orc_ev_deriv_literal(n, a.reshape(-1), V.reshape(-1), np.ascontiguousarray(out["speeds"]),
+                                 float(stress_derivative), d)
+        out["derivatives"] = d
+    if corr_bins:
+        cm = np.zeros(n * 3 * corr_bins * corr_bins)
+        lib.orc_ev_correl_literal(n, a.reshape(-1), V.reshape(-1), int(corr_bins), cm)
+        out["correlations"] = cm.reshape(n, 3, corr_bins, corr_bins)
+    return out

@@ -44,6 +44,9 @@
 #undef private
 #undef protected
 
+#include "spectral_decompositor.h"
+
+#include "lapacke.h"
 #include "umfpack.h"
 
 using namespace sdddstCore;
@@ -393,6 +396,25 @@ void ref_field(int which, long n, const double *dx, const double *dy, double *ou
         if (which == 0) out[i] = f.xy(dx[i], dy[i]);
         else if (which == 1) out[i] = f.xy_diff_x(dx[i], dy[i]);
         else out[i] = f.xy_diff_x2(dx[i], dy[i]);
+    }
+}
+
+/* SpectralDecompositor::decompose (src/spectral_decompositor.cpp:63-201) on
+ * one configuration, through the LAPACKE shim: H = the matrix it hands to
+ * LAPACKE_dsyevd (n x n), w = the eigenvalues it stores, V = eigenvector m at
+ * V[m n ..] through getEigenVectorElement(m, j). */
+void ref_ev_decompose(int n, const double *xyb, int p, const double *pd, double *H, double *w, double *V)
+{
+    std::vector<Dislocation> dis(n);
+    std::vector<PointDefect> pts(p);
+    for (int i = 0; i < n; ++i) dis[i] = Dislocation{xyb[3 * i], xyb[3 * i + 1], xyb[3 * i + 2]};
+    for (int k = 0; k < p; ++k) pts[k] = PointDefect{pd[2 * k], pd[2 * k + 1]};
+    sdddstEV::SpectralDecompositor dec(new AnalyticField);
+    dec.decompose(dis, pts);
+    lapacke_shim_last_input(H, (long)n * n);
+    for (int m = 0; m < n; ++m) {
+        w[m] = dec.getEigenValue(m);
+        for (int j = 0; j < n; ++j) V[(size_t)m * n + j] = dec.getEigenVectorElement(m, j);
     }
 }
 

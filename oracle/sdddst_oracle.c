@@ -21,7 +21,10 @@
  *   solve              src/simulation.cpp:386-396 through the UMFPACK shim
  *   integrate / step   src/simulation.cpp:62-84,398-415,435-650
  * and the CLI's set-up of SimulationData (src/project_parser.cpp:137-298,
- * src/simulation_data.cpp:43-109,208-218).
+ * src/simulation_data.cpp:43-109,208-218); for the eigenvalue analysis the
+ * second field derivative (AnalyticField.cpp:95-132,183-202), the Hessian
+ * (src/spectral_decompositor.cpp:63-165), the eigenvalue derivatives and the
+ * correlation matrices (src/time_series_processor.cpp:104-197,208-247).
  *
  * Its exported calls have the same names and meaning as oracle/ref_harness.cpp
  * so that one Python wrapper (oracle/ref.py) drives either library; tests pin
@@ -43,6 +46,8 @@
 
 #define ORC_EPS 1e-12 /* constants.h:24 */
 #define ORC_FIELD_N 4 /* constants.h:25 */
+
+double orc_xy_diff_x2(double dx, double dy);
 
 /* ------------------------------------------------------------ helpers --- */
 
@@ -848,5 +853,172 @@ void ref_integrate_stage(void *hp, int stage, double *x_out)
 
 void ref_field(int which, long n, const double *dx, const double *dy, double *out)
 {
-    for (long i = 0; i < n; ++i) out[i] = which == 0 ? orc_xy(dx[i], dy[i]) : orc_xy_diff_x(dx[i], dy[i]);
+    for (long i = 0; i < n; ++i)
+        out[i] = which == 0 ? orc_xy(dx[i], dy[i]) : which == 1 ? orc_xy_diff_x(dx[i], dy[i]) : orc_xy_diff_x2(dx[i], dy[i]);
+}
+
+/* ------------------------------------------------ eigenvalue analysis --- */
+/* The --ev-analyzation mode: SpectralDecompositor::decompose
+ * (spectral_decompositor.cpp:63-165) builds the dense Hessian of the
+ * configuration; TimeSeriesProcessor (time_series_processor.cpp:21-247)
+ * derives its observables from the eigenpairs.  The eigensolver itself is
+ * LAPACKE_dsyevd (spectral_decompositor.cpp:188); the Python side of the
+ * oracle uses numpy.linalg.eigh, which calls the same LAPACK driver. */
+
+/* AnalyticField.cpp:95-108: d2/dx2 of fpair (no Taylor branch) */
+static double fpair_dx2(double dx, double cos2piy, double dy)
+{
+    double ch = cosh(M_PI * 2.0 * dx);
+    double sh = sinh(M_PI * 2.0 * dx);
+    double c4y = cos(4.0 * M_PI * dy);
+    double ch4 = cosh(M_PI * 4.0 * dx);
+    double sh4 = sinh(M_PI * 4.0 * dx);
+    return (4.0 * M_PI *
+            (sh * cos2piy * (pow(cos2piy, 2.0) - 2.0) + 2.0 * M_PI * dx * pow(sh, 2.0) * (c4y - 2.0) -
+             M_PI * dx * pow(ch, 3.0) * cos2piy + 0.5 * M_PI * dx * ch * cos2piy * (2.0 * ch4 + c4y - 5.0) +
+             pow(ch, 2.0) * (2.0 * M_PI * dx - sh * cos2piy) + sh4)) /
+           pow(cos2piy - ch, 4.0);
+}
+
+/* AnalyticField.cpp:122-132 */
+static double gimg_dx2(int images, double dx, double cos2piy, double dy)
+{
+    double s = fpair_dx2(dx, cos2piy, dy);
+    for (int k = 1; k <= images; ++k)
+        s = s + fpair_dx2(dx - (double)k, cos2piy, dy) + fpair_dx2(dx + (double)k, cos2piy, dy);
+    return s;
+}
+
+/* AnalyticField::xy_diff_x2, AnalyticField.cpp:183-202 */
+double orc_xy_diff_x2(double dx, double dy)
+{
+    const double n = (double)ORC_FIELD_N;
+    double cy = cos(M_PI * 2.0 * dy);
+    if (dx < 0)
+        return -2.0 * fpair_dx(dx + n + 1.0, cy, dy) - dx * fpair_dx2(dx + n + 1.0, cy, dy) +
+               fpair_dx2(dx - n, cy, dy) * (1.0 + dx) + 2.0 * fpair_dx(dx - n, cy, dy) + fpair_dx2(dx + n, cy, dy) +
+               gimg_dx2(ORC_FIELD_N - 1, dx, cy, dy);
+    return 2.0 * fpair_dx(dx - n - 1.0, cy, dy) + dx * fpair_dx2(dx - n - 1.0, cy, dy) +
+           fpair_dx2(dx + n, cy, dy) * (1.0 - dx) - 2.0 * fpair_dx(dx + n, cy, dy) + fpair_dx2(dx - n, cy, dy) +
+           gimg_dx2(ORC_FIELD_N - 1, dx, cy, dy);
+}
+
+/* spectral_decompositor.cpp:63-165: H (row-major n x n) with
+ * H_ij = b_i b_j xy_diff_x(x_i - x_j, y_i - y_j) for i != j and
+ * H_ii = -sum_{j<i} H_ij - sum_defects b_i d/dx(defect force) - sum_{j>i} H_ji,
+ * accumulated in that order.  The defects use their own scaling: A = 1.6e-3 /
+ * sqrt(defect count), K = 1.65^2 1e6 / 256 * n (:76-84). */
+void orc_ev_hessian(int n, const double *xyb, int p, const double *pd, double *H)
+{
+    double sdA = 0.0, sdK = 0.0;
+    if (p > 0) {
+        sdA = 1e-4 * 16.0 * 1. / sqrt((double)p);
+        sdK = 1.65 * 1.65 * 1e6 / 256.0 * (double)n;
+    }
+    memset(H, 0, sizeof(double) * (size_t)n * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        double sub = 0.0;
+        for (int j = 0; j < i; ++j) {
+            double dx = xyb[3 * i] - xyb[3 * j];
+            normalize(&dx);
+            double dy = xyb[3 * i + 1] - xyb[3 * j + 1];
+            normalize(&dy);
+            double t = xyb[3 * i + 2] * xyb[3 * j + 2] * orc_xy_diff_x(dx, dy);
+            sub += t;
+            H[(size_t)i * n + j] = t;
+            H[(size_t)j * n + i] = t;
+        }
+        H[(size_t)i * n + i] -= sub;
+        for (int k = 0; k < p; ++k) {
+            double dx = xyb[3 * i] - pd[2 * k];
+            normalize(&dx);
+            double dy = xyb[3 * i + 1] - pd[2 * k + 1];
+            normalize(&dy);
+            H[(size_t)i * n + i] -= xyb[3 * i + 2] * pd_force_dx(dx, dy, sdA, sdK);
+        }
+    }
+    for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j) H[(size_t)i * n + i] -= H[(size_t)j * n + i];
+}
+
+/* TimeSeriesProcessor::calculateHessianDerivative (time_series_processor.cpp:208-247) */
+static double ev_hess_deriv(int n, const double *xyb, int i, int j, int k)
+{
+    double dx, dy;
+    if (i == j && j == k) {
+        double sum = 0.0;
+        for (int l = 0; l < n; ++l) {
+            if (l == i) continue;
+            dx = xyb[3 * i] - xyb[3 * l];
+            dy = xyb[3 * i + 1] - xyb[3 * l + 1];
+            normalize(&dx);
+            normalize(&dy);
+            sum += xyb[3 * l + 2] * orc_xy_diff_x2(dx, dy);
+        }
+        return -xyb[3 * i + 2] * sum;
+    }
+    if (i == j || i == k) {
+        const int o = i == j ? k : j;
+        dx = xyb[3 * i] - xyb[3 * o];
+        dy = xyb[3 * i + 1] - xyb[3 * o + 1];
+        normalize(&dx);
+        normalize(&dy);
+        return xyb[3 * i + 2] * xyb[3 * o + 2] * orc_xy_diff_x2(dx, dy);
+    }
+    if (j == k) {
+        dx = xyb[3 * i] - xyb[3 * j];
+        dy = xyb[3 * i + 1] - xyb[3 * j + 1];
+        normalize(&dx);
+        normalize(&dy);
+        return -xyb[3 * i + 2] * xyb[3 * j + 2] * orc_xy_diff_x2(dx, dy);
+    }
+    return 0.0;
+}
+
+/* The eigenvalue derivatives, literally as time_series_processor.cpp:104-121
+ * loops them (n^4 terms; small n only): V holds eigenvector m at V[m n ..],
+ * speeds the velocities at the configuration, sderiv the stress protocol's
+ * getStressDerivative. */
+void orc_ev_deriv_literal(int n, const double *xyb, const double *V, const double *speeds, double sderiv,
+                          double *out)
+{
+    for (int m = 0; m < n; ++m) {
+        double sum = 0.0;
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                double mult = V[(size_t)m * n + i] * V[(size_t)m * n + j] / sderiv;
+                double sub = 0.0;
+                for (int k = 0; k < n; ++k) sub += speeds[k] * ev_hess_deriv(n, xyb, i, j, k);
+                sum += sub * mult;
+            }
+        out[m] = sum;
+    }
+}
+
+/* The correlation matrices of time_series_processor.cpp:145-197: for every
+ * mode m three S x S histograms over the ordered pairs i != j, binned by
+ * (floor((dx + 1/2) S), floor((dy + 1/2) S)) of the minimum-image
+ * separation and weighted by V_mj^2 V_mi^2: equal signs (pp), opposite signs
+ * (pn), all pairs (pppn).  out: [m][pp, pn, pppn][S][S]. */
+void orc_ev_correl_literal(int n, const double *xyb, const double *V, int S, double *out)
+{
+    const size_t ss = (size_t)S * S;
+    memset(out, 0, sizeof(double) * (size_t)n * 3 * ss);
+    for (int m = 0; m < n; ++m) {
+        double *pp = out + (size_t)m * 3 * ss, *pn = pp + ss, *pppn = pn + ss;
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                if (i == j) continue;
+                double dx = xyb[3 * i] - xyb[3 * j];
+                double dy = xyb[3 * i + 1] - xyb[3 * j + 1];
+                normalize(&dx);
+                normalize(&dy);
+                int tx = (int)floor((dx + 0.5) * S);
+                int ty = (int)floor((dy + 0.5) * S);
+                double w = pow(V[(size_t)m * n + j], 2.0) * pow(V[(size_t)m * n + i], 2.0);
+                if (xyb[3 * i + 2] != xyb[3 * j + 2]) pn[(size_t)tx * S + ty] += w;
+                if (xyb[3 * i + 2] == xyb[3 * j + 2]) pp[(size_t)tx * S + ty] += w;
+                pppn[(size_t)tx * S + ty] += w;
+            }
+    }
 }

@@ -41,7 +41,7 @@ EXPORTS = [
     "sdddst_batch_step", "sdddst_batch_get_scalars", "sdddst_batch_get_positions", "sdddst_batch_info",
     "sdddst_direct_stats", "sdddst_profile_direct", "sdddst_precond_apply", "sdddst_set_preconditioner_weights",
     "sdddst_learned_correction", "sdddst_solver_recoveries", "sdddst_batch_stats",
-    "sdddst_batch_profile_pair_sum",
+    "sdddst_batch_profile_pair_sum", "sdddst_ev_hessian", "sdddst_ev_analyze", "sdddst_ev_timings",
 ]
 
 
@@ -116,6 +116,10 @@ def load(path: str = LIB_PATH):
     lib.sdddst_solver_recoveries.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long),
                                              C.POINTER(C.c_long)]
     lib.sdddst_profile_pair_sum.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
+    lib.sdddst_ev_hessian.argtypes = [C.c_void_p, _D, _D]
+    lib.sdddst_ev_analyze.argtypes = [C.c_void_p, _D, C.c_double] + [C.c_void_p] * 6 + [C.c_int, C.c_void_p,
+                                                                                        C.c_void_p, C.c_int]
+    lib.sdddst_ev_timings.argtypes = [C.c_void_p, _D]
     lib.sdddst_vector_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.sdddst_direct_stats.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long),
                                         C.POINTER(C.c_double), C.POINTER(C.c_long), C.POINTER(C.c_int),
@@ -312,6 +316,41 @@ class Engine:
         a, b, c = C.c_long(0), C.c_long(0), C.c_long(0)
         _check(self.lib.sdddst_solver_recoveries(self.h, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
+
+    def ev_hessian(self, xyb) -> np.ndarray:
+        """The dense Hessian of SpectralDecompositor::decompose (n x n)."""
+        a = np.ascontiguousarray(xyb, dtype=np.float64).reshape(-1)
+        H = np.zeros(self.n * self.n)
+        _check(self.lib.sdddst_ev_hessian(self.h, a, H))
+        return H.reshape(self.n, self.n)
+
+    def ev_analyze(self, xyb, sim_time=0.0, nvec=10, deriv=False, corr_bins=0) -> dict:
+        """One configuration of the eigenvalue analysis (sdddst_ev_analyze):
+        eigenvalues, participation, burgers_sum, gan, speeds, eigenvectors
+        (nvec x n), derivatives (when deriv), correlations (n x 3 x S x S
+        when corr_bins = S > 0)."""
+        a = np.ascontiguousarray(xyb, dtype=np.float64).reshape(-1)
+        n = self.n
+        nv = min(int(nvec), n)
+        out = {k: np.zeros(n) for k in ("eigenvalues", "participation", "burgers_sum", "gan", "speeds")}
+        out["eigenvectors"] = np.zeros((nv, n))
+        if deriv:
+            out["derivatives"] = np.zeros(n)
+        if corr_bins:
+            out["correlations"] = np.zeros((n, 3, corr_bins, corr_bins))
+
+        def ptr(k):
+            return out[k].ctypes.data_as(C.c_void_p) if k in out else None
+        _check(self.lib.sdddst_ev_analyze(self.h, a, float(sim_time), ptr("eigenvalues"), ptr("participation"),
+                                          ptr("burgers_sum"), ptr("gan"), ptr("speeds"),
+                                          out["eigenvectors"].ctypes.data_as(C.c_void_p) if nv else None, nv,
+                                          ptr("derivatives"), ptr("correlations"), int(corr_bins)))
+        return out
+
+    def ev_timings(self) -> dict:
+        ms = np.zeros(5)
+        _check(self.lib.sdddst_ev_timings(self.h, ms))
+        return dict(zip(["hessian", "eigensolver", "observables", "derivatives", "correlations"], ms))
 
     def update_params(self, **kw):
         """Changes mutable parameters of the live context (sdddst_update_params)."""

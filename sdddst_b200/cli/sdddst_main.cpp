@@ -8,17 +8,21 @@
 // --hide-copyright.  Option semantics follow ProjectParser::processInput
 // (project_parser.cpp:137-298) field by field; the run is Simulation::run and
 // the log is the reference's 12-column log (simulation.cpp:463-617), written
-// by the host API.  The eigenvalue analysis mode (--ev-analyzation) is not
-// part of this build and is refused.
+// by the host API.  The eigenvalue analysis mode (--ev-analyzation) follows
+// the EV branch of processInput (:299-318) and main (src/main.cpp:36-41) and
+// runs TimeSeriesProcessor on the GPU.
 #include "Fields/AnalyticField.h"
 #include "StressProtocols/fixed_rate_protocol.h"
 #include "StressProtocols/spring_protocol.h"
 #include "StressProtocols/stress_protocol.h"
+#include "data_time_series.h"
 #include "simulation.h"
 #include "simulation_data.h"
+#include "time_series_processor.h"
 
 #include <cmath>
 #include <cstdio>
+#include <exception>
 #include <cstdlib>
 #include <iostream>
 #include <map>
@@ -42,7 +46,7 @@ struct Opt {
 // The option table of project_parser.cpp:39-99 (simulation and EV modes).
 const Opt kOpts[] = {
     {"simulation", Arg::None, nullptr, "run a simulation (default)"},
-    {"ev-analyzation", Arg::None, nullptr, "run eigen value analysation (not part of this build)"},
+    {"ev-analyzation", Arg::None, nullptr, "run eigen value analysation"},
     {"dislocation-configuration", Arg::String, nullptr, "plain text file path containing dislocation data in {x y b} triplets"},
     {"result-dislocation-configuration", Arg::String, nullptr, "path where the result configuration will be stored at the end of the simulation"},
     {"point-defect-configuration", Arg::String, nullptr, "plain text file path containing point defect data in {x y} pairs"},
@@ -274,6 +278,55 @@ std::shared_ptr<SimulationData> simulation_data(const Values &vm)
     return sD;
 }
 
+int as_int(const Values &v, const std::string &k)
+{
+    const std::string s = v.raw(k);
+    char *end = nullptr;
+    const long d = std::strtol(s.c_str(), &end, 10);
+    if (s.empty() || *end != '\0' || d < -2147483648L || d > 2147483647L)
+        die("the argument ('" + s + "') for option '--" + k + "' is invalid", -1);
+    return (int)d;
+}
+
+// The eigenvalue analysis: processInput's EV branch (project_parser.cpp:299-318)
+// and main (src/main.cpp:36-41).  getStressProtocol (:340-348) aborts unless a
+// fixed-rate protocol is given, and is evaluated before getDataTimeSeries
+// (:330-338) as GCC orders the constructor's arguments; getDataTimeSeries
+// needs both the file list and the point-defect file (the reference then
+// dereferences a null series; here that is an error exit).
+int run_ev(const Values &vm)
+{
+    auto sD = std::make_shared<SimulationData>();
+    if (!vm.count.count("result-ev-file") || vm.count.at("result-ev-file") != 1)
+        die("result-ev-file is not defined! Exiting...", 1);
+    sD->eVAnalResultFile = vm.raw("result-ev-file");
+    if (vm.has("calculate-ev-deriv")) sD->calculateDerivativeEVAnal = true;
+    sD->numberOfEigenVecToWrite = as_int(vm, "eigenvector-to-write"); // default 10
+    if (vm.has("write-correlation-matrices")) sD->writeCorrelMatrices = as_int(vm, "write-correlation-matrices");
+    if (!vm.has("fixed-rate-external-stress") || vm.count.at("fixed-rate-external-stress") != 1) {
+        std::cerr << "the eigenvalue analysis needs --fixed-rate-external-stress" << std::endl;
+        std::abort();
+    }
+    auto *protocol = new FixedRateProtocol;
+    protocol->setRate(as_double(vm, "fixed-rate-external-stress"));
+    std::unique_ptr<StressProtocol> owned(protocol);
+    if (!vm.has("pd-configuration") || !vm.has("file-list") || vm.count.at("pd-configuration") != 1 ||
+        vm.count.at("file-list") != 1)
+        die("the eigenvalue analysis needs --file-list and --pd-configuration", 1);
+    try {
+        auto series = std::make_shared<DataTimeSeries>(vm.raw("file-list"), vm.raw("pd-configuration"));
+        sdddstEV::TimeSeriesProcessor processor(sD, series, owned.release());
+        processor.run();
+    } catch (const EngineError &e) {
+        std::cerr << "engine error " << e.code << ": " << e.what() << std::endl;
+        return 3;
+    } catch (const std::exception &e) {
+        std::cerr << e.what() << std::endl;
+        return 2;
+    }
+    return 0;
+}
+
 } // namespace
 
 int main(int argc, char **argv)
@@ -285,8 +338,7 @@ int main(int argc, char **argv)
         print_help();
         return 0;
     }
-    if (vm.has("ev-analyzation") && !vm.has("simulation"))
-        die("ev-analyzation: the eigenvalue analysis is not part of this build", -1);
+    if (vm.has("ev-analyzation") && !vm.has("simulation")) return run_ev(vm);
     std::shared_ptr<SimulationData> sD = simulation_data(vm);
     try {
         Simulation simulation(sD);

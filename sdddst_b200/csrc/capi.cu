@@ -629,6 +629,70 @@ int sdddst_solver_recoveries(void *ctx, long *rebuilds, long *fallbacks, long *r
     return SDDDST_OK;
 }
 
+int sdddst_ev_hessian(void *ctx, const double *xyb, double *H)
+{
+    if (!ctx || !xyb || !H) return fail(SDDDST_ERR_INVALID, "null argument");
+    sd::Engine *e = E(ctx);
+    if (int rc = check_finite(xyb, 3L * e->n, "configuration")) return rc;
+    cudaSetDevice(e->device);
+    try {
+        ScratchConfig sc(e, xyb);
+        if (int rc = sd::ev_hessian(*e, e->d_xs)) return from_engine(e, rc);
+        cudaMemcpyAsync(H, sd::ev_hessian_ptr(*e), sizeof(double) * (size_t)e->n * e->n, cudaMemcpyDeviceToHost,
+                        e->st);
+        return from_engine(e, e->sync_check("Hessian"));
+    } catch (const std::exception &ex) {
+        return fail(SDDDST_ERR_NOMEM, ex.what());
+    }
+}
+
+int sdddst_ev_analyze(void *ctx, const double *xyb, double sim_time, double *eigenvalues, double *participation,
+                      double *burgers_sum, double *gan, double *speeds, double *eigenvectors, int nvec,
+                      double *derivatives, double *correlations, int corr_bins)
+{
+    if (!ctx || !xyb || nvec < 0 || corr_bins < 0 || (correlations && corr_bins == 0) ||
+        (nvec > 0 && !eigenvectors))
+        return fail(SDDDST_ERR_INVALID, "bad argument");
+    sd::Engine *e = E(ctx);
+    if (int rc = check_finite(xyb, 3L * e->n, "configuration")) return rc;
+    if (!(corr_bins <= 4096)) return fail(SDDDST_ERR_INVALID, "correlation sampling size above 4096");
+    cudaSetDevice(e->device);
+    try {
+        ScratchConfig sc(e, xyb);
+        const int n = e->n;
+        // TimeSeriesProcessor::run: the stress at the configuration's time
+        // (Original), then calculateSpeeds without precision-handler updates
+        e->stress_calc(sim_time, 0, e->strain);
+        e->speeds(e->d_xs, e->d_Stmp, e->d_w, 0, false);
+        const bool deriv = derivatives && e->prm.stress_kind == SDDDST_STRESS_FIXED_RATE;
+        if (int rc = sd::ev_analyze(*e, e->d_xs, e->d_Stmp, deriv, e->prm.stress_rate, correlations ? corr_bins : 0))
+            return from_engine(e, rc);
+        const size_t nb = sizeof(double) * n;
+        const double *obs = sd::ev_observables(*e);
+        if (eigenvalues) cudaMemcpyAsync(eigenvalues, sd::ev_values(*e), nb, cudaMemcpyDeviceToHost, e->st);
+        if (participation) cudaMemcpyAsync(participation, obs, nb, cudaMemcpyDeviceToHost, e->st);
+        if (burgers_sum) cudaMemcpyAsync(burgers_sum, obs + n, nb, cudaMemcpyDeviceToHost, e->st);
+        if (gan) cudaMemcpyAsync(gan, obs + 2 * (size_t)n, nb, cudaMemcpyDeviceToHost, e->st);
+        if (derivatives) cudaMemcpyAsync(derivatives, obs + 3 * (size_t)n, nb, cudaMemcpyDeviceToHost, e->st);
+        if (speeds) cudaMemcpyAsync(speeds, e->d_Stmp, nb, cudaMemcpyDeviceToHost, e->st);
+        const int nv = std::min(nvec, n);
+        if (nv > 0) cudaMemcpyAsync(eigenvectors, sd::ev_vectors(*e), nb * nv, cudaMemcpyDeviceToHost, e->st);
+        if (correlations)
+            cudaMemcpyAsync(correlations, sd::ev_correlations(*e), nb * 3 * (size_t)corr_bins * corr_bins,
+                            cudaMemcpyDeviceToHost, e->st);
+        return from_engine(e, e->sync_check("eigenvalue analysis"));
+    } catch (const std::exception &ex) {
+        return fail(SDDDST_ERR_NOMEM, ex.what());
+    }
+}
+
+int sdddst_ev_timings(void *ctx, double *ms5)
+{
+    if (!ctx || !ms5) return fail(SDDDST_ERR_INVALID, "null argument");
+    sd::ev_timings(*E(ctx), ms5);
+    return SDDDST_OK;
+}
+
 int sdddst_direct_stats(void *ctx, long *factorizations, long *perturbed, double *flops, long *front_doubles,
                         int *fronts, int *depth)
 {

@@ -1378,10 +1378,14 @@ template <typename FT> static int factor_impl(Engine &e, Direct &d, double h, co
     cudaMemsetAsync(F, 0, sizeof(FT) * (size_t)d.F_used, st);
     cudaMemsetAsync(e.d_flag, 0, sizeof(int), st);
     cudaMemsetAsync(d.d_npert, 0, 2 * sizeof(int), st);
-    // FP32 fronts: the trailing updates on the tensor cores (compensated TF32)
-    // unless SDDDST_LU_CUDA_CORES is set
+    // FP32 fronts: the trailing updates on the CUDA cores by default; with
+    // SDDDST_LU_TENSOR_CORES set, on the tensor cores (compensated TF32).  At
+    // N = 16384 (31 fronts) the tensor-core updates take 17.4 ms per
+    // factorization against 11.9 ms on the CUDA cores: each 32-deep K chunk
+    // is 12 short MMAs behind a register-staged split of A and B into their
+    // TF32 high and low parts, which the CTA's 128 threads cannot hide.
     const int *list_cur = nullptr;
-    const bool tc = sizeof(FT) == 4 && std::getenv("SDDDST_LU_CUDA_CORES") == nullptr;
+    const bool tc = sizeof(FT) == 4 && std::getenv("SDDDST_LU_TENSOR_CORES") != nullptr;
     if (tc) cudaFuncSetAttribute(update_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
     auto update = [&](unsigned gx, int nf_, cudaStream_t s_, int J_, int mode) {
         if (tc)

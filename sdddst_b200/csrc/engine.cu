@@ -50,6 +50,7 @@ Engine::~Engine()
     fused_free(*this);
     direct_free(*this);
     learned_free(*this);
+    ev_free(*this);
     if (d_xasm) cudaFree(d_xasm);
     if (d_tol_snap) cudaFree(d_tol_snap);
     if (d_astat) cudaFree(d_astat);

@@ -125,6 +125,9 @@ struct Engine {
     void *learned = nullptr;
     double *d_xasm = nullptr; // positions of the last assembly (learned features, LU fallback)
 
+    // ---- eigenvalue analysis (ev.cu): dense Hessian, eigenpairs, observables
+    void *ev = nullptr;
+
     // ---- host scalars (SimulationData / Simulation members)
     double step_size = 1.0, sim_time = 0.0, strain = 0.0;
     double energy = 0.0, energy_accum = 0.0, vsquare = 0.0, vsquare1 = 0.0, vsquare2 = 0.0;
@@ -263,5 +266,16 @@ void learned_invalidate(Engine &e);
 int learned_export(Engine &e, float *host, long cap);
 void learned_free(Engine &e);
 long learned_weight_count();
+
+// eigenvalue analysis (ev.cu)
+int ev_hessian(Engine &e, const double *x);
+const double *ev_hessian_ptr(Engine &e);
+int ev_analyze(Engine &e, const double *x, const double *v, bool deriv, double rate, int corr_bins);
+const double *ev_vectors(Engine &e);
+const double *ev_values(Engine &e);
+const double *ev_observables(Engine &e);
+const double *ev_correlations(Engine &e);
+void ev_timings(Engine &e, double *ms);
+void ev_free(Engine &e);
 
 } // namespace sd

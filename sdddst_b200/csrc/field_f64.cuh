@@ -142,6 +142,40 @@ __device__ __forceinline__ double tau_xy_dx_f64(double dx, double dy)
     return acc * kTwoPiSq;
 }
 
+// AnalyticField::xy_diff_x2 (AnalyticField.cpp:95-132,183-202), the value
+// the reference's eigenvalue derivatives use:
+//   sum_k w_k F(u_k) + 2 sigma (f'(u_end) - f'(u_edge)),  sigma = sign(dx),
+// where the reference's per-image term f_dx2 carries no 2 pi^2 factor (its f
+// and f_dx do), so F = f'' / (2 pi^2):
+//   F(u) = 4 pi / D^2 [S (cy - 2N/D) + pi u ((C - 2 S^2/D)(cy - 2N/D) - 2 (S^2/D)(cy - N/D))]
+// with C = cosh 2 pi u = D + cy.
+__device__ __forceinline__ double tau_xy_dx2_f64(double dx, double dy)
+{
+    Images im;
+    make_images<true>(dx, dy, im);
+    double inv[10];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) inv[k] = im.D[k];
+    batch_rcp<10>(inv);
+    const double twopi = 2.0 * kPi;
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+        const double r = inv[k], S = im.S[k], N = im.N[k], cy = im.cy;
+        const double C = im.D[k] + cy, s2r = S * S * r, a = cy - 2.0 * N * r;
+        const double F = 4.0 * kPi * r * r * (S * a + kPi * im.u[k] * ((C - 2.0 * s2r) * a - 2.0 * s2r * (cy - N * r)));
+        acc += im.w[k] * F;
+    }
+    const int edge = im.pos ? 4 : 8;
+    auto fprime = [&](int k) {
+        const double r = inv[k];
+        return kTwoPiSq * r * r * (im.N[k] + twopi * im.u[k] * im.S[k] * (im.cy - 2.0 * im.N[k] * r));
+    };
+    const double d = fprime(9) - fprime(edge);
+    acc += im.pos ? 2.0 * d : -2.0 * d;
+    return acc;
+}
+
 // Point-defect force term of calculateSpeeds (simulation.cpp:111-128):
 // returns 2 A X(dx) X(dy) ((1-e)/s - K e)/s (subtracted times b_i) and the
 // tolerance distance s = X2(dx) + X2(dy), with X, X2 as in utility.h:42-50.

@@ -39,7 +39,7 @@ def test_option_checks(exe, tmp_path):
     r = _run(exe, "-c", "--no-such-option")
     assert r.returncode == 255 and "unrecognised" in r.stderr
     r = _run(exe, "-c", "--ev-analyzation")
-    assert r.returncode == 255
+    assert r.returncode == 1 and "result-ev-file is not defined" in r.stderr
     r = _run(exe, "-c", "--step-count-limit", "ten")
     assert r.returncode == 255 and "invalid" in r.stderr
     r = _run(exe, "-c", "--calculate-strain=1")

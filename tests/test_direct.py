@@ -136,11 +136,18 @@ def test_direct_matches_gmres_trajectory_config2(engine_lib):
         assert np.abs(x0 - x1).max() <= 1e-9, k
 
 
-def test_direct_mixed_solve_residual(engine_lib):
+@pytest.mark.parametrize("tensor_cores", [False, True])
+def test_direct_mixed_solve_residual(engine_lib, tensor_cores, monkeypatch):
     """SDDDST_SOLVER_DIRECT_MIXED: FP32 fronts, FP64 refinement to the solver
-    tolerance (relative residual 1e-12 against the device's own J)."""
+    tolerance (relative residual 1e-12 against the device's own J), with the
+    trailing updates on the CUDA cores (default) and on the tensor cores
+    (compensated TF32, SDDDST_LU_TENSOR_CORES)."""
     import scipy.sparse as sp
     from sdddst_b200 import capi
+    if tensor_cores:
+        monkeypatch.setenv("SDDDST_LU_TENSOR_CORES", "1")
+    else:
+        monkeypatch.delenv("SDDDST_LU_TENSOR_CORES", raising=False)
     n, p = 4096, 256
     xyb, pd = workloads.dislocations(n, 1, p)
     prm = capi.cli_params(n, 1.0, 1e-7, p=p, pd_scaling=True, stress_kind=capi.STRESS_CONSTANT, stress_value=0.01,
