@@ -9,8 +9,8 @@
 // iteration needs stays on the device:
 //   P1  z = M^-1 V_j (cluster block-Jacobi), written in the user order and in
 //       the cell-sorted order the SpMV gathers from;
-//   P2  w = J z (warp per row over the CTA's rows), then the CTA's partial
-//       dots V_k . w;
+//   P2  w = J z (warp per row over the rows at the CTA's cell-sorted
+//       positions), then the CTA's partial dots V_k . w over those rows;
 //   P3  reduced c1, w -= V c1, partial dots V_k . w and |w|^2 (second
 //       Gram-Schmidt pass);
 //   P4  reduced c2, w -= V c2, V_{j+1} = w / |w| (|w|^2 = |w1|^2 - |c2|^2),
@@ -157,16 +157,19 @@ struct RowDot {
 };
 
 // out_s[row] = v_s[row] + (1 + d_s)/2 h_s (G v_s)[row] (sign -1: rhs_s - that)
-// for the CTA's rows, one warp per row
+// for the rows at the CTA's cell-sorted positions k0 .. k1-1, one warp per
+// row: consecutive rows of a CTA are spatial neighbours, so their gathers
+// from the cell-sorted vector hit the same few kilobytes
 template <typename VT, typename IT, int NS>
-__device__ __forceinline__ void spmv_rows(const FusedArgs &a, int r0, int r1, const double *v0, const double *vs0,
+__device__ __forceinline__ void spmv_rows(const FusedArgs &a, int k0, int k1, const double *v0, const double *vs0,
                                           const double *v1, const double *vs1, double *o0, double *o1, bool act0,
                                           bool act1, bool residual)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const VT *val = static_cast<const VT *>(a.vals);
     const IT *col = static_cast<const IT *>(a.cols);
-    for (int row = r0 + wid; row < r1; row += nw) {
+    for (int k = k0 + wid; k < k1; k += nw) {
+        const int row = a.sorted[k];
         const int s = a.rowptr[row], e = a.rowptr[row + 1];
         double acc0 = 0.0, acc1 = 0.0;
         const double gd = (double)val[s];
@@ -199,12 +202,13 @@ __device__ __forceinline__ void spmv_rows(const FusedArgs &a, int r0, int r1, co
     }
 }
 
-// Per-CTA partial dots over the CTA's rows: task t = (s, k) for s < NS
-// active and k < cnt[s]; vector k is V_s[k] (or w_s itself for k == kw[s]:
-// |w|^2).  One warp per task, lanes strided over the rows.
+// Per-CTA partial dots over the CTA's rows (r0 .. r1-1, or the rows at the
+// cell-sorted positions r0 .. r1-1 when perm is given): task t = (s, k) for
+// s < NS active and k < cnt[s]; vector k is V_s[k] (or w_s itself for
+// k == kw[s]: |w|^2).  One warp per task, lanes strided over the rows.
 template <int NS>
 __device__ __forceinline__ void partial_dots(const FusedArgs &a, int r0, int r1, int n, const int *cnt,
-                                             const int *kw, double *part_pass)
+                                             const int *kw, double *part_pass, const int *perm = nullptr)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int ntask = cnt[0] + (NS == 2 ? cnt[1] : 0);
@@ -214,7 +218,13 @@ __device__ __forceinline__ void partial_dots(const FusedArgs &a, int r0, int r1,
         const FusedSys &S = a.sys[s];
         const double *u = k == kw[s] ? S.w : S.V + (size_t)k * n;
         double acc = 0.0;
-        for (int i = r0 + lane; i < r1; i += 32) acc += u[i] * S.w[i];
+        if (perm)
+            for (int q = r0 + lane; q < r1; q += 32) {
+                const int i = perm[q];
+                acc += u[i] * S.w[i];
+            }
+        else
+            for (int i = r0 + lane; i < r1; i += 32) acc += u[i] * S.w[i];
         acc = warp_sum(acc);
         if (lane == 0) part_pass[((size_t)s * gridDim.x + blockIdx.x) * kKM + k] = acc;
     }
@@ -328,7 +338,7 @@ __global__ void __launch_bounds__(kThreads, 2) fused_gmres_kernel(FusedArgs a)
                 kw[tid] = -1;
             }
             __syncthreads();
-            partial_dots<NS>(a, r0, r1, n, cnt, kw, pass0);
+            partial_dots<NS>(a, r0, r1, n, cnt, kw, pass0, a.sorted);
             grid.sync();
             // P3: c1; w -= V c1; partial dots V_k . w and |w|^2
             reduce_partials<NS>(pass0, cnt, c1);
@@ -451,7 +461,7 @@ __global__ void __launch_bounds__(kThreads, 2) fused_gmres_kernel(FusedArgs a)
             kw[tid] = 0;
         }
         __syncthreads();
-        partial_dots<NS>(a, r0, r1, n, cnt, kw, pass0);
+        partial_dots<NS>(a, r0, r1, n, cnt, kw, pass0, a.sorted);
         grid.sync();
         reduce_partials<NS>(pass0, cnt, c1);
         __syncthreads();

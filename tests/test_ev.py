@@ -166,13 +166,13 @@ def _write_series(tmp_path, sizes, p, seed):
     pdf = str(tmp_path / "defects.fconf")
     with open(pdf, "w") as f:
         for q in pd:
-            f.write(f"{q[0]!r} {q[1]!r}\n")
+            f.write(f"{q[0]:.17g} {q[1]:.17g}\n")
     for k, n in enumerate(sizes):
         xyb, _ = workloads.dislocations(n, seed + 1 + k)
         path = str(tmp_path / f"c{k}.dconf")
         workloads.write_dconf(path, xyb)
         t = 0.5 + 0.75 * k
-        lst.append(f"{t!r} {path}")
+        lst.append(f"{t:.17g} {path}")
         configs.append((t, workloads.read_dconf(path)))
     fl = str(tmp_path / "files.txt")
     with open(fl, "w") as f:
@@ -204,6 +204,7 @@ def test_ev_cli_matches_oracle(engine_lib, port_lib, tmp_path):
     exe = build.build_cli()
     rate, nvec = 2e-3, 3
     fl, pdf, pd, configs = _write_series(tmp_path, (48, 56), 4, 21)
+    assert workloads.read_pdconf(pdf).shape == (4, 2)
     out = str(tmp_path / "ev.gz")
     r = subprocess.run([exe, "-c", "--ev-analyzation", "--file-list", fl, "--pd-configuration", pdf,
                         "--result-ev-file", out, "--fixed-rate-external-stress", repr(rate), "--calculate-ev-deriv",
