@@ -390,8 +390,10 @@ def reference_arm(args):
 def profile_target(args):
     """Small, self-contained launches for ncu captures: the pair-sum kernels
     `reps` times on the workload's configuration, `steps` step attempts, one
-    sparse-LU solve (plain FP64 engine, h = 1e-6), or one inference of the
-    learned preconditioner correction (h = 1e-7)."""
+    sparse-LU solve (plain FP64 engine, h = 1e-6), one inference of the
+    learned preconditioner correction (h = 1e-7), or the eigenvalue analysis
+    of one configuration (`--n` dislocations, 64 point defects; `reps` timed
+    calls after a first one)."""
     from sdddst_b200 import capi
     if args.only in ("direct", "direct_mixed"):
         mixed = args.only == "direct_mixed"
@@ -401,6 +403,10 @@ def profile_target(args):
         x, refinements = eng.solve(1e-6, xyb, rhs)
         print(json.dumps({"target": args.only, "n": args.n, "refinements": refinements, **eng.direct_stats()}))
         eng.close()
+        return
+    if args.only == "ev":
+        import torch
+        print(json.dumps({"target": "ev", **measure_ev(torch, 0, cpu=False, n=args.n, reps=args.reps)}))
         return
     if args.only == "learned":
         eng, _ = make_engine(args.n, args.pairsum, 0, solver=capi.SOLVER_GMRES_LEARNED)
@@ -539,6 +545,59 @@ def measure_batch(torch, steps, warmup, pairsum, rank, world, dist=None, cpu=Fal
     return out
 
 
+def measure_ev(torch, local, cpu=True, n=4096, p=64, reps=3):
+    """The eigenvalue analysis (--ev-analyzation) of one configuration:
+    N = 4096 dislocations (seed 4) with 64 point defects, fixed-rate stress
+    1e-3 at t = 1: Hessian, eigenpairs (cuSOLVER dsyevd), observables and
+    the eigenvalue derivatives, the first 10 eigenvectors read back.  Device
+    phase times from CUDA events; `value` = analysed configurations per
+    second end to end through the C ABI (host configuration in, host
+    results out).  CPU baseline: the oracle's Hessian (C, one core) and
+    numpy.linalg.eigh (LAPACK syevd, all host threads) on an N = 2048 sample
+    of the same workload, scaled by N^2 and N^3."""
+    import time
+    from sdddst_b200 import capi, workloads
+    xyb, pd = workloads.dislocations(n, SEED, p)
+    prm = capi.cli_params(n, 1.0, 1e-6, p=p, pd_scaling=True, stress_kind=capi.STRESS_FIXED_RATE, stress_rate=1e-3,
+                          device=local)
+    e = capi.Engine(prm, xyb, pd)
+    e.ev_analyze(xyb, sim_time=1.0, nvec=10, deriv=True)  # handles, workspaces
+    torch.cuda.synchronize()
+    walls, phases = [], []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        e.ev_analyze(xyb, sim_time=1.0, nvec=10, deriv=True)
+        walls.append(time.perf_counter() - t0)
+        phases.append(e.ev_timings())
+    e.close()
+    best = min(range(reps), key=lambda k: walls[k])
+    ph = phases[best]
+    pairs = n * (n - 1) / 2.0
+    out = {"value": 1.0 / walls[best], "unit": "configurations/s", "n": n, "point_defects": p,
+           "config": "seed 4, fixed-rate stress 1e-3 at t = 1, 10 eigenvectors, derivatives on",
+           "ms": {k: v for k, v in ph.items()}, "wall_ms": walls[best] * 1e3,
+           "hessian_pairs_per_s": pairs / (ph["hessian"] * 1e-3) if ph["hessian"] > 0 else None,
+           "eigensolver": "cuSOLVER Xsyevd (divide and conquer), FP64"}
+    if cpu:
+        import os
+        from oracle import ref
+        m = 2048
+        xs, pds = workloads.dislocations(m, SEED, p)
+        t0 = time.perf_counter()
+        H = ref.ev_hessian(xs, pds)
+        t_h = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        np.linalg.eigh(H)
+        t_e = time.perf_counter() - t0
+        per = t_h * (n / m) ** 2 + t_e * (n / m) ** 3
+        out["cpu_baseline"] = {"value": 1.0 / per, "unit": "configurations/s", "cores": os.cpu_count(),
+                               "kind": "port",
+                               "sample": f"N={m} of the workload: oracle Hessian {t_h:.2f} s (C, one core) + "
+                                         f"numpy.linalg.eigh {t_e:.2f} s (LAPACK syevd, all threads), scaled by "
+                                         f"N^2 and N^3 to N={n}; observables and derivatives excluded"}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -549,11 +608,12 @@ def main():
     ap.add_argument("--n", type=int, default=N_FULL)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--only", default=None, choices=["pairsum", "step", "direct", "direct_mixed", "learned"],
+    ap.add_argument("--only", default=None, choices=["pairsum", "step", "direct", "direct_mixed", "learned", "ev"],
                     help="profiling target: launch only the pair-sum kernels (or only steps) and exit")
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-realisations measurement")
     ap.add_argument("--no-variants", action="store_true", help="skip the preconditioner variants")
+    ap.add_argument("--no-ev", action="store_true", help="skip the eigenvalue-analysis measurement")
     ap.add_argument("--settle", type=int, default=10,
                     help="accepted steps run before the warm-up (the metric's window starts at step 10)")
     ap.add_argument("--cpu-baseline-worker", default=None, choices=["speeds", "jacobian"], help=argparse.SUPPRESS)
@@ -705,6 +765,13 @@ def main():
         except Exception as ex:  # reported, never required for the main line
             batch = {"error": str(ex)[:200]}
 
+    ev_line = None
+    if not args.no_ev and rank == 0:
+        try:
+            ev_line = measure_ev(torch, local, cpu=not args.no_cpu and ws == 1)
+        except Exception as ex:
+            ev_line = {"error": str(ex)[:200]}
+
     cpu = None
     if cpu_proc is not None:
         try:
@@ -736,6 +803,7 @@ def main():
         "position_error_vs_fp64": pos_err,
         "precision_16384": precision,
         "batch_512": batch,
+        "ev_analysis_4096": ev_line,
         "cpu_baseline": cpu,
     }
     if rank == 0:
