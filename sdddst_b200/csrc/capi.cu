@@ -28,6 +28,16 @@ int from_engine(sd::Engine *e, int rc)
 
 sd::Engine *E(void *ctx) { return static_cast<sd::Engine *>(ctx); }
 
+// dst = src; *changed |= 1 where a bit pattern differs
+__global__ void copy_compare_kernel(int n, const double *__restrict__ src, double *__restrict__ dst, int *changed)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = src[i];
+    if (__double_as_longlong(v) != __double_as_longlong(dst[i])) atomicOr(changed, 1);
+    dst[i] = v;
+}
+
 // Rejects a caller array holding NaN or Inf before anything reaches the
 // device (the reference runs on with such values: a NaN velocity is accepted
 // as a step and spreads through the configuration).  Returns 0 or
@@ -476,10 +486,17 @@ int sdddst_upload_positions(void *ctx, const double *x, int recompute)
 {
     if (!ctx || !x) return fail(SDDDST_ERR_INVALID, "null argument");
     sd::Engine *e = E(ctx);
-    e->pre_assembled = false; // the stored pattern no longer matches the next attempt
     if (int rc = check_finite(x, e->n, "positions")) return rc;
     cudaSetDevice(e->device);
-    cudaMemcpyAsync(e->d_x0, x, sizeof(double) * e->n, cudaMemcpyHostToDevice, e->st);
+    // staged and compared: a round trip of the held state keeps the next
+    // attempt's stage I assembly; any changed position drops it
+    cudaMemcpyAsync(e->d_xs, x, sizeof(double) * e->n, cudaMemcpyHostToDevice, e->st);
+    cudaMemsetAsync(e->d_flag, 0, sizeof(int), e->st);
+    copy_compare_kernel<<<(e->n + 255) / 256, 256, 0, e->st>>>(e->n, e->d_xs, e->d_x0, e->d_flag);
+    int changed = 1;
+    cudaMemcpyAsync(&changed, e->d_flag, sizeof(int), cudaMemcpyDeviceToHost, e->st);
+    if (int rc = e->sync_check("upload positions")) return from_engine(e, rc);
+    if (changed || recompute) e->pre_assembled = false;
     if (recompute) {
         e->cur_stress = SDDDST_STAGE_ORIGINAL;
         e->stress_calc(e->sim_time, SDDDST_STAGE_ORIGINAL, e->strain);

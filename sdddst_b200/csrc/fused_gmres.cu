@@ -9,8 +9,8 @@
 // iteration needs stays on the device:
 //   P1  z = M^-1 V_j (cluster block-Jacobi), written in the user order and in
 //       the cell-sorted order the SpMV gathers from;
-//   P2  w = J z (warp per row over the rows at the CTA's cell-sorted
-//       positions), then the CTA's partial dots V_k . w over those rows;
+//   P2  w = J z (warp per row; rows dealt round robin to all warps in
+//       cell-sorted order), then the CTA's partial dots V_k . w over its rows;
 //   P3  reduced c1, w -= V c1, partial dots V_k . w and |w|^2 (second
 //       Gram-Schmidt pass);
 //   P4  reduced c2, w -= V c2, V_{j+1} = w / |w| (|w|^2 = |w1|^2 - |c2|^2),
@@ -156,19 +156,33 @@ struct RowDot {
     }
 };
 
+// The SpMV's rows go round robin over all warps of the grid in cell-sorted
+// order: pass r gives warp w of CTA b the sorted position
+// (b nw + w) + r W (W warps in all).  A CTA's warps take 16 consecutive
+// positions per pass (spatial neighbours: their gathers from the
+// cell-sorted vector share a few kilobytes), and every CTA samples the
+// whole domain, so regions whose rows are slower (denser, or wrapping
+// around the periodic cell) spread over all CTAs instead of stretching the
+// few that own them; the assignment is fixed, so results stay
+// bit-identical run to run.  q-th sorted position of the CTA:
+__device__ __forceinline__ int cta_spmv_pos(int q)
+{
+    const int nw = blockDim.x >> 5;
+    return (int)blockIdx.x * nw + q % nw + (q / nw) * (int)(gridDim.x * nw);
+}
+
 // out_s[row] = v_s[row] + (1 + d_s)/2 h_s (G v_s)[row] (sign -1: rhs_s - that)
-// for the rows at the CTA's cell-sorted positions k0 .. k1-1, one warp per
-// row: consecutive rows of a CTA are spatial neighbours, so their gathers
-// from the cell-sorted vector hit the same few kilobytes
+// for the CTA's SpMV rows, one warp per row
 template <typename VT, typename IT, int NS>
-__device__ __forceinline__ void spmv_rows(const FusedArgs &a, int k0, int k1, const double *v0, const double *vs0,
+__device__ __forceinline__ void spmv_rows(const FusedArgs &a, const double *v0, const double *vs0,
                                           const double *v1, const double *vs1, double *o0, double *o1, bool act0,
                                           bool act1, bool residual)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const VT *val = static_cast<const VT *>(a.vals);
     const IT *col = static_cast<const IT *>(a.cols);
-    for (int k = k0 + wid; k < k1; k += nw) {
+    const int W = gridDim.x * nw;
+    for (int k = (int)blockIdx.x * nw + wid; k < a.n; k += W) {
         const int row = a.sorted[k];
         const int s = a.rowptr[row], e = a.rowptr[row + 1];
         double acc0 = 0.0, acc1 = 0.0;
@@ -202,13 +216,13 @@ __device__ __forceinline__ void spmv_rows(const FusedArgs &a, int k0, int k1, co
     }
 }
 
-// Per-CTA partial dots over the CTA's rows (r0 .. r1-1, or the rows at the
-// cell-sorted positions r0 .. r1-1 when perm is given): task t = (s, k) for
-// s < NS active and k < cnt[s]; vector k is V_s[k] (or w_s itself for
-// k == kw[s]: |w|^2).  One warp per task, lanes strided over the rows.
+// Per-CTA partial dots over the CTA's rows (r0 .. r1-1, or its SpMV rows
+// when spmv_rows is set): task t = (s, k) for s < NS active and k < cnt[s];
+// vector k is V_s[k] (or w_s itself for k == kw[s]: |w|^2).  One warp per
+// task, lanes strided over the rows.
 template <int NS>
 __device__ __forceinline__ void partial_dots(const FusedArgs &a, int r0, int r1, int n, const int *cnt,
-                                             const int *kw, double *part_pass, const int *perm = nullptr)
+                                             const int *kw, double *part_pass, bool spmv_set = false)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int ntask = cnt[0] + (NS == 2 ? cnt[1] : 0);
@@ -218,9 +232,11 @@ __device__ __forceinline__ void partial_dots(const FusedArgs &a, int r0, int r1,
         const FusedSys &S = a.sys[s];
         const double *u = k == kw[s] ? S.w : S.V + (size_t)k * n;
         double acc = 0.0;
-        if (perm)
-            for (int q = r0 + lane; q < r1; q += 32) {
-                const int i = perm[q];
+        if (spmv_set)
+            for (int q = lane;; q += 32) {
+                const int k = cta_spmv_pos(q);
+                if (k >= n) break;
+                const int i = a.sorted[k];
                 acc += u[i] * S.w[i];
             }
         else
@@ -330,7 +346,7 @@ __global__ void __launch_bounds__(kThreads, 2) fused_gmres_kernel(FusedArgs a)
             }
             grid.sync();
             // P2: w = J z on the CTA's rows, then partial dots V_k . w (k <= j)
-            spmv_rows<VT, IT, NS>(a, r0, r1, a.sys[0].z, a.sys[0].zs, NS == 2 ? a.sys[1].z : nullptr,
+            spmv_rows<VT, IT, NS>(a, a.sys[0].z, a.sys[0].zs, NS == 2 ? a.sys[1].z : nullptr,
                                   NS == 2 ? a.sys[1].zs : nullptr, a.sys[0].w, NS == 2 ? a.sys[1].w : nullptr,
                                   act[0] != 0, NS == 2 && act[NS - 1] != 0, false);
             if (tid < 2) {
@@ -338,7 +354,7 @@ __global__ void __launch_bounds__(kThreads, 2) fused_gmres_kernel(FusedArgs a)
                 kw[tid] = -1;
             }
             __syncthreads();
-            partial_dots<NS>(a, r0, r1, n, cnt, kw, pass0, a.sorted);
+            partial_dots<NS>(a, r0, r1, n, cnt, kw, pass0, true);
             grid.sync();
             // P3: c1; w -= V c1; partial dots V_k . w and |w|^2
             reduce_partials<NS>(pass0, cnt, c1);
@@ -453,7 +469,7 @@ __global__ void __launch_bounds__(kThreads, 2) fused_gmres_kernel(FusedArgs a)
             for (int k = r0 + tid; k < r1; k += blockDim.x) S.zs[k] = S.x[a.sorted[k]];
         }
         grid.sync();
-        spmv_rows<VT, IT, NS>(a, r0, r1, a.sys[0].x, a.sys[0].zs, NS == 2 ? a.sys[1].x : nullptr,
+        spmv_rows<VT, IT, NS>(a, a.sys[0].x, a.sys[0].zs, NS == 2 ? a.sys[1].x : nullptr,
                               NS == 2 ? a.sys[1].zs : nullptr, a.sys[0].w, NS == 2 ? a.sys[1].w : nullptr, rs[0] != 0,
                               NS == 2 && rs[NS - 1] != 0, true);
         if (tid < 2) {
@@ -461,7 +477,7 @@ __global__ void __launch_bounds__(kThreads, 2) fused_gmres_kernel(FusedArgs a)
             kw[tid] = 0;
         }
         __syncthreads();
-        partial_dots<NS>(a, r0, r1, n, cnt, kw, pass0, a.sorted);
+        partial_dots<NS>(a, r0, r1, n, cnt, kw, pass0, true);
         grid.sync();
         reduce_partials<NS>(pass0, cnt, c1);
         __syncthreads();
