@@ -9,8 +9,8 @@
 // iteration needs stays on the device:
 //   P1  z = M^-1 V_j (cluster block-Jacobi), written in the user order and in
 //       the cell-sorted order the SpMV gathers from;
-//   P2  w = J z (warp per row; rows dealt round robin to all warps in
-//       cell-sorted order), then the CTA's partial dots V_k . w over its rows;
+//   P2  w = J z (warp per row; rows taken dynamically in cell-sorted order),
+//       then, after a barrier, the CTA's partial dots V_k . w over its rows;
 //   P3  reduced c1, w -= V c1, partial dots V_k . w and |w|^2 (second
 //       Gram-Schmidt pass);
 //   P4  reduced c2, w -= V c2, V_{j+1} = w / |w| (|w|^2 = |w1|^2 - |c2|^2),
@@ -36,6 +36,8 @@ namespace {
 constexpr int kThreads = 512;
 constexpr int kKM = 32; // restart length bound (m <= 31) and partial-sum stride
 constexpr int kStatusSlots = 8; // solves whose statuses one attempt can leave on the device
+constexpr int kPasses = 1024;   // ring of SpMV row counters (a pass zeroes the next one)
+constexpr int kRowChunk = 4;    // sorted positions a warp takes per grab
 
 struct FusedSys {
     double h;
@@ -58,6 +60,7 @@ struct FusedArgs {
     const void *vals;  // G values (VT), diagonal in each row's first slot
     const int *sorted; // cell-sorted position -> dislocation
     double *part;      // per-CTA partial sums: [2 passes][2 systems][grid][kKM]
+    int *ctr;          // SpMV row counters, one per pass (ring of kPasses)
     FusedSys sys[2];
 };
 
@@ -156,73 +159,81 @@ struct RowDot {
     }
 };
 
-// The SpMV's rows go round robin over all warps of the grid in cell-sorted
-// order: pass r gives warp w of CTA b the sorted position
-// (b nw + w) + r W (W warps in all).  A CTA's warps take 16 consecutive
-// positions per pass (spatial neighbours: their gathers from the
-// cell-sorted vector share a few kilobytes), and every CTA samples the
-// whole domain, so regions whose rows are slower (denser, or wrapping
-// around the periodic cell) spread over all CTAs instead of stretching the
-// few that own them; the assignment is fixed, so results stay
-// bit-identical run to run.  q-th sorted position of the CTA:
-__device__ __forceinline__ int cta_spmv_pos(int q)
-{
-    const int nw = blockDim.x >> 5;
-    return (int)blockIdx.x * nw + q % nw + (q / nw) * (int)(gridDim.x * nw);
-}
-
-// out_s[row] = v_s[row] + (1 + d_s)/2 h_s (G v_s)[row] (sign -1: rhs_s - that)
-// for the CTA's SpMV rows, one warp per row
+// one row of the SpMV below
 template <typename VT, typename IT, int NS>
-__device__ __forceinline__ void spmv_rows(const FusedArgs &a, const double *v0, const double *vs0,
-                                          const double *v1, const double *vs1, double *o0, double *o1, bool act0,
-                                          bool act1, bool residual)
+__device__ __forceinline__ void spmv_row(const FusedArgs &a, int row, int lane, const VT *__restrict__ val,
+                                         const IT *__restrict__ col, const double *v0, const double *vs0,
+                                         const double *v1, const double *vs1, double *o0, double *o1, bool act0,
+                                         bool act1, bool residual)
 {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const VT *val = static_cast<const VT *>(a.vals);
-    const IT *col = static_cast<const IT *>(a.cols);
-    const int W = gridDim.x * nw;
-    for (int k = (int)blockIdx.x * nw + wid; k < a.n; k += W) {
-        const int row = a.sorted[k];
-        const int s = a.rowptr[row], e = a.rowptr[row + 1];
-        double acc0 = 0.0, acc1 = 0.0;
-        const double gd = (double)val[s];
-        if (lane == 0) {
-            acc0 = act0 ? gd * v0[row] : 0.0;
-            if (NS == 2) acc1 = act1 ? gd * v1[row] : 0.0;
+    const int s = a.rowptr[row], e = a.rowptr[row + 1];
+    double acc0 = 0.0, acc1 = 0.0;
+    const double gd = (double)val[s];
+    if (lane == 0) {
+        acc0 = act0 ? gd * v0[row] : 0.0;
+        if (NS == 2) acc1 = act1 ? gd * v1[row] : 0.0;
+    }
+    if (NS == 2 && act0 && act1)
+        RowDot<VT, IT, 2>::run(s, e, lane, val, col, vs0, vs1, acc0, acc1);
+    else if (act0)
+        RowDot<VT, IT, 1>::run(s, e, lane, val, col, vs0, vs0, acc0, acc1);
+    else if (NS == 2 && act1)
+        RowDot<VT, IT, 1>::run(s, e, lane, val, col, vs1, vs1, acc1, acc0);
+    acc0 = warp_sum(acc0);
+    if (NS == 2) acc1 = warp_sum(acc1);
+    if (lane == 0) {
+        if (act0) {
+            const FusedSys &S = a.sys[0];
+            const double hh = S.hrow ? S.hrow[row] : S.h;
+            const double y = v0[row] + (1.0 + S.dvec[row]) * 0.5 * hh * acc0;
+            o0[row] = residual ? S.rhs[row] - y : y;
         }
-        if (NS == 2 && act0 && act1)
-            RowDot<VT, IT, 2>::run(s, e, lane, val, col, vs0, vs1, acc0, acc1);
-        else if (act0)
-            RowDot<VT, IT, 1>::run(s, e, lane, val, col, vs0, vs0, acc0, acc1);
-        else if (NS == 2 && act1)
-            RowDot<VT, IT, 1>::run(s, e, lane, val, col, vs1, vs1, acc1, acc0);
-        acc0 = warp_sum(acc0);
-        if (NS == 2) acc1 = warp_sum(acc1);
-        if (lane == 0) {
-            if (act0) {
-                const FusedSys &S = a.sys[0];
-                const double hh = S.hrow ? S.hrow[row] : S.h;
-                const double y = v0[row] + (1.0 + S.dvec[row]) * 0.5 * hh * acc0;
-                o0[row] = residual ? S.rhs[row] - y : y;
-            }
-            if (NS == 2 && act1) {
-                const FusedSys &S = a.sys[1];
-                const double hh = S.hrow ? S.hrow[row] : S.h;
-                const double y = v1[row] + (1.0 + S.dvec[row]) * 0.5 * hh * acc1;
-                o1[row] = residual ? S.rhs[row] - y : y;
-            }
+        if (NS == 2 && act1) {
+            const FusedSys &S = a.sys[1];
+            const double hh = S.hrow ? S.hrow[row] : S.h;
+            const double y = v1[row] + (1.0 + S.dvec[row]) * 0.5 * hh * acc1;
+            o1[row] = residual ? S.rhs[row] - y : y;
         }
     }
 }
 
-// Per-CTA partial dots over the CTA's rows (r0 .. r1-1, or its SpMV rows
-// when spmv_rows is set): task t = (s, k) for s < NS active and k < cnt[s];
-// vector k is V_s[k] (or w_s itself for k == kw[s]: |w|^2).  One warp per
-// task, lanes strided over the rows.
+// out_s[row] = v_s[row] + (1 + d_s)/2 h_s (G v_s)[row] (sign -1: rhs_s - that),
+// one warp per row.  The rows are taken in cell-sorted order, kRowChunk at a
+// time, from the pass's counter: consecutive rows of a warp are spatial
+// neighbours (their gathers from the cell-sorted vector share a few
+// kilobytes), and SMs that run slower (their distance to the memory they
+// gather from differs by up to 40 % in the per-CTA times) simply take fewer
+// rows.  Each row is summed by one warp in a fixed order, so w does not
+// depend on which warp took the row; the dots over w that follow use the
+// static row partition, so results stay bit-identical run to run.  The next
+// grab is issued before the current chunk's rows are processed.
+template <typename VT, typename IT, int NS>
+__device__ __forceinline__ void spmv_rows(const FusedArgs &a, int *ctr, const double *v0, const double *vs0,
+                                          const double *v1, const double *vs1, double *o0, double *o1, bool act0,
+                                          bool act1, bool residual)
+{
+    const int lane = threadIdx.x & 31;
+    const VT *val = static_cast<const VT *>(a.vals);
+    const IT *col = static_cast<const IT *>(a.cols);
+    int g = 0;
+    if (lane == 0) g = atomicAdd(ctr, kRowChunk);
+    g = __shfl_sync(0xffffffffu, g, 0);
+    while (g < a.n) {
+        int gn = 0;
+        if (lane == 0) gn = atomicAdd(ctr, kRowChunk);
+        const int kend = min(g + kRowChunk, a.n);
+        for (int k = g; k < kend; ++k)
+            spmv_row<VT, IT, NS>(a, a.sorted[k], lane, val, col, v0, vs0, v1, vs1, o0, o1, act0, act1, residual);
+        g = __shfl_sync(0xffffffffu, gn, 0);
+    }
+}
+
+// Per-CTA partial dots over the CTA's rows r0 .. r1-1: task t = (s, k) for
+// s < NS active and k < cnt[s]; vector k is V_s[k] (or w_s itself for
+// k == kw[s]: |w|^2).  One warp per task, lanes strided over the rows.
 template <int NS>
 __device__ __forceinline__ void partial_dots(const FusedArgs &a, int r0, int r1, int n, const int *cnt,
-                                             const int *kw, double *part_pass, bool spmv_set = false)
+                                             const int *kw, double *part_pass)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int ntask = cnt[0] + (NS == 2 ? cnt[1] : 0);
@@ -232,15 +243,7 @@ __device__ __forceinline__ void partial_dots(const FusedArgs &a, int r0, int r1,
         const FusedSys &S = a.sys[s];
         const double *u = k == kw[s] ? S.w : S.V + (size_t)k * n;
         double acc = 0.0;
-        if (spmv_set)
-            for (int q = lane;; q += 32) {
-                const int k = cta_spmv_pos(q);
-                if (k >= n) break;
-                const int i = a.sorted[k];
-                acc += u[i] * S.w[i];
-            }
-        else
-            for (int i = r0 + lane; i < r1; i += 32) acc += u[i] * S.w[i];
+        for (int i = r0 + lane; i < r1; i += 32) acc += u[i] * S.w[i];
         acc = warp_sum(acc);
         if (lane == 0) part_pass[((size_t)s * gridDim.x + blockIdx.x) * kKM + k] = acc;
     }
@@ -300,6 +303,8 @@ __global__ void __launch_bounds__(kThreads, 2) fused_gmres_kernel(FusedArgs a)
         cnt[tid] = tid < NS ? 1 : 0;
         kw[tid] = -1;
     }
+    int spass = 0; // SpMV passes so far (the same in every CTA)
+    if (blockIdx.x == 0 && tid == 0) a.ctr[0] = 0;
     grid.sync();
     reduce_partials<NS>(pass0, cnt, c1);
     __syncthreads();
@@ -345,16 +350,19 @@ __global__ void __launch_bounds__(kThreads, 2) fused_gmres_kernel(FusedArgs a)
                 }
             }
             grid.sync();
-            // P2: w = J z on the CTA's rows, then partial dots V_k . w (k <= j)
-            spmv_rows<VT, IT, NS>(a, a.sys[0].z, a.sys[0].zs, NS == 2 ? a.sys[1].z : nullptr,
-                                  NS == 2 ? a.sys[1].zs : nullptr, a.sys[0].w, NS == 2 ? a.sys[1].w : nullptr,
-                                  act[0] != 0, NS == 2 && act[NS - 1] != 0, false);
+            // P2: w = J z (rows taken from the pass's counter), then the
+            // partial dots V_k . w (k <= j) over the CTA's own rows
+            if (blockIdx.x == 0 && tid == 0) a.ctr[(spass + 1) & (kPasses - 1)] = 0;
+            spmv_rows<VT, IT, NS>(a, a.ctr + (spass & (kPasses - 1)), a.sys[0].z, a.sys[0].zs,
+                                  NS == 2 ? a.sys[1].z : nullptr, NS == 2 ? a.sys[1].zs : nullptr, a.sys[0].w,
+                                  NS == 2 ? a.sys[1].w : nullptr, act[0] != 0, NS == 2 && act[NS - 1] != 0, false);
+            ++spass;
             if (tid < 2) {
                 cnt[tid] = (tid < NS && act[tid]) ? j + 1 : 0;
                 kw[tid] = -1;
             }
-            __syncthreads();
-            partial_dots<NS>(a, r0, r1, n, cnt, kw, pass0, true);
+            grid.sync();
+            partial_dots<NS>(a, r0, r1, n, cnt, kw, pass0);
             grid.sync();
             // P3: c1; w -= V c1; partial dots V_k . w and |w|^2
             reduce_partials<NS>(pass0, cnt, c1);
@@ -469,15 +477,17 @@ __global__ void __launch_bounds__(kThreads, 2) fused_gmres_kernel(FusedArgs a)
             for (int k = r0 + tid; k < r1; k += blockDim.x) S.zs[k] = S.x[a.sorted[k]];
         }
         grid.sync();
-        spmv_rows<VT, IT, NS>(a, a.sys[0].x, a.sys[0].zs, NS == 2 ? a.sys[1].x : nullptr,
-                              NS == 2 ? a.sys[1].zs : nullptr, a.sys[0].w, NS == 2 ? a.sys[1].w : nullptr, rs[0] != 0,
-                              NS == 2 && rs[NS - 1] != 0, true);
+        if (blockIdx.x == 0 && tid == 0) a.ctr[(spass + 1) & (kPasses - 1)] = 0;
+        spmv_rows<VT, IT, NS>(a, a.ctr + (spass & (kPasses - 1)), a.sys[0].x, a.sys[0].zs,
+                              NS == 2 ? a.sys[1].x : nullptr, NS == 2 ? a.sys[1].zs : nullptr, a.sys[0].w,
+                              NS == 2 ? a.sys[1].w : nullptr, rs[0] != 0, NS == 2 && rs[NS - 1] != 0, true);
+        ++spass;
         if (tid < 2) {
             cnt[tid] = (tid < NS && rs[tid]) ? 1 : 0;
             kw[tid] = 0;
         }
-        __syncthreads();
-        partial_dots<NS>(a, r0, r1, n, cnt, kw, pass0, true);
+        grid.sync();
+        partial_dots<NS>(a, r0, r1, n, cnt, kw, pass0);
         grid.sync();
         reduce_partials<NS>(pass0, cnt, c1);
         __syncthreads();
@@ -548,6 +558,7 @@ int fused_alloc(Engine &e, int ns)
     if (!e.d_fpart) {
         if (cudaMalloc(&e.d_fpart, sizeof(double) * 2 * 2 * 1024 * kKM) != cudaSuccess) return SDDDST_ERR_NOMEM;
         if (cudaMalloc(&e.d_fstatus, sizeof(double) * 4 * kStatusSlots) != cudaSuccess) return SDDDST_ERR_NOMEM;
+        if (cudaMalloc(&e.d_fctr, sizeof(int) * kPasses) != cudaSuccess) return SDDDST_ERR_NOMEM;
         if (cudaMallocHost(&e.h_fstatus, sizeof(double) * 4 * kStatusSlots) != cudaSuccess) return SDDDST_ERR_NOMEM;
     }
     if (ns == 2 && !e.d_V2) {
@@ -565,6 +576,7 @@ void fused_free(Engine &e)
     double *bufs[] = {e.d_fpart, e.d_fstatus, e.d_V2, e.d_w2, e.d_z2, e.d_zs2, e.d_gI, e.d_solI, e.d_dvecI, e.d_vsI};
     for (double *b : bufs)
         if (b) cudaFree(b);
+    if (e.d_fctr) cudaFree(e.d_fctr);
     if (e.h_fstatus) cudaFreeHost(e.h_fstatus);
 }
 
@@ -589,6 +601,7 @@ int fused_gmres(Engine &e, int ns, const double *h, const double *const *dvec, c
     a.vals = e.valf ? (const void *)e.d_valf : (const void *)e.d_val;
     a.sorted = e.spmv_sorted;
     a.part = e.d_fpart;
+    a.ctr = e.d_fctr;
     double *Vs[2] = {e.d_V, e.d_V2};
     double *ws[2] = {e.d_w, e.d_w2};
     double *zs[2] = {e.d_z, e.d_z2};
