@@ -794,7 +794,8 @@ def main():
                    "step_size_range": h_window,
                    "solver_stats": solver_stats,
                    "gmres_iterations_per_solve": solver_stats["iterations"] / max(1, solver_stats["solves"])},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "accepted": e2e_acc, "attempts": args.steps, "ms_per_step": e2e_ms / max(1, args.steps)},
         "gpu_launches": launches,
         "roofline": roof,
         "clocks": clk,

@@ -9,8 +9,9 @@
 // iteration needs stays on the device:
 //   P1  z = M^-1 V_j (cluster block-Jacobi), written in the user order and in
 //       the cell-sorted order the SpMV gathers from;
-//   P2  w = J z (warp per row; rows taken dynamically in cell-sorted order),
-//       then, after a barrier, the CTA's partial dots V_k . w over its rows;
+//   P2  w = J z (warp per row; CTAs take rows dynamically in cell-sorted
+//       order), then, after a barrier, the CTA's partial dots V_k . w over its
+//       own static rows;
 //   P3  reduced c1, w -= V c1, partial dots V_k . w and |w|^2 (second
 //       Gram-Schmidt pass);
 //   P4  reduced c2, w -= V c2, V_{j+1} = w / |w| (|w|^2 = |w1|^2 - |c2|^2),
@@ -37,7 +38,6 @@ constexpr int kThreads = 512;
 constexpr int kKM = 32; // restart length bound (m <= 31) and partial-sum stride
 constexpr int kStatusSlots = 8; // solves whose statuses one attempt can leave on the device
 constexpr int kPasses = 1024;   // ring of SpMV row counters (a pass zeroes the next one)
-constexpr int kRowChunk = 4;    // sorted positions a warp takes per grab
 
 struct FusedSys {
     double h;
@@ -198,33 +198,36 @@ __device__ __forceinline__ void spmv_row(const FusedArgs &a, int row, int lane, 
 }
 
 // out_s[row] = v_s[row] + (1 + d_s)/2 h_s (G v_s)[row] (sign -1: rhs_s - that),
-// one warp per row.  The rows are taken in cell-sorted order, kRowChunk at a
-// time, from the pass's counter: consecutive rows of a warp are spatial
-// neighbours (their gathers from the cell-sorted vector share a few
-// kilobytes), and SMs that run slower (their distance to the memory they
-// gather from differs by up to 40 % in the per-CTA times) simply take fewer
-// rows.  Each row is summed by one warp in a fixed order, so w does not
-// depend on which warp took the row; the dots over w that follow use the
-// static row partition, so results stay bit-identical run to run.  The next
-// grab is issued before the current chunk's rows are processed.
+// one warp per row.  The CTA takes the rows in cell-sorted order, one per
+// warp per grab, from the pass's counter: its warps work on consecutive
+// sorted positions (spatial neighbours, whose gathers from the cell-sorted
+// vector share a few kilobytes), and SMs that run slower (the per-CTA times
+// of a static split differ by up to 40 %) simply take fewer rows; the tail is
+// one row per warp.  The next grab is issued before the current rows are
+// summed (double-buffered in shared memory, one CTA barrier per grab).  Each
+// row is summed by one warp in a fixed order, so w does not depend on which
+// CTA took it; the dots over w that follow use the static row partition, so
+// results stay bit-identical run to run.
 template <typename VT, typename IT, int NS>
 __device__ __forceinline__ void spmv_rows(const FusedArgs &a, int *ctr, const double *v0, const double *vs0,
                                           const double *v1, const double *vs1, double *o0, double *o1, bool act0,
                                           bool act1, bool residual)
 {
-    const int lane = threadIdx.x & 31;
+    __shared__ int grab[2];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const VT *val = static_cast<const VT *>(a.vals);
     const IT *col = static_cast<const IT *>(a.cols);
-    int g = 0;
-    if (lane == 0) g = atomicAdd(ctr, kRowChunk);
-    g = __shfl_sync(0xffffffffu, g, 0);
+    if (threadIdx.x == 0) grab[0] = atomicAdd(ctr, nw);
+    __syncthreads();
+    int buf = 0;
+    int g = grab[0];
     while (g < a.n) {
-        int gn = 0;
-        if (lane == 0) gn = atomicAdd(ctr, kRowChunk);
-        const int kend = min(g + kRowChunk, a.n);
-        for (int k = g; k < kend; ++k)
-            spmv_row<VT, IT, NS>(a, a.sorted[k], lane, val, col, v0, vs0, v1, vs1, o0, o1, act0, act1, residual);
-        g = __shfl_sync(0xffffffffu, gn, 0);
+        if (threadIdx.x == 0) grab[buf ^ 1] = atomicAdd(ctr, nw);
+        const int k = g + wid;
+        if (k < a.n) spmv_row<VT, IT, NS>(a, a.sorted[k], lane, val, col, v0, vs0, v1, vs1, o0, o1, act0, act1, residual);
+        __syncthreads();
+        buf ^= 1;
+        g = grab[buf];
     }
 }
 
