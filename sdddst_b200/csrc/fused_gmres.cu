@@ -167,6 +167,15 @@ __device__ __forceinline__ void spmv_row(const FusedArgs &a, int row, int lane, 
                                          bool act1, bool residual)
 {
     const int s = a.rowptr[row], e = a.rowptr[row + 1];
+    // the row's values and positions toward L2 at once (one 128-byte line
+    // per lane for each, the first 1024 entries): the loop below walks the
+    // row in 256-entry steps whose loads then wait on L2 instead of DRAM
+    {
+        const char *pv = reinterpret_cast<const char *>(val + s) + 128 * lane;
+        const char *pc = reinterpret_cast<const char *>(col + s) + 128 * lane;
+        if (pv < reinterpret_cast<const char *>(val + e)) asm volatile("prefetch.global.L2 [%0];" ::"l"(pv));
+        if (pc < reinterpret_cast<const char *>(col + e)) asm volatile("prefetch.global.L2 [%0];" ::"l"(pc));
+    }
     double acc0 = 0.0, acc1 = 0.0;
     const double gd = (double)val[s];
     if (lane == 0) {
