@@ -212,9 +212,8 @@ __device__ __forceinline__ void spmv_row(const FusedArgs &a, int row, int lane, 
 // sorted positions (spatial neighbours, whose gathers from the cell-sorted
 // vector share a few kilobytes), and SMs that run slower (the per-CTA times
 // of a static split differ by up to 40 %) simply take fewer rows; the tail is
-// one row per warp.  Grabs run two chunks ahead (three slots in shared
-// memory, one CTA barrier per chunk), so each warp sends its next row toward
-// L2 before summing the current one.  Each
+// one row per warp.  The next grab is issued before the current rows are
+// summed (double-buffered in shared memory, one CTA barrier per grab).  Each
 // row is summed by one warp in a fixed order, so w does not depend on which
 // CTA took it; the dots over w that follow use the static row partition, so
 // results stay bit-identical run to run.
@@ -223,35 +222,21 @@ __device__ __forceinline__ void spmv_rows(const FusedArgs &a, int *ctr, const do
                                           const double *v1, const double *vs1, double *o0, double *o1, bool act0,
                                           bool act1, bool residual)
 {
-    __shared__ int grab[3];
+    __shared__ int grab[2];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const VT *val = static_cast<const VT *>(a.vals);
     const IT *col = static_cast<const IT *>(a.cols);
-    if (threadIdx.x == 0) {
-        grab[0] = atomicAdd(ctr, nw);
-        grab[1] = atomicAdd(ctr, nw);
-    }
+    if (threadIdx.x == 0) grab[0] = atomicAdd(ctr, nw);
     __syncthreads();
-    int slot = 0;
-    int g = grab[0], gn = grab[1];
+    int buf = 0;
+    int g = grab[0];
     while (g < a.n) {
-        // grabs run two chunks ahead, so the warp's next row is known now:
-        // its values and positions go toward L2 while this row is summed
-        if (threadIdx.x == 0) grab[slot == 0 ? 2 : slot - 1] = atomicAdd(ctr, nw);
-        if (gn + wid < a.n) {
-            const int r2 = a.sorted[gn + wid];
-            const int s2 = a.rowptr[r2], e2 = a.rowptr[r2 + 1];
-            const char *pv = reinterpret_cast<const char *>(val + s2) + 128 * lane;
-            const char *pc = reinterpret_cast<const char *>(col + s2) + 128 * lane;
-            if (pv < reinterpret_cast<const char *>(val + e2)) asm volatile("prefetch.global.L2 [%0];" ::"l"(pv));
-            if (pc < reinterpret_cast<const char *>(col + e2)) asm volatile("prefetch.global.L2 [%0];" ::"l"(pc));
-        }
+        if (threadIdx.x == 0) grab[buf ^ 1] = atomicAdd(ctr, nw);
         const int k = g + wid;
         if (k < a.n) spmv_row<VT, IT, NS>(a, a.sorted[k], lane, val, col, v0, vs0, v1, vs1, o0, o1, act0, act1, residual);
         __syncthreads();
-        slot = slot == 2 ? 0 : slot + 1;
-        g = gn;
-        gn = grab[slot == 2 ? 0 : slot + 1];
+        buf ^= 1;
+        g = grab[buf];
     }
 }
 
