@@ -98,6 +98,7 @@ struct Engine {
     // and the second system's Krylov basis and vectors (joint stage I + II)
     double *d_fpart = nullptr, *d_fstatus = nullptr, *h_fstatus = nullptr;
     int *d_fctr = nullptr; // row counters of the device-resident GMRES's SpMV passes
+    int2 *d_fsrow = nullptr; // per cell-sorted position: its CSR row's (start, end)
     double *d_V2 = nullptr, *d_w2 = nullptr, *d_z2 = nullptr, *d_zs2 = nullptr;
     double *d_gI = nullptr, *d_solI = nullptr, *d_dvecI = nullptr, *d_vsI = nullptr; // stage I's g, solution, d, speed
     bool fused = false;                   // the cluster solver runs device-resident (set at init)

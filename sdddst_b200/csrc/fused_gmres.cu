@@ -59,6 +59,7 @@ struct FusedArgs {
     const void *cols;  // cell-sorted column positions (IT), diagonal slot unused
     const void *vals;  // G values (VT), diagonal in each row's first slot
     const int *sorted; // cell-sorted position -> dislocation
+    const int2 *srow;  // cell-sorted position -> its row's (start, end) in the CSR
     double *part;      // per-CTA partial sums: [2 passes][2 systems][kKM][grid] (a sum's partials contiguous)
     int *ctr;          // SpMV row counters, one per pass (ring of kPasses)
     FusedSys sys[2];
@@ -161,12 +162,11 @@ struct RowDot {
 
 // one row of the SpMV below
 template <typename VT, typename IT, int NS>
-__device__ __forceinline__ void spmv_row(const FusedArgs &a, int row, int lane, const VT *__restrict__ val,
-                                         const IT *__restrict__ col, const double *v0, const double *vs0,
-                                         const double *v1, const double *vs1, double *o0, double *o1, bool act0,
-                                         bool act1, bool residual)
+__device__ __forceinline__ void spmv_row(const FusedArgs &a, int row, int s, int e, int lane,
+                                         const VT *__restrict__ val, const IT *__restrict__ col, const double *v0,
+                                         const double *vs0, const double *v1, const double *vs1, double *o0,
+                                         double *o1, bool act0, bool act1, bool residual)
 {
-    const int s = a.rowptr[row], e = a.rowptr[row + 1];
     // the row's values and positions toward L2 at once (one 128-byte line
     // per lane for each, the first 1024 entries): the loop below walks the
     // row in 256-entry steps whose loads then wait on L2 instead of DRAM
@@ -178,9 +178,21 @@ __device__ __forceinline__ void spmv_row(const FusedArgs &a, int row, int lane, 
     }
     double acc0 = 0.0, acc1 = 0.0;
     const double gd = (double)val[s];
+    // the row's scalars for the epilogue, loaded before the sum (lane 0)
+    double f0 = 0.0, f1 = 0.0, r0 = 0.0, r1 = 0.0;
     if (lane == 0) {
         acc0 = act0 ? gd * v0[row] : 0.0;
         if (NS == 2) acc1 = act1 ? gd * v1[row] : 0.0;
+        if (act0) {
+            const FusedSys &S = a.sys[0];
+            f0 = (1.0 + S.dvec[row]) * 0.5 * (S.hrow ? S.hrow[row] : S.h);
+            r0 = residual ? S.rhs[row] : 0.0;
+        }
+        if (NS == 2 && act1) {
+            const FusedSys &S = a.sys[1];
+            f1 = (1.0 + S.dvec[row]) * 0.5 * (S.hrow ? S.hrow[row] : S.h);
+            r1 = residual ? S.rhs[row] : 0.0;
+        }
     }
     if (NS == 2 && act0 && act1)
         RowDot<VT, IT, 2>::run(s, e, lane, val, col, vs0, vs1, acc0, acc1);
@@ -191,17 +203,14 @@ __device__ __forceinline__ void spmv_row(const FusedArgs &a, int row, int lane, 
     acc0 = warp_sum(acc0);
     if (NS == 2) acc1 = warp_sum(acc1);
     if (lane == 0) {
+        // acc includes G_ii v_i; y = v_i + (1 + d_i)/2 h (G v)_i
         if (act0) {
-            const FusedSys &S = a.sys[0];
-            const double hh = S.hrow ? S.hrow[row] : S.h;
-            const double y = v0[row] + (1.0 + S.dvec[row]) * 0.5 * hh * acc0;
-            o0[row] = residual ? S.rhs[row] - y : y;
+            const double y = v0[row] + f0 * acc0;
+            o0[row] = residual ? r0 - y : y;
         }
         if (NS == 2 && act1) {
-            const FusedSys &S = a.sys[1];
-            const double hh = S.hrow ? S.hrow[row] : S.h;
-            const double y = v1[row] + (1.0 + S.dvec[row]) * 0.5 * hh * acc1;
-            o1[row] = residual ? S.rhs[row] - y : y;
+            const double y = v1[row] + f1 * acc1;
+            o1[row] = residual ? r1 - y : y;
         }
     }
 }
@@ -233,7 +242,11 @@ __device__ __forceinline__ void spmv_rows(const FusedArgs &a, int *ctr, const do
     while (g < a.n) {
         if (threadIdx.x == 0) grab[buf ^ 1] = atomicAdd(ctr, nw);
         const int k = g + wid;
-        if (k < a.n) spmv_row<VT, IT, NS>(a, a.sorted[k], lane, val, col, v0, vs0, v1, vs1, o0, o1, act0, act1, residual);
+        if (k < a.n) {
+            const int2 se = a.srow[k]; // loaded beside sorted[k], not after it
+            spmv_row<VT, IT, NS>(a, a.sorted[k], se.x, se.y, lane, val, col, v0, vs0, v1, vs1, o0, o1, act0, act1,
+                                 residual);
+        }
         __syncthreads();
         buf ^= 1;
         g = grab[buf];
@@ -528,6 +541,16 @@ __global__ void __launch_bounds__(kThreads, 2) fused_gmres_kernel(FusedArgs a)
     }
 }
 
+// (start, end) of the row at each cell-sorted position
+__global__ void sorted_rows_kernel(int n, const int *__restrict__ sorted, const int *__restrict__ rowptr,
+                                   int2 *__restrict__ srow)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int r = sorted[k];
+    srow[k] = make_int2(rowptr[r], rowptr[r + 1]);
+}
+
 template <typename VT, typename IT, int NS>
 const void *kernel_ptr()
 {
@@ -571,6 +594,7 @@ int fused_alloc(Engine &e, int ns)
         if (cudaMalloc(&e.d_fpart, sizeof(double) * 2 * 2 * 1024 * kKM) != cudaSuccess) return SDDDST_ERR_NOMEM;
         if (cudaMalloc(&e.d_fstatus, sizeof(double) * 4 * kStatusSlots) != cudaSuccess) return SDDDST_ERR_NOMEM;
         if (cudaMalloc(&e.d_fctr, sizeof(int) * kPasses) != cudaSuccess) return SDDDST_ERR_NOMEM;
+        if (cudaMalloc(&e.d_fsrow, sizeof(int2) * (size_t)e.n) != cudaSuccess) return SDDDST_ERR_NOMEM;
         if (cudaMallocHost(&e.h_fstatus, sizeof(double) * 4 * kStatusSlots) != cudaSuccess) return SDDDST_ERR_NOMEM;
     }
     if (ns == 2 && !e.d_V2) {
@@ -589,6 +613,7 @@ void fused_free(Engine &e)
     for (double *b : bufs)
         if (b) cudaFree(b);
     if (e.d_fctr) cudaFree(e.d_fctr);
+    if (e.d_fsrow) cudaFree(e.d_fsrow);
     if (e.h_fstatus) cudaFreeHost(e.h_fstatus);
 }
 
@@ -614,6 +639,9 @@ int fused_gmres(Engine &e, int ns, const double *h, const double *const *dvec, c
     a.sorted = e.spmv_sorted;
     a.part = e.d_fpart;
     a.ctr = e.d_fctr;
+    sorted_rows_kernel<<<(e.n + 255) / 256, 256, 0, e.st>>>(e.n, e.spmv_sorted, e.d_rowptr, e.d_fsrow);
+    e.launches++;
+    a.srow = e.d_fsrow;
     double *Vs[2] = {e.d_V, e.d_V2};
     double *ws[2] = {e.d_w, e.d_w2};
     double *zs[2] = {e.d_z, e.d_z2};
