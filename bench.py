@@ -343,45 +343,46 @@ def finish_cpu_baseline(procs, timeout=900):
 def reference_arm(args):
     """The reference's own CPU code for one step attempt at the full workload:
     the five calculateSpeeds and three calculateJacobian calls of a
-    zero-stress attempt (simulation.cpp:62-84,435-650), executed one after
-    the other on one core (the reference is single-threaded) on the N = 32768
-    configuration and timed as one step.  The UMFPACK factorization and
-    solve are excluded (UMFPACK is not installed; the harness's stand-in LU
-    would only make the reference slower).  One such attempt takes about
-    ten minutes, so the arm times one attempt whatever --steps asks for,
-    after a warm-up of one small call."""
+    zero-stress attempt (simulation.cpp:62-84,435-650) at N = 32768.  The
+    reference is single-threaded and an attempt runs its calls one after
+    the other on one core, so the attempt's time is the sum of the eight
+    calls' times; to keep the run within a few minutes the eight calls run
+    at once, each in its own process on its own host core (the calls are
+    compute-bound; they share no data), and their times are summed.  The
+    UMFPACK factorization and solve are excluded (UMFPACK is not installed;
+    the harness's stand-in LU would only make the reference slower).  One
+    attempt is timed whatever --steps asks for."""
     ws, rank, _ = _dist()
     if rank != 0:
         return
     n = args.n
-    sim, xyb, kind = _ref_sim(n)
-    from oracle import ref
-    small = ref.Sim(np.ascontiguousarray(xyb[:512]), None, ref.params(cutoff_multiplier=CUTOFF_M, prec=PREC,
-                                                                       step_size=H0),
-                    "ref" if kind == "reference" else "port")
-    small.speeds(np.ascontiguousarray(xyb[:512]))  # warm-up: library pages, allocator
-    calls = []
-    cap = _jacobian_cap(n)
+    kinds = ["speeds", "jacobian", "speeds", "speeds", "jacobian", "speeds", "jacobian", "speeds"]
     t0 = time.perf_counter()
-    for what in ("speeds", "jacobian", "speeds", "speeds", "jacobian", "speeds", "jacobian", "speeds"):
-        c0 = time.perf_counter()
-        if what == "speeds":
-            sim.speeds(xyb)
-        else:
-            sim.jacobian(H0, xyb, cap=cap)
-        calls.append((what, time.perf_counter() - c0))
-    t = time.perf_counter() - t0
+    procs = [subprocess.Popen([sys.executable, os.path.abspath(__file__), "--cpu-baseline-worker", which,
+                               "--n", str(n)], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+             for which in kinds]
+    calls, kind = [], None
+    for which, proc in zip(kinds, procs):
+        out, err = proc.communicate(timeout=1800)
+        if proc.returncode != 0:
+            raise RuntimeError(err.strip().splitlines()[-1] if err.strip() else f"rc {proc.returncode}")
+        r = json.loads(out.strip().splitlines()[-1])
+        kind = r["kind"]
+        calls.append((which, (r["t_speeds"] if which == "speeds" else r["t_jacobian"])[0]))
+    wall = time.perf_counter() - t0
+    t = sum(c for _, c in calls)
     v = 1.0 / t
     t_sp = [c for w, c in calls if w == "speeds"]
     t_jac = [c for w, c in calls if w == "jacobian"]
-    sample = (f"one zero-stress step attempt of the reference at the full N={n} configuration on one core: "
-              f"5 calculateSpeeds ({min(t_sp):.1f}-{max(t_sp):.1f} s each) and 3 calculateJacobian "
-              f"({min(t_jac):.1f}-{max(t_jac):.1f} s each) run in sequence, {t:.1f} s; UMFPACK solve excluded")
+    sample = (f"one zero-stress step attempt of the reference at the full N={n} configuration: 5 calculateSpeeds "
+              f"({min(t_sp):.1f}-{max(t_sp):.1f} s each) and 3 calculateJacobian ({min(t_jac):.1f}-{max(t_jac):.1f} s "
+              f"each), each call on its own core at the same time ({wall:.0f} s wall), summed to the {t:.1f} s "
+              f"one core takes for the attempt; UMFPACK solve excluded")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": 1,
             "requested_steps": args.steps, "warmup": 0, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"n{n}_m{CUTOFF_M}_seed{SEED}", "N": n, "cutoff_multiplier": CUTOFF_M,
-                       "prec": PREC, "parallelism": "none (single-threaded reference)"},
+                       "prec": PREC, "parallelism": "none (single-threaded reference; calls timed concurrently)"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
