@@ -84,11 +84,15 @@ struct RowDot;
 template <int NS>
 struct RowDot<float, unsigned short, NS> {
     // 16-byte value and 8-byte position loads from the first multiple of four
-    // in the row on, the unaligned head and the tail entry by entry
+    // in the row on, the unaligned head and the tail entry by entry.  A step
+    // issues the loads of four 128-entry chunks (512 entries: most of a row)
+    // before any of their gathers, so a warp has 3 KB of the CSR stream in
+    // flight instead of waiting on it chunk by chunk
     __device__ __forceinline__ static void run(int s, int e, int lane, const float *__restrict__ val,
                                                const unsigned short *__restrict__ col, const double *__restrict__ a,
                                                const double *__restrict__ b, double &acc0, double &acc1)
     {
+        constexpr int kU = 4;
         const int q0 = s + 1;
         const int qa = min(e, (q0 + 3) & ~3);
         if (q0 + lane < qa) {
@@ -97,42 +101,35 @@ struct RowDot<float, unsigned short, NS> {
             acc0 += g * a[c];
             if (NS == 2) acc1 += g * b[c];
         }
-        // two 128-entry chunks per step: both chunks' value and position
-        // loads are issued before their gathers (twice the loads in flight
-        // per warp at two CTAs per SM)
-        for (int q = qa + 4 * lane; q + 3 < e; q += 256) {
-            const bool two = q + 131 < e;
-            const float4 w = *reinterpret_cast<const float4 *>(val + q);
-            const uint2 c = *reinterpret_cast<const uint2 *>(col + q);
-            float4 w2 = make_float4(0.f, 0.f, 0.f, 0.f);
-            uint2 cc = make_uint2(0u, 0u);
-            if (two) {
-                w2 = *reinterpret_cast<const float4 *>(val + q + 128);
-                cc = *reinterpret_cast<const uint2 *>(col + q + 128);
+        for (int q = qa + 4 * lane; q + 3 < e; q += 128 * kU) {
+            float4 w[kU];
+            uint2 c[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int qq = q + 128 * u;
+                if (u == 0 || qq + 3 < e) {
+                    w[u] = *reinterpret_cast<const float4 *>(val + qq);
+                    c[u] = *reinterpret_cast<const uint2 *>(col + qq);
+                } else {
+                    w[u] = make_float4(0.f, 0.f, 0.f, 0.f); // position 0, weight 0
+                    c[u] = make_uint2(0u, 0u);
+                }
             }
-            const int c0 = c.x & 0xffffu, c1 = c.x >> 16, c2 = c.y & 0xffffu, c3 = c.y >> 16;
-            const int d0 = cc.x & 0xffffu, d1 = cc.x >> 16, d2 = cc.y & 0xffffu, d3 = cc.y >> 16;
-            const double a0 = a[c0], a1 = a[c1], a2 = a[c2], a3 = a[c3];
-            const double a4 = a[d0], a5 = a[d1], a6 = a[d2], a7 = a[d3]; // position 0 when !two (w2 = 0)
-            acc0 += (double)w.x * a0;
-            acc0 += (double)w.y * a1;
-            acc0 += (double)w.z * a2;
-            acc0 += (double)w.w * a3;
-            acc0 += (double)w2.x * a4;
-            acc0 += (double)w2.y * a5;
-            acc0 += (double)w2.z * a6;
-            acc0 += (double)w2.w * a7;
-            if (NS == 2) {
-                const double b0 = b[c0], b1 = b[c1], b2 = b[c2], b3 = b[c3];
-                const double b4 = b[d0], b5 = b[d1], b6 = b[d2], b7 = b[d3];
-                acc1 += (double)w.x * b0;
-                acc1 += (double)w.y * b1;
-                acc1 += (double)w.z * b2;
-                acc1 += (double)w.w * b3;
-                acc1 += (double)w2.x * b4;
-                acc1 += (double)w2.y * b5;
-                acc1 += (double)w2.z * b6;
-                acc1 += (double)w2.w * b7;
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int c0 = c[u].x & 0xffffu, c1 = c[u].x >> 16, c2 = c[u].y & 0xffffu, c3 = c[u].y >> 16;
+                const double a0 = a[c0], a1 = a[c1], a2 = a[c2], a3 = a[c3];
+                acc0 += (double)w[u].x * a0;
+                acc0 += (double)w[u].y * a1;
+                acc0 += (double)w[u].z * a2;
+                acc0 += (double)w[u].w * a3;
+                if (NS == 2) {
+                    const double b0 = b[c0], b1 = b[c1], b2 = b[c2], b3 = b[c3];
+                    acc1 += (double)w[u].x * b0;
+                    acc1 += (double)w[u].y * b1;
+                    acc1 += (double)w[u].z * b2;
+                    acc1 += (double)w[u].w * b3;
+                }
             }
         }
         const int qt = qa + ((e - qa) & ~3);
