@@ -83,61 +83,32 @@ struct RowDot;
 
 template <int NS>
 struct RowDot<float, unsigned short, NS> {
-    // 16-byte value and 8-byte position loads from the first multiple of four
-    // in the row on, the unaligned head and the tail entry by entry.  A step
-    // issues the loads of four 128-entry chunks (512 entries: most of a row)
-    // before any of their gathers, so a warp has 3 KB of the CSR stream in
-    // flight instead of waiting on it chunk by chunk
+    // Lane l takes entries q + l + 32 u (u < 8) of each 256-entry step: the
+    // value and position loads are coalesced scalar loads, and, since a row's
+    // positions run in cell-sorted order, the 32 lanes of one gather read
+    // neighbouring doubles (two or three cache lines) -- the gathers, not the
+    // CSR stream, set the SpMV's pace in L1, and a lane holding four
+    // consecutive entries instead spreads each gather over about sixteen lines
     __device__ __forceinline__ static void run(int s, int e, int lane, const float *__restrict__ val,
                                                const unsigned short *__restrict__ col, const double *__restrict__ a,
                                                const double *__restrict__ b, double &acc0, double &acc1)
     {
-        constexpr int kU = 4;
-        const int q0 = s + 1;
-        const int qa = min(e, (q0 + 3) & ~3);
-        if (q0 + lane < qa) {
-            const double g = (double)val[q0 + lane];
-            const int c = col[q0 + lane];
-            acc0 += g * a[c];
-            if (NS == 2) acc1 += g * b[c];
-        }
-        for (int q = qa + 4 * lane; q + 3 < e; q += 128 * kU) {
-            float4 w[kU];
-            uint2 c[kU];
+        constexpr int kU = 8;
+        for (int q = s + 1 + lane; q < e; q += 32 * kU) {
+            float w[kU];
+            int c[kU];
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
-                const int qq = q + 128 * u;
-                if (u == 0 || qq + 3 < e) {
-                    w[u] = *reinterpret_cast<const float4 *>(val + qq);
-                    c[u] = *reinterpret_cast<const uint2 *>(col + qq);
-                } else {
-                    w[u] = make_float4(0.f, 0.f, 0.f, 0.f); // position 0, weight 0
-                    c[u] = make_uint2(0u, 0u);
-                }
+                const int qq = q + 32 * u;
+                const bool in = qq < e;
+                w[u] = in ? val[qq] : 0.0f; // position 0, weight 0 past the row
+                c[u] = in ? (int)col[qq] : 0;
             }
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
-                const int c0 = c[u].x & 0xffffu, c1 = c[u].x >> 16, c2 = c[u].y & 0xffffu, c3 = c[u].y >> 16;
-                const double a0 = a[c0], a1 = a[c1], a2 = a[c2], a3 = a[c3];
-                acc0 += (double)w[u].x * a0;
-                acc0 += (double)w[u].y * a1;
-                acc0 += (double)w[u].z * a2;
-                acc0 += (double)w[u].w * a3;
-                if (NS == 2) {
-                    const double b0 = b[c0], b1 = b[c1], b2 = b[c2], b3 = b[c3];
-                    acc1 += (double)w[u].x * b0;
-                    acc1 += (double)w[u].y * b1;
-                    acc1 += (double)w[u].z * b2;
-                    acc1 += (double)w[u].w * b3;
-                }
+                acc0 += (double)w[u] * a[c[u]];
+                if (NS == 2) acc1 += (double)w[u] * b[c[u]];
             }
-        }
-        const int qt = qa + ((e - qa) & ~3);
-        if (qt + lane < e) {
-            const double g = (double)val[qt + lane];
-            const int c = col[qt + lane];
-            acc0 += g * a[c];
-            if (NS == 2) acc1 += g * b[c];
         }
     }
 };
