@@ -94,14 +94,8 @@ __device__ __forceinline__ float ex2_fast(float x)
 constexpr float kPiLog2eF = 4.532360141827193f;   // pi log2(e)
 constexpr float kSinhSplitF = 0.15915494309189535f; // |pi dx| = 0.5
 constexpr float kPiSqF = 9.869604401089358f;
-constexpr float kEPiF = 23.140692632779267f;           // e^{pi}
-constexpr float kEmPiF = 0.04321391826377226f;         // e^{-pi}
-constexpr float kEQuarterPiF = 2.1932800507380152f;    // e^{pi / 4}
 
-// The same with e^{pi dx} and e^{-pi dx} supplied by the caller (the pair
-// tiles form them as products of per-dislocation exponentials, which takes
-// the two ex2 per pair off the SFU).
-__device__ __forceinline__ float2 tau_xy_f32x2_e(float2 dx, float2 sn, float2 ep, float2 epi, float2 &s_out)
+__device__ __forceinline__ float2 tau_xy_f32x2(float2 dx, float2 sn, float2 &s_out)
 {
     const float2 sn2 = mul2(sn, sn);
     const float2 cy = fma2(sn2, f2c(-2.0f), f2c(1.0f));
@@ -111,6 +105,12 @@ __device__ __forceinline__ float2 tau_xy_f32x2_e(float2 dx, float2 sn, float2 ep
     q = fma2(q, x2, f2c(5.167712780049969f));
     q = fma2(q, x2, f2c(3.141592653589793f));
     q = mul2(dx, q);
+    const float2 xk = mul2(dx, f2c(kPiLog2eF));
+    float2 ep, epi;
+    ep.x = ex2_fast(xk.x);
+    ep.y = ex2_fast(xk.y);
+    epi.x = ex2_fast(-xk.x);
+    epi.y = ex2_fast(-xk.y);
     const float2 shx = fma2(ep, f2c(0.5f), mul2(epi, f2c(-0.5f)));
     float2 sh;
     sh.x = fabsf(dx.x) < kSinhSplitF ? q.x : shx.x;
@@ -143,17 +143,6 @@ __device__ __forceinline__ float2 tau_xy_f32x2_e(float2 dx, float2 sn, float2 ep
     const float2 c2 = fma2(mul2(cy, cy), f2c(16.0f * kQN2SQ), f2c(-8.0f * kQN2SQ));
     const float2 far2 = fma2(c2, g2, mul2(cy, g1));
     return add2(near2, far2);
-}
-
-__device__ __forceinline__ float2 tau_xy_f32x2(float2 dx, float2 sn, float2 &s_out)
-{
-    const float2 xk = mul2(dx, f2c(kPiLog2eF));
-    float2 ep, epi;
-    ep.x = ex2_fast(xk.x);
-    ep.y = ex2_fast(xk.y);
-    epi.x = ex2_fast(-xk.x);
-    epi.y = ex2_fast(-xk.y);
-    return tau_xy_f32x2_e(dx, sn, ep, epi, s_out);
 }
 
 } // namespace sd

@@ -81,35 +81,110 @@ __device__ __forceinline__ double block_row(const FusedSys &S, int i, const doub
 template <typename VT, typename IT, int NS>
 struct RowDot;
 
-template <int NS>
-struct RowDot<float, unsigned short, NS> {
-    // Lane l takes entries q + l + 32 u (u < 8) of each 256-entry step: the
-    // value and position loads are coalesced scalar loads, and, since a row's
-    // positions run in cell-sorted order, the 32 lanes of one gather read
-    // neighbouring doubles (two or three cache lines) -- the gathers, not the
-    // CSR stream, set the SpMV's pace in L1, and a lane holding four
-    // consecutive entries instead spreads each gather over about sixteen lines
+// FP32 values, 16-bit cell-sorted positions.  Two forms, measured on the
+// N=32768 workload (SpMV phase of a solve, about five passes):
+//   one vector (stage III): a lane holds four consecutive entries (16-byte
+//   value and 8-byte position loads), two 128-entry chunks per step: 185 us;
+//   lanes on consecutive entries (scalar coalesced loads): 209 us;
+//   two vectors (stages I+II): 385 us and 345 us -- with two gathers per
+//   entry the gathers' spread over cache lines dominates, and consecutive
+//   lanes on consecutive entries read neighbouring doubles.
+template <>
+struct RowDot<float, unsigned short, 1> {
     __device__ __forceinline__ static void run(int s, int e, int lane, const float *__restrict__ val,
                                                const unsigned short *__restrict__ col, const double *__restrict__ a,
                                                const double *__restrict__ b, double &acc0, double &acc1)
     {
-        constexpr int kU = 8;
-        for (int q = s + 1 + lane; q < e; q += 32 * kU) {
-            float w[kU];
-            int c[kU];
-#pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                const int qq = q + 32 * u;
-                const bool in = qq < e;
-                w[u] = in ? val[qq] : 0.0f; // position 0, weight 0 past the row
-                c[u] = in ? (int)col[qq] : 0;
+        (void)b;
+        (void)acc1;
+        const int q0 = s + 1;
+        const int qa = min(e, (q0 + 3) & ~3);
+        if (q0 + lane < qa) acc0 += (double)val[q0 + lane] * a[col[q0 + lane]];
+        // both chunks' value and position loads are issued before their gathers
+        for (int q = qa + 4 * lane; q + 3 < e; q += 256) {
+            const bool two = q + 131 < e;
+            const float4 w = *reinterpret_cast<const float4 *>(val + q);
+            const uint2 c = *reinterpret_cast<const uint2 *>(col + q);
+            float4 w2 = make_float4(0.f, 0.f, 0.f, 0.f);
+            uint2 cc = make_uint2(0u, 0u);
+            if (two) {
+                w2 = *reinterpret_cast<const float4 *>(val + q + 128);
+                cc = *reinterpret_cast<const uint2 *>(col + q + 128);
             }
-#pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                acc0 += (double)w[u] * a[c[u]];
-                if (NS == 2) acc1 += (double)w[u] * b[c[u]];
-            }
+            const double a0 = a[c.x & 0xffffu], a1 = a[c.x >> 16], a2 = a[c.y & 0xffffu], a3 = a[c.y >> 16];
+            const double a4 = a[cc.x & 0xffffu], a5 = a[cc.x >> 16], a6 = a[cc.y & 0xffffu],
+                         a7 = a[cc.y >> 16]; // position 0 when !two (w2 = 0)
+            acc0 += (double)w.x * a0;
+            acc0 += (double)w.y * a1;
+            acc0 += (double)w.z * a2;
+            acc0 += (double)w.w * a3;
+            acc0 += (double)w2.x * a4;
+            acc0 += (double)w2.y * a5;
+            acc0 += (double)w2.z * a6;
+            acc0 += (double)w2.w * a7;
         }
+        const int qt = qa + ((e - qa) & ~3);
+        if (qt + lane < e) acc0 += (double)val[qt + lane] * a[col[qt + lane]];
+    }
+};
+
+// lanes on consecutive entries, one (kTwo false) or two vectors
+template <bool kTwo>
+__device__ __forceinline__ void row_dot_coalesced(int s, int e, int lane, const float *__restrict__ val,
+                                                  const unsigned short *__restrict__ col,
+                                                  const double *__restrict__ a, const double *__restrict__ b,
+                                                  double &acc0, double &acc1)
+{
+    constexpr int kU = 8;
+    for (int q = s + 1 + lane; q < e; q += 32 * kU) {
+        float w[kU];
+        int c[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int qq = q + 32 * u;
+            const bool in = qq < e;
+            w[u] = in ? val[qq] : 0.0f; // position 0, weight 0 past the row
+            c[u] = in ? (int)col[qq] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            acc0 += (double)w[u] * a[c[u]];
+            if (kTwo) acc1 += (double)w[u] * b[c[u]];
+        }
+    }
+}
+
+template <>
+struct RowDot<float, unsigned short, 2> {
+    __device__ __forceinline__ static void run(int s, int e, int lane, const float *__restrict__ val,
+                                               const unsigned short *__restrict__ col, const double *__restrict__ a,
+                                               const double *__restrict__ b, double &acc0, double &acc1)
+    {
+        row_dot_coalesced<true>(s, e, lane, val, col, a, b, acc0, acc1);
+    }
+};
+
+// One active vector inside a kernel built for NS systems: the joint kernel
+// (NS = 2) keeps the coalesced form, whose registers it already holds.
+template <typename VT, typename IT, int NS>
+struct RowDot1 {
+    __device__ __forceinline__ static void run(int s, int e, int lane, const VT *__restrict__ val,
+                                               const IT *__restrict__ col, const double *__restrict__ a,
+                                               double &acc)
+    {
+        double unused = 0.0;
+        RowDot<VT, IT, 1>::run(s, e, lane, val, col, a, a, acc, unused);
+    }
+};
+
+template <>
+struct RowDot1<float, unsigned short, 2> {
+    __device__ __forceinline__ static void run(int s, int e, int lane, const float *__restrict__ val,
+                                               const unsigned short *__restrict__ col,
+                                               const double *__restrict__ a, double &acc)
+    {
+        double unused = 0.0;
+        row_dot_coalesced<false>(s, e, lane, val, col, a, a, acc, unused);
     }
 };
 
@@ -165,9 +240,9 @@ __device__ __forceinline__ void spmv_row(const FusedArgs &a, int row, int s, int
     if (NS == 2 && act0 && act1)
         RowDot<VT, IT, 2>::run(s, e, lane, val, col, vs0, vs1, acc0, acc1);
     else if (act0)
-        RowDot<VT, IT, 1>::run(s, e, lane, val, col, vs0, vs0, acc0, acc1);
+        RowDot1<VT, IT, NS>::run(s, e, lane, val, col, vs0, acc0);
     else if (NS == 2 && act1)
-        RowDot<VT, IT, 1>::run(s, e, lane, val, col, vs1, vs1, acc1, acc0);
+        RowDot1<VT, IT, NS>::run(s, e, lane, val, col, vs1, acc1);
     acc0 = warp_sum(acc0);
     if (NS == 2) acc1 = warp_sum(acc1);
     if (lane == 0) {

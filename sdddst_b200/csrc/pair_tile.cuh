@@ -108,9 +108,7 @@ __device__ __forceinline__ double min_image(double d)
 // Mixed-precision tiles.  Separations in FP64, rounded once to FP32: dx as
 // the minimum-image difference, sin(pi dy) as s_i c_j - c_i s_j from
 // per-dislocation s = sin(pi y), c = cos(pi y) (FP64, formed once per tile
-// and dislocation); e^{+-pi dx} as FP32 products of per-dislocation
-// e^{+-pi x} (formed once per tile and dislocation in FP64, rounded once)
-// and e^{-+pi} for a wrapped pair, so the field needs no exponential per pair.  Field terms in packed FP32 for two columns at a time
+// and dislocation).  Field terms in packed FP32 for two columns at a time
 // (tau_xy_f32x2, which returns tau2 = tau_xy / pi^2); row and column partials
 // summed in FP32 over 16 terms, then carried in FP64:
 //   row i:    sum_j (pi^2 b_j) tau2_ij,  times b_i at the end;
@@ -118,14 +116,12 @@ __device__ __forceinline__ double min_image(double d)
 // Interior tiles (I < J, full blocks) skip every validity test.
 template <int T, bool kChecked>
 __device__ __forceinline__ void f32_tile_body(const double *sx, const double *sy, const double *ssn,
-                                              const double *scs, const float *sbp, const float *sem,
-                                              const float *sep, const float *brow, double xi, double yi, double si,
-                                              double ci, float ei, float eim, int n, int j0, int tid, bool row_ok,
+                                              const double *scs, const float *sbp, const float *brow, double xi,
+                                              double yi, double si, double ci, int n, int j0, int tid, bool row_ok,
                                               bool diag, int i, float *tb, double *colsum_w, double &acc,
                                               unsigned long long *minr2, float r2_track, float s_track)
 {
     const int lane = tid & 31;
-    const double m52 = 6755399441055744.0; // 1.5 * 2^52: rint by an add and a subtract
     for (int c0 = 0; c0 < T; c0 += 32) {
         float2 racc = f2c(0.0f);
 #pragma unroll
@@ -134,17 +130,7 @@ __device__ __forceinline__ void f32_tile_body(const double *sx, const double *sy
             const double2 X = *reinterpret_cast<const double2 *>(sx + jj);
             const double2 S = *reinterpret_cast<const double2 *>(ssn + jj);
             const double2 C = *reinterpret_cast<const double2 *>(scs + jj);
-            const float2 EM = *reinterpret_cast<const float2 *>(sem + jj);
-            const float2 EP = *reinterpret_cast<const float2 *>(sep + jj);
-            // minimum image d - rint(d); e^{+-pi dx} = e^{+-pi x_i} e^{-+pi x_j} e^{-+pi rint(d)}
-            const double da = xi - X.x, db = xi - X.y;
-            const double ra = __dadd_rn(__dadd_rn(da, m52), -m52), rb = __dadd_rn(__dadd_rn(db, m52), -m52);
-            float2 dx = make_float2(__double2float_rn(da - ra), __double2float_rn(db - rb));
-            const float2 fsh = make_float2(ra > 0.0 ? kEmPiF : ra < 0.0 ? kEPiF : 1.0f,
-                                           rb > 0.0 ? kEmPiF : rb < 0.0 ? kEPiF : 1.0f);
-            const float2 fshi = make_float2(ra > 0.0 ? kEPiF : ra < 0.0 ? kEmPiF : 1.0f,
-                                            rb > 0.0 ? kEPiF : rb < 0.0 ? kEmPiF : 1.0f);
-            float2 ep = mul2(mul2(f2c(ei), EM), fsh), epi = mul2(mul2(f2c(eim), EP), fshi);
+            float2 dx = make_float2(__double2float_rn(min_image(xi - X.x)), __double2float_rn(min_image(xi - X.y)));
             float2 sn = make_float2(__double2float_rn(fma(si, C.x, -ci * S.x)),
                                     __double2float_rn(fma(si, C.y, -ci * S.y)));
             bool va = true, vb = true;
@@ -154,18 +140,14 @@ __device__ __forceinline__ void f32_tile_body(const double *sx, const double *sy
                 if (!va) {
                     dx.x = 0.25f;
                     sn.x = 0.70710678f;
-                    ep.x = kEQuarterPiF;
-                    epi.x = 1.0f / kEQuarterPiF;
                 }
                 if (!vb) {
                     dx.y = 0.25f;
                     sn.y = 0.70710678f;
-                    ep.y = kEQuarterPiF;
-                    epi.y = 1.0f / kEQuarterPiF;
                 }
             }
             float2 s;
-            float2 t = tau_xy_f32x2_e(dx, sn, ep, epi, s);
+            float2 t = tau_xy_f32x2(dx, sn, s);
             if (kChecked) {
                 t.x = va ? t.x : 0.0f;
                 t.y = vb ? t.y : 0.0f;
@@ -219,8 +201,6 @@ __device__ __forceinline__ void pair_tile_f32(const double *__restrict__ xw, con
     __shared__ __align__(16) double ssn[T];
     __shared__ __align__(16) double scs[T];
     __shared__ __align__(8) float sbp[T];
-    __shared__ __align__(8) float sem[T]; // e^{-pi x_j}
-    __shared__ __align__(8) float sep[T]; // e^{+pi x_j}
     __shared__ __align__(8) float brow[W][64];
     __shared__ __align__(8) float tbuf[W][16 * 66];
     __shared__ __align__(16) double colsum[W][T];
@@ -235,9 +215,6 @@ __device__ __forceinline__ void pair_tile_f32(const double *__restrict__ xw, con
         double sj, cj;
         sincospi(yj, &sj, &cj);
         sx[tid] = ok ? xw[j] : 0.0;
-        const double ex = exp(kPi * (ok ? xw[j] : 0.0));
-        sem[tid] = (float)(1.0 / ex);
-        sep[tid] = (float)ex;
         sy[tid] = yj;
         ssn[tid] = sj;
         scs[tid] = cj;
@@ -250,8 +227,6 @@ __device__ __forceinline__ void pair_tile_f32(const double *__restrict__ xw, con
     const double bi = row_ok ? b[i] : 0.0;
     double si, ci;
     sincospi(yi, &si, &ci);
-    const double exi = exp(kPi * xi);
-    const float ei = (float)exi, eim = (float)(1.0 / exi);
     brow[warp][2 * lane] = brow[warp][2 * lane + 1] = kPiSqF * (float)bi;
     const bool diag = (I == J);
     const bool checked = diag || (j0 + T > n) || (I * T + T > n);
@@ -262,11 +237,11 @@ __device__ __forceinline__ void pair_tile_f32(const double *__restrict__ xw, con
     __syncthreads();
     double acc = 0.0;
     if (checked)
-        f32_tile_body<T, true>(sx, sy, ssn, scs, sbp, sem, sep, brow[warp], xi, yi, si, ci, ei, eim, n, j0, tid,
-                               row_ok, diag, i, tbuf[warp], colsum[warp], acc, minr2, r2_track, s_track);
+        f32_tile_body<T, true>(sx, sy, ssn, scs, sbp, brow[warp], xi, yi, si, ci, n, j0, tid, row_ok, diag, i,
+                               tbuf[warp], colsum[warp], acc, minr2, r2_track, s_track);
     else
-        f32_tile_body<T, false>(sx, sy, ssn, scs, sbp, sem, sep, brow[warp], xi, yi, si, ci, ei, eim, n, j0, tid,
-                                row_ok, diag, i, tbuf[warp], colsum[warp], acc, minr2, r2_track, s_track);
+        f32_tile_body<T, false>(sx, sy, ssn, scs, sbp, brow[warp], xi, yi, si, ci, n, j0, tid, row_ok, diag, i,
+                                tbuf[warp], colsum[warp], acc, minr2, r2_track, s_track);
     __syncthreads();
     double ctot = 0.0;
 #pragma unroll
