@@ -344,6 +344,26 @@ int sdddst_set_preconditioner_weights(void *ctx, const unsigned short *bf16, lon
  * first slot).  Requires loaded weights; no counterpart in the reference. */
 int sdddst_learned_correction(void *ctx, double h, float *values, long cap, long *nnz);
 
+/* Training of the learned correction on the device (the network of
+ * sdddst_set_preconditioner_weights): hand-written forward and backward
+ * kernels, node products and weight gradients on the tensor cores (BF16
+ * operands, FP32 accumulation), Adam on FP32 master weights with global-norm
+ * clipping at 1; the BF16 weights the inference reads follow every step.
+ * The context should use SDDDST_SOLVER_GMRES_LEARNED (its cluster
+ * threshold is the one the correction is trained against).
+ *   init:    FP32 starting weights (count = the flat weight count);
+ *   step:    the Jacobian J(h) at the context's accepted configuration, its
+ *            cluster inverse B and `probes` (1..8) random sign probes Z from
+ *            `seed`: loss2[0] = ||Z - J B Z||^2 / ||Z||^2 (B alone),
+ *            loss2[1] = ||Z - J (B + C) Z||^2 / ||Z||^2 (the loss), both
+ *            before the update; with apply, one Adam step at rate lr; grad
+ *            (optional, count floats) the gradient of loss2[1];
+ *   weights: the FP32 master weights. */
+int sdddst_learned_train_init(void *ctx, const float *weights, long count);
+int sdddst_learned_train_step(void *ctx, double h, int probes, double lr, unsigned long long seed, int apply,
+                              double *loss2, float *grad);
+int sdddst_learned_train_weights(void *ctx, float *weights, long count);
+
 /* ---- Batches of independent systems (a population of random realisations).
  * `count` systems of sizes[k] dislocations, concatenated in xyb (sum of sizes
  * rows of {x, y, b}), share the parameters of `common` (n, p and the stress

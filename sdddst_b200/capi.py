@@ -42,6 +42,7 @@ EXPORTS = [
     "sdddst_direct_stats", "sdddst_profile_direct", "sdddst_precond_apply", "sdddst_set_preconditioner_weights",
     "sdddst_learned_correction", "sdddst_solver_recoveries", "sdddst_batch_stats",
     "sdddst_batch_profile_pair_sum", "sdddst_ev_hessian", "sdddst_ev_analyze", "sdddst_ev_timings",
+    "sdddst_learned_train_init", "sdddst_learned_train_step", "sdddst_learned_train_weights",
 ]
 
 
@@ -120,6 +121,11 @@ def load(path: str = LIB_PATH):
     lib.sdddst_ev_analyze.argtypes = [C.c_void_p, _D, C.c_double] + [C.c_void_p] * 6 + [C.c_int, C.c_void_p,
                                                                                         C.c_void_p, C.c_int]
     lib.sdddst_ev_timings.argtypes = [C.c_void_p, _D]
+    _F = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+    lib.sdddst_learned_train_init.argtypes = [C.c_void_p, _F, C.c_long]
+    lib.sdddst_learned_train_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_double, C.c_ulonglong, C.c_int,
+                                              _D, C.c_void_p]
+    lib.sdddst_learned_train_weights.argtypes = [C.c_void_p, _F, C.c_long]
     lib.sdddst_vector_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.sdddst_direct_stats.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long),
                                         C.POINTER(C.c_double), C.POINTER(C.c_long), C.POINTER(C.c_int),
@@ -316,6 +322,28 @@ class Engine:
         a, b, c = C.c_long(0), C.c_long(0), C.c_long(0)
         _check(self.lib.sdddst_solver_recoveries(self.h, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
+
+    def learned_train_init(self, weights_fp32):
+        """Starts training the learned correction from FP32 weights."""
+        w = np.ascontiguousarray(weights_fp32, dtype=np.float32)
+        _check(self.lib.sdddst_learned_train_init(self.h, w, w.size))
+
+    def learned_train_step(self, h, probes=8, lr=1e-3, seed=0, apply=True, grad=False):
+        """One training step on J(h) at the accepted configuration: returns
+        (loss of B alone, loss of B + C[, gradient])."""
+        from sdddst_b200.learned import weight_count
+        loss = np.zeros(2)
+        g = np.zeros(weight_count(), dtype=np.float32) if grad else None
+        _check(self.lib.sdddst_learned_train_step(self.h, float(h), int(probes), float(lr), int(seed) & (2**64 - 1),
+                                                  int(bool(apply)), loss,
+                                                  g.ctypes.data_as(C.c_void_p) if grad else None))
+        return (loss[0], loss[1], g) if grad else (loss[0], loss[1])
+
+    def learned_train_weights(self) -> np.ndarray:
+        from sdddst_b200.learned import weight_count
+        w = np.zeros(weight_count(), dtype=np.float32)
+        _check(self.lib.sdddst_learned_train_weights(self.h, w, w.size))
+        return w
 
     def ev_hessian(self, xyb) -> np.ndarray:
         """The dense Hessian of SpectralDecompositor::decompose (n x n)."""

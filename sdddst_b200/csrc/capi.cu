@@ -42,6 +42,14 @@ __global__ void copy_compare_kernel(int n, const double *__restrict__ src, doubl
 // device (the reference runs on with such values: a NaN velocity is accepted
 // as a step and spreads through the configuration).  Returns 0 or
 // SDDDST_ERR_NONFINITE with the first offending entry named.
+int check_finite_f(const float *a, long count, const char *what)
+{
+    for (long k = 0; k < count; ++k)
+        if (!std::isfinite(a[k]))
+            return fail(SDDDST_ERR_NONFINITE, std::string(what) + ": non-finite value at index " + std::to_string(k));
+    return 0;
+}
+
 int check_finite(const double *a, long count, const char *what)
 {
     for (long k = 0; k < count; ++k)
@@ -606,6 +614,36 @@ int sdddst_set_preconditioner_weights(void *ctx, const unsigned short *bf16, lon
     sd::Engine *e = E(ctx);
     cudaSetDevice(e->device);
     return from_engine(e, sd::learned_set_weights(*e, bf16, count));
+}
+
+int sdddst_learned_train_init(void *ctx, const float *weights, long count)
+{
+    if (!ctx || !weights) return fail(SDDDST_ERR_INVALID, "null argument");
+    if (int rc = check_finite_f(weights, count, "weights")) return rc;
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    return from_engine(e, sd::learned_train_init(*e, weights, count));
+}
+
+int sdddst_learned_train_step(void *ctx, double h, int probes, double lr, unsigned long long seed, int apply,
+                              double *loss2, float *grad)
+{
+    if (!ctx || !(h > 0) || !(lr >= 0)) return fail(SDDDST_ERR_INVALID, "bad argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    try {
+        return from_engine(e, sd::learned_train_step(*e, h, probes, lr, seed, apply != 0, loss2, grad));
+    } catch (const std::exception &ex) {
+        return fail(SDDDST_ERR_NOMEM, ex.what());
+    }
+}
+
+int sdddst_learned_train_weights(void *ctx, float *weights, long count)
+{
+    if (!ctx || !weights) return fail(SDDDST_ERR_INVALID, "null argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    return from_engine(e, sd::learned_train_weights(*e, weights, count));
 }
 
 int sdddst_learned_correction(void *ctx, double h, float *values, long cap, long *nnz)

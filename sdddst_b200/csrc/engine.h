@@ -268,6 +268,13 @@ void learned_invalidate(Engine &e);
 int learned_export(Engine &e, float *host, long cap);
 void learned_free(Engine &e);
 long learned_weight_count();
+int learned_ensure(Engine &e);
+// training of the learned correction on the device (learned_train.cu)
+int learned_train_init(Engine &e, const float *W0, long count);
+int learned_train_step(Engine &e, double h, int k, double lr, unsigned long long seed, bool apply, double *loss,
+                       float *grad);
+int learned_train_weights(Engine &e, float *W, long count);
+void learned_train_free(void *p);
 
 // eigenvalue analysis (ev.cu)
 int ev_hessian(Engine &e, const double *x);

@@ -170,6 +170,42 @@ def weight_count():
     return H * NODE_F + H + LAYERS * per_layer + H * H + H + H * H + H * EDGE_F + H + 1 + H + 1
 
 
+def init_weights(seed: int = 0) -> np.ndarray:
+    """Flat FP32 starting weights for the device trainer: every layer as
+    PyTorch's nn.Linear initialises it (weights and biases uniform in
+    +-1/sqrt(fan_in)), the output layers (w_o, b_o, w_d, b_d) at zero, so the
+    correction starts as the analytic first-order term."""
+    rng = np.random.default_rng(seed)
+    parts = []
+
+    def lin(out_f, in_f, bias=True):
+        b = 1.0 / np.sqrt(in_f)
+        parts.append(rng.uniform(-b, b, out_f * in_f))
+        if bias:
+            parts.append(rng.uniform(-b, b, out_f))
+
+    lin(H, NODE_F)
+    for _ in range(LAYERS):
+        lin(H, H)              # P, b_P
+        lin(H, H, bias=False)  # Q
+        lin(H, EDGE_F, False)  # R
+        lin(H, 2 * H)          # U, b_U
+    lin(H, H)                  # P_o, b_Po
+    lin(H, H, bias=False)      # Q_o
+    lin(H, EDGE_F, False)      # R_o
+    parts.append(np.zeros(H + 1))  # w_o, b_o
+    parts.append(np.zeros(H + 1))  # w_d, b_d
+    w = np.concatenate(parts).astype(np.float32)
+    assert w.size == weight_count()
+    return w
+
+
+def bf16_bits(w: np.ndarray) -> np.ndarray:
+    """FP32 -> BF16 bit patterns (uint16), round to nearest even."""
+    bits = np.ascontiguousarray(w, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    return ((bits + 0x7FFF + ((bits >> 16) & 1)) >> 16).astype(np.uint16)
+
+
 def pack_bf16(net) -> np.ndarray:
     """Flat BF16 bit patterns (uint16), round to nearest even."""
     flat = np.concatenate([t.detach().float().cpu().numpy().ravel() for t in weight_tensors(net)])

@@ -1,128 +1,125 @@
 """Trains the learned correction C of the cluster preconditioner (see
-sdddst_b200/learned.py) and writes sdddst_b200/learned_weights.npz.
+sdddst_b200/learned.py) on the device and writes
+sdddst_b200/learned_weights.npz.
 
-    python -m sdddst_b200.learned_train [--sizes 4096 8192] [--seeds 11 12]
-                                        [--attempts 16] [--probes 8] [--iters 2500]
+    python -m sdddst_b200.learned_train [--jacobians 20000] [--sizes 4096 8192 16384 32768]
+                                        [--probes 8] [--lr 1e-3] [--heldout 16]
 
-Data: for every accepted configuration of runs of the mixed-precision method
-(cutoff multiplier 2, precision 1e-5, zero stress; seeds other than the
-benchmark workload's), the Jacobians J(h) and J(h/2) of the next step's
-full and half steps, k random sign probes Z and the cluster preconditioner's
-B Z (sdddst_precond_apply).  Loss: the probe estimate of the right
-preconditioned residual, ||Z - J (B + C) Z||^2 / ||Z||^2.  The last run is
-held out for validation; the file records the held-out loss of B alone, of
-B plus the analytic first-order correction (c_ij = -1 across blocks) and of
-B plus the trained correction.
+Every training step is one call of sdddst_learned_train_step: the device
+assembles the Jacobian J(h) of the engine's accepted configuration, builds
+its cluster inverse B, draws sign probes Z, runs the network forward, the
+loss ||Z - J (B + C) Z||^2 / ||Z||^2 and its gradient with hand-written
+kernels (node products and weight gradients on the tensor cores, BF16
+operands, FP32 accumulation) and one Adam step on the FP32 master weights
+(global-norm clipping at 1, cosine-decayed learning rate).  No PyTorch.
+
+Data: the Jacobians the method itself generates.  Runs of the mixed
+learned-preconditioned method (cutoff multiplier 2, precision 1e-5, zero
+stress) at N taken in turn from --sizes with seeds other than the benchmark
+workload's; after every accepted step the network trains on J(h) and on
+J(h/2) of the next step's full and half steps, until --jacobians Jacobians
+have been used.  A held-out run (N = 8192, seed 12) provides --heldout
+states; the file records their loss with B alone, with the first-order
+correction (the starting network: zero output layers) and with the trained
+correction.
 """
 from __future__ import annotations
 
 import argparse
 import json
-import random
+import math
 import sys
 import time
 
 import numpy as np
 
 
-def generate(n, seed, attempts, k, device, log):
-    import torch
+def _engine(n, seed):
     from sdddst_b200 import capi, workloads
-    from sdddst_b200.learned import Graph
     xyb, _ = workloads.dislocations(n, seed)
-    eng = capi.Engine(capi.cli_params(n, 2.0, 1e-5, step_size=1e-6, pairsum=capi.PAIRSUM_FP32), xyb)
-    out = []
-    for a in range(attempts):
-        eng.step()
-        sc = eng.scalars()
-        h, cut = sc["step_size"], sc["cutoff"]
-        cfg = eng.config(0)
-        for hh in (h, 0.5 * h):
-            rp, col, val, d = eng.jacobian(hh, cfg)
-            Z = (torch.randint(0, 2, (k, n), device=device, dtype=torch.float64) * 2 - 1).contiguous()
-            BZ = torch.empty_like(Z)
-            blk = torch.empty(n, dtype=torch.int32, device=device)
-            torch.cuda.synchronize()
-            eng.precond_apply(hh, k, Z.data_ptr(), BZ.data_ptr(), blk.data_ptr())
-            g = Graph(rp, col, val, d, cfg[:, 0], cfg[:, 1], cut, blk.cpu().numpy(), device)
-            Zt, BZt = Z.T.contiguous(), BZ.T.contiguous()
-            out.append((g, Zt, Zt - g.apply_J(BZt)))
-    log(f"  N={n} seed={seed}: {len(out)} Jacobians, nnz/row {int(rp[-1]) / n:.0f}, final h {h:.3e}")
-    eng.close()
-    return out
+    return capi.Engine(capi.cli_params(n, 2.0, 1e-5, step_size=1e-6, pairsum=capi.PAIRSUM_FP32,
+                                       solver=capi.SOLVER_GMRES_LEARNED), xyb)
 
 
-def losses(net, samples):
-    import torch
-    lb = ln = lt = 0.0
-    with torch.no_grad():
-        for g, Z, R0 in samples:
-            zz = float((Z ** 2).sum())
-            lb += float((R0 ** 2).sum()) / zz
-            same = g.edge_f[:, 4].double()
-            ce = -(1.0 - same)
-            R1 = R0 - g.apply_J(g.apply_C(ce, torch.zeros(g.n, device=Z.device, dtype=torch.float64), Z))
-            ln += float((R1 ** 2).sum()) / zz
-            c_e, c_d = net(g)
-            R2 = R0 - g.apply_J(g.apply_C(c_e, c_d, Z))
-            lt += float((R2 ** 2).sum()) / zz
-    m = max(1, len(samples))
-    return lb / m, ln / m, lt / m
+def heldout_states(count, w0):
+    """(engine, [(configuration, step size), ...]) of a held-out run."""
+    e = _engine(8192, 12)
+    e.learned_train_init(w0)
+    states = []
+    while len(states) < count:
+        if e.step():
+            sc = e.scalars()
+            states.append((e.config(0), sc["step_size"]))
+    return e, states
+
+
+def evaluate(e, states, probes, weights):
+    """Mean held-out losses (B alone, B + C) for the given FP32 weights."""
+    e.learned_train_init(weights)
+    lb = lc = 0.0
+    for k, (cfg, h) in enumerate(states):
+        sc = e.scalars()
+        e.set_state(cfg, h, sc["sim_time"], sc["energy"], sc["strain"], False)
+        b, c = e.learned_train_step(h, probes=probes, lr=0.0, seed=10_000 + k, apply=False)
+        lb += b
+        lc += c
+    return lb / len(states), lc / len(states)
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--sizes", type=int, nargs="+", default=[4096, 8192])
-    ap.add_argument("--seeds", type=int, nargs="+", default=[11, 12])
-    ap.add_argument("--attempts", type=int, default=16)
+    ap.add_argument("--jacobians", type=int, default=20000)
+    ap.add_argument("--sizes", type=int, nargs="+", default=[4096, 8192, 16384, 32768])
     ap.add_argument("--probes", type=int, default=8)
-    ap.add_argument("--iters", type=int, default=2500)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--steps-per-run", type=int, default=400, help="accepted steps before the next run")
+    ap.add_argument("--heldout", type=int, default=16)
     ap.add_argument("--out", default=None)
     args = ap.parse_args(argv)
-    import torch
     from sdddst_b200 import build, learned
     build.build()
-    torch.manual_seed(0)
-    random.seed(0)
-    dev = "cuda"
     log = lambda s: print(s, flush=True)
     t0 = time.time()
-    runs = [(n, s) for n in args.sizes for s in args.seeds]
-    data = [generate(n, s, args.attempts, args.probes, dev, log) for n, s in runs]
-    train = [x for run in data[:-1] for x in run]
-    val = data[-1]
-    log(f"data: {len(train)} training, {len(val)} held-out Jacobians in {time.time() - t0:.0f} s")
-    net = learned.make_net().to(dev)
-    with torch.no_grad():  # start from the correction being zero: M = B
-        net.wo.weight.zero_()
-        net.wo.bias.zero_()
-        net.wd.weight.zero_()
-        net.wd.bias.zero_()
-    opt = torch.optim.Adam(net.parameters(), lr=args.lr)
-    sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, args.iters)
+    w0 = learned.init_weights(0)
+    ev, states = heldout_states(args.heldout, w0)
+    lb0, lf0 = evaluate(ev, states, args.probes, w0)
+    log(f"held-out: B {lb0:.4e}  B + first order {lf0:.4e}")
+    weights = w0
+    used = 0
+    run = 0
     hist = []
-    for it in range(args.iters):
-        g, Z, R0 = random.choice(train)
-        c_e, c_d = net(g)
-        R = R0 - g.apply_J(g.apply_C(c_e, c_d, Z))
-        loss = (R ** 2).sum() / (Z ** 2).sum()
-        opt.zero_grad()
-        loss.backward()
-        torch.nn.utils.clip_grad_norm_(net.parameters(), 1.0)
-        opt.step()
-        sched.step()
-        if it % 250 == 0 or it == args.iters - 1:
-            lb, ln, lt = losses(net, val)
-            hist.append({"iter": it, "train": float(loss), "val_B": lb, "val_B_neumann": ln, "val_learned": lt})
-            log(f"iter {it}: train {float(loss):.4e}  held-out: B {lb:.4e}  B+neumann {ln:.4e}  learned {lt:.4e}")
-    # the weights as the device will use them (BF16), evaluated once more
-    bf16 = learned.pack_bf16(net)
-    learned.unpack_into(net, bf16)
-    lb, ln, lt = losses(net, val)
-    meta = {"sizes": args.sizes, "seeds": args.seeds, "attempts": args.attempts, "probes": args.probes,
-            "iters": args.iters, "train_jacobians": len(train), "heldout_jacobians": len(val),
-            "heldout_loss": {"B": lb, "B_plus_first_order": ln, "B_plus_learned_bf16": lt},
+    sizes_used = {}
+    while used < args.jacobians:
+        n = args.sizes[run % len(args.sizes)]
+        seed = 100 + run
+        e = _engine(n, seed)
+        e.learned_train_init(weights)
+        # continue the optimiser state across runs: the moments restart, the
+        # schedule continues
+        accepted = 0
+        while accepted < args.steps_per_run and used < args.jacobians:
+            if not e.step():
+                continue
+            accepted += 1
+            h = e.scalars()["step_size"]
+            for hh in (h, 0.5 * h):
+                lr = args.lr * 0.5 * (1.0 + math.cos(math.pi * used / args.jacobians))
+                b, c = e.learned_train_step(hh, probes=args.probes, lr=lr, seed=used)
+                used += 1
+                sizes_used[n] = sizes_used.get(n, 0) + 1
+                if used % 1000 == 0:
+                    log(f"{used} Jacobians ({time.time() - t0:.0f} s): N={n} B {b:.3e}  B + C {c:.3e}")
+        weights = e.learned_train_weights()
+        e.close()
+        hb, hc = evaluate(ev, states, args.probes, weights)
+        hist.append({"jacobians": used, "heldout_B": hb, "heldout_learned": hc})
+        log(f"run {run} (N={n}) done: {used} Jacobians, held-out B + C {hc:.4e}")
+        run += 1
+    hb, hc = evaluate(ev, states, args.probes, weights)
+    bf16 = learned.bf16_bits(weights)
+    meta = {"trainer": "device (csrc/learned_train.cu)", "jacobians": used, "sizes": sizes_used,
+            "probes": args.probes, "lr": args.lr, "runs": run, "heldout_states": len(states),
+            "heldout_loss": {"B": lb0, "B_plus_first_order": lf0, "B_plus_learned_bf16": hc},
             "history": hist, "seconds": time.time() - t0}
     log(json.dumps(meta["heldout_loss"]))
     np.savez(args.out or learned.WEIGHTS_FILE, bf16=bf16, meta=np.array(json.dumps(meta)))
