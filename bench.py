@@ -409,6 +409,21 @@ def profile_target(args):
         import torch
         print(json.dumps({"target": "ev", **measure_ev(torch, 0, cpu=False, n=args.n, reps=args.reps)}))
         return
+    if args.only == "learned_train":
+        # device training steps of the learned correction on J(h) of the
+        # workload's configuration: `reps` timed steps after one
+        from sdddst_b200 import learned
+        eng, _ = make_engine(args.n, args.pairsum, 0, solver=capi.SOLVER_GMRES_LEARNED)
+        eng.learned_train_init(learned.init_weights(0))
+        eng.learned_train_step(1e-6, probes=8, lr=1e-3, seed=0)
+        t0 = time.perf_counter()
+        for r in range(args.reps):
+            lb, lc = eng.learned_train_step(1e-6, probes=8, lr=1e-3, seed=1 + r)
+        dt = (time.perf_counter() - t0) / max(1, args.reps)
+        print(json.dumps({"target": "learned_train", "n": args.n, "ms_per_step": dt * 1e3, "loss_B": lb,
+                          "loss_B_plus_C": lc}))
+        eng.close()
+        return
     if args.only == "learned":
         eng, _ = make_engine(args.n, args.pairsum, 0, solver=capi.SOLVER_GMRES_LEARNED)
         eng.set_preconditioner_weights()
@@ -609,7 +624,8 @@ def main():
     ap.add_argument("--n", type=int, default=N_FULL)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--only", default=None, choices=["pairsum", "step", "direct", "direct_mixed", "learned", "ev"],
+    ap.add_argument("--only", default=None,
+                    choices=["pairsum", "step", "direct", "direct_mixed", "learned", "learned_train", "ev"],
                     help="profiling target: launch only the pair-sum kernels (or only steps) and exit")
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-realisations measurement")
