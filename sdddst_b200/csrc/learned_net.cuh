@@ -131,42 +131,45 @@ __global__ void node_in_kernel(int n, const float *__restrict__ nf, const __nv_b
     hout[idx] = fmaxf(acc, 0.0f);
 }
 
-// per-edge pass, one warp per row: lane l holds channels l and l + 32.
+// per-edge pass, one warp per row, 8 rows per block of 256 threads: lane l
+// holds channels 2l and 2l + 1 (one 4-byte BF16 pair of qh_j per edge,
+// packed FP32 arithmetic); a chunk's 32 edges have their features formed one
+// per lane and staged in shared memory, every lane then reads them back
+// (two 16-byte broadcast loads per edge).
 // kOut = false: agg_i = mean_j relu(ph_i + qh_j + R e_ij);
 // kOut = true:  C_ij = (w_o . relu(ph_i + qh_j + R e_ij) + b_o) A_ij / (J_ii J_jj)
 template <typename VT, bool kOut>
-__global__ void edge_kernel(int n, double h, const int *__restrict__ rowptr, const int *__restrict__ col,
-                            const VT *__restrict__ val, const double *__restrict__ dvec,
-                            const double *__restrict__ jii, const double *__restrict__ x,
-                            const double *__restrict__ y, const int *__restrict__ blk, double cutoff,
-                            const float *__restrict__ ph, const __nv_bfloat16 *__restrict__ qh,
-                            const __nv_bfloat16 *__restrict__ w, long oR, long owo, long owob,
-                            float *__restrict__ agg, float *__restrict__ cval, float *__restrict__ craw)
+__global__ void __launch_bounds__(256)
+    edge_kernel(int n, double h, const int *__restrict__ rowptr, const int *__restrict__ col,
+                const VT *__restrict__ val, const double *__restrict__ dvec, const double *__restrict__ jii,
+                const double *__restrict__ x, const double *__restrict__ y, const int *__restrict__ blk,
+                double cutoff, const float *__restrict__ ph, const __nv_bfloat16 *__restrict__ qh,
+                const __nv_bfloat16 *__restrict__ w, long oR, long owo, long owob, float *__restrict__ agg,
+                float *__restrict__ cval, float *__restrict__ craw)
 {
+    __shared__ __align__(16) float sfeat[8][32][8]; // per warp: e0..e3 | e4, j (bits), -, -
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wib = (threadIdx.x >> 5) & 7;
     if (i >= n) return;
-    const int c0 = lane, c1 = lane + 32;
-    float r0[kEF], r1[kEF];
+    const int c0 = 2 * lane;
+    float2 rf[kEF];
 #pragma unroll
-    for (int f = 0; f < kEF; ++f) {
-        r0[f] = bf(w, oR + c0 * kEF + f);
-        r1[f] = bf(w, oR + c1 * kEF + f);
-    }
-    float wo0 = 0.0f, wo1 = 0.0f, bo = 0.0f;
+    for (int f = 0; f < kEF; ++f) rf[f] = make_float2(bf(w, oR + c0 * kEF + f), bf(w, oR + (c0 + 1) * kEF + f));
+    float2 wo = make_float2(0.0f, 0.0f);
+    float bo = 0.0f;
     if (kOut) {
-        wo0 = bf(w, owo + c0);
-        wo1 = bf(w, owo + c1);
+        wo = make_float2(bf(w, owo + c0), bf(w, owo + c0 + 1));
         bo = bf(w, owob);
     }
-    const float p0 = ph[(long)i * kH + c0], p1 = ph[(long)i * kH + c1];
+    const float2 pp = *reinterpret_cast<const float2 *>(ph + (long)i * kH + c0);
     const double di = (1.0 + dvec[i]) * 0.5 * h;
     const double ji = jii[i];
     const double xi = x[i], yi = y[i];
     const int bi = blk[i];
     const float inv_pos = (float)(1.0 / (kPosScale * cutoff));
-    float s0 = 0.0f, s1 = 0.0f;
+    float2 s = make_float2(0.0f, 0.0f);
     int cnt = 0;
+    float *my = &sfeat[wib][lane][0];
     const int qs = rowptr[i], qe = rowptr[i + 1];
     for (int q0 = qs; q0 < qe; q0 += 32) {
         const int q = q0 + lane;
@@ -191,33 +194,33 @@ __global__ void edge_kernel(int n, double h, const int *__restrict__ rowptr, con
             }
         }
         cnt += __popc(__ballot_sync(0xffffffffu, j >= 0));
+        *reinterpret_cast<float4 *>(my) = make_float4(e0, e1, e2, e3);
+        *reinterpret_cast<float4 *>(my + 4) = make_float4(e4, __int_as_float(j), 0.0f, 0.0f);
+        __syncwarp();
         // the chunk's 32 edges unrolled: independent gathers of qh_j; the
         // output pass leaves lane t's two-channel partial of edge t in v[t]
         float v[32];
 #pragma unroll
         for (int t = 0; t < 32; ++t) {
-            const int jt = __shfl_sync(0xffffffffu, j, t);
-            const float f0 = __shfl_sync(0xffffffffu, e0, t), f1 = __shfl_sync(0xffffffffu, e1, t);
-            const float f2 = __shfl_sync(0xffffffffu, e2, t), f3 = __shfl_sync(0xffffffffu, e3, t);
-            const float f4 = __shfl_sync(0xffffffffu, e4, t);
-            float a = 0.0f, b = 0.0f;
+            const float4 fa = *reinterpret_cast<const float4 *>(&sfeat[wib][t][0]);
+            const float4 fb = *reinterpret_cast<const float4 *>(&sfeat[wib][t][4]);
+            const int jt = __float_as_int(fb.y);
+            float2 a = make_float2(0.0f, 0.0f);
             if (jt >= 0) {
-                a = p0 + __bfloat162float(qh[(long)jt * kH + c0]);
-                b = p1 + __bfloat162float(qh[(long)jt * kH + c1]);
-                a = fmaf(r0[0], f0, a); a = fmaf(r0[1], f1, a); a = fmaf(r0[2], f2, a);
-                a = fmaf(r0[3], f3, a); a = fmaf(r0[4], f4, a);
-                b = fmaf(r1[0], f0, b); b = fmaf(r1[1], f1, b); b = fmaf(r1[2], f2, b);
-                b = fmaf(r1[3], f3, b); b = fmaf(r1[4], f4, b);
-                a = fmaxf(a, 0.0f);
-                b = fmaxf(b, 0.0f);
+                const __nv_bfloat162 qv = *reinterpret_cast<const __nv_bfloat162 *>(qh + (long)jt * kH + c0);
+                a = __fadd2_rn(pp, __bfloat1622float2(qv));
+                a = __ffma2_rn(rf[0], make_float2(fa.x, fa.x), a);
+                a = __ffma2_rn(rf[1], make_float2(fa.y, fa.y), a);
+                a = __ffma2_rn(rf[2], make_float2(fa.z, fa.z), a);
+                a = __ffma2_rn(rf[3], make_float2(fa.w, fa.w), a);
+                a = __ffma2_rn(rf[4], make_float2(fb.x, fb.x), a);
+                a.x = fmaxf(a.x, 0.0f);
+                a.y = fmaxf(a.y, 0.0f);
             }
-            if (kOut) {
-                v[t] = fmaf(wo0, a, wo1 * b);
-            } else {
-                s0 += a;
-                s1 += b;
-            }
+            if (kOut) v[t] = fmaf(wo.x, a.x, wo.y * a.y);
+            else s = __fadd2_rn(s, a);
         }
+        __syncwarp(); // the next chunk overwrites the staged features
         if (kOut) {
             // reduce-scatter over the warp: afterwards lane l holds the sum
             // over all lanes of v[l] in v[0] (31 shuffles for 32 edges)
@@ -240,8 +243,7 @@ __global__ void edge_kernel(int n, double h, const int *__restrict__ rowptr, con
     }
     if (!kOut) {
         const float inv = 1.0f / (float)max(cnt, 1);
-        agg[(long)i * kH + c0] = s0 * inv;
-        agg[(long)i * kH + c1] = s1 * inv;
+        *reinterpret_cast<float2 *>(agg + (long)i * kH + c0) = make_float2(s.x * inv, s.y * inv);
     }
 }
 

@@ -10,7 +10,8 @@
 //     M = diag(c)^-1 J (M_ii = 1/c_i + h G_ii, M_ij = h G_ij);
 //   * every dislocation points to its strongest neighbour with s >= theta;
 //     following pointers never decreases s, so each chain ends in a mutual
-//     pair, whose smaller index roots the cluster (pointer jumping);
+//     pair, whose smaller index roots the cluster (one bounded walk per
+//     dislocation);
 //   * clusters are listed contiguously, members in ascending index order,
 //     and cut into blocks of at most kMaxBlock;
 //   * one warp per block builds the dense block of J, inverts it by
@@ -92,30 +93,31 @@ __global__ void msorted_kernel(int n, double h, const int *__restrict__ sorted, 
     msrt[k] = m != 0.0 ? (VT)(1.0 / fabs(m)) : (VT)0;
 }
 
-__global__ void root_init_kernel(int n, const int *__restrict__ ptr, int *__restrict__ parent)
+// Cluster root of every dislocation in one pass: a dislocation that points
+// to itself, or the smaller index of a mutual pair, is a root; every other
+// one follows the pointers for at most kRootWalk steps and takes the root it
+// reaches, or becomes its own root when none is reached within them (a chain
+// longer than that, or a tie cycle).  Roots count their members.
+constexpr int kRootWalk = 4096;
+
+__device__ __forceinline__ bool is_root(const int *__restrict__ ptr, int i, int p)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int p = ptr[i];
-    if (p == i || (ptr[p] == i && i < p)) parent[i] = i;
-    else parent[i] = p;
+    return p == i || (ptr[p] == i && i < p);
 }
 
-__global__ void jump_kernel(int n, const int *__restrict__ in, int *__restrict__ out)
+__global__ void root_walk_kernel(int n, const int *__restrict__ ptr, int *__restrict__ root, int *__restrict__ count)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = in[in[i]];
-}
-
-// After jumping, a node whose parent is not a root (a chain longer than the
-// jumps covered, or a tie cycle) becomes its own root.
-__global__ void root_fix_kernel(int n, int *__restrict__ parent, int *__restrict__ count)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    int r = parent[i];
-    if (parent[r] != r) r = i;
-    parent[i] = r;
+    int r = i, p = ptr[i];
+    int steps = 0;
+    while (!is_root(ptr, r, p) && steps < kRootWalk) {
+        r = p;
+        p = ptr[r];
+        ++steps;
+    }
+    if (!is_root(ptr, r, p)) r = i;
+    root[i] = r;
     atomicAdd(&count[r], 1);
 }
 
@@ -306,7 +308,7 @@ int precond_build(Engine &e, Cluster &c, double h, const double *dvec, bool chec
     cudaStream_t st = e.st;
     const unsigned nb256 = (unsigned)((n + 255) / 256);
     const double theta = cluster_theta(e);
-    int *ptr = c.ptr, *par = c.parent, *par2 = c.tmp;
+    int *ptr = c.ptr, *par = c.parent;
     // single system: M_jj in the cell-sorted order (the SpMV's staging buffer,
     // free until the solve), read through the CSR's sorted column positions
     const bool srt = e.col_s_valid && !e.d_hrow;
@@ -322,19 +324,14 @@ int precond_build(Engine &e, Cluster &c, double h, const double *dvec, bool chec
                                                               e.d_gdiag, dvec, ptr, e.d_col_s, msrt, e.spmv_sorted);
     }
     if (srt) e.launches++;
-    root_init_kernel<<<nb256, 256, 0, st>>>(n, ptr, par);
-    for (int it = 0; it < 12; ++it) {
-        jump_kernel<<<nb256, 256, 0, st>>>(n, par, par2);
-        std::swap(par, par2);
-    }
     cudaMemsetAsync(c.count, 0, sizeof(int) * (n + 1), st);
     cudaMemsetAsync(c.fill, 0, sizeof(int) * (n + 1), st);
-    root_fix_kernel<<<nb256, 256, 0, st>>>(n, par, c.count);
+    root_walk_kernel<<<nb256, 256, 0, st>>>(n, ptr, par, c.count);
     e.launches += launch_scan(e, c.count, n, c.start, st) - 1;
     member_scatter_kernel<<<nb256, 256, 0, st>>>(n, par, c.start, c.fill, c.tmp2);
     cluster_sort_kernel<<<nb256, 256, 0, st>>>(n, c.count, c.start, c.tmp2, c.members, c.nblk);
     e.launches += launch_scan(e, c.nblk, n, c.bbase, st) - 1;
-    e.launches += 19;
+    e.launches += 6;
     // the block count stays on the device (pc_bbase[n]); the block kernels
     // run over n (an upper bound) and return beyond it, and the inverses'
     // storage is sized for the bound sum k^2 <= kMaxBlock n once

@@ -72,26 +72,51 @@ __global__ void wrap_kernel(int n, const double *__restrict__ x, double *__restr
 
 // Per-dislocation finish: sum of the nblk partials in fixed order, point
 // defects (simulation.cpp:111-128), S = pair + defect sum, v = S + b tau_ext
-// (simulation.cpp:129), and the tolerance update from min r^2.
-__global__ void speeds_finish_kernel(int n, int nblk, const double *__restrict__ part, const double *__restrict__ x,
-                                     const double *__restrict__ y, const double *__restrict__ b, int p,
-                                     const double *__restrict__ pdx, const double *__restrict__ pdy, double A,
-                                     double K, double tau_ext, double *__restrict__ S, double *__restrict__ v,
-                                     const unsigned long long *__restrict__ minr2, double *__restrict__ tol,
-                                     double prec_sqr, int update_tol, double *__restrict__ minr2_out)
+// (simulation.cpp:129), and the tolerance update from min r^2.  A block of
+// kFinishGroups warps serves 32 dislocations: warp g sums the g-th quarter of
+// the partials (lanes on consecutive dislocations: each load is one 256-byte
+// row segment, sixteen in flight per warp), and the quarters are combined in
+// order by warp 0.
+constexpr int kFinishGroups = 4;
+
+__device__ __forceinline__ void neumaier_add(double &acc, double &comp, double v)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    // compensated (Neumaier) FP64 sum of the per-tile partials, in a fixed
-    // order: the tile partials themselves are FP64 sums of at most one
-    // tile's pairs, so the long reduction is this one
+    const double t = acc + v;
+    comp += fabs(acc) >= fabs(v) ? (acc - t) + v : (v - t) + acc;
+    acc = t;
+}
+
+__global__ void __launch_bounds__(32 * kFinishGroups)
+    speeds_finish_kernel(int n, int nblk, const double *__restrict__ part, const double *__restrict__ x,
+                         const double *__restrict__ y, const double *__restrict__ b, int p,
+                         const double *__restrict__ pdx, const double *__restrict__ pdy, double A, double K,
+                         double tau_ext, double *__restrict__ S, double *__restrict__ v,
+                         const unsigned long long *__restrict__ minr2, double *__restrict__ tol, double prec_sqr,
+                         int update_tol, double *__restrict__ minr2_out)
+{
+    __shared__ double sacc[kFinishGroups][32], scomp[kFinishGroups][32];
+    const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+    const int i = blockIdx.x * 32 + lane;
+    // compensated (Neumaier) FP64 sums of the per-tile partials: the tile
+    // partials themselves are FP64 sums of at most one tile's pairs, so the
+    // long reduction is this one
+    const int per = (nblk + kFinishGroups - 1) / kFinishGroups;
+    const int L0 = g * per, L1 = min(nblk, L0 + per);
     double acc = 0.0, comp = 0.0;
+    if (i < n) {
 #pragma unroll 16
-    for (int L = 0; L < nblk; ++L) { // unrolled: sixteen loads in flight per round trip
-        const double v = part[(size_t)L * n + i];
-        const double t = acc + v;
-        comp += fabs(acc) >= fabs(v) ? (acc - t) + v : (v - t) + acc;
-        acc = t;
+        for (int L = L0; L < L1; ++L) neumaier_add(acc, comp, part[(size_t)L * n + i]);
+    }
+    sacc[g][lane] = acc;
+    scomp[g][lane] = comp;
+    __syncthreads();
+    if (g != 0 || i >= n) return;
+    acc = 0.0;
+    comp = 0.0;
+#pragma unroll
+    for (int k = 0; k < kFinishGroups; ++k) {
+        neumaier_add(acc, comp, sacc[k][lane]);
+        comp += scomp[k][lane];
     }
     acc += comp;
     double smin = update_tol ? __longlong_as_double((long long)minr2[i]) : 0.0;
@@ -100,8 +125,8 @@ __global__ void speeds_finish_kernel(int n, int nblk, const double *__restrict__
         double dx = wrap_half(xi - pdx[q]);
         double dy = wrap_half(yi - pdy[q]);
         double s;
-        double g = pd_force_f64(dx, dy, A, K, &s);
-        acc -= g * bi;
+        const double f = pd_force_f64(dx, dy, A, K, &s);
+        acc -= f * bi;
         if (s < smin) smin = s;
     }
     if (S) S[i] = acc;
@@ -166,7 +191,7 @@ void launch_speeds_finish(const Engine &e, const double *x, double tau_ext, doub
     const int n = e.n;
     const int T = pair_tile_size(n);
     const int nblk = (n + T - 1) / T;
-    speeds_finish_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, nblk, e.d_part, x, e.d_y, e.d_b, e.p, e.d_pdx, e.d_pdy,
+    speeds_finish_kernel<<<(n + 31) / 32, 32 * kFinishGroups, 0, st>>>(n, nblk, e.d_part, x, e.d_y, e.d_b, e.p, e.d_pdx, e.d_pdy,
                                                          e.A, e.KASQR, tau_ext, S, v, e.d_minr2, e.d_tol,
                                                          e.prec * e.prec, update_tol, e.d_minr2_out);
 }
@@ -189,7 +214,7 @@ void launch_speeds_raw(int n, const double *x, const double *y, const double *b,
         pair_tiles_kernel<128, 0><<<(unsigned)tiles, 128, 0, st>>>(x, y, b, n, nblk, part, nullptr, 0.0);
     else
         pair_tiles_kernel<64, 0><<<(unsigned)tiles, 64, 0, st>>>(x, y, b, n, nblk, part, nullptr, 0.0);
-    speeds_finish_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, nblk, part, x, y, b, 0, nullptr, nullptr, 0.0, 0.0,
+    speeds_finish_kernel<<<(n + 31) / 32, 32 * kFinishGroups, 0, st>>>(n, nblk, part, x, y, b, 0, nullptr, nullptr, 0.0, 0.0,
                                                          tau_ext, nullptr, v, nullptr, nullptr, 0.0, 0, nullptr);
 }
 
