@@ -551,6 +551,31 @@ int sdddst_profile_pair_sum(void *ctx, int reps, double *ms_per_launch)
     return from_engine(e, rc);
 }
 
+// Internal check of the exclusive scan the assembly and the preconditioner
+// build use (not part of the public header): out[0..m] from in[0..m-1], both
+// device pointers, on the context's stream, with scratch sized for m.
+int sdddst_internal_scan(void *ctx, const int *in, int m, int *out)
+{
+    if (!ctx || !in || !out || m < 1) return fail(SDDDST_ERR_INVALID, "bad argument");
+    sd::Engine *e = E(ctx);
+    cudaSetDevice(e->device);
+    int *saved = e->d_scan_tmp;
+    const int saved_cap = e->scan_tmp_cap;
+    const int need = 2 * ((m + 2047) / 2048) + 2;
+    int *tmp = nullptr;
+    if (need > saved_cap) {
+        if (cudaMalloc(&tmp, sizeof(int) * need) != cudaSuccess) return fail(SDDDST_ERR_NOMEM, "scan scratch");
+        e->d_scan_tmp = tmp;
+        e->scan_tmp_cap = need;
+    }
+    e->launches += sd::launch_scan(*e, in, m, out, e->st);
+    const int rc = e->sync_check("scan");
+    e->d_scan_tmp = saved;
+    e->scan_tmp_cap = saved_cap;
+    if (tmp) cudaFree(tmp);
+    return from_engine(e, rc);
+}
+
 int sdddst_profile_direct(void *ctx, double h, int reps, double *factor_ms, double *solve_ms)
 {
     if (!ctx || !factor_ms || !solve_ms || reps < 1 || !(h > 0)) return fail(SDDDST_ERR_INVALID, "bad argument");

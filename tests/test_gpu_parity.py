@@ -412,6 +412,30 @@ def test_jacobian_multiblock_scan_n20001(engine_lib, port_lib):
     assert np.linalg.norm(J @ x - rhs) <= 1e-12 * np.linalg.norm(rhs)
 
 
+@pytest.mark.parametrize("m", [1000, 2048, 2049, 16385, 20001, 131072, 131073, 300001])
+def test_scan_routes_match_cumsum(engine_lib, m):
+    """The exclusive scan behind the CSR row pointers and the preconditioner's
+    offsets, on each of its routes (one block up to 2048 entries, one launch
+    of self-offsetting chunks up to 64 x 2048, three launches above), against
+    numpy's cumulative sum."""
+    import ctypes as C
+    import torch
+    from sdddst_b200 import capi
+    xyb, _ = workloads.dislocations(256, 0)
+    e = capi.Engine(capi.cli_params(256, 0.5, 1e-6), xyb)
+    vals = np.random.default_rng(m).integers(0, 700, m).astype(np.int32)
+    src = torch.tensor(vals, device="cuda")
+    dst = torch.full((m + 1,), -7, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    fn = e.lib.sdddst_internal_scan
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    fn.restype = C.c_int
+    assert fn(e.h, src.data_ptr(), m, dst.data_ptr()) == 0
+    want = np.concatenate([[0], np.cumsum(vals, dtype=np.int64)])
+    assert np.array_equal(dst.cpu().numpy().astype(np.int64), want)
+    e.close()
+
+
 def test_solve_with_restarts_matches_dense(engine_lib, port_lib):
     """The device-resident GMRES with a restart length of 4 (several restart
     cycles: the true residual recomputed, the basis rebuilt) against a dense
