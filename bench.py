@@ -416,17 +416,18 @@ def profile_target(args):
         return
     if args.only == "learned_train":
         # device training steps of the learned correction on J(h) of the
-        # workload's configuration: `reps` timed steps after one
+        # workload's configuration at a step size of its settled window
+        # (h = 1e-9): `reps` timed steps (each waits for its losses) after one
         from sdddst_b200 import learned
         eng, _ = make_engine(args.n, args.pairsum, 0, solver=capi.SOLVER_GMRES_LEARNED)
         eng.learned_train_init(learned.init_weights(0))
-        eng.learned_train_step(1e-6, probes=8, lr=1e-3, seed=0)
+        lb, lc = eng.learned_train_step(1e-9, probes=8, lr=1e-5, seed=0)
         t0 = time.perf_counter()
         for r in range(args.reps):
-            lb, lc = eng.learned_train_step(1e-6, probes=8, lr=1e-3, seed=1 + r)
+            eng.learned_train_step(1e-9, probes=8, lr=1e-5, seed=1 + r)
         dt = (time.perf_counter() - t0) / max(1, args.reps)
-        print(json.dumps({"target": "learned_train", "n": args.n, "ms_per_step": dt * 1e3, "loss_B": lb,
-                          "loss_B_plus_C": lc}))
+        print(json.dumps({"target": "learned_train", "n": args.n, "ms_per_step": dt * 1e3, "h": 1e-9,
+                          "loss_B": lb, "loss_B_plus_first_order": lc}))
         eng.close()
         return
     if args.only == "learned":

@@ -356,8 +356,9 @@ int sdddst_learned_correction(void *ctx, double h, float *values, long cap, long
  *            cluster inverse B and `probes` (1..8) random sign probes Z from
  *            `seed`: loss2[0] = ||Z - J B Z||^2 / ||Z||^2 (B alone),
  *            loss2[1] = ||Z - J (B + C) Z||^2 / ||Z||^2 (the loss), both
- *            before the update; with apply, one Adam step at rate lr; grad
- *            (optional, count floats) the gradient of loss2[1];
+ *            before the update; with apply, one Adam step at rate lr on
+ *            the ratio loss2[1] / loss2[0] (scale-free across step sizes);
+ *            grad (optional, count floats) the gradient of that ratio;
  *   weights: the FP32 master weights. */
 int sdddst_learned_train_init(void *ctx, const float *weights, long count);
 int sdddst_learned_train_step(void *ctx, double h, int probes, double lr, unsigned long long seed, int apply,

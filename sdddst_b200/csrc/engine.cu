@@ -38,8 +38,7 @@ Engine::~Engine()
                     d_g, d_sol, d_dvec, d_tol, d_tol_last, d_minr2, d_part, d_pdx, d_pdy, d_cell,
                     d_cell_count, d_cell_start, d_cell_fill, d_sorted, d_rowcnt, d_rowptr, d_col, d_val,
                     d_V, d_w, d_z, d_r, d_hcol, d_partials, d_gs_partials, d_scal, d_y_small, d_ys, d_bs, d_flag, d_xw,
-                    d_gdiag, d_valf, d_col_s, d_col_s16, d_vsort, d_xsrt, d_ysrt, d_bsrt, d_scan_tmp,
-                    d_fmask, d_fpre, d_segtab, d_fmode};
+                    d_gdiag, d_valf, d_col_s, d_col_s16, d_vsort, d_xsrt, d_ysrt, d_bsrt, d_scan_tmp};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (h_scal) cudaFreeHost(h_scal);
@@ -181,7 +180,6 @@ int Engine::init(const sdddst_params &p_, const double *xyb, const double *pd)
     scan_tmp_cap = 2 * ((n + 2047) / 2048) + 2;
     rc |= dalloc(&d_scan_tmp, scan_tmp_cap);
     rc |= dalloc(&d_flag, 4);
-    rc |= dalloc(&d_fmode, 1);
     rc |= dalloc(&d_V, (size_t)(restart + 1) * n);
     rc |= dalloc(&d_hcol, 2 * (restart + 1) + 4);
     rc |= dalloc(&d_partials, (size_t)red_blocks * 32 + 64);

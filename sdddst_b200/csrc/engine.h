@@ -74,11 +74,6 @@ struct Engine {
     double *d_hrow = nullptr;  // per-row step size of a batch of systems (null: one system, scalar h)
     long nnz_cap = 0, nnz = 0;
     int *d_flag = nullptr; // device-side error flag of the assembly
-    // the count pass's kept-candidate masks for the fill (jacobian.cu, FillAux)
-    unsigned *d_fmask = nullptr;
-    unsigned short *d_fpre = nullptr;
-    int *d_segtab = nullptr, *d_fmode = nullptr;
-    long segtab_cap = 0;
     bool assembled_valid = false;
     const double *assembled_for = nullptr;
 

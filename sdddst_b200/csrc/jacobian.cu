@@ -274,23 +274,6 @@ struct CellScan {
     float kb_f, ka_f;              // the same from FP32 copies of the positions, with a wider margin
 };
 
-// What the count pass leaves for the fill (single system, 3x3 blocks staged):
-// bit t of mask[r * kMaskWords + t / 32] tells whether candidate t of the
-// 3x3 block of cell-sorted row r is in the row's pattern, pre[] holds the
-// number of pattern entries before each word, segtab[cell * 10 + s] the
-// offset of the block's s-th cell (s = 9: the block's size), and *mode is
-// 0 when every block was staged (the fill then evaluates each unordered pair
-// once and writes it to both rows).
-constexpr int kMaskWords = 128;
-
-struct FillAux {
-    unsigned *mask;
-    unsigned short *pre;
-    int *segtab;
-    const int *cell; // cell of each dislocation (index order)
-    int *mode;
-};
-
 // Minimum-image difference in FP32 for positions already wrapped into
 // [-0.5, 0.5): d - rint(d) with rint as the add/subtract of 1.5 * 2^23.
 __device__ __forceinline__ float wrap_diff_f32(float d)
@@ -510,96 +493,6 @@ __device__ void row_values(int i, double xi, double yi, double bi, const CellSca
     }
 }
 
-// Slot in row r's CSR of staged candidate t of its block (t = ncand: the row's end).
-__device__ __forceinline__ int mask_slot(const FillAux &aux, long mrow, int t, int ncand, int base, int rowend)
-{
-    if (t >= ncand) return rowend;
-    const long w = mrow + (t >> 5);
-    return base + 1 + aux.pre[w] + __popc(aux.mask[w] & ((1u << (t & 31)) - 1u));
-}
-
-// Slot u of the owned runs (start st[s], length ln[s], s = 0..8, in order).
-__device__ __forceinline__ int owned_slot(int u, const int (&st)[9], const int (&ln)[9])
-{
-    int q = -1;
-#pragma unroll
-    for (int s = 0; s < 9; ++s) {
-        if (q < 0 && u < ln[s]) q = st[s] + u;
-        if (q < 0) u -= ln[s];
-    }
-    return q;
-}
-
-// FP32 values of row i's owned entries (columns later in the cell-sorted
-// order: the tail of the row's own cell and the whole neighbour cells of
-// larger index), each written to its own slot and to the mirror slot in the
-// column's row, which the mask of that row locates: candidate position of
-// row i in the column's block (the block's offset of row i's cell + row i's
-// offset in its cell), then the entries before it.  G_ij is the same number
-// from either row (dx = x[max] - x[min]; b_i b_j), so both rows read what
-// each would have computed.  Two entries per lane through the packed field.
-__device__ void row_values_owned(int i, double xi, double yi, double bi, int cx, int cy, int roff, int G,
-                                 const CellScan &cs, const FillAux &aux, double c, double c2, const int (&st)[9],
-                                 const int (&ln)[9], int total, const int *__restrict__ rowptr,
-                                 const int *__restrict__ col, const int *__restrict__ col_s, float *__restrict__ val,
-                                 const double *__restrict__ bs, long cap, int *__restrict__ flag, double ic2, int lane)
-{
-    for (int u0 = 0; u0 < total; u0 += 64) {
-        int qs[2];
-        qs[0] = u0 + lane < total ? owned_slot(u0 + lane, st, ln) : -1;
-        qs[1] = u0 + lane + 32 < total ? owned_slot(u0 + lane + 32, st, ln) : -1;
-        double dxs[2], dys[2], ws[2], bss[2];
-        int js[2], kss[2];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            js[u] = kss[u] = -1;
-            if (qs[u] < 0) { // a stand-in pair, never stored
-                dxs[u] = dys[u] = 0.25;
-                ws[u] = bss[u] = 0.0;
-                continue;
-            }
-            const int j = col[qs[u]], ks = col_s[qs[u]];
-            js[u] = j;
-            kss[u] = ks;
-            const double xj = cs.xs[ks], yj = cs.ys[ks];
-            dxs[u] = wrap_diff_f64(i < j ? xj - xi : xi - xj); // x[hi] - x[lo]
-            dys[u] = wrap_diff_f64(i < j ? yj - yi : yi - yj);
-            const double r2 = r2_exact(dxs[u], dys[u]);
-            float wf = 1.0f;
-            if (r2 > c2) {
-                const float t = sqrtf((float)r2) - (float)c;
-                wf = __expf(-(t * t) * (float)ic2);
-            }
-            ws[u] = (double)wf;
-            bss[u] = bs[ks];
-        }
-        const float2 t = tau_xy_dx_f32x2(make_float2(__double2float_rn(dxs[0]), __double2float_rn(dxs[1])),
-                                         make_float2(__double2float_rn(dys[0]), __double2float_rn(dys[1])));
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            if (qs[u] < 0) continue;
-            const float v = (float)(bi * bss[u] * (double)(u ? t.y : t.x) * ws[u]);
-            val[qs[u]] = v;
-            const int j = js[u];
-            const int cj = aux.cell[j];
-            int ox = cx - cj % G, oy = cy - cj / G; // row i's cell seen from the column's cell
-            ox = ox > 1 ? ox - G : (ox < -1 ? ox + G : ox);
-            oy = oy > 1 ? oy - G : (oy < -1 ? oy + G : oy);
-            bool ok = ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1;
-            const int ti = ok ? aux.segtab[cj * 10 + (oy + 1) * 3 + (ox + 1)] + roff : -1;
-            ok = ok && ti >= 0 && ti < 32 * kMaskWords;
-            if (ok) {
-                const long mw = (long)kss[u] * kMaskWords + (ti >> 5);
-                const int qm = rowptr[j] + 1 + aux.pre[mw] + __popc(aux.mask[mw] & ((1u << (ti & 31)) - 1u));
-                const int je = rowptr[j + 1];
-                ok = qm < je && (long)je <= cap;
-                if (ok) val[qm] = v;
-            }
-            if (!ok) atomicExch(flag, 1); // not the symmetric pattern the count pass saw
-        }
-    }
-}
-
 // Count (kFill = false) or fill (kFill = true) pass over the rows of one
 // cell.  Block (cell, part) stages the cell's 3x3 neighbour block (FP32
 // copies of the wrapped positions and the indices of up to kCandCap
@@ -615,7 +508,6 @@ __device__ void row_values_owned(int i, double xi, double yi, double bi, int cx,
 // the FP64 test instead.  Both routes visit candidates in the same order and
 // make the same decisions, so the CSR is the same either way.
 constexpr int kCandCap = 4096;
-static_assert(kCandCap == 32 * kMaskWords, "one mask bit per staged candidate");
 constexpr int kCellThreads = 256;
 constexpr size_t kCellSmem = (size_t)kCandCap * (2 * sizeof(float) + sizeof(int));
 
@@ -643,13 +535,12 @@ __device__ __forceinline__ bool staged_kept(int i, double xi, double yi, float x
 }
 
 template <bool kFill, typename VT>
-__global__ void __launch_bounds__(kCellThreads, sizeof(VT) == sizeof(float) ? 4 : 1) cell_rows_kernel(
+__global__ void __launch_bounds__(kCellThreads) cell_rows_kernel(
     int parts, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ b, CellScan cs,
     double c, double c2, double ic2, int *__restrict__ rowcnt, const int *__restrict__ rowptr, int *__restrict__ col,
     VT *__restrict__ val, double *__restrict__ gdiag, int p, const double *__restrict__ pdx,
     const double *__restrict__ pdy, double A, double K, int *__restrict__ flag, const double *__restrict__ tab_dx,
-    int *__restrict__ col_s, unsigned short *__restrict__ col_s16, const double *__restrict__ bs, long cap,
-    FillAux aux)
+    int *__restrict__ col_s, unsigned short *__restrict__ col_s16, const double *__restrict__ bs, long cap)
 {
     extern __shared__ __align__(16) unsigned char cell_smem[];
     float *sxc = reinterpret_cast<float *>(cell_smem);
@@ -659,7 +550,6 @@ __global__ void __launch_bounds__(kCellThreads, sizeof(VT) == sizeof(float) ? 4 
 
     const int G = cs.G;
     const int cell = blockIdx.x / parts, part = blockIdx.x % parts;
-    const int cx = cell % G, cy = cell / G;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int r0 = cs.start[cell], r1 = cs.start[cell + 1];
     const int chunk = (r1 - r0 + parts - 1) / parts;
@@ -670,6 +560,7 @@ __global__ void __launch_bounds__(kCellThreads, sizeof(VT) == sizeof(float) ? 4 
     int ncand = 0;
     if (G >= 3) {
         if (threadIdx.x == 0) {
+            const int cx = cell % G, cy = cell / G;
             int nseg = 0, off = 0;
             for_neighbour_cells(cx, cy, G, [&](int nc) {
                 seg_start[nseg] = cs.start[nc];
@@ -682,7 +573,6 @@ __global__ void __launch_bounds__(kCellThreads, sizeof(VT) == sizeof(float) ? 4 
         __syncthreads();
         ncand = seg_off[9];
         staged = ncand <= kCandCap;
-        if (!kFill && aux.segtab && part == 0 && threadIdx.x < 10) aux.segtab[cell * 10 + threadIdx.x] = seg_off[threadIdx.x];
         if (staged) {
             for (int t = threadIdx.x; t < ncand; t += blockDim.x) {
                 int sgi = 0;
@@ -695,9 +585,6 @@ __global__ void __launch_bounds__(kCellThreads, sizeof(VT) == sizeof(float) ? 4 
             __syncthreads();
         }
     }
-    if (!kFill && !staged && aux.mode && threadIdx.x == 0) atomicOr(aux.mode, 1); // no pair written twice
-    // the fill evaluates each unordered pair once when every block was staged
-    const bool sym = kFill && sizeof(VT) == sizeof(float) && !tab_dx && staged && aux.mask && *aux.mode == 0;
     for (int r = rbeg + warp; r < rend; r += nwarps) {
         const int i = cs.sorted[r];
         const double xi = x[i], yi = y[i];
@@ -706,37 +593,15 @@ __global__ void __launch_bounds__(kCellThreads, sizeof(VT) == sizeof(float) ? 4 
         if (!kFill) {
             int cnt = 0;
             if (staged) {
-                // one ballot per 32 candidates: the row's mask words and the
-                // entries before each, stored 32 words at a time
-                unsigned mw = 0u;
-                int pw = 0;
-                const long mrow = (long)r * kMaskWords;
-#pragma unroll 2
-                for (int t0 = 0; t0 < ncand; t0 += 32) {
-                    const int t = t0 + lane;
-                    const bool hit = t < ncand && t != own &&
-                                     staged_kept(i, xi, yi, xif, yif, t, sxc, syc, sjc, seg_start, seg_off, c, c2,
-                                                 ic2, cs);
-                    const unsigned m = __ballot_sync(0xffffffffu, hit);
-                    const int w = t0 >> 5;
-                    if ((w & 31) == lane) {
-                        mw = m;
-                        pw = cnt;
-                    }
-                    cnt += __popc(m);
-                    if (aux.mask && ((w & 31) == 31 || t0 + 32 >= ncand)) {
-                        const int wl = (w & ~31) + lane;
-                        if (wl <= w) {
-                            aux.mask[mrow + wl] = mw;
-                            aux.pre[mrow + wl] = (unsigned short)pw;
-                        }
-                    }
-                }
+#pragma unroll 4
+                for (int t = lane; t < ncand; t += 32)
+                    cnt += t != own &&
+                           staged_kept(i, xi, yi, xif, yif, t, sxc, syc, sjc, seg_start, seg_off, c, c2, ic2, cs);
             } else {
                 cnt = row_count_global(i, xi, yi, cs, c, c2, ic2, lane);
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
             }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
             if (lane == 0) rowcnt[i] = cnt + 1;
         } else {
             const int base = rowptr[i], rowend = rowptr[i + 1];
@@ -745,25 +610,15 @@ __global__ void __launch_bounds__(kCellThreads, sizeof(VT) == sizeof(float) ? 4 
                 continue;
             }
             int pos = base + 1;
-            const long mrow = (long)r * kMaskWords;
             if (staged) {
                 int sgi = 0; // segment of the chunk's first candidate (candidates ascend)
-                unsigned mwl = 0u;
                 for (int t0 = 0; t0 < ncand; t0 += 32) {
                     const int t = t0 + lane;
-                    unsigned m;
-                    if (aux.mask) { // the count pass's decisions, 32 words per load
-                        const int w = t0 >> 5;
-                        if ((w & 31) == 0) mwl = aux.mask[mrow + w + lane];
-                        m = __shfl_sync(0xffffffffu, mwl, w & 31);
-                    } else {
-                        bool hit = false;
-                        if (t < ncand && t != own)
-                            hit = staged_kept(i, xi, yi, xif, yif, t, sxc, syc, sjc, seg_start, seg_off, c, c2,
-                                              ic2, cs);
-                        m = __ballot_sync(0xffffffffu, hit);
-                    }
-                    const bool hit = (m >> lane) & 1u;
+                    bool hit = false;
+                    if (t < ncand && t != own)
+                        hit = staged_kept(i, xi, yi, xif, yif, t, sxc, syc, sjc, seg_start, seg_off, c, c2, ic2,
+                                          cs);
+                    const unsigned m = __ballot_sync(0xffffffffu, hit);
                     const int at = pos + __popc(m & ((1u << lane) - 1u));
                     if (hit && at < rowend) {
                         int sg = sgi;
@@ -784,63 +639,9 @@ __global__ void __launch_bounds__(kCellThreads, sizeof(VT) == sizeof(float) ? 4 
                 if (lane == 0) atomicExch(flag, 1);
                 continue;
             }
-            if (sym) {
-                // owned runs: lanes 0..9 locate the block's cell boundaries in
-                // the row, lane 10 the row's own candidate
-                const int tb = lane < 10 ? seg_off[lane] : (lane == 10 ? own : ncand);
-                const int bnd = min(max(mask_slot(aux, mrow, tb, ncand, base, rowend), base + 1), rowend);
-                const int oslot = __shfl_sync(0xffffffffu, bnd, 10);
-                int st[9], ln[9], total = 0;
-#pragma unroll
-                for (int sg = 0; sg < 9; ++sg) {
-                    const int b0 = __shfl_sync(0xffffffffu, bnd, sg), b1 = __shfl_sync(0xffffffffu, bnd, sg + 1);
-                    int yy = cy + sg / 3 - 1, xx = cx + sg % 3 - 1;
-                    yy = yy < 0 ? yy + G : (yy >= G ? yy - G : yy);
-                    xx = xx < 0 ? xx + G : (xx >= G ? xx - G : xx);
-                    st[sg] = sg == 4 ? oslot : b0;
-                    ln[sg] = max(sg == 4 ? b1 - oslot : (yy * G + xx > cell ? b1 - b0 : 0), 0);
-                    total += ln[sg];
-                }
-                if (lane == 0) col[base] = i;
-                row_values_owned(i, xi, yi, b[i], cx, cy, r - seg_start[4], G, cs, aux, c, c2, st, ln, total,
-                                 rowptr, col, col_s, reinterpret_cast<float *>(val), bs, cap, flag, ic2, lane);
-                double pd = 0.0;
-                for (int q = lane; q < p; q += 32) {
-                    const double dx = wrap_half(xi - pdx[q]), dy = wrap_half(yi - pdy[q]);
-                    double w;
-                    if (pair_kept(r2_exact(dx, dy), c, c2, ic2, &w)) pd += b[i] * pd_force_dx_f64(dx, dy, A, K) * w;
-                }
-                pd = warp_sum(pd);
-                if (lane == 0) gdiag[i] = pd; // the diagonal pass adds the row sum
-                continue;
-            }
             row_values<VT>(i, xi, yi, b[i], cs, c, c2, ic2, base, rowend, col, col_s, val, gdiag, p, pdx, pdy, A, K,
                            tab_dx, bs, lane);
         }
-    }
-}
-
-// Diagonal after a fill that wrote each pair once into both rows: G_ii =
-// -(row sum + the point-defect seed the fill left in gdiag), the row summed
-// in the order the per-row fill uses (lane-strided, then across the warp),
-// so the value is the same bits either way.  Nothing to do when the fill
-// ran per row (*mode != 0).  One warp per row.
-__global__ void diag_sum_kernel(int n, const int *__restrict__ mode, const int *__restrict__ rowptr,
-                                float *__restrict__ val, double *__restrict__ gdiag, long cap)
-{
-    if (*mode != 0) return;
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (i >= n) return;
-    const int base = rowptr[i], end = rowptr[i + 1];
-    if ((long)end > cap) return; // the fill skipped the row (storage overflow, flagged)
-    double rs = 0.0;
-    for (int q = base + 1 + lane; q < end; q += 32) rs += (double)val[q];
-    rs = warp_sum(rs);
-    if (lane == 0) {
-        const double g = -(rs + gdiag[i]);
-        val[base] = (float)g;
-        gdiag[i] = g;
     }
 }
 
@@ -935,35 +736,6 @@ static int cell_parts(const Engine &e, int ncell)
     return ncell >= want ? 1 : (want + ncell - 1) / ncell;
 }
 
-// Count-pass masks (kMaskWords words and prefix counts per row) and the
-// cells' block offsets, allocated on first use.
-static int fill_aux_alloc(Engine &e, int ncell)
-{
-    if (!e.d_fmask) {
-        if (cudaMalloc(&e.d_fmask, sizeof(unsigned) * (size_t)e.n * kMaskWords) != cudaSuccess) return SDDDST_ERR_NOMEM;
-        if (cudaMalloc(&e.d_fpre, sizeof(unsigned short) * (size_t)e.n * kMaskWords) != cudaSuccess)
-            return SDDDST_ERR_NOMEM;
-    }
-    if ((long)ncell * 10 > e.segtab_cap) {
-        if (e.d_segtab) cudaFree(e.d_segtab);
-        e.d_segtab = nullptr;
-        e.segtab_cap = 0;
-        if (cudaMalloc(&e.d_segtab, sizeof(int) * (size_t)ncell * 10) != cudaSuccess) return SDDDST_ERR_NOMEM;
-        e.segtab_cap = (long)ncell * 10;
-    }
-    return 0;
-}
-
-// The diagonal pass of a single-evaluation FP32 fill (a no-op on the device
-// when a block was not staged and the fill ran per row).
-static void launch_diag_sum(Engine &e, cudaStream_t st)
-{
-    const int wpb = 8;
-    diag_sum_kernel<<<(e.n + wpb - 1) / wpb, 32 * wpb, 0, st>>>(e.n, e.d_fmode, e.d_rowptr, e.d_valf, e.d_gdiag,
-                                                                e.nnz_cap);
-    e.launches++;
-}
-
 // With defer, nothing waits for the device: the row counts are not read
 // back (the fill is bounded by the current storage and flags an overflow
 // with 2 in d_flag) and the fill's flag is left for the caller to read;
@@ -986,24 +758,9 @@ int jacobian_assemble(Engine &e, const double *x, bool defer)
                 (float)(rp * rp * (1.0 - rel)), (float)(rp * rp * (1.0 + rel))};
     const int parts = cell_parts(e, ncell);
     const unsigned nb = (unsigned)(ncell * parts);
-    FillAux aux{nullptr, nullptr, nullptr, e.d_cell, e.d_fmode};
-    if (G >= 3) {
-        if (int rc = fill_aux_alloc(e, ncell)) {
-            e.err = "jacobian: mask allocation failed";
-            return rc;
-        }
-        aux.mask = e.d_fmask;
-        aux.pre = e.d_fpre;
-        aux.segtab = e.d_segtab;
-    }
-    cudaMemsetAsync(e.d_fmode, 0, sizeof(int), st);
-    // the FP32 analytic fill evaluates each pair once when every block is
-    // staged (decided on the device: *d_fmode), the diagonal then in a pass
-    // of its own
-    const bool sym_fill = e.valf && !e.d_tab_dx && aux.mask;
     cell_rows_kernel<false, float><<<nb, kCellThreads, kCellSmem, st>>>(
         parts, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr, e.d_rowcnt, nullptr, nullptr,
-        nullptr, nullptr, 0, nullptr, nullptr, 0.0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, 0L, aux);
+        nullptr, nullptr, 0, nullptr, nullptr, 0.0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, 0L);
     e.launches += launch_scan(e, e.d_rowcnt, n, e.d_rowptr, st) - 1;
     e.launches += 8;
     if (defer) {
@@ -1012,13 +769,12 @@ int jacobian_assemble(Engine &e, const double *x, bool defer)
             cell_rows_kernel<true, float><<<nb, kCellThreads, kCellSmem, st>>>(
                 parts, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr, nullptr, e.d_rowptr,
                 e.d_col, e.d_valf, e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag, e.d_tab_dx, e.d_col_s,
-                e.d_col_s16, e.d_bsrt, e.nnz_cap, aux);
+                e.d_col_s16, e.d_bsrt, e.nnz_cap);
         else
             cell_rows_kernel<true, double><<<nb, kCellThreads, kCellSmem, st>>>(
                 parts, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr, nullptr, e.d_rowptr,
                 e.d_col, e.d_val, e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag, e.d_tab_dx, e.d_col_s,
-                e.d_col_s16, e.d_bsrt, e.nnz_cap, aux);
-        if (sym_fill) launch_diag_sum(e, st);
+                e.d_col_s16, e.d_bsrt, e.nnz_cap);
         e.launches += 1;
         e.nnz = -1;
         e.col_s_valid = true;
@@ -1044,13 +800,12 @@ int jacobian_assemble(Engine &e, const double *x, bool defer)
         cell_rows_kernel<true, float><<<nb, kCellThreads, kCellSmem, st>>>(
             parts, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr, nullptr, e.d_rowptr, e.d_col,
             e.d_valf, e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag, e.d_tab_dx, e.d_col_s, e.d_col_s16,
-            e.d_bsrt, e.nnz_cap, aux);
+            e.d_bsrt, e.nnz_cap);
     else
         cell_rows_kernel<true, double><<<nb, kCellThreads, kCellSmem, st>>>(
             parts, x, e.d_y, e.d_b, cs, e.cutoff, e.cutoff_sqr, e.one_per_cutoff_sqr, nullptr, e.d_rowptr, e.d_col,
             e.d_val, e.d_gdiag, e.p, e.d_pdx, e.d_pdy, e.A, e.KASQR, e.d_flag, e.d_tab_dx, e.d_col_s, e.d_col_s16,
-            e.d_bsrt, e.nnz_cap, aux);
-    if (sym_fill) launch_diag_sum(e, st);
+            e.d_bsrt, e.nnz_cap);
     e.launches += 1;
     int flag = 0;
     cudaMemcpyAsync(&flag, e.d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);

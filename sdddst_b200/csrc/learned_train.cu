@@ -145,8 +145,20 @@ __global__ void sub_sq_kernel(long m, const double *__restrict__ b, const double
 }
 
 // x *= s elementwise
-__global__ void scale_kernel(long m, double s, double *__restrict__ x)
+// x *= num / (sum of the np partials in ref): the residual's gradient
+// relative to |R0|^2, so every Jacobian's step is scale-free (the loss with B
+// alone spans decades over the step sizes a run visits)
+__global__ void scale_by_sum_kernel(long m, double num, const double *__restrict__ ref, int np, double *__restrict__ x)
 {
+    __shared__ double sh[8];
+    double r = 0.0;
+    for (int b = threadIdx.x; b < np; b += blockDim.x) r += ref[b];
+    r = warp_sum(r);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = r;
+    __syncthreads();
+    double tot = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += sh[w];
+    const double s = tot > 0.0 ? num / tot : 0.0;
     for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (long)gridDim.x * blockDim.x) x[t] *= s;
 }
 
@@ -1067,8 +1079,8 @@ int train_step_impl(Engine &e, const VT *val, double h, int k, double lr, unsign
     capply_kernel<<<wrows, 256, 0, st>>>(n, k, e.d_rowptr, e.d_col, L.d_cval, T.Z, T.T1);
     jmul_kernel<VT><<<wrows, 256, 0, st>>>(n, k, h, e.d_rowptr, e.d_col, val, T.dvec, T.T1, T.T2, false, 1.0);
     sub_sq_kernel<<<kSubCTAs, 256, 0, st>>>(nk, T.R0, T.T2, T.T1, T.dpart + kSubCTAs); // T1 = R
-    // dR = 2 R / (n k); Gm = -J^T dR (into T2)
-    scale_kernel<<<kSubCTAs, 256, 0, st>>>(nk, 2.0 / (double)nk, T.T1);
+    // the step follows |R|^2 / |R0|^2: dR = 2 R / |R0|^2; Gm = -J^T dR (into T2)
+    scale_by_sum_kernel<<<kSubCTAs, 256, 0, st>>>(nk, 2.0, T.dpart, kSubCTAs, T.T1);
     jmul_kernel<VT><<<wrows, 256, 0, st>>>(n, k, h, e.d_rowptr, e.d_col, val, T.dvec, T.T1, T.T2, true, -1.0);
     const double *Gm = T.T2;
     cudaMemsetAsync(T.g, 0, sizeof(float) * T.nw, st);

@@ -3,7 +3,7 @@ sdddst_b200/learned.py) on the device and writes
 sdddst_b200/learned_weights.npz.
 
     python -m sdddst_b200.learned_train [--jacobians 20000] [--sizes 4096 8192 16384 32768]
-                                        [--probes 8] [--lr 1e-3] [--heldout 16]
+                                        [--probes 8] [--lr 1e-5] [--heldout 16] [--settle 10]
 
 Every training step is one call of sdddst_learned_train_step: the device
 assembles the Jacobian J(h) of the engine's accepted configuration, builds
@@ -21,7 +21,11 @@ J(h/2) of the next step's full and half steps, until --jacobians Jacobians
 have been used.  A held-out run (N = 8192, seed 12) provides --heldout
 states; the file records their loss with B alone, with the first-order
 correction (the starting network: zero output layers) and with the trained
-correction.
+correction.  The file keeps the checkpoint (taken after each run, the start
+included) with the lowest held-out loss.  Each step follows the loss relative
+to the loss with B alone, so Jacobians of every step size weigh alike, and
+each run's first --settle accepted steps (the initial step-size transient)
+are skipped.
 """
 from __future__ import annotations
 
@@ -41,15 +45,19 @@ def _engine(n, seed):
                                        solver=capi.SOLVER_GMRES_LEARNED), xyb)
 
 
-def heldout_states(count, w0):
-    """(engine, [(configuration, step size), ...]) of a held-out run."""
+def heldout_states(count, w0, settle):
+    """(engine, [(configuration, step size), ...]) of a held-out run, from
+    its accepted steps after the first `settle`."""
     e = _engine(8192, 12)
     e.learned_train_init(w0)
     states = []
+    accepted = 0
     while len(states) < count:
         if e.step():
-            sc = e.scalars()
-            states.append((e.config(0), sc["step_size"]))
+            accepted += 1
+            if accepted > settle:
+                sc = e.scalars()
+                states.append((e.config(0), sc["step_size"]))
     return e, states
 
 
@@ -71,20 +79,29 @@ def main(argv=None):
     ap.add_argument("--jacobians", type=int, default=20000)
     ap.add_argument("--sizes", type=int, nargs="+", default=[4096, 8192, 16384, 32768])
     ap.add_argument("--probes", type=int, default=8)
-    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr", type=float, default=1e-5)
+    ap.add_argument("--settle", type=int, default=10,
+                    help="accepted steps of each run (and of the held-out run) before its Jacobians are used")
     ap.add_argument("--steps-per-run", type=int, default=400, help="accepted steps before the next run")
     ap.add_argument("--heldout", type=int, default=16)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--compare", default=None, help="a weight file whose held-out loss the record also states")
     args = ap.parse_args(argv)
     from sdddst_b200 import build, learned
     build.build()
     log = lambda s: print(s, flush=True)
     t0 = time.time()
     w0 = learned.init_weights(0)
-    ev, states = heldout_states(args.heldout, w0)
+    ev, states = heldout_states(args.heldout, w0, args.settle)
     lb0, lf0 = evaluate(ev, states, args.probes, w0)
     log(f"held-out: B {lb0:.4e}  B + first order {lf0:.4e}")
+    lcmp = None
+    if args.compare:
+        bits = learned.load_weights(args.compare).astype(np.uint32) << 16
+        lcmp = evaluate(ev, states, args.probes, bits.view(np.float32))[1]
+        log(f"held-out: B + {args.compare} {lcmp:.4e}")
     weights = w0
+    best, best_loss, best_at = w0, lf0, 0
     used = 0
     run = 0
     hist = []
@@ -97,10 +114,12 @@ def main(argv=None):
         # continue the optimiser state across runs: the moments restart, the
         # schedule continues
         accepted = 0
-        while accepted < args.steps_per_run and used < args.jacobians:
+        while accepted < args.steps_per_run + args.settle and used < args.jacobians:
             if not e.step():
                 continue
             accepted += 1
+            if accepted <= args.settle:  # the initial step-size transient
+                continue
             h = e.scalars()["step_size"]
             for hh in (h, 0.5 * h):
                 lr = args.lr * 0.5 * (1.0 + math.cos(math.pi * used / args.jacobians))
@@ -113,14 +132,19 @@ def main(argv=None):
         e.close()
         hb, hc = evaluate(ev, states, args.probes, weights)
         hist.append({"jacobians": used, "heldout_B": hb, "heldout_learned": hc})
+        if hc < best_loss:
+            best, best_loss, best_at = weights, hc, used
         log(f"run {run} (N={n}) done: {used} Jacobians, held-out B + C {hc:.4e}")
         run += 1
-    hb, hc = evaluate(ev, states, args.probes, weights)
-    bf16 = learned.bf16_bits(weights)
+    # the checkpoint with the lowest held-out loss (the start included)
+    bf16 = learned.bf16_bits(best)
     meta = {"trainer": "device (csrc/learned_train.cu)", "jacobians": used, "sizes": sizes_used,
-            "probes": args.probes, "lr": args.lr, "runs": run, "heldout_states": len(states),
-            "heldout_loss": {"B": lb0, "B_plus_first_order": lf0, "B_plus_learned_bf16": hc},
-            "history": hist, "seconds": time.time() - t0}
+            "probes": args.probes, "lr": args.lr, "settle": args.settle, "runs": run,
+            "heldout_states": len(states),
+            "heldout_loss": {"B": lb0, "B_plus_first_order": lf0, "B_plus_learned_bf16": best_loss,
+                             "B_plus_last": hist[-1]["heldout_learned"] if hist else lf0,
+                "B_plus_compared": lcmp},
+            "kept_checkpoint_after_jacobians": best_at, "history": hist, "seconds": time.time() - t0}
     log(json.dumps(meta["heldout_loss"]))
     np.savez(args.out or learned.WEIGHTS_FILE, bf16=bf16, meta=np.array(json.dumps(meta)))
 
