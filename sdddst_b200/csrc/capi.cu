@@ -551,6 +551,16 @@ int sdddst_profile_pair_sum(void *ctx, int reps, double *ms_per_launch)
     return from_engine(e, rc);
 }
 
+// Internal counters of the learned correction (not part of the public
+// header): network inferences, rescales onto a second step size of the same
+// assembly, and remaps onto a new assembly.
+int sdddst_internal_learned_counts(void *ctx, long *inferences, long *rescales, long *remaps)
+{
+    if (!ctx || !inferences || !rescales || !remaps) return fail(SDDDST_ERR_INVALID, "null argument");
+    sd::learned_counts(*E(ctx), inferences, rescales, remaps);
+    return SDDDST_OK;
+}
+
 // Internal check of the exclusive scan the assembly and the preconditioner
 // build use (not part of the public header): out[0..m] from in[0..m-1], both
 // device pointers, on the context's stream, with scratch sized for m.

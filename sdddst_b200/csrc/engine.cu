@@ -385,6 +385,10 @@ int Engine::prepare_solver(double h, bool same_assembly)
         // assembly (stage II's h/2 after stage I's h) rescales its outputs
         if (same_assembly && prm.solver == SDDDST_SOLVER_GMRES_LEARNED && learned_rescale(*this, h, d_dvec))
             return 0;
+        // a new assembly right after an inference (stage III after stage I)
+        // carries that inference's outputs onto its pattern
+        if (!same_assembly && prm.solver == SDDDST_SOLVER_GMRES_LEARNED && learned_remap(*this, h, d_dvec))
+            return 0;
         return learned_build(*this, h, d_dvec, d_xasm, prm.solver == SDDDST_SOLVER_GMRES_NEUMANN);
     }
     return 0;

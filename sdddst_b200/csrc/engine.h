@@ -264,6 +264,8 @@ int learned_set_weights(Engine &e, const unsigned short *bf16, long count);
 int learned_build(Engine &e, double h, const double *dvec, const double *x, bool analytic);
 void learned_apply_add(Engine &e, const double *v, double *z);
 bool learned_rescale(Engine &e, double h, const double *dvec);
+bool learned_remap(Engine &e, double h, const double *dvec);
+void learned_counts(Engine &e, long *inferences, long *rescales, long *remaps);
 void learned_invalidate(Engine &e);
 int learned_export(Engine &e, float *host, long cap);
 void learned_free(Engine &e);

@@ -33,6 +33,8 @@
 #include "engine.h"
 #include "learned_net.cuh"
 
+#include <utility>
+
 namespace sd {
 
 using namespace ln;
@@ -146,6 +148,43 @@ __global__ void rescale_kernel(int n, double h, const int *__restrict__ rowptr, 
     }
 }
 
+// The network's raw outputs of the previous assembly's pattern (rp0, col0)
+// carried onto the current one, one warp per row: a row whose columns are
+// unchanged copies them; otherwise every entry looks for its column in the
+// old row, first within eight slots of its own offset (a few entries came or
+// went), then over the whole row, and takes 0 where the column is new (the
+// network's part of c_ij, leaving the analytic first-order value).
+__global__ void remap_raw_kernel(int n, const int *__restrict__ rp, const int *__restrict__ col,
+                                 const int *__restrict__ rp0, const int *__restrict__ col0,
+                                 const float *__restrict__ raw0, float *__restrict__ raw)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const int s = rp[i], e = rp[i + 1], s0 = rp0[i], e0 = rp0[i + 1];
+    const int len = e - s, len0 = e0 - s0;
+    bool same = len == len0;
+    if (same)
+        for (int k = lane; k < len; k += 32) same = same && col[s + k] == col0[s0 + k];
+    same = __all_sync(0xffffffffu, same);
+    if (same) {
+        for (int k = lane; k < len; k += 32) raw[s + k] = raw0[s0 + k];
+        return;
+    }
+    for (int k = 1 + lane; k < len; k += 32) { // slot 0 is the diagonal
+        const int j = col[s + k];
+        int at = -1;
+        for (int d = 0; d <= 8 && at < 0; ++d) {
+            if (k + d < len0 && col0[s0 + k + d] == j) at = k + d;
+            else if (d > 0 && k - d >= 1 && k - d < len0 && col0[s0 + k - d] == j) at = k - d;
+        }
+        for (int k0 = 1; k0 < len0 && at < 0; ++k0)
+            if (col0[s0 + k0] == j) at = k0;
+        raw[s + k] = at >= 0 ? raw0[s0 + at] : 0.0f;
+    }
+    if (lane == 0) raw[s] = raw0[s0];
+}
+
 // z += C v, one warp per row
 __global__ void apply_kernel(int n, const int *__restrict__ rowptr, const int *__restrict__ col,
                              const float *__restrict__ cval, const double *__restrict__ v, double *__restrict__ z)
@@ -220,12 +259,15 @@ int learned_set_weights(Engine &e, const unsigned short *bf16, long count)
     L.off = o;
     cudaMemcpyAsync(L.d_w, bf16, sizeof(unsigned short) * o.total, cudaMemcpyHostToDevice, e.st);
     L.has_weights = true;
+    L.raw_valid = L.prev_valid = false; // outputs of other weights are not reused
     return e.sync_check("learned weights");
 }
 
 // C for the assembled J(h); the cluster preconditioner must be built (its
 // block indices are an edge feature).  analytic: the first-order
 // block-Neumann correction without the network.
+static void keep_pattern(Engine &e, Learned &L);
+
 int learned_build(Engine &e, double h, const double *dvec, const double *x, bool analytic)
 {
     if (!analytic && !(e.learned && LN(e)->has_weights)) {
@@ -237,8 +279,14 @@ int learned_build(Engine &e, double h, const double *dvec, const double *x, bool
     if (e.nnz > L.cval_cap) {
         if (L.d_cval) cudaFree(L.d_cval);
         if (L.d_craw) cudaFree(L.d_craw);
+        if (L.d_craw0) cudaFree(L.d_craw0);
+        if (L.d_col0) cudaFree(L.d_col0);
         L.d_cval = nullptr;
         L.d_craw = nullptr;
+        L.d_craw0 = nullptr; // the remap buffers follow cval_cap (they swap with d_craw)
+        L.d_col0 = nullptr;
+        L.col0_cap = 0;
+        L.prev_valid = false;
         L.cval_cap = 0;
         const long cap = e.nnz + e.nnz / 8;
         if (cudaMalloc(&L.d_cval, sizeof(float) * cap) != cudaSuccess ||
@@ -328,7 +376,53 @@ int learned_build(Engine &e, double h, const double *dvec, const double *x, bool
     e.launches += 4 + 3 * kLayers + 2;
     L.builds++;
     L.raw_valid = true;
+    keep_pattern(e, L);
+    L.remaps = 0;
     return 0;
+}
+
+// The current pattern becomes the one the raw outputs belong to.
+static void keep_pattern(Engine &e, Learned &L)
+{
+    L.prev_valid = false;
+    if (e.nnz <= 0 || e.d_hrow || e.nnz > L.cval_cap) return;
+    if (L.col0_cap != L.cval_cap) { // d_craw0 swaps with d_craw: the same capacity
+        if (L.d_col0) cudaFree(L.d_col0);
+        if (L.d_craw0) cudaFree(L.d_craw0);
+        L.d_col0 = nullptr;
+        L.d_craw0 = nullptr;
+        L.col0_cap = 0;
+        if (cudaMalloc(&L.d_col0, sizeof(int) * L.cval_cap) != cudaSuccess ||
+            cudaMalloc(&L.d_craw0, sizeof(float) * L.cval_cap) != cudaSuccess)
+            return; // no remapping: the next assembly runs the network
+        L.col0_cap = L.cval_cap;
+    }
+    if (!L.d_rp0 && cudaMalloc(&L.d_rp0, sizeof(int) * (e.n + 1)) != cudaSuccess) return;
+    cudaMemcpyAsync(L.d_rp0, e.d_rowptr, sizeof(int) * (e.n + 1), cudaMemcpyDeviceToDevice, e.st);
+    cudaMemcpyAsync(L.d_col0, e.d_col, sizeof(int) * e.nnz, cudaMemcpyDeviceToDevice, e.st);
+    L.prev_valid = true;
+}
+
+// C of the network for J(h) on a new assembly from the outputs of the
+// inference on the previous one (one remap per inference: the stage III
+// assembly of an attempt reuses the inference of its stage I, whose
+// positions differ by a half step); false when that is not possible: run
+// learned_build.
+bool learned_remap(Engine &e, double h, const double *dvec)
+{
+    Learned *Lp = LN(e);
+    if (!Lp || !Lp->has_weights || !Lp->prev_valid || Lp->remaps >= 1 || e.d_hrow) return false;
+    Learned &L = *Lp;
+    if (e.nnz <= 0 || e.nnz > L.cval_cap || L.col0_cap != L.cval_cap) return false;
+    const unsigned wrows = (unsigned)((e.n + 7) / 8);
+    remap_raw_kernel<<<wrows, 256, 0, e.st>>>(e.n, e.d_rowptr, e.d_col, L.d_rp0, L.d_col0, L.d_craw, L.d_craw0);
+    std::swap(L.d_craw, L.d_craw0); // both hold cval_cap floats
+    e.launches++;
+    L.raw_valid = true;
+    L.remaps++;
+    L.remap_count++;
+    keep_pattern(e, L);
+    return learned_rescale(e, h, dvec);
 }
 
 // C of the network for J(h) from the outputs of the last inference on the
@@ -347,6 +441,14 @@ bool learned_rescale(Engine &e, double h, const double *dvec)
     e.launches++;
     Lp->rescales++;
     return true;
+}
+
+void learned_counts(Engine &e, long *inferences, long *rescales, long *remaps)
+{
+    const Learned *L = LN(e);
+    *inferences = L ? L->builds : 0;
+    *rescales = L ? L->rescales : 0;
+    *remaps = L ? L->remap_count : 0;
 }
 
 // a new assembly: the network's outputs no longer match the pattern
@@ -394,7 +496,7 @@ void learned_free(Engine &e)
     Learned *L = LN(e);
     if (!L) return;
     void *bufs[] = {L->d_w, L->d_nf, L->d_h, L->d_ph, L->d_qh, L->d_agg, L->d_jii, L->d_cval, L->d_crow, L->d_ccnt,
-                    L->d_ccol, L->d_cv, L->d_err, L->d_craw, L->d_crawd};
+                    L->d_ccol, L->d_cv, L->d_err, L->d_craw, L->d_crawd, L->d_rp0, L->d_col0, L->d_craw0};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (L->h_err) cudaFreeHost(L->h_err);

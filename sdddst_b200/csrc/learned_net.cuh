@@ -75,6 +75,14 @@ struct Learned {
     long cval_cap = 0, ccap = 0;
     long builds = 0, rescales = 0;
     bool raw_valid = false; // d_craw / d_crawd hold the outputs of an inference on the current assembly
+    // the pattern those outputs belong to (row pointers, columns), kept across
+    // the next assembly so its C can reuse them (learned_remap)
+    int *d_rp0 = nullptr, *d_col0 = nullptr;
+    float *d_craw0 = nullptr; // remap target
+    long col0_cap = 0;
+    bool prev_valid = false;
+    int remaps = 0;           // assemblies served by remapping since the last inference
+    long remap_count = 0;
     void *train = nullptr;  // training state (learned_train.cu)
 };
 

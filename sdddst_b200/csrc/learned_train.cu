@@ -1052,6 +1052,7 @@ int train_step_impl(Engine &e, const VT *val, double h, int k, double lr, unsign
         }
         L.cval_cap = cap;
     }
+    L.prev_valid = false; // d_craw now receives this step's forward: nothing to remap from
     feat_kernel<VT><<<wrows, 256, 0, st>>>(n, h, e.d_rowptr, e.d_col, val, e.d_gdiag, T.dvec, L.d_nf, L.d_jii);
     // probes, R0 = Z - J B Z
     probe_kernel<<<(unsigned)((nk + 255) / 256), 256, 0, st>>>(n, k, seed, T.Z);

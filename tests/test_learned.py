@@ -84,3 +84,12 @@ def test_learned_solver_matches_cluster_trajectory(engine_lib):
         assert a.step() == b.step(), k
         assert np.abs(a.config(0)[:, 0] - b.config(0)[:, 0]).max() <= 1e-9, k
     assert a.solver_stats()[0] > 0
+    # one inference per attempt: stage II rescales it, stage III's assembly
+    # remaps it onto its own pattern
+    import ctypes as C
+    fn = a.lib.sdddst_internal_learned_counts
+    fn.argtypes = [C.c_void_p] + [C.POINTER(C.c_long)] * 3
+    fn.restype = C.c_int
+    inf, resc, remap = C.c_long(), C.c_long(), C.c_long()
+    assert fn(a.h, C.byref(inf), C.byref(resc), C.byref(remap)) == 0
+    assert remap.value > 0 and inf.value <= 11, (inf.value, resc.value, remap.value)
