@@ -143,7 +143,7 @@ def main(argv=None):
             "heldout_states": len(states),
             "heldout_loss": {"B": lb0, "B_plus_first_order": lf0, "B_plus_learned_bf16": best_loss,
                              "B_plus_last": hist[-1]["heldout_learned"] if hist else lf0,
-                "B_plus_compared": lcmp},
+                             "B_plus_compared": lcmp},
             "kept_checkpoint_after_jacobians": best_at, "history": hist, "seconds": time.time() - t0}
     log(json.dumps(meta["heldout_loss"]))
     np.savez(args.out or learned.WEIGHTS_FILE, bf16=bf16, meta=np.array(json.dumps(meta)))
