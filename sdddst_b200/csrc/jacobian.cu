@@ -431,8 +431,9 @@ __device__ void row_values(int i, double xi, double yi, double bi, const CellSca
                 dys[u] = wrap_diff_f64(i < j ? yj - yi : yi - yj);
                 const double r2 = r2_exact(dxs[u], dys[u]);
                 float wf = 1.0f;
-                if (r2 > c2) {
-                    const float t = sqrtf((float)r2) - (float)c;
+                if (r2 > c2) { // the weight of an FP32 value: r from the FP32 reciprocal square root
+                    const float r2f = (float)r2;
+                    const float t = r2f * rsqrtf(r2f) - (float)c;
                     wf = __expf(-(t * t) * (float)ic2);
                 }
                 ws[u] = (double)wf;
@@ -440,11 +441,13 @@ __device__ void row_values(int i, double xi, double yi, double bi, const CellSca
             }
             const float2 t = tau_xy_dx_f32x2(make_float2(__double2float_rn(dxs[0]), __double2float_rn(dxs[1])),
                                              make_float2(__double2float_rn(dys[0]), __double2float_rn(dys[1])));
-            const VT va = (VT)(bi * bss[0] * (double)t.x * ws[0]);
+            // b_i b_j is +-1 (0 for a stand-in): the product runs in FP32, the
+            // precision it is stored in, and is the same from either row
+            const VT va = (VT)((float)(bi * bss[0]) * (t.x * (float)ws[0]));
             val[qa] = va;
             rs += (double)va;
             if (hb) {
-                const VT vb = (VT)(bi * bss[1] * (double)t.y * ws[1]);
+                const VT vb = (VT)((float)(bi * bss[1]) * (t.y * (float)ws[1]));
                 val[qb] = vb;
                 rs += (double)vb;
             }
