@@ -184,33 +184,17 @@ __global__ void block_meta_kernel(const int *__restrict__ nbp, const int *__rest
     sq[b] = k * k;
 }
 
-// One warp per block: dense J block, Gauss-Jordan inverse with partial
-// pivoting, written row-major at binv[off[b]].
+// Dense J block b (k >= 2 members from bstart s), Gauss-Jordan inverse with
+// partial pivoting by one warp in M, written row-major at binv[off[b]];
+// false when the block is singular.
 template <typename VT>
-__global__ void block_invert_kernel(const int *__restrict__ nbp, double h0, const double *__restrict__ hrow, const int *__restrict__ bstart,
-                                    const int *__restrict__ blen,
-                                    const int *__restrict__ members, const int *__restrict__ blk_of,
-                                    const int *__restrict__ loc, const int *__restrict__ off,
-                                    const int *__restrict__ rowptr, const int *__restrict__ col,
-                                    const VT *__restrict__ val, const double *__restrict__ gdiag,
-                                    const double *__restrict__ dvec, double *__restrict__ binv,
-                                    int *__restrict__ flag)
+__device__ bool invert_block_warp(int b, int k, int s, double h, const int *__restrict__ members,
+                                  const int *__restrict__ blk_of, const int *__restrict__ loc,
+                                  const int *__restrict__ off, const int *__restrict__ rowptr,
+                                  const int *__restrict__ col, const VT *__restrict__ val,
+                                  const double *__restrict__ gdiag, const double *__restrict__ dvec,
+                                  double *__restrict__ binv, double (*M)[2 * kMaxBlock + 1], int lane)
 {
-    __shared__ double A[2][kMaxBlock][2 * kMaxBlock + 1];
-    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = blockIdx.x * 2 + wib;
-    if (b >= *nbp) return;
-    const int k = blen[b], s = bstart[b];
-    double(*M)[2 * kMaxBlock + 1] = A[wib];
-    const double h = hrow ? hrow[members[s]] : h0; // a block lies inside one system
-    if (k == 1) {
-        if (lane == 0) {
-            const int i = members[s];
-            const double jii = 1.0 + (1.0 + dvec[i]) * 0.5 * h * gdiag[i];
-            binv[off[b]] = 1.0 / jii;
-        }
-        return;
-    }
     for (int r = 0; r < k; ++r)
         for (int c = lane; c < 2 * k; c += 32) M[r][c] = (c - k == r) ? 1.0 : 0.0;
     __syncwarp();
@@ -262,13 +246,52 @@ __global__ void block_invert_kernel(const int *__restrict__ nbp, double h0, cons
         }
         __syncwarp();
     }
-    if (singular) {
-        if (lane == 0) atomicExch(flag, 1);
-        return;
-    }
+    if (singular) return false;
     double *dst = binv + off[b];
     for (int r = 0; r < k; ++r)
         for (int c = lane; c < k; c += 32) dst[r * k + c] = M[r][k + c];
+    __syncwarp();
+    return true;
+}
+
+// Each warp serves 32 consecutive blocks: a one-member block (most of them)
+// is inverted by its own lane, and the warp then takes the larger blocks
+// of its group one after another.
+template <typename VT>
+__global__ void block_invert_kernel(const int *__restrict__ nbp, double h0, const double *__restrict__ hrow, const int *__restrict__ bstart,
+                                    const int *__restrict__ blen,
+                                    const int *__restrict__ members, const int *__restrict__ blk_of,
+                                    const int *__restrict__ loc, const int *__restrict__ off,
+                                    const int *__restrict__ rowptr, const int *__restrict__ col,
+                                    const VT *__restrict__ val, const double *__restrict__ gdiag,
+                                    const double *__restrict__ dvec, double *__restrict__ binv,
+                                    int *__restrict__ flag)
+{
+    __shared__ double A[2][kMaxBlock][2 * kMaxBlock + 1];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b0 = (blockIdx.x * 2 + wib) * 32;
+    const int nb = *nbp;
+    if (b0 >= nb) return;
+    const int bl = b0 + lane;
+    const int kl = bl < nb ? blen[bl] : 0;
+    if (kl == 1) {
+        const int i = members[bstart[bl]];
+        const double h = hrow ? hrow[i] : h0;
+        const double jii = 1.0 + (1.0 + dvec[i]) * 0.5 * h * gdiag[i];
+        binv[off[bl]] = 1.0 / jii;
+    }
+    unsigned multi = __ballot_sync(0xffffffffu, kl > 1);
+    while (multi) {
+        const int l = __ffs(multi) - 1;
+        multi &= multi - 1u;
+        const int b = b0 + l;
+        const int k = blen[b], s = bstart[b];
+        const double h = hrow ? hrow[members[s]] : h0; // a block lies inside one system
+        if (!invert_block_warp<VT>(b, k, s, h, members, blk_of, loc, off, rowptr, col, val, gdiag, dvec, binv,
+                                   A[wib], lane) &&
+            lane == 0)
+            atomicExch(flag, 1);
+    }
 }
 
 // z = M^-1 v, one thread per dislocation i: its row loc[i] of its block's
@@ -353,7 +376,7 @@ int precond_build(Engine &e, Cluster &c, double h, const double *dvec, bool chec
                                              c.sq);
     e.launches += launch_scan(e, c.sq, n, c.off, st) - 1;
     cudaMemsetAsync(c.flag, 0, sizeof(int), st);
-    const unsigned ib = (unsigned)((n + 1) / 2);
+    const unsigned ib = (unsigned)((n + 63) / 64); // 32 blocks per warp, two warps per CTA
     if (e.valf)
         block_invert_kernel<float><<<ib, 64, 0, st>>>(nbp, h, e.d_hrow, c.bstart, c.blen, c.members,
                                                       c.blk_of, c.loc, c.off, e.d_rowptr, e.d_col, e.d_valf,
