@@ -14,9 +14,10 @@
 //     dislocation);
 //   * clusters are listed contiguously, members in ascending index order,
 //     and cut into blocks of at most kMaxBlock;
-//   * one warp per block builds the dense block of J, inverts it by
-//     Gauss-Jordan elimination with partial pivoting in shared memory, and
-//     stores the inverse; applying M^-1 is one small dense product per block.
+//   * a one-member block is inverted by one lane; a warp builds each larger
+//     block of J densely, inverts it by Gauss-Jordan elimination with
+//     partial pivoting in shared memory, and stores the inverse; applying
+//     M^-1 is one small dense product per block.
 #include "engine.h"
 #include "common.cuh"
 
