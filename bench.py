@@ -811,7 +811,9 @@ def main():
         "config": {"workload": f"n{args.n}_m{CUTOFF_M}_seed{SEED}", "N": args.n, "cutoff_multiplier": CUTOFF_M,
                    "prec": PREC, "initial_step": H0, "pairsum": args.pairsum,
                    "solver": "gmres(30) fp64 to a 1e-10 relative residual, cluster block-Jacobi preconditioner",
-                   "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas" if ws > 1 else "none",
+                   "arms": "value: the fastest preconditioner (cluster); learned_precond: the learned correction; "
+                           "plain_fp64: the plain FP64 direct-solve path",
+                   "l2":"flushed between timed steps (256 MiB write)", "parallelism": "replicas" if ws > 1 else "none",
                    "accepted": accepted, "attempts": args.steps, "final_step_size": sc["step_size"],
                    "window": f"attempts after {settled} accepted steps and {args.warmup} warm-up attempts",
                    "step_size_range": h_window,
