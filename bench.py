@@ -813,7 +813,7 @@ def main():
                    "solver": "gmres(30) fp64 to a 1e-10 relative residual, cluster block-Jacobi preconditioner",
                    "arms": "value: the fastest preconditioner (cluster); learned_precond: the learned correction; "
                            "plain_fp64: the plain FP64 direct-solve path",
-                   "l2":"flushed between timed steps (256 MiB write)", "parallelism": "replicas" if ws > 1 else "none",
+                   "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas" if ws > 1 else "none",
                    "accepted": accepted, "attempts": args.steps, "final_step_size": sc["step_size"],
                    "window": f"attempts after {settled} accepted steps and {args.warmup} warm-up attempts",
                    "step_size_range": h_window,
