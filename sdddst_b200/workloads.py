@@ -7,7 +7,7 @@ read identical states.  Every generator uses ``numpy.random.default_rng(seed)``
 
 * dislocation positions ``rng.uniform(-0.5, 0.5, (N, 2))`` (column 0 = x,
   column 1 = y), i.e. the reference's simulation cell [-0.5, 0.5)^2
-  (README.md "Configuration files");
+  (the reference's README.md, "Configuration files");
 * Burgers signs ``rng.permutation([+1]*(N//2) + [-1]*(N - N//2))``;
 * point defects ``rng.uniform(-0.5, 0.5, (P, 2))``, after the dislocations.
 
